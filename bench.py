@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark: implicit time steps of 256^3 TVD convection-diffusion on one B200.
+
+Workload (one "step" = one implicit Euler step of the reference's driver loop:
+Build, BiCGStab2 solve to a 1e-10 relative residual, CopyTo, ExchangeHaloCells,
+CopyDataVectorsToOldTimeStep): periodic unit cube, 256^3 cells, FP64,
+D = 1e-4, divergence-free seeded velocity (cell Peclet 5, CFL 0.5), van Leer
+TVD by deferred correction, Jacobi-preconditioned BiCGStab(2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dare|reference]
+
+Prints one JSON line.  ``value`` is steps/s with every input resident in HBM;
+``e2e`` is the same metric through the public API with the field uploaded from
+and downloaded to pinned host memory every step.  Under torchrun (N > 1) each
+rank runs an independent replica (the path is not sharded here), timing is
+the max over ranks and ``value`` counts the steps of all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "implicit steps/s (256^3 TVD convection-diffusion, Jacobi-BiCGStab2 to 1e-10)"
+UNIT = "steps/s"
+# Algorithmic bytes per cell and launch (FP64, each operand streamed once; the
+# SpMV inputs at the 6 neighbours come from cache).  See DESIGN.md.
+BYTES_PER_CELL = {
+    "assemble": 8 + 8 + 24 + 56 + 8 + 8,   # phi, phi_old, 3 face velocities; 7 diagonals, rhs, x0
+    "step1": 88,    # r, u, 6 off-diagonals, r_hat; u', v
+    "step2": 112,   # r, v, 6 off-diagonals, u, x, r_hat; r', s, x
+    "step3": 88,    # s, v, 6 off-diagonals, r_hat; v', w
+    "step4": 120,   # s, w, 6 off-diagonals, r, u, v; u, r, s', t
+    "step5": 88,    # x, r, s, t, u, v, w, r_hat; x, r, u
+}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["dare", "reference"], default="dare")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ----------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(prefix="dare_clocks_", suffix=".csv")
+        self.proc = None
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-i",
+                 str(gpu_index), "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, n: int):
+    """DRAM bytes per launch from the committed ncu summary (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            t = json.load(fh)
+        ent = t[kernel]
+        return ent["bytes_per_cell"] * n ** 3
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------------
+# CPU (oracle) arm: the reference's algorithm restated on the host cores
+# ----------------------------------------------------------------------------
+def cpu_steps(case, steps: int, n: int):
+    from oracle import oracle as O
+    og = O.make_grid(3, case["n"], case["size"], 2, case["periodic"])
+    fv = [np.ascontiguousarray(a) for a in case["face_vel"]]
+    desc = O.AssemblyDesc(og, dt=case["dt"], D=case["D"], face_vel=fv, limiter=O.LIM_VANLEER)
+    phi = np.ascontiguousarray(case["phi0"].reshape(-1)).copy()
+    old = phi.copy()
+    times, iters = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        diag, rhs, mask = O.assemble(desc, phi, old)
+        rp, cols, vals = O.export_csr(og, diag, mask)
+        x0 = O.field_to_vector(og, phi)
+        x, info = O.bicgstab2(rp, cols, vals, rhs, x0, 1e-10 * float(np.linalg.norm(rhs)), 5000)
+        O.copy_to_field(og, x, phi)
+        O.exchange_halo(og, phi)
+        old[:] = phi
+        times.append(time.perf_counter() - t0)
+        iters.append(info["iters"])
+        del diag, rp, cols, vals
+    return times, iters, O.num_threads()
+
+
+def host_case(n, seed):
+    from dare_b200 import workloads as W
+    return W.tvd_convection_diffusion(n=n, seed=seed)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    case = host_case(args.n, args.seed)
+    times, iters, cores = cpu_steps(case, args.warmup + args.steps, args.n)
+    timed = times[args.warmup:]
+    total = sum(timed)
+    value = len(timed) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded divergence-free velocity, smooth scalar)",
+        "config": {"workload": f"TVD convection-diffusion {args.n}^3 periodic, van Leer, D=1e-4, Pe 5, CFL 0.5, "
+                               "Jacobi-BiCGStab2 to 1e-10 relative", "cells": args.n ** 3},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{len(timed)} full implicit steps of the {args.n}^3 workload (CPU oracle: "
+                                   "assembly, CSR build, BiCGStab2, copy back), OpenMP on all host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iterations_per_step": statistics.mean(iters),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+def run_dare(args):
+    import torch
+
+    import dare_b200 as D
+    from dare_b200 import workloads as W
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+
+    n = args.n
+    case = W.tvd_convection_diffusion(n=n, seed=args.seed, device=dev)
+    ctx = D.Context(local)
+    grid = D.Grid(ctx, case["n"], case["size"], 2, case["periodic"])
+    field = D.Field(grid, 2)
+    phi0 = case["phi0"].reshape(-1).cpu().numpy()
+    field.upload(phi0, 0)
+    field.upload(phi0, 1)
+    system = D.MatrixSystem(grid)
+    vel = [D.DeviceArray.from_tensor(case["face_vel"][d]) for d in range(3)]
+    asm = D.Assembly(dt=case["dt"], D=case["D"], face_vel=tuple(vel), limiter="VANLEER")
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+
+    for _ in range(args.warmup):
+        D.timestep(system, field, asm, solver)
+    ctx.set_profiling(True)
+    ctx.reset_kernel_stats()
+    ctx.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    clocks = ClockSampler(local)
+    launches0 = ctx.launch_count
+    iters = []
+    barrier()
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        rep = D.timestep(system, field, asm, solver)
+        iters.append(rep["iters"])
+        if not rep["converged"]:
+            raise RuntimeError(f"solve did not converge: {rep}")
+    ms = ctx.timer_stop()
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.launch_count - launches0
+    ms = max_over_ranks(ms)
+    value = world * args.steps / (ms * 1e-3)
+
+    # per-kernel durations (CUDA events on the launching stream, timed region)
+    kstats = {}
+    for name in BYTES_PER_CELL:
+        tot, cnt = ctx.kernel_stats(name)
+        if cnt:
+            kstats[name] = {"ms_total": tot, "launches": cnt, "ms_avg": tot / cnt}
+    ctx.set_profiling(False)
+    dom = max(kstats, key=lambda k: kstats[k]["ms_total"]) if kstats else None
+    peak, peak_kind = measured_peak_hbm()
+    roofline = None
+    if dom:
+        algo = BYTES_PER_CELL[dom] * n ** 3
+        achieved = algo / (kstats[dom]["ms_avg"] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(dom, n),
+                    "algorithmic_bytes": algo}
+        roofline["kernels"] = {k: {**v, "GBps": BYTES_PER_CELL[k] * n ** 3 / (v["ms_avg"] * 1e-3) / 1e9}
+                               for k, v in kstats.items()}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(grid.num_cells_ghosted, dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = field.download(0)
+        barrier()
+        ctx.synchronize()
+        ctx.timer_start()
+        for _ in range(args.steps):
+            field.upload(host, 0)
+            field.copy_to_old()
+            D.timestep(system, field, asm, solver)
+            host[:] = field.download(0)
+        ems = max_over_ranks(ctx.timer_stop())
+        barrier()
+        nbytes = grid.num_cells_ghosted * 8
+        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        hcase = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in case.items() if k != "face_vel"}
+        hcase["face_vel"] = [a.cpu().numpy() for a in case["face_vel"]]
+        times, citers, cores = cpu_steps(hcase, args.cpu_steps, n)
+        cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{len(times)} full implicit steps of the same {n}^3 workload from the same initial "
+                         f"field (CPU oracle, OpenMP), iterations {citers}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded divergence-free velocity, smooth scalar in [0,1])",
+            "config": {"workload": f"TVD convection-diffusion {n}^3 periodic, van Leer, D=1e-4, Pe 5, CFL 0.5, "
+                                   "Jacobi-BiCGStab2 to 1e-10 relative",
+                       "cells": n ** 3, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (system ~3.6 GB per GPU)"},
+            "time_to_residual_ms": ms / args.steps, "iterations_per_step": statistics.mean(iters),
+            "cell_updates_per_s": value * n ** 3,
+            "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_dare(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

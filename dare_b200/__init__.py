@@ -1,0 +1,445 @@
+"""dare_b200 -- B200-native finite-volume hot path of hpc-dave/dare.
+
+Python binding of the C ABI in ``include/dare_gpu.h`` (``libdare_gpu.so``,
+hand-written CUDA for sm_100a).  There is no CPU fallback: every object here
+drives device kernels, and importing a handle class without the built library
+raises ``RuntimeError``.
+
+The classes mirror the reference's host API for the path:
+
+=====================  ====================================================
+reference (C++)         here
+=====================  ====================================================
+Grid::Cartesian<Dim>    :class:`Grid`
+Data::Field             :class:`Field` (time levels of ghosted GridVectors)
+Matrix::Trilinos<SC>    :class:`MatrixSystem` (``build``, ``copy_to``, CSR export)
+Matrix::BiCGStab2       :class:`BiCGStab2` (``"Convergence Tolerance"``,
+                        ``"Maximum Iterations"`` parameter names)
+=====================  ====================================================
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdare_gpu.so")
+
+CENTER, WEST, EAST, SOUTH, NORTH, BOTTOM, TOP = range(7)
+BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN = 0, 1, 2
+LIMITER = {"CDS": 0, "UPWIND": 1, "VANALBADA": 2, "MINMOD": 3, "VANLEER": 4}
+PREC_NONE, PREC_JACOBI = 0, 1
+PRECISION_FP64, PRECISION_FP32_REFINE = 0, 1
+SOLVE_STATUS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "nan"}
+KERNEL_IDS = {"assemble": 0, "step1": 3, "step2": 4, "step3": 5, "step4": 6, "step5": 7}
+
+
+class GridInfo(C.Structure):
+    _fields_ = [("dim", C.c_int), ("num_ghost", C.c_int), ("n", C.c_int64 * 3), ("n_ghosted", C.c_int64 * 3),
+                ("num_cells", C.c_int64), ("num_cells_ghosted", C.c_int64), ("dx", C.c_double * 3),
+                ("volume", C.c_double), ("area", C.c_double * 3), ("periodic", C.c_int * 3)]
+
+
+class AssemblyDesc(C.Structure):
+    _fields_ = [("dt", C.c_double), ("diffusion", C.c_int), ("D", C.c_double), ("face_D", C.c_void_p * 3),
+                ("convection", C.c_int), ("limiter", C.c_int), ("vel", C.c_double * 3),
+                ("face_vel", C.c_void_p * 3)]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_it", C.c_int), ("precond", C.c_int), ("precision", C.c_int),
+                ("inner_rel_tol", C.c_double), ("inner_max_it", C.c_int), ("max_refinements", C.c_int),
+                ("check_every", C.c_int), ("compute_true_residual", C.c_int), ("tol_relative", C.c_int)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("iters", C.c_int), ("converged", C.c_int), ("status", C.c_int), ("breakdown_step", C.c_int),
+                ("res_abs", C.c_double), ("true_res_abs", C.c_double), ("b_norm", C.c_double),
+                ("refinements", C.c_int), ("inner_iters", C.c_int), ("fallback_used", C.c_int),
+                ("tol_abs", C.c_double)]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["status_name"] = SOLVE_STATUS.get(self.status, str(self.status))
+        return d
+
+
+# every symbol declared in include/dare_gpu.h: (name, restype, argtypes)
+_P = C.c_void_p
+_SIGS = [
+    ("dare_ctx_create", C.c_int, [C.c_int, C.POINTER(_P)]),
+    ("dare_ctx_destroy", C.c_int, [_P]),
+    ("dare_ctx_set_stream", C.c_int, [_P, _P]),
+    ("dare_ctx_get_stream", _P, [_P]),
+    ("dare_ctx_synchronize", C.c_int, [_P]),
+    ("dare_ctx_last_error", C.c_char_p, [_P]),
+    ("dare_ctx_launch_count", C.c_int64, [_P]),
+    ("dare_ctx_set_profiling", C.c_int, [_P, C.c_int]),
+    ("dare_ctx_reset_kernel_stats", C.c_int, [_P]),
+    ("dare_ctx_kernel_stats", C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    ("dare_ctx_timer_start", C.c_int, [_P]),
+    ("dare_ctx_timer_stop", C.c_int, [_P, C.POINTER(C.c_double)]),
+    ("dare_grid_create", C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(_P)]),
+    ("dare_grid_destroy", C.c_int, [_P]),
+    ("dare_grid_get_info", C.c_int, [_P, C.POINTER(GridInfo)]),
+    ("dare_field_create", C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    ("dare_field_destroy", C.c_int, [_P]),
+    ("dare_field_upload", C.c_int, [_P, C.c_int, _P]),
+    ("dare_field_download", C.c_int, [_P, C.c_int, _P]),
+    ("dare_field_device_ptr", _P, [_P, C.c_int]),
+    ("dare_field_exchange_halo", C.c_int, [_P]),
+    ("dare_field_copy_to_old", C.c_int, [_P]),
+    ("dare_system_create", C.c_int, [_P, C.POINTER(_P)]),
+    ("dare_system_destroy", C.c_int, [_P]),
+    ("dare_system_set_bc", C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
+    ("dare_assemble", C.c_int, [_P, C.POINTER(AssemblyDesc), _P]),
+    ("dare_system_set_coefficients", C.c_int, [_P, _P, _P, _P]),
+    ("dare_system_get_coefficients", C.c_int, [_P, _P, _P]),
+    ("dare_system_set_initial_guess", C.c_int, [_P, _P]),
+    ("dare_system_get_solution", C.c_int, [_P, _P]),
+    ("dare_system_device_ptr", _P, [_P, C.c_int]),
+    ("dare_system_csr_nnz", C.c_int64, [_P]),
+    ("dare_system_export_csr", C.c_int, [_P, _P, _P, _P]),
+    ("dare_system_copy_to", C.c_int, [_P, _P]),
+    ("dare_solver_params_default", None, [C.POINTER(SolverParams)]),
+    ("dare_bicgstab2_solve", C.c_int, [_P, C.POINTER(SolverParams), C.POINTER(SolveReport)]),
+    ("dare_timestep", C.c_int, [_P, _P, C.POINTER(AssemblyDesc), C.POINTER(SolverParams),
+                                C.POINTER(SolveReport)]),
+    ("dare_face_average", C.c_int, [_P, _P, C.POINTER(_P)]),
+]
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib():
+    """Load libdare_gpu.so (fails loudly: there is no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"dare_b200: {LIB_PATH} is missing; build it with `python -m dare_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in _SIGS:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class DareError(RuntimeError):
+    pass
+
+
+def _check(rc: int, ctx=None, what: str = ""):
+    if rc != 0:
+        msg = lib().dare_ctx_last_error(ctx).decode() if ctx else ""
+        raise DareError(f"{what} failed with status {rc}: {msg}")
+
+
+def _ptr(a: np.ndarray):
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One device and one CUDA stream (dare_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        rc = lib().dare_ctx_create(device, C.byref(h))
+        if rc != 0:
+            raise DareError(f"dare_ctx_create(device={device}) failed with status {rc}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dare_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        _check(lib().dare_ctx_synchronize(self.h), self.h, "synchronize")
+
+    def set_stream(self, stream_ptr: int | None):
+        _check(lib().dare_ctx_set_stream(self.h, stream_ptr), self.h, "set_stream")
+
+    @property
+    def stream(self) -> int:
+        return lib().dare_ctx_get_stream(self.h) or 0
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().dare_ctx_launch_count(self.h))
+
+    def set_profiling(self, on: bool):
+        _check(lib().dare_ctx_set_profiling(self.h, int(on)), self.h, "set_profiling")
+
+    def reset_kernel_stats(self):
+        lib().dare_ctx_reset_kernel_stats(self.h)
+
+    def timer_start(self):
+        _check(lib().dare_ctx_timer_start(self.h), self.h, "timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        _check(lib().dare_ctx_timer_stop(self.h, C.byref(ms)), self.h, "timer_stop")
+        return ms.value
+
+    def kernel_stats(self, name: str):
+        ms = C.c_double()
+        n = C.c_int64()
+        _check(lib().dare_ctx_kernel_stats(self.h, KERNEL_IDS[name], C.byref(ms), C.byref(n)), self.h, "stats")
+        return ms.value, n.value
+
+
+class Grid:
+    """Cartesian grid on one rank (Grid::Cartesian<Dim> + CartesianRepresentation)."""
+
+    def __init__(self, ctx: Context, n, size=None, num_ghost: int = 2, periodic=None):
+        dim = len(n)
+        self.ctx = ctx
+        nn = (C.c_int64 * 3)(*(list(n) + [1] * (3 - dim)))
+        sz = list(size) if size is not None else [1.0] * dim
+        ss = (C.c_double * 3)(*(sz + [1.0] * (3 - dim)))
+        pp_ = list(periodic) if periodic is not None else [0] * dim
+        pp = (C.c_int * 3)(*([int(x) for x in pp_] + [0] * (3 - dim)))
+        h = C.c_void_p()
+        _check(lib().dare_grid_create(ctx.h, dim, nn, ss, num_ghost, pp, C.byref(h)), ctx.h, "grid_create")
+        self.h = h
+        info = GridInfo()
+        lib().dare_grid_get_info(h, C.byref(info))
+        self.info = info
+        self.dim = dim
+        self.n = tuple(int(info.n[d]) for d in range(3))
+        self.ghosted_shape = tuple(int(info.n_ghosted[d]) for d in range(3))
+        self.num_cells = int(info.num_cells)
+        self.num_cells_ghosted = int(info.num_cells_ghosted)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dare_grid_destroy(self.h)
+            self.h = None
+
+    @property
+    def dx(self):
+        return [self.info.dx[d] for d in range(3)]
+
+    @property
+    def volume(self):
+        return self.info.volume
+
+    @property
+    def area(self):
+        return [self.info.area[d] for d in range(3)]
+
+    def face_shape(self, d: int):
+        s = list(self.n)
+        s[d] += 1
+        return tuple(s)
+
+
+class Field:
+    """Time levels of ghosted grid vectors on the device (Data::Field)."""
+
+    def __init__(self, grid: Grid, num_levels: int = 2):
+        self.grid = grid
+        h = C.c_void_p()
+        _check(lib().dare_field_create(grid.h, num_levels, C.byref(h)), grid.ctx.h, "field_create")
+        self.h = h
+        self.num_levels = num_levels
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dare_field_destroy(self.h)
+            self.h = None
+
+    def upload(self, values: np.ndarray, level: int = 0):
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if a.size != self.grid.num_cells_ghosted:
+            raise ValueError("field upload expects the ghosted layout")
+        _check(lib().dare_field_upload(self.h, level, _ptr(a)), self.grid.ctx.h, "field_upload")
+
+    def download(self, level: int = 0) -> np.ndarray:
+        a = np.empty(self.grid.num_cells_ghosted, dtype=np.float64)
+        _check(lib().dare_field_download(self.h, level, _ptr(a)), self.grid.ctx.h, "field_download")
+        return a
+
+    def device_ptr(self, level: int = 0) -> int:
+        return lib().dare_field_device_ptr(self.h, level)
+
+    def exchange_halo(self):
+        _check(lib().dare_field_exchange_halo(self.h), self.grid.ctx.h, "exchange_halo")
+
+    def copy_to_old(self):
+        _check(lib().dare_field_copy_to_old(self.h), self.grid.ctx.h, "copy_to_old")
+
+
+class DeviceArray:
+    """A plain device buffer owned by a torch tensor (plumbing for face arrays)."""
+
+    def __init__(self, host: np.ndarray | None, device: int = 0):
+        import torch
+        self.t = None if host is None else torch.from_numpy(
+            np.ascontiguousarray(host, dtype=np.float64)).to(f"cuda:{device}")
+
+    @classmethod
+    def from_tensor(cls, t) -> "DeviceArray":
+        a = cls(None)
+        a.t = t.contiguous()
+        return a
+
+    @property
+    def ptr(self) -> int:
+        return self.t.data_ptr()
+
+
+@dataclass
+class Assembly:
+    """Descriptor of the fused per-cell functor (see dare_assembly_desc)."""
+    dt: float = 0.0
+    D: float | None = None
+    face_D: tuple | None = None        # 3 device pointers (int) or DeviceArray
+    vel: tuple | None = None           # constant velocity
+    face_vel: tuple | None = None      # 3 device pointers (int) or DeviceArray
+    limiter: str = "VANLEER"
+
+    def to_c(self) -> AssemblyDesc:
+        a = AssemblyDesc()
+        a.dt = self.dt
+        if self.face_D is not None:
+            a.diffusion = 2
+            for d, p in enumerate(self.face_D):
+                a.face_D[d] = p.ptr if isinstance(p, DeviceArray) else p
+        elif self.D is not None:
+            a.diffusion = 1
+            a.D = float(self.D)
+        if self.face_vel is not None:
+            a.convection = 2
+            for d, p in enumerate(self.face_vel):
+                a.face_vel[d] = p.ptr if isinstance(p, DeviceArray) else p
+        elif self.vel is not None:
+            a.convection = 1
+            for d, v in enumerate(self.vel):
+                a.vel[d] = float(v)
+        a.limiter = LIMITER[self.limiter]
+        return a
+
+
+class MatrixSystem:
+    """Structured 7-diagonal system A x = B (Matrix::Trilinos<SC>)."""
+
+    def __init__(self, grid: Grid):
+        self.grid = grid
+        h = C.c_void_p()
+        _check(lib().dare_system_create(grid.h, C.byref(h)), grid.ctx.h, "system_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dare_system_destroy(self.h)
+            self.h = None
+
+    def set_bc(self, face: int, kind: int, value: float = 0.0):
+        _check(lib().dare_system_set_bc(self.h, face, kind, value), self.grid.ctx.h, "set_bc")
+
+    def build(self, field: Field, assembly: Assembly):
+        """Trilinos<SC>::Build with the fused functor; x0 = field level 0."""
+        desc = assembly.to_c()
+        _check(lib().dare_assemble(self.h, C.byref(desc), field.h), self.grid.ctx.h, "assemble")
+
+    def set_coefficients(self, diag: np.ndarray | None, rhs: np.ndarray | None = None, x0: np.ndarray | None = None):
+        d = None if diag is None else np.ascontiguousarray(diag, dtype=np.float64)
+        r = None if rhs is None else np.ascontiguousarray(rhs, dtype=np.float64)
+        x = None if x0 is None else np.ascontiguousarray(x0, dtype=np.float64)
+        _check(lib().dare_system_set_coefficients(self.h, _ptr(d), _ptr(r), _ptr(x)), self.grid.ctx.h, "set_coef")
+
+    def coefficients(self):
+        n = self.grid.num_cells
+        diag = np.empty((7, n), dtype=np.float64)
+        rhs = np.empty(n, dtype=np.float64)
+        _check(lib().dare_system_get_coefficients(self.h, _ptr(diag), _ptr(rhs)), self.grid.ctx.h, "get_coef")
+        return diag, rhs
+
+    def solution(self) -> np.ndarray:
+        x = np.empty(self.grid.num_cells, dtype=np.float64)
+        _check(lib().dare_system_get_solution(self.h, _ptr(x)), self.grid.ctx.h, "get_solution")
+        return x
+
+    def set_initial_guess(self, x0: np.ndarray):
+        self.set_coefficients(None, None, x0)
+
+    def device_ptr(self, which: int) -> int:
+        return lib().dare_system_device_ptr(self.h, which)
+
+    def export_csr(self):
+        nnz = int(lib().dare_system_csr_nnz(self.h))
+        n = self.grid.num_cells
+        rowptr = np.empty(n + 1, dtype=np.int64)
+        cols = np.empty(nnz, dtype=np.int64)
+        vals = np.empty(nnz, dtype=np.float64)
+        _check(lib().dare_system_export_csr(self.h, _ptr(rowptr), _ptr(cols), _ptr(vals)), self.grid.ctx.h, "csr")
+        return rowptr, cols, vals
+
+    def copy_to(self, field: Field):
+        _check(lib().dare_system_copy_to(self.h, field.h), self.grid.ctx.h, "copy_to")
+
+
+class BiCGStab2:
+    """BiCGStab(2) with the reference's parameter names (Matrix::BiCGStab2)."""
+
+    def __init__(self, params: dict | None = None, precond: str = "JACOBI", precision: str = "FP64"):
+        p = SolverParams()
+        lib().dare_solver_params_default(C.byref(p))
+        params = params or {}
+        if "Convergence Tolerance" in params:
+            p.tol = float(params["Convergence Tolerance"])
+        if "Maximum Iterations" in params:
+            p.max_it = int(params["Maximum Iterations"])
+        p.precond = {"NONE": PREC_NONE, "JACOBI": PREC_JACOBI}[precond.upper()]
+        p.precision = {"FP64": PRECISION_FP64, "FP32_REFINE": PRECISION_FP32_REFINE}[precision.upper()]
+        for k, v in params.items():
+            if hasattr(p, k):
+                setattr(p, k, v)
+        self.params = p
+        self.report = None
+
+    def solve(self, system: MatrixSystem) -> dict:
+        rep = SolveReport()
+        _check(lib().dare_bicgstab2_solve(system.h, C.byref(self.params), C.byref(rep)), system.grid.ctx.h,
+               "bicgstab2_solve")
+        self.report = rep.as_dict()
+        return self.report
+
+    def get_num_iters(self) -> int:
+        return self.report["iters"] if self.report else 0
+
+
+def timestep(system: MatrixSystem, field: Field, assembly: Assembly, solver: BiCGStab2) -> dict:
+    """Build, Solve, CopyTo, ExchangeHaloCells, CopyDataVectorsToOldTimeStep on the device."""
+    desc = assembly.to_c()
+    rep = SolveReport()
+    _check(lib().dare_timestep(system.h, field.h, C.byref(desc), C.byref(solver.params), C.byref(rep)),
+           system.grid.ctx.h, "timestep")
+    solver.report = rep.as_dict()
+    return solver.report
+
+
+def face_average(grid: Grid, cell_D_ptr: int, face_ptrs) -> None:
+    arr = (C.c_void_p * 3)(*[p.ptr if isinstance(p, DeviceArray) else p for p in face_ptrs])
+    _check(lib().dare_face_average(grid.h, cell_D_ptr, arr), grid.ctx.h, "face_average")

@@ -1,0 +1,93 @@
+// dare_step.cu -- one implicit time step of the reference's driver loop
+// (test/Verification/counter_diffusion1D.cpp:170-217 and
+// advection_periodic2D.cpp:160-196): Build, Solve, CopyTo,
+// ExchangeHaloCells, CopyDataVectorsToOldTimeStep -- all on the device,
+// control returning to the host only for the solver's status.
+#include <cstring>
+
+#include "dare_internal.cuh"
+
+using namespace dare_gpu;
+
+int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_report* rep);
+namespace dare_gpu {
+int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old);
+int launch_scatter(dare_ctx* ctx, const GridDev& g, const double* x, double* phi);
+int launch_halo(dare_ctx* ctx, const GridDev& g, double* phi);
+}  // namespace dare_gpu
+
+extern "C" {
+
+int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc, const dare_solver_params* p,
+                  dare_solve_report* rep) {
+    if (!s || !f || !desc || !p || !rep || f->grid != s->grid) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = s->grid->ctx;
+    cudaSetDevice(ctx->device);
+    const double* phi = f->level[0];
+    const double* phi_old = f->num_levels > 1 ? f->level[1] : f->level[0];
+    const bool prof = ctx->profiling != 0;
+    if (prof) DARE_CUDA(ctx, cudaEventRecord(ctx->ev[12], ctx->stream));
+    int rc = launch_assemble(s, desc, phi, phi_old);                 // Trilinos::Build
+    if (rc) return rc;
+    if (prof) DARE_CUDA(ctx, cudaEventRecord(ctx->ev[13], ctx->stream));
+    rc = dare_bicgstab2_solve(s, p, rep);                            // TrilinosSolver::Solve
+    if (rc) return rc;
+    if (prof) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev[12], ctx->ev[13]) == cudaSuccess) {
+            ctx->stat_ms[KID_ASSEMBLE] += ms;
+            ctx->stat_n[KID_ASSEMBLE] += 1;
+        }
+    }
+    rc = launch_scatter(ctx, s->grid->dev, s->x, f->level[0]);       // Trilinos::CopyTo
+    if (rc) return rc;
+    rc = launch_halo(ctx, s->grid->dev, f->level[0]);                // Field::ExchangeHaloCells
+    if (rc) return rc;
+    return dare_field_copy_to_old(f);                                // CopyDataVectorsToOldTimeStep
+}
+
+int dare_ctx_set_profiling(dare_ctx* ctx, int on) {
+    if (!ctx) return DARE_ERR_BAD_ARG;
+    if (on) {
+        for (auto& e : ctx->ev)
+            if (!e) DARE_CUDA(ctx, cudaEventCreate(&e));
+    }
+    ctx->profiling = on ? 1 : 0;
+    return DARE_OK;
+}
+
+int dare_ctx_reset_kernel_stats(dare_ctx* ctx) {
+    if (!ctx) return DARE_ERR_BAD_ARG;
+    std::memset(ctx->stat_ms, 0, sizeof(ctx->stat_ms));
+    std::memset(ctx->stat_n, 0, sizeof(ctx->stat_n));
+    return DARE_OK;
+}
+
+int dare_ctx_kernel_stats(const dare_ctx* ctx, int kernel_id, double* total_ms, int64_t* count) {
+    if (!ctx || kernel_id < 0 || kernel_id >= KID_COUNT || !total_ms || !count) return DARE_ERR_BAD_ARG;
+    *total_ms = ctx->stat_ms[kernel_id];
+    *count = ctx->stat_n[kernel_id];
+    return DARE_OK;
+}
+
+int dare_ctx_timer_start(dare_ctx* ctx) {
+    if (!ctx) return DARE_ERR_BAD_ARG;
+    if (!ctx->ev[14]) {
+        DARE_CUDA(ctx, cudaEventCreate(&ctx->ev[14]));
+        DARE_CUDA(ctx, cudaEventCreate(&ctx->ev[15]));
+    }
+    DARE_CUDA(ctx, cudaEventRecord(ctx->ev[14], ctx->stream));
+    return DARE_OK;
+}
+
+int dare_ctx_timer_stop(dare_ctx* ctx, double* ms) {
+    if (!ctx || !ms || !ctx->ev[14]) return DARE_ERR_BAD_ARG;
+    DARE_CUDA(ctx, cudaEventRecord(ctx->ev[15], ctx->stream));
+    DARE_CUDA(ctx, cudaEventSynchronize(ctx->ev[15]));
+    float f = 0.f;
+    DARE_CUDA(ctx, cudaEventElapsedTime(&f, ctx->ev[14], ctx->ev[15]));
+    *ms = f;
+    return DARE_OK;
+}
+
+}  // extern "C"

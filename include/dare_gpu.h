@@ -1,0 +1,225 @@
+/*
+ * dare_gpu.h -- C ABI of the B200-native finite-volume hot path.
+ *
+ * Drop-in boundary for hpc-dave/dare's implicit step: Cartesian grid and
+ * numbering, ghosted fields with the periodic halo fill, assembly of the
+ * per-cell 7-point coefficients (DDT + diffusion + TVD convection + boundary
+ * folding), and the BiCGStab(2) solve.  Every entry point is plain C: opaque
+ * handles, plain pointers and sizes, int status codes (0 = OK, never aborts).
+ * Host arrays passed in or out are caller-owned; device memory belongs to the
+ * context.  A context is thread-compatible (one host thread at a time) and
+ * issues all work on one CUDA stream.
+ *
+ * Citations are file:line in the hpc-dave/dare source tree.
+ */
+#ifndef DARE_GPU_H_
+#define DARE_GPU_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DARE_API __attribute__((visibility("default")))
+#else
+#define DARE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference throws or MPI_Aborts instead:
+ *      BiCGStab2.inl:139-160, ExecutionManager.cpp:72-77) -------------------- */
+#define DARE_OK 0
+#define DARE_ERR_BAD_ARG (-1)
+#define DARE_ERR_CUDA (-2)
+#define DARE_ERR_OOM (-3)
+#define DARE_ERR_STATE (-4)
+#define DARE_ERR_UNSUPPORTED (-5)
+
+/* ---- neighbour slots: CartesianNeighbor (Grid/Cartesian/CartesianMesh.h:67-77) */
+#define DARE_CENTER 0
+#define DARE_WEST 1
+#define DARE_EAST 2
+#define DARE_SOUTH 3
+#define DARE_NORTH 4
+#define DARE_BOTTOM 5
+#define DARE_TOP 6
+
+/* ---- boundary conditions folded into boundary rows
+ *      (test/Verification/counter_diffusion1D.cpp:123-146) ------------------- */
+#define DARE_BC_PERIODIC 0
+#define DARE_BC_DIRICHLET 1
+#define DARE_BC_NEUMANN 2
+
+/* ---- flux limiters: Equations/FluxLimiter.h:41-173 (+ van Leer, new) ------ */
+#define DARE_LIMITER_CDS 0
+#define DARE_LIMITER_UPWIND 1
+#define DARE_LIMITER_VANALBADA 2
+#define DARE_LIMITER_MINMOD 3
+#define DARE_LIMITER_VANLEER 4
+
+/* ---- preconditioners (right, TrilinosSolver.inl:84-85) --------------------- */
+#define DARE_PREC_NONE 0
+#define DARE_PREC_JACOBI 1
+
+/* ---- solver precision modes ------------------------------------------------ */
+#define DARE_PRECISION_FP64 0
+#define DARE_PRECISION_FP32_REFINE 1
+
+/* ---- solve status (BiCGStab2.inl:322-571) ---------------------------------- */
+#define DARE_SOLVE_CONVERGED 0
+#define DARE_SOLVE_MAXIT 1
+#define DARE_SOLVE_BREAKDOWN 2   /* breakdown_step holds the reference step 3/4/7/14/20/21 */
+#define DARE_SOLVE_NAN 3
+
+typedef struct dare_ctx dare_ctx;
+typedef struct dare_grid dare_grid;
+typedef struct dare_field dare_field;
+typedef struct dare_system dare_system;
+
+typedef struct {
+    int dim;
+    int num_ghost;
+    int64_t n[3];              /* internal cells per dimension (1 when inactive) */
+    int64_t n_ghosted[3];      /* incl. ghost layers in active dimensions */
+    int64_t num_cells;         /* internal */
+    int64_t num_cells_ghosted;
+    double dx[3];
+    double volume;
+    double area[3];
+    int periodic[3];
+} dare_grid_info;
+
+/* Assembly description: the composed user functor of the reference's time
+ * loops,
+ *     mb  = ddt(field);  mb += div(TVD(vel) * field);  mb -= div(D, grad(mb));
+ *     then Dirichlet / Neumann folding on non-periodic faces (W,E,S,N,B,T),
+ * replacing Trilinos<SC>::Build(grep, field, functor) (MatrixSystem/Trilinos.h:107-111).
+ * Face arrays live in device memory with the staggered face layout
+ *     x-faces (nx+1, ny, nz), y-faces (nx, ny+1, nz), z-faces (nx, ny, nz+1),
+ * entry [i][j][k] of the x-faces being the face between cells i-1 and i. */
+typedef struct {
+    double dt;                       /* > 0: implicit-Euler DDT (DDT.inl:39-81) */
+    int diffusion;                   /* 0 none, 1 scalar D, 2 face arrays */
+    double D;
+    const double* face_D[3];
+    int convection;                  /* 0 none, 1 constant velocity, 2 face velocity arrays */
+    int limiter;                     /* DARE_LIMITER_* */
+    double vel[3];
+    const double* face_vel[3];
+} dare_assembly_desc;
+
+typedef struct {
+    double tol;             /* ABSOLUTE tolerance on ||r||_2 (stop criterion RNORM,
+                               BiCGStab2.inl:34,561-565); tol_abs = rel * ||b|| for a relative one */
+    int max_it;             /* "Maximum Iterations" */
+    int precond;            /* DARE_PREC_NONE / DARE_PREC_JACOBI */
+    int precision;          /* DARE_PRECISION_FP64 / DARE_PRECISION_FP32_REFINE */
+    double inner_rel_tol;   /* FP32 inner solve: relative reduction per refinement (e.g. 1e-5) */
+    int inner_max_it;       /* FP32 inner solve iteration cap per refinement */
+    int max_refinements;
+    int check_every;        /* iterations between host status polls (0 = default) */
+    int compute_true_residual; /* report ||b - A x||_2 in FP64 after the solve */
+    int tol_relative;       /* 1: stop on ||r|| <= tol * ||b||_2 (||b|| computed on the device) */
+} dare_solver_params;
+
+typedef struct {
+    int iters;              /* reference num_iteration (k) */
+    int converged;
+    int status;             /* DARE_SOLVE_* */
+    int breakdown_step;
+    double res_abs;         /* last recurrence residual check (reference norm_residual) */
+    double true_res_abs;    /* ||b - A x||_2, FP64 (if requested) */
+    double b_norm;          /* ||b||_2 */
+    int refinements;        /* FP32_REFINE: outer FP64 corrections */
+    int inner_iters;        /* FP32_REFINE: total inner iterations */
+    int fallback_used;      /* FP32_REFINE: fell back to the FP64 solve */
+    double tol_abs;         /* absolute tolerance that was applied */
+} dare_solve_report;
+
+/* ---- context --------------------------------------------------------------- */
+DARE_API int dare_ctx_create(int device, dare_ctx** out);
+DARE_API int dare_ctx_destroy(dare_ctx* ctx);
+/* Use an external cudaStream_t (NULL restores the context's own stream). */
+DARE_API int dare_ctx_set_stream(dare_ctx* ctx, void* stream);
+DARE_API void* dare_ctx_get_stream(dare_ctx* ctx);
+DARE_API int dare_ctx_synchronize(dare_ctx* ctx);
+DARE_API const char* dare_ctx_last_error(const dare_ctx* ctx);
+/* Kernel launches this context issued since creation (for launch accounting). */
+DARE_API int64_t dare_ctx_launch_count(const dare_ctx* ctx);
+/* Optional per-kernel CUDA-event timing on the context's stream (no reference
+ * counterpart: the reference has no timers).  Kernel ids: 0 assembly,
+ * 3..7 the five fused BiCGStab(2) kernels (steps 5-7, 8-11, 12-14, 15-23, 24-25). */
+DARE_API int dare_ctx_set_profiling(dare_ctx* ctx, int on);
+DARE_API int dare_ctx_reset_kernel_stats(dare_ctx* ctx);
+DARE_API int dare_ctx_kernel_stats(const dare_ctx* ctx, int kernel_id, double* total_ms, int64_t* count);
+/* Wall time of the work issued on the context's stream between start and stop,
+ * from CUDA events (stop synchronizes). */
+DARE_API int dare_ctx_timer_start(dare_ctx* ctx);
+DARE_API int dare_ctx_timer_stop(dare_ctx* ctx, double* ms);
+
+/* ---- grid: Cartesian<Dim> + CartesianRepresentation (np = 1)
+ *      Grid/Cartesian/CartesianMesh.inl:33-112, CartesianRepresentation.inl:31-227 */
+DARE_API int dare_grid_create(dare_ctx* ctx, int dim, const int64_t n[3], const double size[3],
+                     int num_ghost, const int periodic[3], dare_grid** out);
+DARE_API int dare_grid_destroy(dare_grid* g);
+DARE_API int dare_grid_get_info(const dare_grid* g, dare_grid_info* info);
+
+/* ---- field: Field<Grid,SC,1> time levels of ghosted GridVectors
+ *      Data/Field.h:47-138, Data/GridVector.h:42-251 (level 0 = new, 1 = old) */
+DARE_API int dare_field_create(dare_grid* g, int num_levels, dare_field** out);
+DARE_API int dare_field_destroy(dare_field* f);
+DARE_API int dare_field_upload(dare_field* f, int level, const double* host_ghosted);
+DARE_API int dare_field_download(dare_field* f, int level, double* host_ghosted);
+DARE_API double* dare_field_device_ptr(dare_field* f, int level);
+/* Field::ExchangeHaloCells (Field.inl:100-103): periodic face ghosts of level 0 */
+DARE_API int dare_field_exchange_halo(dare_field* f);
+/* Field::CopyDataVectorsToOldTimeStep (Field.inl:88-93) */
+DARE_API int dare_field_copy_to_old(dare_field* f);
+
+/* ---- linear system: the structured 7-diagonal form of Trilinos<SC>'s A, x, B
+ *      (MatrixSystem/Trilinos.h:51-314) -------------------------------------- */
+DARE_API int dare_system_create(dare_grid* g, dare_system** out);
+DARE_API int dare_system_destroy(dare_system* s);
+/* face: DARE_WEST..DARE_TOP; non-periodic faces need DIRICHLET or NEUMANN */
+DARE_API int dare_system_set_bc(dare_system* s, int face, int type, double value);
+/* Trilinos<SC>::Build -> BuildNew (Trilinos.inl:48-60,285-385) with the fused
+ * functor above; x0 = field level 0 (the initial guess). DDT reads level 1 when
+ * the field has 2+ levels, else level 0; convection reads level 0. */
+DARE_API int dare_assemble(dare_system* s, const dare_assembly_desc* desc, dare_field* field);
+/* Replace coefficients with user-built MatrixBlocks (host SoA: diag[7][ncells]
+ * in slot order CENTER..TOP, removed entries 0), rhs and initial guess. */
+DARE_API int dare_system_set_coefficients(dare_system* s, const double* diag7, const double* rhs,
+                                 const double* x0);
+DARE_API int dare_system_get_coefficients(dare_system* s, double* diag7, double* rhs);
+DARE_API int dare_system_set_initial_guess(dare_system* s, const double* x0);
+DARE_API int dare_system_get_solution(dare_system* s, double* x);
+DARE_API double* dare_system_device_ptr(dare_system* s, int which); /* 0..6 diag, 7 rhs, 8 x */
+/* CSR export for parity (MatrixBlock::Finalize, MatrixBlock_Cartesian.inl:127-240;
+ * rows sorted by column as Tpetra fillComplete / Trilinos::PrintRow, Trilinos.inl:185-212) */
+DARE_API int64_t dare_system_csr_nnz(dare_system* s);
+DARE_API int dare_system_export_csr(dare_system* s, int64_t* rowptr, int64_t* cols, double* vals);
+/* Trilinos::CopyTo (Trilinos.inl:166-177): solution into field level 0 */
+DARE_API int dare_system_copy_to(dare_system* s, dare_field* f);
+
+/* ---- solve: TrilinosSolver::Solve(BumbleBee, "BICGSTAB2", M, A, x, B, p)
+ *      (TrilinosSolver.inl:69-93) -> BiCGStab2::Solve (BiCGStab2.inl:166-582) */
+DARE_API void dare_solver_params_default(dare_solver_params* p);
+DARE_API int dare_bicgstab2_solve(dare_system* s, const dare_solver_params* p, dare_solve_report* rep);
+
+/* One implicit time step of the reference's driver loop
+ * (test/Verification/counter_diffusion1D.cpp:170-217): Build, Solve, CopyTo,
+ * ExchangeHaloCells, CopyDataVectorsToOldTimeStep. */
+DARE_API int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
+                  const dare_solver_params* p, dare_solve_report* rep);
+
+/* Face diffusivity as the linear interpolation of cell values to faces
+ * (Interpolation_Cartesian.h:139-158: (D_lo + D_hi) * 1/2, periodic wrap on
+ * periodic faces, boundary faces take the adjacent cell value).
+ * cell_D: device, internal cells; face_D[d]: device, face layout above. */
+DARE_API int dare_face_average(dare_grid* g, const double* cell_D, double* face_D[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DARE_GPU_H_ */

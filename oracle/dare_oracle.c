@@ -221,6 +221,13 @@ static int64_t face_index(const dor_grid* g, int d, int64_t i, int64_t j, int64_
     }
 }
 
+/* Upper face of cell index i along d.  On a periodic dimension the staggered
+ * field has n faces and its halo wraps (CartesianRepresentation.inl:64-76),
+ * so face n is face 0. */
+static int64_t upper_face(const dor_grid* g, int d, int64_t i) {
+    return (g->periodic[d] && i + 1 == g->n[d]) ? 0 : i + 1;
+}
+
 /* One cell of the composed user functor
  *     mb  = ddt(field);                      DDT.inl:39-81, Set  MatrixBlock_Cartesian.inl:480-497
  *     mb += div(TVD(vel) * field);           TVD_Cartesian.inl:185-261, Divergence_Cartesian.inl:139-207
@@ -269,7 +276,7 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
             } else {                              /* face velocities: TVD_Cartesian.inl:26-38 */
                 int64_t fi[3] = {i, j, k};
                 vlo = a->face_vel[d][face_index(g, d, fi[0], fi[1], fi[2])];
-                fi[d] += 1;
+                fi[d] = upper_face(g, d, fi[d]);
                 vup = a->face_vel[d][face_index(g, d, fi[0], fi[1], fi[2])];
             }
             const int64_t s = lstride[d];
@@ -344,7 +351,7 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
             } else {
                 int64_t fi[3] = {i, j, k};
                 Dlo = a->face_D[d][face_index(g, d, fi[0], fi[1], fi[2])];
-                fi[d] += 1;
+                fi[d] = upper_face(g, d, fi[d]);
                 Dup = a->face_D[d][face_index(g, d, fi[0], fi[1], fi[2])];
             }
             nb[lo] = (-dn) * Dlo;

@@ -1,0 +1,118 @@
+"""Shared test helpers: oracle-side time loop and the reference's solver
+functors (test infrastructure; used by tests only)."""
+import numpy as np
+
+from oracle import oracle as O
+
+
+def oracle_grid(case, ng=2):
+    n = case["n"]
+    dim = len([x for x in n])
+    return O.make_grid(dim, n, case.get("size"), ng, case.get("periodic"))
+
+
+def oracle_assembly(og, case, face_D=None):
+    bc = {int(k): v for k, v in case.get("bc", {}).items()}
+    lim = {"CDS": O.LIM_CDS, "UPWIND": O.LIM_UPWIND, "VANALBADA": O.LIM_VANALBADA, "MINMOD": O.LIM_MINMOD,
+           "VANLEER": O.LIM_VANLEER}[case.get("limiter", "VANLEER")]
+    fv = case.get("face_vel")
+    fv = None if fv is None else [np.ascontiguousarray(np.asarray(a), dtype=np.float64) for a in fv]
+    return O.AssemblyDesc(og, dt=case.get("dt", 0.0), D=case.get("D"), face_D=face_D, vel=case.get("vel"),
+                          face_vel=fv, limiter=lim, bc=bc)
+
+
+def oracle_timeloop(case, steps, precond=O.PREC_JACOBI, face_D=None, max_it=5000):
+    """The reference's driver loop on the CPU oracle: Build, Solve, CopyTo,
+    ExchangeHaloCells, CopyDataVectorsToOldTimeStep (counter_diffusion1D.cpp:170-217)."""
+    og = oracle_grid(case)
+    desc = oracle_assembly(og, case, face_D)
+    phi = np.ascontiguousarray(np.asarray(case["phi0"], dtype=np.float64).reshape(-1)).copy()
+    old = phi.copy()
+    history, iters = [], []
+    for _ in range(steps):
+        diag, rhs, mask = O.assemble(desc, phi, old)
+        rowptr, cols, vals = O.export_csr(og, diag, mask)
+        x0 = O.field_to_vector(og, phi)
+        tol = case.get("rel_tol", 1e-10) * float(np.linalg.norm(rhs))
+        x, info = O.bicgstab2(rowptr, cols, vals, rhs, x0, tol=tol, max_it=max_it, precond=precond)
+        O.copy_to_field(og, x, phi)
+        O.exchange_halo(og, phi)
+        old[:] = phi
+        history.append(phi.copy())
+        iters.append(info["iters"])
+    return history, iters
+
+
+def interior(phi, shape, ng=2, dim=3):
+    a = np.asarray(phi).reshape(shape)
+    sl = tuple(slice(ng, s - ng) if d < dim else slice(None) for d, s in enumerate(shape))
+    return a[sl]
+
+
+def rel_l2(a, b):
+    a = np.asarray(a).ravel()
+    b = np.asarray(b).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def profile_functor_diag(dim, n, west=0.0, east=1.0):
+    """SoA coefficients of test_integration_Cartesian_Trilinos.cpp SolveScalar(X)
+    (1D :99-130, 2D :245-294, 3D :602-672): centre 2*dim, neighbours -1,
+    Dirichlet mirror on W/E, Neumann on the other faces; removed slots 0."""
+    nn = list(n) + [1] * (3 - dim)
+    N = nn[0] * nn[1] * nn[2]
+    diag = np.zeros((7, N))
+    rhs = np.zeros(N)
+    x0 = np.zeros(N)
+    idx = np.indices(nn).reshape(3, -1)
+    diag[0] = 2.0 * dim
+    for d in range(dim):
+        lo, hi = 2 * d + 1, 2 * d + 2
+        at_lo = idx[d] == 0
+        at_hi = idx[d] == nn[d] - 1
+        diag[lo] = np.where(at_lo, 0.0, -1.0)
+        diag[hi] = np.where(at_hi, 0.0, -1.0)
+        if d == 0:
+            diag[0] += at_lo * 1.0 + at_hi * 1.0
+            rhs = np.where(at_lo, 2.0 * west, rhs)
+            rhs = np.where(at_hi, 2.0 * east, rhs)
+            x0 = np.where(at_lo, west, x0)
+            x0 = np.where(at_hi, east, x0)
+        else:
+            diag[0] -= at_lo * 1.0 + at_hi * 1.0
+    return diag, rhs, x0
+
+
+def coupled_components_diag(ncell=23, ncomp=4):
+    """MatrixSystem/test/test_TrilinosSolver.cpp:120-165 as a 2D structured
+    grid (cells along x, interleaved components along y)."""
+    N = ncell * ncomp
+    diag = np.zeros((7, N))
+    rhs = np.zeros(N)
+    x0 = np.full(N, 0.5)
+    node = np.repeat(np.arange(ncell), ncomp)
+    comp = np.tile(np.arange(ncomp), ncell)
+    left, right = node == 0, node == ncell - 1
+    diag[0] = np.where(left | right, 3.0, 2.0)
+    diag[1] = np.where(left, 0.0, -1.0)   # WEST  (row - N)
+    diag[2] = np.where(right, 0.0, -1.0)  # EAST  (row + N)
+    rhs = np.where(right, 2.0, 0.0)
+    x0 = np.where(left, 0.0, np.where(right, 1.0, x0))
+    diag[3] = np.where(comp == 0, 0.0, -1.0)           # SOUTH (row - 1)
+    diag[4] = np.where(comp == ncomp - 1, 0.0, -1.0)   # NORTH (row + 1)
+    diag[0] += (comp != 0) * 1.0 + (comp != ncomp - 1) * 1.0
+    return diag, rhs, x0
+
+
+def diag_to_csr(dim, n, diag, periodic=None):
+    """CSR of SoA coefficients with the Finalize pattern (removed = out of range)."""
+    og = O.make_grid(dim, n, None, 2, periodic)
+    nn = list(n) + [1] * (3 - dim)
+    idx = np.indices(nn).reshape(3, -1)
+    mask = np.ones(idx.shape[1], dtype=np.uint8)
+    pp = list(periodic or [0] * dim) + [0] * (3 - dim)
+    for d in range(dim):
+        lo = np.ones(idx.shape[1], dtype=bool) if pp[d] else idx[d] > 0
+        hi = np.ones(idx.shape[1], dtype=bool) if pp[d] else idx[d] < nn[d] - 1
+        mask |= (lo.astype(np.uint8) << (2 * d + 1)) | (hi.astype(np.uint8) << (2 * d + 2))
+    return O.export_csr(og, np.ascontiguousarray(diag), mask)

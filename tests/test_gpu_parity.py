@@ -1,0 +1,285 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Bars: cell numbering, ghost fill and the exported CSR pattern bit-exact;
+assembled FP64 coefficients bit-exact (the assembly kernel keeps the
+reference's operation order and no FMA contraction; the contract allows
+1e-13 relative); solutions within 1e-9 relative L2 at the same tolerance.
+"""
+import numpy as np
+import pytest
+
+import dare_b200 as D
+from dare_b200 import workloads as W
+from oracle import oracle as O
+from tests.helpers import (coupled_components_diag, diag_to_csr, interior, oracle_assembly, oracle_grid,
+                           oracle_timeloop, profile_functor_diag, rel_l2)
+
+pytestmark = pytest.mark.gpu
+
+SOL_TOL = 1e-9   # relative L2, solutions at the same residual tolerance
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = D.Context(0)
+    yield c
+    c.synchronize()
+
+
+def _gpu_case(ctx, case):
+    dim = len(case["n"])
+    g = D.Grid(ctx, case["n"], case.get("size"), 2, case.get("periodic"))
+    f = D.Field(g, 2)
+    phi = np.ascontiguousarray(np.asarray(case["phi0"], dtype=np.float64).reshape(-1))
+    f.upload(phi, 0)
+    f.upload(np.ascontiguousarray(np.asarray(case.get("phi_old", phi), dtype=np.float64).reshape(-1)), 1)
+    s = D.MatrixSystem(g)
+    for face, (kind, val) in case.get("bc", {}).items():
+        s.set_bc(int(face), kind, val)
+    keep = []
+    face_vel = None
+    if case.get("face_vel") is not None:
+        keep = [D.DeviceArray(np.asarray(a)) for a in case["face_vel"]]
+        face_vel = tuple(keep)
+    face_D = None
+    if case.get("face_D") is not None:
+        fd = [D.DeviceArray(np.asarray(a)) for a in case["face_D"]]
+        keep += fd
+        face_D = tuple(fd)
+    asm = D.Assembly(dt=case.get("dt", 0.0), D=case.get("D"), face_D=face_D, vel=case.get("vel"),
+                     face_vel=face_vel, limiter=case.get("limiter", "VANLEER"))
+    return g, f, s, asm, keep, dim
+
+
+def _random_case(kind, seed=0):
+    rng = np.random.default_rng(seed)
+    if kind == "diffusion3d":
+        n = (12, 10, 9)
+        phi = rng.random(tuple(x + 4 for x in n))
+        return {"n": n, "size": (1.0, 2.0, 0.5), "periodic": (0, 0, 0), "dt": 0.01, "D": 1e-3, "phi0": phi,
+                "phi_old": rng.random(phi.shape),
+                "bc": {1: (1, 1.0), 2: (1, 0.0), 3: (2, 0.0), 4: (1, 0.25), 5: (2, 0.0), 6: (2, 0.0)}}
+    if kind.startswith("tvd3d"):
+        lim = kind.split("-")[1]
+        c = W.tvd_convection_diffusion(n=16, seed=seed)
+        c["limiter"] = lim
+        return c
+    if kind == "facediff3d":
+        c = W.heterogeneous(n=16, seed=seed)
+        Dc = c["cell_D"]
+        faces = []
+        for d in range(3):
+            lo = np.roll(Dc, 1, axis=d)
+            f = (lo + Dc) * 0.5
+            first = [slice(None)] * 3
+            first[d] = slice(0, 1)
+            faces.append(np.concatenate([f, f[tuple(first)]], axis=d))
+        c["face_D"] = faces
+        return c
+    if kind == "mixed3d":
+        n = (5, 7, 9)
+        phi = rng.random(tuple(x + 4 for x in n)) - 0.5
+        return {"n": n, "size": (1.0, 1.0, 1.0), "periodic": (1, 0, 0), "dt": 0.05, "D": 2e-3,
+                "vel": (0.3, -0.2, 0.1), "limiter": "MINMOD", "phi0": phi,
+                "bc": {3: (1, 1.0), 4: (2, 0.0), 5: (1, -1.0), 6: (1, 0.5)}}
+    if kind == "tvd2d":
+        n = (11, 13)
+        phi = rng.random((15, 17, 1))
+        return {"n": n, "size": (1.0, 2.0), "periodic": (1, 1), "dt": 0.02, "D": 1e-3, "vel": (-0.4, 0.7),
+                "limiter": "VANALBADA", "phi0": phi}
+    if kind == "tvd1d":
+        phi = rng.random((14, 1, 1))
+        return {"n": (10,), "size": (1.0,), "periodic": (0,), "dt": 0.1, "D": 0.5, "vel": (-1.0,),
+                "limiter": "VANLEER", "phi0": phi, "bc": {1: (2, 0.0), 2: (1, 2.0)}}
+    raise KeyError(kind)
+
+
+ASM_CASES = ["diffusion3d", "tvd3d-VANLEER", "tvd3d-CDS", "tvd3d-UPWIND", "tvd3d-MINMOD", "tvd3d-VANALBADA",
+             "facediff3d", "mixed3d", "tvd2d", "tvd1d"]
+
+
+@pytest.mark.parametrize("kind", ASM_CASES)
+def test_assembly_bit_exact(ctx, kind):
+    case = _random_case(kind)
+    if kind == "facediff3d":
+        case["D"] = None
+    g, f, s, asm, keep, dim = _gpu_case(ctx, case)
+    s.build(f, asm)
+    diag, rhs = s.coefficients()
+    x0 = s.solution()
+    og = oracle_grid(case)
+    desc = oracle_assembly(og, case, face_D=case.get("face_D"))
+    phi = np.ascontiguousarray(np.asarray(case["phi0"], dtype=np.float64).reshape(-1))
+    old = np.ascontiguousarray(np.asarray(case.get("phi_old", case["phi0"]), dtype=np.float64).reshape(-1))
+    odiag, orhs, omask = O.assemble(desc, phi, old)
+    np.testing.assert_array_equal(diag, odiag)
+    np.testing.assert_array_equal(rhs, orhs)
+    np.testing.assert_array_equal(x0, O.field_to_vector(og, phi))
+    # CSR export: identical pattern and values
+    rp, cols, vals = s.export_csr()
+    orp, ocols, ovals = O.export_csr(og, odiag, omask)
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(cols, ocols)
+    np.testing.assert_array_equal(vals, ovals)
+
+
+@pytest.mark.parametrize("dims,periodic", [((9, 8, 7), (1, 1, 1)), ((9, 8, 7), (0, 1, 0)), ((6, 5), (1, 0)),
+                                           ((10,), (1,)), ((10,), (0,))])
+def test_halo_exchange_bit_exact(ctx, dims, periodic):
+    g = D.Grid(ctx, dims, None, 2, periodic)
+    og = O.make_grid(len(dims), dims, None, 2, periodic)
+    phi = np.random.default_rng(1).random(g.num_cells_ghosted)
+    f = D.Field(g, 2)
+    f.upload(phi)
+    f.exchange_halo()
+    got = f.download()
+    ref = phi.copy()
+    O.exchange_halo(og, ref)
+    np.testing.assert_array_equal(got, ref)
+    # CopyDataVectorsToOldTimeStep
+    f.copy_to_old()
+    np.testing.assert_array_equal(f.download(1), ref)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("precond", ["NONE", "JACOBI"])
+def test_bicgstab2_linear_profile(ctx, dim, precond):
+    """test_integration_Cartesian_Trilinos.cpp SolveScalar(X): BiCGStab2,
+    tolerance 1e-14, solution = linear profile within 1e-8."""
+    n = [20 + d for d in range(dim)]
+    diag, rhs, x0 = profile_functor_diag(dim, n)
+    g = D.Grid(ctx, n, [1.0 + d for d in range(dim)], 2, None)
+    s = D.MatrixSystem(g)
+    s.set_coefficients(diag, rhs, x0)
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-14, "Maximum Iterations": 5000}, precond=precond)
+    rep = solver.solve(s)
+    assert rep["converged"], rep
+    x = s.solution()
+    nn = n + [1] * (3 - dim)
+    i = np.repeat(np.arange(nn[0]), nn[1] * nn[2])
+    assert np.max(np.abs(x - (i + 0.5) / nn[0])) < 1e-8
+    rp, cols, vals = diag_to_csr(dim, n, diag)
+    ox, info = O.bicgstab2(rp, cols, vals, rhs, x0, 1e-14, 5000,
+                           O.PREC_JACOBI if precond == "JACOBI" else O.PREC_NONE)
+    assert rel_l2(x, ox) < SOL_TOL
+    assert abs(rep["iters"] - info["iters"]) <= max(2, info["iters"] // 10)
+
+
+def test_bicgstab2_coupled_components(ctx):
+    """MatrixSystem/test/test_TrilinosSolver.cpp:98-205 (BumbleBee BICGSTAB2,
+    tolerance 1e-12), as a 23 x 4 structured grid."""
+    diag, rhs, x0 = coupled_components_diag()
+    g = D.Grid(ctx, (23, 4), None, 2, None)
+    s = D.MatrixSystem(g)
+    s.set_coefficients(diag, rhs, x0)
+    for precond in ("NONE", "JACOBI"):
+        s.set_initial_guess(x0)
+        rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 5000}, precond=precond).solve(s)
+        assert rep["converged"], rep
+        x = s.solution()
+        node = np.repeat(np.arange(23), 4)
+        assert np.max(np.abs(x - (node + 0.5) / 23)) < 1e-8
+
+
+def _gpu_timeloop(ctx, case, steps, precond="JACOBI"):
+    g, f, s, asm, keep, dim = _gpu_case(ctx, case)
+    solver = D.BiCGStab2({"Convergence Tolerance": case.get("rel_tol", 1e-10), "Maximum Iterations": 5000,
+                          "tol_relative": 1}, precond=precond)
+    hist, iters = [], []
+    for _ in range(steps):
+        rep = D.timestep(s, f, asm, solver)
+        assert rep["converged"], rep
+        hist.append(f.download(0))
+        iters.append(rep["iters"])
+    return hist, iters, g
+
+
+@pytest.mark.parametrize("kind", ["gaussian", "tvd"])
+def test_timeloop_matches_oracle(ctx, kind):
+    if kind == "gaussian":
+        case = W.gaussian_diffusion(n=20, steps=3)
+    else:
+        case = W.tvd_convection_diffusion(n=24, steps=3)
+    hist, iters, g = _gpu_timeloop(ctx, case, 3)
+    ohist, oiters = oracle_timeloop(case, 3)
+    for a, b in zip(hist, ohist):
+        assert rel_l2(interior(a, g.ghosted_shape), interior(b, g.ghosted_shape)) < SOL_TOL
+        # the periodic halo is refilled identically
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * np.abs(b).max())
+    for a, b in zip(iters, oiters):
+        assert abs(a - b) <= 2
+
+
+def test_analytical_slab_diffusion(ctx):
+    """Companion of the Gaussian diffusion workload against
+    AnalyticalSolutions/Diffusion.h (phi = 0 at t = 0, Dirichlet 1 at x = 1,
+    zero gradient at x = 0; tau = D t / L^2).  The reference asserts no
+    threshold; the bar here is first-order-in-time implicit Euler."""
+    n, D_, dt, steps = 32, 1.0, 1e-3, 20
+    case = {"n": (n, 3, 3), "size": (1.0, 1.0, 1.0), "periodic": (0, 0, 0), "dt": dt, "D": D_,
+            "phi0": np.zeros((n + 4, 7, 7)), "rel_tol": 1e-12,
+            "bc": {1: (2, 0.0), 2: (1, 1.0), 3: (2, 0.0), 4: (2, 0.0), 5: (2, 0.0), 6: (2, 0.0)}}
+    hist, _, g = _gpu_timeloop(ctx, case, steps)
+    phi = interior(hist[-1], g.ghosted_shape)[:, 1, 1]
+    zeta = (np.arange(n) + 0.5) / n
+    exact = np.array([O.diffusion_n0d1(D_ * dt * steps, z) for z in zeta])
+    err = np.abs(phi - exact)
+    assert err.mean() < 5e-3 and err.max() < 2e-2, (err.mean(), err.max())
+
+
+def test_breakdown_and_limits_report_status(ctx):
+    n = (6, 5, 4)
+    g = D.Grid(ctx, n, None, 2, (1, 1, 1))
+    s = D.MatrixSystem(g)
+    N = g.num_cells
+    diag = np.zeros((7, N))
+    diag[0] = 7.0
+    diag[1:] = -1.0
+    rhs = np.random.default_rng(3).random(N)
+    # iteration budget: max_it = 1 stops with k = 2 > 1 (BiCGStab2.inl:322-326)
+    s.set_coefficients(diag, rhs, np.zeros(N))
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-300, "Maximum Iterations": 1}).solve(s)
+    assert rep["status_name"] == "max_iterations" and not rep["converged"] and rep["iters"] == 2
+    # zero residual at the start: converged with k = 0
+    s.set_coefficients(diag, np.zeros(N), np.zeros(N))
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 10}).solve(s)
+    assert rep["converged"] and rep["iters"] == 0
+    # NaN injected into the rhs: reported, not looped on
+    bad = rhs.copy()
+    bad[5] = np.nan
+    s.set_coefficients(diag, bad, np.zeros(N))
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 50}).solve(s)
+    assert rep["status_name"] == "nan" and not rep["converged"]
+    # a zero matrix without preconditioning breaks down at step (7): gamma = 0
+    s.set_coefficients(np.zeros((7, N)), rhs, np.zeros(N))
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 50}, precond="NONE").solve(s)
+    assert rep["status_name"] == "breakdown" and rep["breakdown_step"] == 7
+    # the context is still usable afterwards
+    s.set_coefficients(diag, rhs, np.zeros(N))
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 100}).solve(s)
+    assert rep["converged"]
+
+
+def test_face_average_matches_interpolation(ctx):
+    n = (7, 6, 5)
+    g = D.Grid(ctx, n, None, 2, (1, 0, 1))
+    cell = np.random.default_rng(4).random(n)
+    dc = D.DeviceArray(cell)
+    faces = [D.DeviceArray(np.zeros(g.face_shape(d))) for d in range(3)]
+    D.face_average(g, dc.ptr, faces)
+    ctx.synchronize()
+    for d, per in enumerate((1, 0, 1)):
+        got = faces[d].t.cpu().numpy()
+        lo = np.roll(cell, 1, axis=d)
+        exp_inner = (lo + cell) * 0.5
+        sl = [slice(None)] * 3
+        sl[d] = slice(0, n[d])
+        if per:
+            np.testing.assert_array_equal(got[tuple(sl)], exp_inner)
+        else:
+            sl2 = [slice(None)] * 3
+            sl2[d] = slice(1, n[d])
+            np.testing.assert_array_equal(got[tuple(sl2)], exp_inner[tuple(sl2)])
+            sl0 = [slice(None)] * 3
+            sl0[d] = 0
+            np.testing.assert_array_equal(got[tuple(sl0)], np.take(cell, 0, axis=d))
