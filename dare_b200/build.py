@@ -32,6 +32,7 @@ SOURCES = {
     "dare_core.cu": [],
     "dare_assembly.cu": ["--fmad=false"],
     "dare_bicgstab2.cu": [],
+    "dare_mixed.cu": [],
     "dare_step.cu": [],
 }
 

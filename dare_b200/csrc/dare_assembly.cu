@@ -69,9 +69,10 @@ __device__ __forceinline__ int upper_face(const GridDev& g, int d, int i) {
 }
 
 // ApplyDivergence of a face matrix stencil (Divergence_Cartesian.inl:143-181)
+template <int DIM>
 __device__ __forceinline__ void apply_divergence(const GridDev& g, const double nb[7], const double cc[7],
                                                  double sc[7]) {
-    const int dim = g.dim;
+    constexpr int dim = DIM;
     const double* A = g.area;
 #pragma unroll
     for (int p = 0; p < 7; p++) sc[p] = 0.;
@@ -93,11 +94,11 @@ __device__ __forceinline__ void apply_divergence(const GridDev& g, const double 
     }
 }
 
+template <int DIM>
 __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const double* __restrict__ phi,
                                                   const double* __restrict__ phi_old, double* __restrict__ diag,
                                                   double* __restrict__ rhs_out, double* __restrict__ x0) {
     const int64_t n = g.ncell;
-    const int dim = g.dim;
     const int64_t lstride[3] = {(int64_t)g.gn[1] * g.gn[2], g.gn[2], 1};
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
         const unsigned cc_ = (unsigned)c, nz = (unsigned)g.n[2], ny = (unsigned)g.n[1];
@@ -123,7 +124,8 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             double nb[7], cf[7], rr[7];
 #pragma unroll
             for (int p = 0; p < 7; p++) nb[p] = cf[p] = rr[p] = 0.;
-            for (int d = 0; d < dim; d++) {
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
                 const int lo = 2 * d + 1, up = 2 * d + 2;
                 double vlo, vup;
                 if (a.convection == 1) {
@@ -159,12 +161,12 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
                 }
             }
             double sc[7];
-            apply_divergence(g, nb, cf, sc);
+            apply_divergence<DIM>(g, nb, cf, sc);
 #pragma unroll
             for (int p = 0; p < 7; p++) sc[p] *= 1.;
             double srhs = g.area[0] * (rr[DARE_EAST] - rr[DARE_WEST]);
-            if (dim > 1) srhs += g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
-            if (dim > 2) srhs += g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
+            if (DIM > 1) srhs += g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
+            if (DIM > 2) srhs += g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
 #pragma unroll
             for (int p = 0; p < 7; p++) coef[p] += sc[p];       // MatrixBlock::Add
             rhs += srhs;
@@ -174,7 +176,8 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             double nb[7], cf[7];
 #pragma unroll
             for (int p = 0; p < 7; p++) nb[p] = cf[p] = 0.;
-            for (int d = 0; d < dim; d++) {
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
                 const double dn = 1. / g.dx[d];
                 const int lo = 2 * d + 1, up = 2 * d + 2;
                 double Dlo, Dup;
@@ -192,14 +195,16 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
                 cf[up] = (-dn) * Dup;
             }
             double sc[7];
-            apply_divergence(g, nb, cf, sc);
+            apply_divergence<DIM>(g, nb, cf, sc);
 #pragma unroll
             for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
             rhs += -1. * 0.;
         }
 
-        for (int d = 0; d < dim; d++) {                    // boundary folding
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {                    // boundary folding
             if (g.periodic[d]) continue;
+#pragma unroll
             for (int side = 0; side < 2; side++) {
                 const int face = 2 * d + 1 + side;
                 const bool on_boundary = side == 0 ? (idx[d] == 0) : (idx[d] == g.n[d] - 1);
@@ -248,7 +253,12 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
         a.limiter > DARE_LIMITER_VANLEER)
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: bad descriptor");
     const int blocks = grid_blocks(ctx, g.ncell, 256, 8);
-    k_assemble<<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
+    if (g.dim == 3)
+        k_assemble<3><<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
+    else if (g.dim == 2)
+        k_assemble<2><<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
+    else
+        k_assemble<1><<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }

@@ -37,6 +37,8 @@ int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
         if (cudaEventElapsedTime(&ms, ctx->ev[12], ctx->ev[13]) == cudaSuccess) {
             ctx->stat_ms[KID_ASSEMBLE] += ms;
             ctx->stat_n[KID_ASSEMBLE] += 1;
+        } else {
+            cudaGetLastError();
         }
     }
     rc = launch_scatter(ctx, s->grid->dev, s->x, f->level[0]);       // Trilinos::CopyTo

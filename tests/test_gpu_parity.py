@@ -283,3 +283,66 @@ def test_face_average_matches_interpolation(ctx):
             sl0 = [slice(None)] * 3
             sl0[d] = 0
             np.testing.assert_array_equal(got[tuple(sl0)], np.take(cell, 0, axis=d))
+
+
+def _hetero_system(ctx, n, seed=0):
+    c = W.heterogeneous(n=n, seed=seed)
+    Dc = c["cell_D"]
+    faces = []
+    for d in range(3):
+        f = (np.roll(Dc, 1, axis=d) + Dc) * 0.5
+        first = [slice(None)] * 3
+        first[d] = slice(0, 1)
+        faces.append(np.concatenate([f, f[tuple(first)]], axis=d))
+    c["face_D"] = faces
+    c["D"] = None
+    g, f, s, asm, keep, dim = _gpu_case(ctx, c)
+    s.build(f, asm)
+    return c, g, f, s, asm, keep
+
+
+def test_mixed_precision_refinement_matches_fp64(ctx):
+    """FP32 inner BiCGStab2 + FP64 refinement reaches the FP64 residual and
+    the FP64 oracle solution (heterogeneous-D TVD operator)."""
+    c, g, f, s, asm, keep = _hetero_system(ctx, 24)
+    diag, rhs = s.coefficients()
+    x0 = s.solution()
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 500, "tol_relative": 1},
+                      precision="FP32_REFINE").solve(s)
+    assert rep["converged"] and not rep["fallback_used"], rep
+    assert rep["refinements"] >= 2
+    assert rep["true_res_abs"] <= 1e-12 * rep["b_norm"] * 1.0000001
+    x = s.solution()
+    og = oracle_grid(c)
+    mask = np.full(g.num_cells, 127, dtype=np.uint8)
+    rp, cols, vals = O.export_csr(og, np.ascontiguousarray(diag), mask)
+    ox, info = O.bicgstab2(rp, cols, vals, rhs, x0, 1e-12 * np.linalg.norm(rhs), 500)
+    assert info["converged"]
+    assert rel_l2(x, ox) < SOL_TOL
+
+
+def test_mixed_precision_fallback(ctx):
+    """An inner budget too small to contract the residual engages the FP64 fallback."""
+    c, g, f, s, asm, keep = _hetero_system(ctx, 16, seed=1)
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 500, "tol_relative": 1,
+                       "inner_max_it": 1, "inner_rel_tol": 1e-30, "max_refinements": 2},
+                      precision="FP32_REFINE").solve(s)
+    assert rep["converged"] and rep["fallback_used"] == 1, rep
+    assert rep["true_res_abs"] <= 1e-10 * rep["b_norm"] * 1.0000001
+
+
+def test_profiling_mode_same_result(ctx):
+    """Per-kernel event timing launches the same kernels directly; results match the graph path."""
+    case = W.tvd_convection_diffusion(n=20, steps=2)
+    hist_a, it_a, g = _gpu_timeloop(ctx, case, 2)
+    ctx.set_profiling(True)
+    ctx.reset_kernel_stats()
+    try:
+        hist_b, it_b, _ = _gpu_timeloop(ctx, case, 2)
+        stats = {k: ctx.kernel_stats(k) for k in ("assemble", "step1", "step4")}
+    finally:
+        ctx.set_profiling(False)
+    assert it_a == it_b
+    for a, b in zip(hist_a, hist_b):
+        np.testing.assert_array_equal(a, b)
+    assert stats["assemble"][1] == 2 and stats["assemble"][0] > 0
