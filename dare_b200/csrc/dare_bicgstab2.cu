@@ -56,18 +56,18 @@ MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem) {
     int tj = 256 / tk;
     while (tj > 1 && tj / 2 >= n1) tj /= 2;
     m.block = dim3(tk, tj, 1);
-    const int gx = (n2 + tk - 1) / tk, gy = (n1 + tj - 1) / tj;
-    const int64_t tiles = (int64_t)gx * gy;
-    int64_t target = (int64_t)ctx->num_sms * 24;          // several waves keep the tail short
-    if (target > kMaxBlocks) target = kMaxBlocks;
-    int64_t nchunk = (target + tiles - 1) / tiles;
-    if (nchunk > kMaxBlocks / tiles) nchunk = kMaxBlocks / tiles;
-    if (nchunk > n0) nchunk = n0;
-    if (nchunk < 1) nchunk = 1;
-    m.chunk = (int)((n0 + nchunk - 1) / nchunk);
-    nchunk = (n0 + m.chunk - 1) / m.chunk;
-    m.grid = dim3(gx, gy, (unsigned)nchunk);
-    m.nblocks = (int)(tiles * nchunk);
+    m.tiles_x = (n2 + tk - 1) / tk;
+    m.tiles_y = (n1 + tj - 1) / tj;
+    const int64_t tiles = (int64_t)m.tiles_x * m.tiles_y;
+    // Longest plane run that still leaves ~4 items per resident block (the
+    // dynamic queue then ends with a short tail); each run re-reads 2 planes.
+    const int64_t want = (int64_t)ctx->num_sms * 3 * 4;
+    int planes = 32;
+    while (planes > 4 && tiles * ((n0 + planes - 1) / planes) < want) planes /= 2;
+    while (tiles * ((n0 + planes - 1) / planes) > kMaxBlocks && planes < n0) planes *= 2;
+    if (planes > n0) planes = n0;
+    m.planes = planes;
+    m.nitems = (int)(tiles * ((n0 + planes - 1) / planes));
     m.smem = 2 * (size_t)(tk + 2) * (tj + 2) * elem;
     return m;
 }
@@ -122,7 +122,16 @@ template VecsT<float> carve_vecs<float>(float*, int64_t, float*, const float*);
 template <typename T, bool UNIT>
 int launch_init(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const OpT<T>& op, const VecsT<T>& vs,
                 SolverState* st, double* partials) {
-    FInit<T, UNIT> f{op, vs.x, vs.b, vs.r[0], vs.rh, vs.u[0], vs.v[0], vs.w};
+    using F = FInit<T, UNIT>;
+    F f{};
+    f.zs[0] = vs.x;
+    set_coef_streams<T, UNIT, F::NP>(op, f.ps);
+    f.ps[F::NC] = vs.b;
+    f.r = vs.r[0];
+    f.rh = vs.rh;
+    f.u = vs.u[0];
+    f.v = vs.v[0];
+    f.w = vs.w;
     return launch_march(ctx, g, m, f, st, partials);
 }
 template int launch_init<double, true>(dare_ctx*, const GridDev&, const MarchCfg&, const OpT<double>&,
@@ -140,17 +149,53 @@ int launch_iteration(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbl
     const int a = par, b = 1 - par;
     cudaStream_t sm = ctx->stream;
     int rc;
+    using F1 = FStep1<T, UNIT>;
+    using F2 = FStep2<T, UNIT>;
+    using F3 = FStep3<T, UNIT>;
+    using F4 = FStep4<T, UNIT>;
+    constexpr int NC = NCoef<UNIT>::value;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[0], sm));
-    FStep1<T, UNIT> f1{op, vs.r[a], vs.u[a], vs.rh, vs.u[b], vs.v[0], T(0)};
+    F1 f1{};
+    f1.zs[0] = vs.r[a];
+    f1.zs[1] = vs.u[a];
+    set_coef_streams<T, UNIT, F1::NP>(op, f1.ps);
+    f1.ps[NC] = vs.rh;
+    f1.u_out = vs.u[b];
+    f1.v = vs.v[0];
     if ((rc = launch_march(ctx, g, m, f1, st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[1], sm));
-    FStep2<T, UNIT> f2{op, vs.r[a], vs.v[0], vs.u[b], vs.rh, vs.r[b], vs.s[0], vs.x, T(0)};
+    F2 f2{};
+    f2.zs[0] = vs.v[0];
+    f2.zs[1] = vs.r[a];
+    set_coef_streams<T, UNIT, F2::NP>(op, f2.ps);
+    f2.ps[NC] = vs.rh;
+    f2.ps[NC + 1] = vs.u[b];
+    f2.ps[NC + 2] = vs.x;
+    f2.r_out = vs.r[b];
+    f2.s = vs.s[0];
+    f2.x = vs.x;
     if ((rc = launch_march(ctx, g, m, f2, st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[2], sm));
-    FStep3<T, UNIT> f3{op, vs.s[0], vs.v[0], vs.rh, vs.v[1], vs.w, T(0)};
+    F3 f3{};
+    f3.zs[0] = vs.s[0];
+    f3.zs[1] = vs.v[0];
+    set_coef_streams<T, UNIT, F3::NP>(op, f3.ps);
+    f3.ps[NC] = vs.rh;
+    f3.v_out = vs.v[1];
+    f3.w = vs.w;
     if ((rc = launch_march(ctx, g, m, f3, st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[3], sm));
-    FStep4<T, UNIT> f4{op, vs.u[b], vs.r[b], vs.v[1], vs.s[0], vs.w, vs.s[1], vs.t, T(0), T(0)};
+    F4 f4{};
+    f4.zs[0] = vs.w;
+    f4.zs[1] = vs.s[0];
+    set_coef_streams<T, UNIT, F4::NP>(op, f4.ps);
+    f4.ps[NC] = vs.r[b];
+    f4.ps[NC + 1] = vs.u[b];
+    f4.ps[NC + 2] = vs.v[1];
+    f4.u = vs.u[b];
+    f4.r = vs.r[b];
+    f4.s_out = vs.s[1];
+    f4.t = vs.t;
     if ((rc = launch_march(ctx, g, m, f4, st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[4], sm));
     k_step5<T><<<sblocks, 256, 0, sm>>>(g.ncell, vs.x, vs.r[b], vs.s[1], vs.t, vs.u[b], vs.v[1], vs.w, vs.rh, st,
@@ -168,7 +213,11 @@ template int launch_iteration<float, true>(dare_ctx*, const GridDev&, const Marc
 
 int launch_true_residual(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const OpT<double>& op,
                          const double* x, const double* b, SolverState* st, double* partials, double* out) {
-    FResidual<double> f{op, x, b, out};
+    FResidual<double> f{};
+    f.zs[0] = x;
+    set_coef_streams<double, false, 8>(op, f.ps);
+    f.ps[7] = b;
+    f.out = out;
     return launch_march(ctx, g, m, f, st, partials);
 }
 
@@ -177,7 +226,11 @@ int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double
     const int eb = grid_blocks(ctx, g.ncell, 256, 8);
     k_invdiag<<<eb, 256, 0, ctx->stream>>>(diag, invd, g.ncell);
     DARE_LAUNCHED(ctx);
-    FFold f{diag, invd, ahat, g.ncell};
+    FFold f{};
+    f.zs[0] = invd;
+    for (int q = 0; q < 6; q++) f.ps[q] = diag + (q + 1) * g.ncell;
+    f.ahat = ahat;
+    f.n = g.ncell;
     return launch_march(ctx, g, m, f, st, partials);
 }
 
@@ -288,14 +341,14 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
 
     OpT<double> full{s->diag, s->diag + n, n};
     OpT<double> folded{nullptr, ws->ahat, n};
-    if (jacobi) {
-        if ((rc = launch_fold(ctx, g, m, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
-    }
-    SolverState init{};
+    SolverState init{};   // also zeroes the reduction and queue counters
     init.tol = p->tol;
     init.max_it = p->max_it;
     init.tol_relative = p->tol_relative;
     DARE_CUDA(ctx, cudaMemcpyAsync(ws->st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    if (jacobi) {
+        if ((rc = launch_fold(ctx, g, m, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
+    }
     VecsT<double> vs = carve_vecs<double>(ws->vec, n, s->x, s->rhs);
     rc = jacobi ? launch_init<double, true>(ctx, g, m, folded, vs, ws->st, ws->partials)
                 : launch_init<double, false>(ctx, g, m, full, vs, ws->st, ws->partials);

@@ -15,7 +15,9 @@ struct SolverState {
     double alpha, beta, rho0, rho1, gamma, omega1, omega2, mu, nu, tau;
     double rnorm, rnorm0, bnorm2, tol;
     int k, max_it, done, status, step, tol_relative;
-    unsigned int count;
+    unsigned int count;   // reduction arrivals (reset by the last arrival)
+    unsigned int queue;   // next work item of a marching kernel
+    unsigned int exitc;   // blocks that left a marching kernel (the last resets queue)
 };
 
 template <typename T>
@@ -38,10 +40,13 @@ struct VecsT {
     T* t;
 };
 
+// Work decomposition of the marching kernels: (j,k) tiles of block.x by
+// block.y cells, runs of `planes` i-planes; item = chunk * tiles + tile.
 struct MarchCfg {
-    dim3 grid, block;
-    int chunk = 1;
-    int nblocks = 1;
+    dim3 block;
+    int tiles_x = 1, tiles_y = 1;
+    int planes = 1;
+    int nitems = 1;
     size_t smem = 0;
 };
 

@@ -1,6 +1,17 @@
 // dare_march.cuh -- device side of the BiCGStab(2) kernels: the scalar
 // recurrences of BiCGStab2.inl, the fused stencil functors and the
 // plane-marching stencil kernel they run in.
+//
+// The marching kernel is persistent: one grid of (blocks per SM x SMs)
+// blocks pulls equal work items -- a (j,k) tile and a run of i-planes -- from
+// a device queue.  Inside an item the block walks along i.  Every plane is
+// staged in shared memory by asynchronous copies (cp.async): the inputs of the
+// fused SpMV operand with a one-cell j/k halo, and the per-cell streams of the
+// centre step (coefficients, vectors).  A ring of three stages keeps the
+// copies of planes i+1 and i+2 in flight while plane i computes, so HBM
+// latency hides behind the arithmetic without holding data in registers.
+// Dot-product partials are kept per item and summed in item order by the
+// last item, so results do not depend on which block took which item.
 #pragma once
 
 #include "dare_bicgstab2.cuh"
@@ -8,7 +19,7 @@
 namespace dare_gpu {
 
 // ---------------------------------------------------------------------------
-// scalar recurrences, run by thread 0 of the last block of a kernel
+// scalar recurrences, run by thread 0 of the block that finishes last
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void finish(SolverState* st, int status, int step) {
     st->status = status;
@@ -105,39 +116,55 @@ __device__ inline void finish_update(SolverState* st, const double* tot) {      
 }
 
 // ---------------------------------------------------------------------------
-// fused stencil functors for the marching kernel
-//   z(c):      the fused SpMV input at cell c
-//   center():  everything done at the cell (writes, the SpMV row, dot terms)
-//   done():    the scalar step, thread 0 of the last block
+// operator rows: p[0..5] = W,E,S,N,B,T off-diagonals, p[6] = centre (general
+// operator only); z[0..6] = C,W,E,S,N,B,T values of the SpMV operand
 // ---------------------------------------------------------------------------
+template <bool UNIT>
+struct NCoef {
+    static constexpr int value = UNIT ? 6 : 7;
+};
+
 template <typename T, bool UNIT>
-__device__ __forceinline__ T apply7(const OpT<T>& op, int64_t c, const T z[7]) {
-    const int64_t n = op.n;
-    T y = UNIT ? z[0] : op.c[c] * z[0];
-    y += op.off[c] * z[1];
-    y += op.off[n + c] * z[2];
-    y += op.off[2 * n + c] * z[3];
-    y += op.off[3 * n + c] * z[4];
-    y += op.off[4 * n + c] * z[5];
-    y += op.off[5 * n + c] * z[6];
+__device__ __forceinline__ T apply_pre(const T* p, const T (&z)[7]) {
+    T y = UNIT ? z[0] : p[6] * z[0];
+    y += p[0] * z[1];
+    y += p[1] * z[2];
+    y += p[2] * z[3];
+    y += p[3] * z[4];
+    y += p[4] * z[5];
+    y += p[5] * z[6];
     return y;
 }
+
+template <typename T, bool UNIT, int NP>
+__host__ __device__ inline void set_coef_streams(const OpT<T>& op, const T* (&ps)[NP]) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) ps[q] = op.off + q * op.n;
+    if (!UNIT) ps[6] = op.c;
+}
+
+// ---------------------------------------------------------------------------
+// fused stencil functors (plain data, built on the host)
+//   zs[NZ] / zc(a, b):   the SpMV operand z = zc(zs[0][c], zs[1][c])
+//   ps[NP]:              per-cell streams staged for the centre step
+//   center(c, z, p, acc): writes, the SpMV row, dot-product terms
+//   done(st, tot):       the scalar step, by the block finishing the last item
+// ---------------------------------------------------------------------------
 
 // K0: r = b - Op x; r_hat_0 = r; u = v = w = 0; sums <r,r>, <b,b>
 template <typename T, bool UNIT>
 struct FInit {
     using type = T;
-    static constexpr int Q = 2;
+    static constexpr int Q = 2, NZ = 1, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = false;
-    OpT<T> op;
-    const T* x;
-    const T* b;
+    const T* zs[2];   // x
+    const T* ps[NP];  // coefficients, b
     T *r, *rh, *u, *v, *w;
     __device__ void load(const SolverState*) {}
-    __device__ T z(int64_t c) const { return x[c]; }
-    __device__ void center(int64_t c, const T zz[7], double* acc) const {
-        const T bc = b[c];
-        const T rr = bc - apply7<T, UNIT>(op, c, zz);
+    __device__ T zc(T a, T) const { return a; }
+    __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
+        const T bc = p[NC];
+        const T rr = bc - apply_pre<T, UNIT>(p, zz);
         r[c] = rr;
         rh[c] = rr;
         u[c] = T(0);
@@ -153,19 +180,19 @@ struct FInit {
 template <typename T, bool UNIT>
 struct FStep1 {
     using type = T;
-    static constexpr int Q = 1;
+    static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
-    OpT<T> op;
-    const T *r, *u_in, *rh;
+    const T* zs[2];   // r, u
+    const T* ps[NP];  // coefficients, r_hat_0
     T *u_out, *v;
     T beta;
     __device__ void load(const SolverState* st) { beta = (T)st->beta; }
-    __device__ T z(int64_t c) const { return r[c] - beta * u_in[c]; }
-    __device__ void center(int64_t c, const T zz[7], double* acc) const {
+    __device__ T zc(T r, T u) const { return r - beta * u; }
+    __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
         u_out[c] = zz[0];
-        const T vc = apply7<T, UNIT>(op, c, zz);
+        const T vc = apply_pre<T, UNIT>(p, zz);
         v[c] = vc;
-        acc[0] += (double)vc * (double)rh[c];
+        acc[0] += (double)vc * (double)p[NC];
     }
     __device__ void done(SolverState* st, const double* tot) const { finish_gamma(st, tot, 7); }
 };
@@ -174,20 +201,20 @@ struct FStep1 {
 template <typename T, bool UNIT>
 struct FStep2 {
     using type = T;
-    static constexpr int Q = 1;
+    static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 3;
     static constexpr bool kCheckDone = true;
-    OpT<T> op;
-    const T *r_in, *v, *u, *rh;
+    const T* zs[2];   // v, r
+    const T* ps[NP];  // coefficients, r_hat_0, u, x
     T *r_out, *s, *x;
     T alpha;
     __device__ void load(const SolverState* st) { alpha = (T)st->alpha; }
-    __device__ T z(int64_t c) const { return -alpha * v[c] + r_in[c]; }
-    __device__ void center(int64_t c, const T zz[7], double* acc) const {
+    __device__ T zc(T v, T r) const { return -alpha * v + r; }
+    __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
         r_out[c] = zz[0];
-        const T sc = apply7<T, UNIT>(op, c, zz);
+        const T sc = apply_pre<T, UNIT>(p, zz);
         s[c] = sc;
-        x[c] = alpha * u[c] + x[c];
-        acc[0] += (double)rh[c] * (double)sc;
+        x[c] = alpha * p[NC + 1] + p[NC + 2];
+        acc[0] += (double)p[NC] * (double)sc;
     }
     __device__ void done(SolverState* st, const double* tot) const { finish_rho(st, tot); }
 };
@@ -196,19 +223,19 @@ struct FStep2 {
 template <typename T, bool UNIT>
 struct FStep3 {
     using type = T;
-    static constexpr int Q = 1;
+    static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
-    OpT<T> op;
-    const T *s, *v_in, *rh;
+    const T* zs[2];   // s, v
+    const T* ps[NP];  // coefficients, r_hat_0
     T *v_out, *w;
     T beta;
     __device__ void load(const SolverState* st) { beta = (T)st->beta; }
-    __device__ T z(int64_t c) const { return s[c] - beta * v_in[c]; }
-    __device__ void center(int64_t c, const T zz[7], double* acc) const {
+    __device__ T zc(T s, T v) const { return s - beta * v; }
+    __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
         v_out[c] = zz[0];
-        const T wc = apply7<T, UNIT>(op, c, zz);
+        const T wc = apply_pre<T, UNIT>(p, zz);
         w[c] = wc;
-        acc[0] += (double)wc * (double)rh[c];
+        acc[0] += (double)wc * (double)p[NC];
     }
     __device__ void done(SolverState* st, const double* tot) const { finish_gamma(st, tot, 14); }
 };
@@ -218,25 +245,24 @@ struct FStep3 {
 template <typename T, bool UNIT>
 struct FStep4 {
     using type = T;
-    static constexpr int Q = 5;
+    static constexpr int Q = 5, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 3;
     static constexpr bool kCheckDone = true;
-    OpT<T> op;
-    T *u, *r;
-    const T *v, *s_in, *w;
-    T *s_out, *t;
+    const T* zs[2];   // w, s
+    const T* ps[NP];  // coefficients, r, u, v
+    T *u, *r, *s_out, *t;
     T alpha, beta;
     __device__ void load(const SolverState* st) {
         alpha = (T)st->alpha;
         beta = (T)st->beta;
     }
-    __device__ T z(int64_t c) const { return -alpha * w[c] + s_in[c]; }
-    __device__ void center(int64_t c, const T zz[7], double* acc) const {
-        const T rc = r[c];
-        u[c] = rc - beta * u[c];
-        const T rn = -alpha * v[c] + rc;
+    __device__ T zc(T w, T s) const { return -alpha * w + s; }
+    __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
+        const T rc = p[NC];
+        u[c] = rc - beta * p[NC + 1];
+        const T rn = -alpha * p[NC + 2] + rc;
         r[c] = rn;
         s_out[c] = zz[0];
-        const T tc = apply7<T, UNIT>(op, c, zz);
+        const T tc = apply_pre<T, UNIT>(p, zz);
         t[c] = tc;
         const double dr = rn, ds = zz[0], dt = tc;
         acc[0] += dr * ds;
@@ -248,123 +274,279 @@ struct FStep4 {
     __device__ void done(SolverState* st, const double* tot) const { finish_omega(st, tot); }
 };
 
-// ||b - A x||^2 with a general operator, written to *out
+// ||b - A x||_2 with the general operator, written to *out
 template <typename T>
 struct FResidual {
     using type = T;
-    static constexpr int Q = 1;
+    static constexpr int Q = 1, NZ = 1, NP = 8;
     static constexpr bool kCheckDone = false;
-    OpT<T> op;
-    const T* x;
-    const T* b;
+    const T* zs[2];   // x
+    const T* ps[NP];  // 7 coefficients, b
     double* out;
     __device__ void load(const SolverState*) {}
-    __device__ T z(int64_t c) const { return x[c]; }
-    __device__ void center(int64_t c, const T zz[7], double* acc) const {
-        const double r = (double)b[c] - (double)apply7<T, false>(op, c, zz);
+    __device__ T zc(T a, T) const { return a; }
+    __device__ void center(int64_t, const T (&zz)[7], const T* p, double* acc) const {
+        const double r = (double)p[7] - (double)apply_pre<T, false>(p, zz);
         acc[0] += r * r;
     }
     __device__ void done(SolverState*, const double* tot) const { *out = sqrt(tot[0]); }
 };
 
-// Ahat[p][c] = A[p][c] * invd[neighbour_p(c)] (removed neighbours read 0)
+// Ahat[q][c] = A[q][c] * invd[neighbour_q(c)] (removed neighbours read 0)
 struct FFold {
     using type = double;
-    static constexpr int Q = 0;
+    static constexpr int Q = 0, NZ = 1, NP = 6;
     static constexpr bool kCheckDone = false;
-    const double* diag;
-    const double* invd;
+    const double* zs[2];   // invd
+    const double* ps[NP];  // the 6 off-diagonals of A
     double* ahat;
     int64_t n;
     __device__ void load(const SolverState*) {}
-    __device__ double z(int64_t c) const { return invd[c]; }
-    __device__ void center(int64_t c, const double zz[7], double*) const {
+    __device__ double zc(double a, double) const { return a; }
+    __device__ void center(int64_t c, const double (&zz)[7], const double* p, double*) const {
 #pragma unroll
-        for (int p = 1; p < 7; p++) ahat[(p - 1) * n + c] = diag[p * n + c] * zz[p];
+        for (int q = 0; q < 6; q++) ahat[q * n + c] = p[q] * zz[q + 1];
     }
     __device__ void done(SolverState*, const double*) const {}
 };
 
 // ---------------------------------------------------------------------------
-// the plane-marching kernel
+// item reduction: partials are indexed by item; the item whose counter
+// increment completes the set sums them in item order.
+// ---------------------------------------------------------------------------
+template <int Q>
+__device__ bool item_reduce(double (&v)[Q], double* __restrict__ partials, int item, int nitems,
+                            unsigned int* counter, double (&tot)[Q]) {
+    __shared__ double sh[32 * kMaxQ];
+    __shared__ bool is_last;
+    block_sum<Q>(v, sh);
+    const int tid = thread_linear();
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) partials[q * kMaxBlocks + item] = v[q];
+        __threadfence();
+        const unsigned prev = atomicAdd(counter, 1u);
+        is_last = (prev == (unsigned)nitems - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double a[Q];
+#pragma unroll
+    for (int q = 0; q < Q; q++) a[q] = 0.;
+    const int nt = blockDim.x * blockDim.y;
+    for (int b = tid; b < nitems; b += nt) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) a[q] += __ldcg(partials + q * kMaxBlocks + b);
+    }
+    block_sum<Q>(a, sh);
+#pragma unroll
+    for (int q = 0; q < Q; q++) tot[q] = a[q];
+    if (tid == 0) *counter = 0u;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// asynchronous global -> shared copies (zero-filled when src_bytes == 0)
+// ---------------------------------------------------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int src = valid ? BYTES : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Shared-memory bytes of one marching block for functor K.
+template <class K>
+__host__ __device__ constexpr size_t march_stage_elems(int tk, int tj) {
+    return (size_t)K::NZ * (tk + 2) * (tj + 2) + (size_t)K::NP * tk * tj;
+}
+template <class K>
+inline size_t march_smem_bytes(const MarchCfg& m) {
+    return 3 * march_stage_elems<K>(m.block.x, m.block.y) * sizeof(typename K::type);
+}
+
+// ---------------------------------------------------------------------------
+// the persistent plane-marching kernel
 // ---------------------------------------------------------------------------
 template <class K>
-__global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* st, double* partials, int chunk) {
+__global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* st, double* partials, MarchCfg m) {
     using T = typename K::type;
+    constexpr int NZ = K::NZ, NP = K::NP;
+    constexpr int QA = K::Q > 0 ? K::Q : 1;
     if (K::kCheckDone && st->done) return;
     K k = kern;
     k.load(st);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* tile = reinterpret_cast<T*>(smem_raw);
+    T* smem = reinterpret_cast<T*>(smem_raw);
+    __shared__ int s_item;
     const int TK = blockDim.x, TJ = blockDim.y;
     const int W = TK + 2, H = TJ + 2;
+    const int ZT = W * H;                       // one staged operand tile
+    const int STAGE = NZ * ZT + NP * TK * TJ;   // elements per stage
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int kk = blockIdx.x * TK + tx, jj = blockIdx.y * TJ + ty;
+    const int tid = tx + TK * ty;
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
-    const int i0 = blockIdx.z * chunk;
-    const int i1 = min(i0 + chunk, n0);
-    const bool inside = jj < n1 && kk < n2;
-    const bool edge = jj <= n1 && kk <= n2;   // the first row / column past the grid is read as halo
     const int p0 = g.periodic[0], p1 = g.periodic[1], p2 = g.periodic[2];
+    const int64_t plane = (int64_t)n1 * n2;
+    const int tiles = m.tiles_x * m.tiles_y;
 
-    // fused input at (i, j, kx); wrapped on periodic dimensions, 0 outside
-    auto Zat = [&](int i, int j, int kx) -> T {
-        if (i < 0) {
-            if (!p0) return T(0);
-            i += n0;
-        } else if (i >= n0) {
-            if (!p0) return T(0);
-            i -= n0;
-        }
-        if (j < 0) {
-            if (!p1) return T(0);
-            j += n1;
-        } else if (j >= n1) {
-            if (!p1) return T(0);
-            j -= n1;
-        }
-        if (kx < 0) {
-            if (!p2) return T(0);
-            kx += n2;
-        } else if (kx >= n2) {
-            if (!p2) return T(0);
-            kx -= n2;
-        }
-        if ((unsigned)i >= (unsigned)n0 || (unsigned)j >= (unsigned)n1 || (unsigned)kx >= (unsigned)n2) return T(0);
-        return k.z(((int64_t)i * n1 + j) * n2 + kx);
-    };
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(&st->queue, 1u);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= m.nitems) break;
+        const int tile_id = item % tiles;
+        const int chunk = item / tiles;
+        const int kk = (tile_id % m.tiles_x) * TK + tx;
+        const int jj = (tile_id / m.tiles_x) * TJ + ty;
+        const int i0 = chunk * m.planes;
+        const int i1 = min(i0 + m.planes, n0);
+        const bool inside = jj < n1 && kk < n2;
+        const bool edge = jj <= n1 && kk <= n2;   // the first row / column past the grid is read as halo
+        const bool hS = inside && ty == 0, hN = inside && ty == TJ - 1;
+        const bool hB = inside && tx == 0, hT = inside && tx == TK - 1;
 
-    double acc[K::Q > 0 ? K::Q : 1];
+        // in-plane position (j, kx) -> wrapped offset, or -1 when outside (zero)
+        auto jk_offset = [&](int j, int kx) -> int64_t {
+            if (j < 0) {
+                if (!p1) return -1;
+                j += n1;
+            } else if (j >= n1) {
+                if (!p1) return -1;
+                j -= n1;
+            }
+            if (kx < 0) {
+                if (!p2) return -1;
+                kx += n2;
+            } else if (kx >= n2) {
+                if (!p2) return -1;
+                kx -= n2;
+            }
+            if ((unsigned)j >= (unsigned)n1 || (unsigned)kx >= (unsigned)n2) return -1;
+            return (int64_t)j * n2 + kx;
+        };
+        const int64_t o_c = edge ? jk_offset(jj, kk) : -1;
+        const int64_t o_s = hS ? jk_offset(jj - 1, kk) : -1;
+        const int64_t o_n = hN ? jk_offset(jj + 1, kk) : -1;
+        const int64_t o_b = hB ? jk_offset(jj, kk - 1) : -1;
+        const int64_t o_t = hT ? jk_offset(jj, kk + 1) : -1;
+        const int64_t o_own = inside ? (int64_t)jj * n2 + kk : 0;
+
+        // Stage plane p into ring slot `slot`: operand inputs with halo, and
+        // (when `full`) the per-cell streams.  Out-of-range planes are zeros.
+        auto stage = [&](int p, int slot, bool full) {
+            T* sb = smem + (size_t)slot * STAGE;
+            bool pv = true;
+            int pp = p;
+            if (pp < 0) {
+                pv = p0;
+                pp += n0;
+            } else if (pp >= n0) {
+                pv = p0;
+                pp -= n0;
+            }
+            const int64_t base = (int64_t)pp * plane;
 #pragma unroll
-    for (int q = 0; q < (K::Q > 0 ? K::Q : 1); q++) acc[q] = 0.;
-    T zprev = inside ? Zat(i0 - 1, jj, kk) : T(0);
-    T zcur = edge ? Zat(i0, jj, kk) : T(0);
-    int buf = 0;
-    for (int i = i0; i < i1; i++) {
-        const T znext = edge ? Zat(i + 1, jj, kk) : T(0);
-        T* tb = tile + buf * W * H;
-        tb[(ty + 1) * W + tx + 1] = zcur;
-        if (inside) {
-            if (ty == 0) tb[tx + 1] = Zat(i, jj - 1, kk);
-            if (ty == TJ - 1) tb[(TJ + 1) * W + tx + 1] = Zat(i, jj + 1, kk);
-            if (tx == 0) tb[(ty + 1) * W] = Zat(i, jj, kk - 1);
-            if (tx == TK - 1) tb[(ty + 1) * W + TK + 1] = Zat(i, jj, kk + 1);
+            for (int z = 0; z < NZ; z++) {
+                const T* src = k.zs[z];
+                T* zt = sb + z * ZT;
+                cp_async<sizeof(T)>(zt + (ty + 1) * W + tx + 1, src + base + (o_c < 0 ? 0 : o_c), pv && o_c >= 0);
+                if (hS) cp_async<sizeof(T)>(zt + tx + 1, src + base + (o_s < 0 ? 0 : o_s), pv && o_s >= 0);
+                if (hN) cp_async<sizeof(T)>(zt + (TJ + 1) * W + tx + 1, src + base + (o_n < 0 ? 0 : o_n),
+                                            pv && o_n >= 0);
+                if (hB) cp_async<sizeof(T)>(zt + (ty + 1) * W, src + base + (o_b < 0 ? 0 : o_b), pv && o_b >= 0);
+                if (hT) cp_async<sizeof(T)>(zt + (ty + 1) * W + TK + 1, src + base + (o_t < 0 ? 0 : o_t),
+                                            pv && o_t >= 0);
+            }
+            if (full && inside) {
+                T* pt = sb + NZ * ZT + tid;
+#pragma unroll
+                for (int q = 0; q < NP; q++) cp_async<sizeof(T)>(pt + q * TK * TJ, k.ps[q] + base + o_own, true);
+            }
+        };
+        auto slot_of = [&](int p) { return (p - i0 + 1) % 3; };
+        auto zval = [&](const T* sb, int row, int col) -> T {
+            const T a = sb[row * W + col];
+            const T b = NZ > 1 ? sb[ZT + row * W + col] : T(0);
+            return k.zc(a, b);
+        };
+
+        double acc[QA];
+#pragma unroll
+        for (int q = 0; q < QA; q++) acc[q] = 0.;
+        // prologue: planes i0-1 (operand only), i0, i0+1
+        stage(i0 - 1, slot_of(i0 - 1), false);
+        cp_async_commit();
+        stage(i0, slot_of(i0), true);
+        cp_async_commit();
+        stage(i0 + 1, slot_of(i0 + 1), i0 + 1 < i1);
+        cp_async_commit();
+        cp_async_wait<2>();
+        __syncthreads();
+        T zprev = inside ? zval(smem + (size_t)slot_of(i0 - 1) * STAGE, ty + 1, tx + 1) : T(0);
+        __syncthreads();
+        for (int i = i0; i < i1; i++) {
+            if (i + 2 <= i1) stage(i + 2, slot_of(i + 2), i + 2 < i1);   // reuses the slot of plane i-1
+            cp_async_commit();
+            cp_async_wait<1>();                 // planes i and i+1 have landed
+            __syncthreads();
+            const T* sb = smem + (size_t)slot_of(i) * STAGE;
+            const T* sn = smem + (size_t)slot_of(i + 1) * STAGE;
+            if (inside) {
+                const T zcur = zval(sb, ty + 1, tx + 1);
+                const T z7[7] = {zcur, zprev, zval(sn, ty + 1, tx + 1), zval(sb, ty, tx + 1), zval(sb, ty + 2, tx + 1),
+                                 zval(sb, ty + 1, tx), zval(sb, ty + 1, tx + 2)};
+                T pv[NP];
+#pragma unroll
+                for (int q = 0; q < NP; q++) pv[q] = sb[NZ * ZT + q * TK * TJ + tid];
+                k.center((int64_t)i * plane + o_own, z7, pv, acc);
+                zprev = zcur;
+            }
+            __syncthreads();                    // slot of plane i is free for plane i+3
+        }
+        cp_async_wait<0>();
+        if constexpr (K::Q > 0) {
+            double tot[K::Q];
+            if (item_reduce<K::Q>(acc, partials, item, m.nitems, &st->count, tot) && tid == 0) k.done(st, tot);
         }
         __syncthreads();
-        if (inside) {
-            const T z7[7] = {zcur, zprev, znext, tb[ty * W + tx + 1], tb[(ty + 2) * W + tx + 1],
-                             tb[(ty + 1) * W + tx], tb[(ty + 1) * W + tx + 2]};
-            k.center(((int64_t)i * n1 + jj) * n2 + kk, z7, acc);
+    }
+    // the last block out resets the queue for the next launch
+    if (tid == 0) {
+        const unsigned prev = atomicAdd(&st->exitc, 1u);
+        if (prev == gridDim.x - 1) {
+            st->queue = 0u;
+            st->exitc = 0u;
+            __threadfence();
         }
-        zprev = zcur;
-        zcur = znext;
-        buf ^= 1;
     }
-    if constexpr (K::Q > 0) {
-        double tot[K::Q];
-        if (!grid_reduce<K::Q>(acc, partials, &st->count, tot)) return;
-        if (threadIdx.x == 0 && threadIdx.y == 0) k.done(st, tot);
+}
+
+template <class K>
+inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
+                        double* partials) {
+    if (m.nitems > kMaxBlocks) return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
+    const size_t smem = march_smem_bytes<K>(m);
+    static int per_sm = 0;
+    static size_t per_sm_smem = 0;
+    if (per_sm == 0 || per_sm_smem != smem) {
+        if (smem > 48 * 1024)
+            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K>, m.block.x * m.block.y, smem);
+        if (per_sm < 1) per_sm = 1;
+        per_sm_smem = smem;
     }
+    int blocks = per_sm * ctx->num_sms;
+    if (blocks > m.nitems) blocks = m.nitems;
+    k_march<K><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, m);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
 }
 
 // K5: (24) x = x + w1 r + w2 s + alpha u; (25) r = r - w1 s - w2 t; ||r||;
@@ -403,15 +585,6 @@ static __global__ void k_invdiag(const double* __restrict__ dc, double* __restri
 static __global__ void k_scale(int64_t n, const double* __restrict__ invd, double* __restrict__ x) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
         x[c] = invd[c] * x[c];
-}
-
-template <class K>
-inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
-                        double* partials) {
-    if (m.nblocks > kMaxBlocks) return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
-    k_march<K><<<m.grid, m.block, m.smem, ctx->stream>>>(g, kern, st, partials, m.chunk);
-    DARE_LAUNCHED(ctx);
-    return DARE_OK;
 }
 
 }  // namespace dare_gpu

@@ -61,18 +61,17 @@ static __global__ void __launch_bounds__(256) k_norm(int64_t n, const double* __
 // r = b - A x in FP64; r32 = (float) r; dy = 0; ||r||_2 -> *out
 struct FRefResidual {
     using type = double;
-    static constexpr int Q = 1;
+    static constexpr int Q = 1, NZ = 1, NP = 8;
     static constexpr bool kCheckDone = false;
-    OpT<double> op;
-    const double* x;
-    const double* b;
+    const double* zs[2];   // x
+    const double* ps[NP];  // 7 coefficients, b
     float* r32;
     float* dy;
     double* out;
     __device__ void load(const SolverState*) {}
-    __device__ double z(int64_t c) const { return x[c]; }
-    __device__ void center(int64_t c, const double zz[7], double* acc) const {
-        const double r = b[c] - apply7<double, false>(op, c, zz);
+    __device__ double zc(double a, double) const { return a; }
+    __device__ void center(int64_t c, const double (&zz)[7], const double* p, double* acc) const {
+        const double r = p[7] - apply_pre<double, false>(p, zz);
         r32[c] = (float)r;
         dy[c] = 0.f;
         acc[0] += r * r;
@@ -137,7 +136,13 @@ int dare_bicgstab2_refine(dare_system* s, const dare_solver_params* p, dare_solv
     bool converged = false;
     int refinements = 0, inner_total = 0;
     for (int it = 0; it <= p->max_refinements; it++) {
-        FRefResidual fr{full, s->x, s->rhs, r32, dy, scratch};
+        FRefResidual fr{};
+        fr.zs[0] = s->x;
+        set_coef_streams<double, false, 8>(full, fr.ps);
+        fr.ps[7] = s->rhs;
+        fr.r32 = r32;
+        fr.dy = dy;
+        fr.out = scratch;
         if ((rc = launch_march(ctx, g, m, fr, ws->st, ws->partials))) return rc;
         if ((rc = read_scalar(ctx, scratch, &rnorm))) return rc;
         if (rnorm <= tol_abs) {
