@@ -63,7 +63,26 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    build_examples(force, verbose)
     return LIB
+
+
+EXAMPLES = {"example_diffusion": os.path.join(HERE, "cxx", "example_diffusion.cpp")}
+BIN = os.path.join(HERE, "bin")
+
+
+def build_examples(force: bool = False, verbose: bool = False) -> None:
+    """C++ programs written against include/dare_gpu.hpp, linked to the library."""
+    os.makedirs(BIN, exist_ok=True)
+    hdrs = [os.path.join(ROOT, "include", "dare_gpu.hpp"), os.path.join(ROOT, "include", "dare_gpu.h"), LIB]
+    for name, src in EXAMPLES.items():
+        exe = os.path.join(BIN, name)
+        if force or _stale(exe, [src] + hdrs):
+            cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), src, "-L", HERE,
+                   "-ldare_gpu", "-Wl,-rpath,$ORIGIN/..", "-o", exe]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
 
 
 def main(argv=None) -> int:

@@ -62,6 +62,14 @@ def test_solver_defaults_match_reference():
     assert p.tol == 1e-8 and p.max_it == 100 and p.precond == dare_b200.PREC_JACOBI
 
 
+def test_cxx_header_compiles(tmp_path):
+    src = tmp_path / "t.cpp"
+    src.write_text('#include "dare_gpu.hpp"\nint main() { dare_b200::BiCGStab2 s({{"Maximum Iterations", 7}});'
+                   ' return s.Params().max_it == 7 ? 0 : 1; }\n')
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                    str(src)], check=True)
+
+
 def test_no_product_import_of_oracle():
     # the product package never imports the CPU checker
     for f in glob.glob(os.path.join(ROOT, "dare_b200", "**", "*.py"), recursive=True):

@@ -331,6 +331,31 @@ def test_mixed_precision_fallback(ctx):
     assert rep["true_res_abs"] <= 1e-10 * rep["b_norm"] * 1.0000001
 
 
+def test_cxx_host_api_example(tmp_path):
+    """The C++ API (include/dare_gpu.hpp) drives the same path: a DaRe-style
+    time loop in C++ matches the oracle's loop on the same inputs."""
+    import json
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "dare_b200", "bin", "example_diffusion")
+    n, steps = 20, 3
+    out = tmp_path / "phi.bin"
+    res = subprocess.run([exe, str(n), str(steps), str(out)], capture_output=True, text=True, timeout=120)
+    assert res.returncode == 0, res.stderr
+    line = json.loads(res.stdout.strip().splitlines()[-1])
+    got = np.fromfile(out, dtype=np.float64)
+    c = (np.arange(n) + 0.5) / n - 0.5
+    r2 = c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2
+    case = {"n": (n, n, n), "size": (1.0, 1.0, 1.0), "periodic": (0, 0, 0), "dt": 1e-2, "D": 1e-3,
+            "phi0": W.ghosted(np, None, np.exp(-r2 / (2.0 * 0.01))), "rel_tol": 1e-10,
+            "bc": {1: (1, 1.0), 2: (1, 0.0), 3: (2, 0.0), 4: (2, 0.0), 5: (2, 0.0), 6: (2, 0.0)}}
+    ohist, oiters = oracle_timeloop(case, steps)
+    shape = (n + 4, n + 4, n + 4)
+    assert rel_l2(interior(got, shape), interior(ohist[-1], shape)) < SOL_TOL
+    assert all(abs(a - b) <= 2 for a, b in zip(line["iters"], oiters))
+
+
 def test_profiling_mode_same_result(ctx):
     """Per-kernel event timing launches the same kernels directly; results match the graph path."""
     case = W.tvd_convection_diffusion(n=20, steps=2)
