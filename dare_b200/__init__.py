@@ -110,6 +110,8 @@ _SIGS = [
     ("dare_timestep", C.c_int, [_P, _P, C.POINTER(AssemblyDesc), C.POINTER(SolverParams),
                                 C.POINTER(SolveReport)]),
     ("dare_face_average", C.c_int, [_P, _P, C.POINTER(_P)]),
+    ("dare_residual_norm_noalloc", C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int), _P, _P, _P, _P,
+                                             _P, C.c_char_p, C.c_int]),
 ]
 
 _lib = None

@@ -34,6 +34,7 @@ SOURCES = {
     "dare_bicgstab2.cu": [],
     "dare_mixed.cu": [],
     "dare_step.cu": [],
+    "dare_noalloc.cu": [],
 }
 
 

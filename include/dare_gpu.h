@@ -219,6 +219,27 @@ DARE_API int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_de
  * cell_D: device, internal cells; face_D[d]: device, face layout above. */
 DARE_API int dare_face_average(dare_grid* g, const double* cell_D, double* face_D[3]);
 
+/* ---- residual norm without device allocation -------------------------------
+ * No counterpart in the reference (DaRe computes residuals inside Tpetra).
+ * ||b - A x||_2 of a structured 7-point system given as plain device arrays
+ * (diag7: 7 x ncells in slot order CENTER..TOP, x, b over internal cells,
+ * ordinal (i*ny + j)*nz + k; neighbours past a non-periodic face are ignored),
+ * written as one double to the device pointer norm_out, on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).  It is for callers that cannot
+ * call cudaMalloc mid-run -- host codes whose device memory is owned by their
+ * own allocator or budget, or that must not stall other streams with the
+ * device synchronization cudaMalloc implies: it allocates nothing and keeps
+ * its scratch (4096 partial sums plus counters, about 33 KB per device) in a
+ * fixed device array held until process exit.  Grids whose (j,k) plane needs
+ * more than 4096 tiles of 32 x 8 cells (ny*nz above about 1M) are rejected
+ * with DARE_ERR_UNSUPPORTED and a message in `err` (may be NULL).  All calls
+ * on a device share that array: calls that overlap on the GPU race and must
+ * be serialized by the caller.  The first call on a device looks up the
+ * array's device address, so make it before capturing any stream there. */
+DARE_API int dare_residual_norm_noalloc(int dim, const int64_t n[3], const int periodic[3], const double* diag7,
+                                        const double* x, const double* b, double* norm_out, void* stream,
+                                        char* err, int err_len);
+
 #ifdef __cplusplus
 }
 #endif
