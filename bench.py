@@ -115,13 +115,18 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+NCU_NAMES = {"assemble": "k_assemble", "step1": "k_march<FStep1>", "step2": "k_march<FStep2>",
+             "step3": "k_march<FStep3>", "step4": "k_march<FStep4>", "step5": "k_step5"}
+
+
 def ncu_traffic(kernel: str, n: int):
-    """DRAM bytes per launch from the committed ncu summary (profiles/traffic.json)."""
+    """DRAM bytes per launch (read + write) from the committed ncu summary
+    (profiles/traffic.json: per-cell figures of a 128^3 capture, scaled by
+    the cell count)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
             t = json.load(fh)
-        ent = t[kernel]
-        return ent["bytes_per_cell"] * n ** 3
+        return t[NCU_NAMES[kernel]]["bytes_per_cell"] * n ** 3
     except Exception:
         return None
 
