@@ -29,6 +29,8 @@ struct AsmParams {
     const double* face_vel[3];
     int bc_type[6];
     double bc_value[6];
+    double tt;      // (V * 1) / dt, the DDT weight (evaluated once on the host: same IEEE result)
+    double dn[3];   // 1 / dx per dimension (Gradient_Cartesian.inl:30-34)
 };
 
 __device__ __forceinline__ double limiter_value(int kind, double r) {
@@ -94,28 +96,76 @@ __device__ __forceinline__ void apply_divergence(const GridDev& g, const double 
     }
 }
 
+// One TVD face (TVD_Cartesian.inl:199-258).  The stencil line along the face
+// normal is (m2, m1, c0, p1, p2) = phi at offsets -2..+2; `upper` selects the
+// upper face.  Writes the face matrix stencil (neighbour, centre, rhs).
+__device__ __forceinline__ void tvd_face(bool upper, double m2, double m1, double c0, double p1, double p2,
+                                         double v, int limiter, double& nb, double& cf, double& rr) {
+    const int vp = v >= 0., vn = !(v >= 0.);
+    double pUU, pU, pD;
+    if (!upper) {   // UU = i + vn - 2 vp, U = i - vp, D = i - vn
+        pUU = vp ? m2 : p1;
+        pU = vp ? m1 : c0;
+        pD = vp ? c0 : m1;
+    } else {        // UU = i + 2 vn - vp, U = i + vn, D = i + vp
+        pUU = vp ? m1 : p2;
+        pU = vp ? c0 : p1;
+        pD = vp ? p1 : c0;
+    }
+    const double r = (pU - pUU) / (pD - pU);
+    const double psi = limiter_value(limiter, r);
+    if (!upper) {
+        nb = ((double)vp * v) * 1.;
+        cf = ((double)vn * v) * 1.;
+    } else {
+        nb = ((double)vn * v) * 1.;
+        cf = ((double)vp * v) * 1.;
+    }
+    rr = ((-0.5 * psi) * (pD - pU)) * v;
+}
+
+// Column-marching assembly: a thread owns one (j,k) column and walks along i
+// through `planes` planes, keeping phi(i-2..i+2) and the x-face velocity in
+// registers; addresses advance by constant strides (no per-cell index
+// division).  The arithmetic per cell is exactly the per-cell functor above.
 template <int DIM>
 __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const double* __restrict__ phi,
                                                   const double* __restrict__ phi_old, double* __restrict__ diag,
-                                                  double* __restrict__ rhs_out, double* __restrict__ x0) {
+                                                  double* __restrict__ rhs_out, double* __restrict__ x0,
+                                                  int planes) {
+    const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+    const int jj = blockIdx.y * blockDim.y + threadIdx.y;
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    if (jj >= n1 || kk >= n2) return;
+    const int i0 = blockIdx.z * planes;
+    const int i1 = min(i0 + planes, n0);
+    if (i0 >= i1) return;
     const int64_t n = g.ncell;
-    const int64_t lstride[3] = {(int64_t)g.gn[1] * g.gn[2], g.gn[2], 1};
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
-        const unsigned cc_ = (unsigned)c, nz = (unsigned)g.n[2], ny = (unsigned)g.n[1];
-        const unsigned row = cc_ / nz;
-        const int k = (int)(cc_ - row * nz);
-        const int i = (int)(row / ny);
-        const int j = (int)(row - (unsigned)i * ny);
-        const int idx[3] = {i, j, k};
-        const int64_t loc = local_index(g, i, j, k);
+    const int64_t S0 = (int64_t)g.gn[1] * g.gn[2], S1 = g.gn[2];
+    const int64_t nplane = (int64_t)n1 * n2;
+    const int64_t jk = (int64_t)jj * n2 + kk;
+    int64_t loc = local_index(g, i0, jj, kk);
+    int64_t c = (int64_t)i0 * nplane + jk;
+    // face-array offsets: x-faces (n0+1, n1, n2), y-faces (n0, n1+1, n2), z-faces (n0, n1, n2+1)
+    const int64_t fy_plane = (int64_t)(n1 + 1) * n2, fz_plane = (int64_t)n1 * (n2 + 1);
+    int64_t fy_lo = (int64_t)i0 * fy_plane + (int64_t)jj * n2 + kk;
+    int64_t fy_up = (int64_t)i0 * fy_plane + (int64_t)upper_face(g, 1, jj) * n2 + kk;
+    int64_t fz_lo = (int64_t)i0 * fz_plane + (int64_t)jj * (n2 + 1) + kk;
+    int64_t fz_up = (int64_t)i0 * fz_plane + (int64_t)jj * (n2 + 1) + upper_face(g, 2, kk);
+    double w0 = phi[loc - 2 * S0], w1 = phi[loc - S0], w2 = phi[loc], w3 = phi[loc + S0], w4 = phi[loc + 2 * S0];
+    double vx_lo = 0., Dx_lo = 0.;
+    if (a.convection == 2) vx_lo = a.face_vel[0][(int64_t)i0 * nplane + jk];
+    if (a.diffusion == 2) Dx_lo = a.face_D[0][(int64_t)i0 * nplane + jk];
+
+    for (int i = i0; i < i1; i++) {
+        const int64_t fx_up = (int64_t)upper_face(g, 0, i) * nplane + jk;
         double coef[7];
 #pragma unroll
         for (int p = 0; p < 7; p++) coef[p] = 0.;
         double rhs = 0.;
-        const double phi_c = phi[loc];
 
         if (a.dt > 0.) {                                   // DDT, weights (1, 1)
-            const double tt = (g.volume * 1.) / a.dt;
+            const double tt = a.tt;
             coef[DARE_CENTER] = tt;
             rhs = 0. + tt * phi_old[loc];
         }
@@ -124,41 +174,37 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             double nb[7], cf[7], rr[7];
 #pragma unroll
             for (int p = 0; p < 7; p++) nb[p] = cf[p] = rr[p] = 0.;
-#pragma unroll
-            for (int d = 0; d < DIM; d++) {
-                const int lo = 2 * d + 1, up = 2 * d + 2;
-                double vlo, vup;
+            double vlo, vup;
+            // x (always active)
+            if (a.convection == 1) {
+                vlo = vup = a.vel[0];
+            } else {
+                vlo = vx_lo;
+                vup = a.face_vel[0][fx_up];
+            }
+            tvd_face(false, w0, w1, w2, w3, w4, vlo, a.limiter, nb[DARE_WEST], cf[DARE_WEST], rr[DARE_WEST]);
+            tvd_face(true, w0, w1, w2, w3, w4, vup, a.limiter, nb[DARE_EAST], cf[DARE_EAST], rr[DARE_EAST]);
+            if (DIM > 1) {
+                const double m2 = phi[loc - 2 * S1], m1 = phi[loc - S1], p1 = phi[loc + S1], p2 = phi[loc + 2 * S1];
                 if (a.convection == 1) {
-                    vlo = vup = a.vel[d];
+                    vlo = vup = a.vel[1];
                 } else {
-                    int fi[3] = {i, j, k};
-                    vlo = a.face_vel[d][face_index(g, d, fi[0], fi[1], fi[2])];
-                    fi[d] = upper_face(g, d, fi[d]);
-                    vup = a.face_vel[d][face_index(g, d, fi[0], fi[1], fi[2])];
+                    vlo = a.face_vel[1][fy_lo];
+                    vup = a.face_vel[1][fy_up];
                 }
-                const int64_t s = lstride[d];
-                {   // lower face (TVD_Cartesian.inl:199-227)
-                    const int vp = vlo >= 0., vn = !(vlo >= 0.);
-                    const double pUU = phi[loc + (int64_t)(vn - 2 * vp) * s];
-                    const double pU = phi[loc - (int64_t)vp * s];
-                    const double pD = phi[loc - (int64_t)vn * s];
-                    const double r = (pU - pUU) / (pD - pU);
-                    const double psi = limiter_value(a.limiter, r);
-                    nb[lo] = ((double)vp * vlo) * 1.;
-                    cf[lo] = ((double)vn * vlo) * 1.;
-                    rr[lo] = ((-0.5 * psi) * (pD - pU)) * vlo;
+                tvd_face(false, m2, m1, w2, p1, p2, vlo, a.limiter, nb[DARE_SOUTH], cf[DARE_SOUTH], rr[DARE_SOUTH]);
+                tvd_face(true, m2, m1, w2, p1, p2, vup, a.limiter, nb[DARE_NORTH], cf[DARE_NORTH], rr[DARE_NORTH]);
+            }
+            if (DIM > 2) {
+                const double m2 = phi[loc - 2], m1 = phi[loc - 1], p1 = phi[loc + 1], p2 = phi[loc + 2];
+                if (a.convection == 1) {
+                    vlo = vup = a.vel[2];
+                } else {
+                    vlo = a.face_vel[2][fz_lo];
+                    vup = a.face_vel[2][fz_up];
                 }
-                {   // upper face (TVD_Cartesian.inl:229-258)
-                    const int vp = vup >= 0., vn = !(vup >= 0.);
-                    const double pUU = phi[loc + (int64_t)(2 * vn - vp) * s];
-                    const double pU = phi[loc + (int64_t)vn * s];
-                    const double pD = phi[loc + (int64_t)vp * s];
-                    const double r = (pU - pUU) / (pD - pU);
-                    const double psi = limiter_value(a.limiter, r);
-                    nb[up] = ((double)vn * vup) * 1.;
-                    cf[up] = ((double)vp * vup) * 1.;
-                    rr[up] = ((-0.5 * psi) * (pD - pU)) * vup;
-                }
+                tvd_face(false, m2, m1, w2, p1, p2, vlo, a.limiter, nb[DARE_BOTTOM], cf[DARE_BOTTOM], rr[DARE_BOTTOM]);
+                tvd_face(true, m2, m1, w2, p1, p2, vup, a.limiter, nb[DARE_TOP], cf[DARE_TOP], rr[DARE_TOP]);
             }
             double sc[7];
             apply_divergence<DIM>(g, nb, cf, sc);
@@ -173,26 +219,29 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
         }
 
         if (a.diffusion) {                                 // mb -= div(D, grad(mb))
+            double Dlo[3], Dup[3];
+            if (a.diffusion == 1) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) Dlo[d] = Dup[d] = a.D;
+            } else {
+                Dlo[0] = Dx_lo;
+                Dup[0] = a.face_D[0][fx_up];
+                Dlo[1] = DIM > 1 ? a.face_D[1][fy_lo] : 0.;
+                Dup[1] = DIM > 1 ? a.face_D[1][fy_up] : 0.;
+                Dlo[2] = DIM > 2 ? a.face_D[2][fz_lo] : 0.;
+                Dup[2] = DIM > 2 ? a.face_D[2][fz_up] : 0.;
+            }
             double nb[7], cf[7];
 #pragma unroll
             for (int p = 0; p < 7; p++) nb[p] = cf[p] = 0.;
 #pragma unroll
             for (int d = 0; d < DIM; d++) {
-                const double dn = 1. / g.dx[d];
+                const double dn = a.dn[d];
                 const int lo = 2 * d + 1, up = 2 * d + 2;
-                double Dlo, Dup;
-                if (a.diffusion == 1) {
-                    Dlo = Dup = a.D;
-                } else {
-                    int fi[3] = {i, j, k};
-                    Dlo = a.face_D[d][face_index(g, d, fi[0], fi[1], fi[2])];
-                    fi[d] = upper_face(g, d, fi[d]);
-                    Dup = a.face_D[d][face_index(g, d, fi[0], fi[1], fi[2])];
-                }
-                nb[lo] = (-dn) * Dlo;
-                cf[lo] = dn * Dlo;
-                nb[up] = dn * Dup;
-                cf[up] = (-dn) * Dup;
+                nb[lo] = (-dn) * Dlo[d];
+                cf[lo] = dn * Dlo[d];
+                nb[up] = dn * Dup[d];
+                cf[up] = (-dn) * Dup[d];
             }
             double sc[7];
             apply_divergence<DIM>(g, nb, cf, sc);
@@ -201,6 +250,7 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             rhs += -1. * 0.;
         }
 
+        const int idx[3] = {i, jj, kk};
 #pragma unroll
         for (int d = 0; d < DIM; d++) {                    // boundary folding
             if (g.periodic[d]) continue;
@@ -222,7 +272,24 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
 #pragma unroll
         for (int p = 0; p < 7; p++) diag[p * n + c] = coef[p];
         rhs_out[c] = rhs;
-        x0[c] = phi_c;
+        x0[c] = w2;
+
+        // advance one plane
+        if (i + 1 < i1) {
+            w0 = w1;
+            w1 = w2;
+            w2 = w3;
+            w3 = w4;
+            w4 = phi[loc + 3 * S0];
+            if (a.convection == 2) vx_lo = a.face_vel[0][fx_up];
+            if (a.diffusion == 2) Dx_lo = a.face_D[0][fx_up];
+        }
+        loc += S0;
+        c += nplane;
+        fy_lo += fy_plane;
+        fy_up += fy_plane;
+        fz_lo += fz_plane;
+        fz_up += fz_plane;
     }
 }
 
@@ -244,6 +311,8 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
         a.bc_type[f] = s->bc_type[f];
         a.bc_value[f] = s->bc_value[f];
     }
+    a.tt = a.dt > 0. ? (g.volume * 1.) / a.dt : 0.;
+    for (int d = 0; d < 3; d++) a.dn[d] = 1. / g.dx[d];
     for (int d = 0; d < g.dim; d++) {
         if (a.diffusion == 2 && !a.face_D[d]) return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: face_D missing");
         if (a.convection == 2 && !a.face_vel[d])
@@ -252,13 +321,26 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
     if (a.diffusion < 0 || a.diffusion > 2 || a.convection < 0 || a.convection > 2 || a.limiter < 0 ||
         a.limiter > DARE_LIMITER_VANLEER)
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: bad descriptor");
-    const int blocks = grid_blocks(ctx, g.ncell, 256, 8);
+    // (j,k) tiles of tk x tj columns, runs of `planes` i-planes per block
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int tk = n2 > 16 ? 32 : n2 > 8 ? 16 : n2 > 4 ? 8 : n2 > 2 ? 4 : 1;
+    int tj = 256 / tk;
+    while (tj > 1 && tj / 2 >= n1) tj /= 2;
+    const int gx = (n2 + tk - 1) / tk, gy = (n1 + tj - 1) / tj;
+    const int64_t tiles = (int64_t)gx * gy;
+    int64_t nchunk = (2 * 8 * (int64_t)ctx->num_sms + tiles - 1) / tiles;
+    if (nchunk > n0) nchunk = n0;
+    if (nchunk < 1) nchunk = 1;
+    int planes = (int)((n0 + nchunk - 1) / nchunk);
+    if (planes < 2 && n0 >= 2) planes = 2;
+    nchunk = (n0 + planes - 1) / planes;
+    const dim3 grid(gx, gy, (unsigned)nchunk), block(tk, tj, 1);
     if (g.dim == 3)
-        k_assemble<3><<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
+        k_assemble<3><<<grid, block, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x, planes);
     else if (g.dim == 2)
-        k_assemble<2><<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
+        k_assemble<2><<<grid, block, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x, planes);
     else
-        k_assemble<1><<<blocks, 256, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x);
+        k_assemble<1><<<grid, block, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x, planes);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
