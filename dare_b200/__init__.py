@@ -112,7 +112,25 @@ _SIGS = [
     ("dare_face_average", C.c_int, [_P, _P, C.POINTER(_P)]),
     ("dare_residual_norm_noalloc", C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int), _P, _P, _P, _P,
                                              _P, C.c_char_p, C.c_int]),
+    ("dare_batch_create", C.c_int, [_P, C.c_int, _P, C.POINTER(_P)]),
+    ("dare_batch_destroy", C.c_int, [_P]),
+    ("dare_batch_num_cells", C.c_int64, [_P, C.c_int]),
+    ("dare_batch_set_field", C.c_int, [_P, C.c_int, _P]),
+    ("dare_batch_get_field", C.c_int, [_P, C.c_int, _P]),
+    ("dare_batch_solve", C.c_int, [_P, _P, _P]),
+    ("dare_batch_autotune", C.c_int, [_P, _P, C.POINTER(C.c_int)]),
+    ("dare_batch_get_tuning", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
 ]
+
+
+class BatchInstance(C.Structure):
+    _fields_ = [("n", C.c_int64 * 3), ("size", C.c_double * 3), ("D", C.c_double), ("dt", C.c_double),
+                ("bc_type", C.c_int * 6), ("bc_value", C.c_double * 6)]
+
+
+class BatchReport(C.Structure):
+    _fields_ = [("iters", C.c_int), ("converged", C.c_int), ("status", C.c_int), ("breakdown_step", C.c_int),
+                ("res_abs", C.c_double), ("b_norm", C.c_double), ("tol_abs", C.c_double)]
 
 _lib = None
 
@@ -445,3 +463,65 @@ def timestep(system: MatrixSystem, field: Field, assembly: Assembly, solver: BiC
 def face_average(grid: Grid, cell_D_ptr: int, face_ptrs) -> None:
     arr = (C.c_void_p * 3)(*[p.ptr if isinstance(p, DeviceArray) else p for p in face_ptrs])
     _check(lib().dare_face_average(grid.h, cell_D_ptr, arr), grid.ctx.h, "face_average")
+
+
+class Batch:
+    """Many independent implicit diffusion steps solved in one persistent launch.
+
+    ``instances``: dicts with ``n`` (3 ints), ``size`` (3 floats), ``D``, ``dt``,
+    ``bc`` = {face: (kind, value)} for faces WEST..TOP (Dirichlet/Neumann).
+    """
+
+    def __init__(self, ctx: Context, instances):
+        self.ctx = ctx
+        arr = (BatchInstance * len(instances))()
+        for q, ins in enumerate(instances):
+            a = arr[q]
+            for d in range(3):
+                a.n[d] = int(ins["n"][d])
+                a.size[d] = float(ins.get("size", (1.0, 1.0, 1.0))[d])
+            a.D = float(ins["D"])
+            a.dt = float(ins["dt"])
+            for face in range(1, 7):
+                kind, val = ins["bc"].get(face, (BC_NEUMANN, 0.0))
+                a.bc_type[face - 1] = kind
+                a.bc_value[face - 1] = val
+        h = C.c_void_p()
+        _check(lib().dare_batch_create(ctx.h, len(instances), arr, C.byref(h)), ctx.h, "batch_create")
+        self.h = h
+        self.count = len(instances)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dare_batch_destroy(self.h)
+            self.h = None
+
+    def num_cells(self, idx: int) -> int:
+        return int(lib().dare_batch_num_cells(self.h, idx))
+
+    def set_field(self, idx: int, values: np.ndarray):
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if a.size != self.num_cells(idx):
+            raise ValueError("batch field size")
+        _check(lib().dare_batch_set_field(self.h, idx, _ptr(a)), self.ctx.h, "batch_set_field")
+
+    def get_field(self, idx: int) -> np.ndarray:
+        a = np.empty(self.num_cells(idx), dtype=np.float64)
+        _check(lib().dare_batch_get_field(self.h, idx, _ptr(a)), self.ctx.h, "batch_get_field")
+        return a
+
+    def solve(self, solver: "BiCGStab2", reports: bool = True):
+        rep = (BatchReport * self.count)() if reports else None
+        _check(lib().dare_batch_solve(self.h, C.byref(solver.params), rep), self.ctx.h, "batch_solve")
+        if not reports:
+            return None
+        return [{"iters": r.iters, "converged": bool(r.converged), "status": SOLVE_STATUS.get(r.status, r.status),
+                 "breakdown_step": r.breakdown_step, "res_abs": r.res_abs, "b_norm": r.b_norm, "tol_abs": r.tol_abs}
+                for r in rep]
+
+    def autotune(self, solver: "BiCGStab2") -> dict:
+        blk = C.c_int()
+        _check(lib().dare_batch_autotune(self.h, C.byref(solver.params), C.byref(blk)), self.ctx.h, "autotune")
+        vec = (C.c_int * 8)()
+        lib().dare_batch_get_tuning(self.h, C.byref(blk), vec)
+        return {"block": blk.value, "cells_per_thread_by_size": list(vec)}

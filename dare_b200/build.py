@@ -35,6 +35,7 @@ SOURCES = {
     "dare_mixed.cu": [],
     "dare_step.cu": [],
     "dare_noalloc.cu": [],
+    "dare_batched.cu": [],
 }
 
 

@@ -182,3 +182,20 @@ def heterogeneous(n=512, seed=0, peclet=5.0, cfl=0.5, steps=1, device=None):
         "n": nn, "size": (1.0, 1.0, 1.0), "periodic": (1, 1, 1), "cell_D": Dc, "median_D": med, "dt": dt,
         "steps": steps, "u_max": u_max, "face_vel": faces, "phi0": phi, "limiter": "VANLEER", "rel_tol": 1e-10,
     }
+
+
+def batched_diffusion(count=4096, seed=0, sides=(16, 24, 32, 48, 64), dt=1e-2, d_range=(1e-5, 1e-2)):
+    """Batch of independent cubes: side uniform from `sides`, unit size, D
+    log-uniform in `d_range`, one random face Dirichlet with a U[0,1] value,
+    Neumann on the other five, phi_0 = 0, one implicit step of `dt`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        side = int(rng.choice(sides))
+        D = float(np.exp(rng.uniform(np.log(d_range[0]), np.log(d_range[1]))))
+        face = int(rng.integers(1, 7))
+        val = float(rng.uniform(0.0, 1.0))
+        bc = {f: (2, 0.0) for f in range(1, 7)}
+        bc[face] = (1, val)
+        out.append({"n": (side, side, side), "size": (1.0, 1.0, 1.0), "D": D, "dt": dt, "bc": bc})
+    return out

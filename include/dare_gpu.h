@@ -219,6 +219,46 @@ DARE_API int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_de
  * cell_D: device, internal cells; face_D[d]: device, face layout above. */
 DARE_API int dare_face_average(dare_grid* g, const double* cell_D, double* face_D[3]);
 
+/* ---- batched uneven solves -------------------------------------------------
+ * Many independent 3D boxes, each one implicit-Euler diffusion step
+ * (DDT + div(D grad), Dirichlet/Neumann folding per face: the functor of
+ * test/Verification/counter_diffusion1D.cpp:113-146 in 3D), each solved by
+ * Jacobi-BiCGStab(2) (BiCGStab2.inl:166-582) with its own tolerance check and
+ * status, all in one persistent launch.  Fields are internal cells,
+ * ordinal (i*ny + j)*nz + k; the field is the initial guess and phi_old. */
+typedef struct {
+    int64_t n[3];          /* cells per dimension (>= 3 each) */
+    double size[3];        /* box lengths */
+    double D;              /* constant diffusivity */
+    double dt;             /* implicit Euler step */
+    int bc_type[6];        /* W,E,S,N,B,T: DARE_BC_DIRICHLET or DARE_BC_NEUMANN */
+    double bc_value[6];
+} dare_batch_instance;
+
+typedef struct {
+    int iters;
+    int converged;
+    int status;            /* DARE_SOLVE_* */
+    int breakdown_step;
+    double res_abs;        /* last recurrence residual (or true residual after a tau = 0 exit) */
+    double b_norm;
+    double tol_abs;
+} dare_batch_report;
+
+typedef struct dare_batch dare_batch;
+DARE_API int dare_batch_create(dare_ctx* ctx, int count, const dare_batch_instance* inst, dare_batch** out);
+DARE_API int dare_batch_destroy(dare_batch* bt);
+DARE_API int64_t dare_batch_num_cells(const dare_batch* bt, int idx);
+DARE_API int dare_batch_set_field(dare_batch* bt, int idx, const double* host_phi);
+DARE_API int dare_batch_get_field(dare_batch* bt, int idx, double* host_phi);
+/* Solves every instance (p: tol, tol_relative, max_it; Jacobi, FP64). The
+ * fields are replaced by the solutions; reports (host, count entries) may be NULL. */
+DARE_API int dare_batch_solve(dare_batch* bt, const dare_solver_params* p, dare_batch_report* reports);
+/* Picks the block size and the cells each thread handles per sweep (per size
+ * class) by timing solves of the current fields, which are restored. */
+DARE_API int dare_batch_autotune(dare_batch* bt, const dare_solver_params* p, int* chosen_block);
+DARE_API int dare_batch_get_tuning(const dare_batch* bt, int* block, int vec_by_size[8]);
+
 /* ---- residual norm without device allocation -------------------------------
  * No counterpart in the reference (DaRe computes residuals inside Tpetra).
  * ||b - A x||_2 of a structured 7-point system given as plain device arrays
