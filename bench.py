@@ -57,6 +57,10 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["tvd", "gauss64", "hetero", "batched"], default="tvd",
+                    help="tvd: the headline 256^3 line; the others print their own measurement line")
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--no-autotune", action="store_true")
     return ap.parse_args(argv)
 
 
@@ -281,7 +285,7 @@ def run_dare(args):
     e2e = None
     if not args.no_e2e:
         host = torch.empty(grid.num_cells_ghosted, dtype=torch.float64, pin_memory=True).numpy()
-        host[:] = field.download(0)
+        field.download(0, out=host)
         barrier()
         ctx.synchronize()
         ctx.timer_start()
@@ -289,7 +293,7 @@ def run_dare(args):
             field.upload(host, 0)
             field.copy_to_old()
             D.timestep(system, field, asm, solver)
-            host[:] = field.download(0)
+            field.download(0, out=host)
         ems = max_over_ranks(ctx.timer_stop())
         barrier()
         nbytes = grid.num_cells_ghosted * 8
@@ -326,10 +330,172 @@ def run_dare(args):
     return 0
 
 
+# ----------------------------------------------------------------------------
+# the other configurations (reported in DESIGN.md / profiles/, not the headline)
+# ----------------------------------------------------------------------------
+def _gpu_setup_field(D, ctx, case):
+    grid = D.Grid(ctx, case["n"], case["size"], 2, case["periodic"])
+    field = D.Field(grid, 2)
+    return grid, field
+
+
+def run_gauss64(args):
+    """64^3 transient diffusion (Gaussian bump, Dirichlet x, Neumann elsewhere), 10 steps."""
+    import dare_b200 as D
+    from dare_b200 import workloads as W
+    from oracle import oracle as O
+    from tests.helpers import oracle_timeloop
+    case = W.gaussian_diffusion(n=64, seed=args.seed, steps=10)
+    ctx = D.Context(0)
+    grid, field = _gpu_setup_field(D, ctx, case)
+    system = D.MatrixSystem(grid)
+    for face, (kind, val) in case["bc"].items():
+        system.set_bc(face, kind, val)
+    asm = D.Assembly(dt=case["dt"], D=case["D"])
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    phi0 = np.ascontiguousarray(case["phi0"].reshape(-1))
+
+    def trajectory():
+        field.upload(phi0, 0)
+        field.upload(phi0, 1)
+        its = []
+        ctx.timer_start()
+        for _ in range(case["steps"]):
+            its.append(D.timestep(system, field, asm, solver)["iters"])
+        return ctx.timer_stop(), its
+
+    for _ in range(max(1, args.warmup)):
+        trajectory()
+    ms, its = trajectory()
+    got = field.download(0)
+    t0 = time.perf_counter()
+    hist, oits = oracle_timeloop(case, case["steps"])
+    cpu_s = time.perf_counter() - t0
+    err = float(np.linalg.norm(got - hist[-1]) / np.linalg.norm(hist[-1]))
+    print(json.dumps({"workload": "gaussian diffusion 64^3, 10 implicit steps, Jacobi-BiCGStab2 1e-10",
+                      "metric": "implicit steps/s", "value": case["steps"] / (ms * 1e-3), "ms_total": ms,
+                      "iterations": its, "oracle_iterations": oits, "rel_l2_vs_oracle": err,
+                      "cpu_baseline": {"value": case["steps"] / cpu_s, "unit": "steps/s", "cores": O.num_threads(),
+                                       "kind": "port"}}), flush=True)
+    return 0
+
+
+def run_hetero(args):
+    """Heterogeneous-D TVD operator (log-normal D, box-filtered): FP64 plain vs
+    FP32-inner / FP64-refinement per step, error of the latter vs the former."""
+    import torch
+
+    import dare_b200 as D
+    from dare_b200 import workloads as W
+    n = args.n
+    dev = "cuda:0"
+    case = W.heterogeneous(n=n, seed=args.seed, device=dev)
+    ctx = D.Context(0)
+    grid, field = _gpu_setup_field(D, ctx, case)
+    phi0 = case["phi0"].reshape(-1).cpu().numpy()
+    field.upload(phi0, 0)
+    field.upload(phi0, 1)
+    cell_D = case["cell_D"].contiguous()
+    faceD = [D.DeviceArray.from_tensor(torch.empty(grid.face_shape(d), dtype=torch.float64, device=dev))
+             for d in range(3)]
+    D.face_average(grid, cell_D.data_ptr(), faceD)
+    vel = [D.DeviceArray.from_tensor(case["face_vel"][d]) for d in range(3)]
+    dt = case["dt"]
+    del case
+    torch.cuda.empty_cache()
+    system = D.MatrixSystem(grid)
+    asm = D.Assembly(dt=dt, face_D=tuple(faceD), face_vel=tuple(vel))
+    p64 = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    p32 = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1},
+                      precision="FP32_REFINE")
+    x64 = torch.empty(grid.num_cells, dtype=torch.float64, device=dev)
+    rows = []
+    for step in range(args.warmup + args.steps):
+        system.build(field, asm)
+        ctx.timer_start()
+        r64 = p64.solve(system)
+        t64 = ctx.timer_stop()
+        x64.copy_(torch.from_numpy(system.solution()).to(dev))
+        system.build(field, asm)
+        ctx.timer_start()
+        r32 = p32.solve(system)
+        t32 = ctx.timer_stop()
+        x32 = torch.from_numpy(system.solution()).to(dev)
+        err = float((x32 - x64).norm() / x64.norm())
+        system.copy_to(field)
+        field.exchange_halo()
+        field.copy_to_old()
+        if step >= args.warmup:
+            rows.append({"fp64_ms": t64, "fp64_iters": r64["iters"], "refine_ms": t32,
+                         "refinements": r32["refinements"], "inner_iters": r32["inner_iters"],
+                         "fallback": r32["fallback_used"], "rel_l2_vs_fp64": err,
+                         "true_res_rel": r32["true_res_abs"] / r32["b_norm"]})
+    print(json.dumps({"workload": f"heterogeneous-D TVD convection-diffusion {n}^3 periodic, Pe 5 at median D",
+                      "steps": rows,
+                      "fp64_ms_mean": statistics.mean(r["fp64_ms"] for r in rows),
+                      "refine_ms_mean": statistics.mean(r["refine_ms"] for r in rows)}), flush=True)
+    return 0
+
+
+def run_batched(args):
+    """4096 independent diffusion boxes (sides 16-64), one implicit step each, one launch."""
+    import dare_b200 as D
+    from dare_b200 import workloads as W
+    from oracle import oracle as O
+    inst =W.batched_diffusion(count=args.batch, seed=args.seed)
+    cells = int(sum(np.prod(i["n"]) for i in inst))
+    ctx = D.Context(0)
+    bt = D.Batch(ctx, inst)
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 10000, "tol_relative": 1})
+    tuning = bt.autotune(solver) if not args.no_autotune else None
+    for _ in range(args.warmup):
+        bt.zero_fields()
+        bt.solve(solver, reports=False)
+    times = []
+    for _ in range(args.steps):
+        bt.zero_fields()
+        ctx.synchronize()
+        ctx.timer_start()
+        bt.solve(solver, reports=False)
+        times.append(ctx.timer_stop())
+    bt.zero_fields()
+    reps = bt.solve(solver)
+    its = [r["iters"] for r in reps]
+    # CPU baseline on a bounded sample of the batch, scaled by cells
+    rng = np.random.default_rng(1)
+    sample = rng.choice(len(inst), size=min(64, len(inst)), replace=False)
+    t0 = time.perf_counter()
+    scells = 0
+    for q in sample:
+        ins = inst[q]
+        g = O.make_grid(3, ins["n"], ins["size"], 2, (0, 0, 0))
+        z = np.zeros(int(np.prod(O.ghosted_shape(g))))
+        diag, rhs, mask = O.assemble(O.AssemblyDesc(g, dt=ins["dt"], D=ins["D"], bc=ins["bc"]), z, z)
+        rp, cols, vals = O.export_csr(g, diag, mask)
+        O.bicgstab2(rp, cols, vals, rhs, np.zeros(len(rhs)), 1e-10 * np.linalg.norm(rhs), 10000)
+        scells += int(np.prod(ins["n"]))
+    cpu_s = (time.perf_counter() - t0) * cells / scells
+    ms = statistics.median(times)
+    print(json.dumps({"workload": f"{len(inst)} diffusion boxes, sides 16-64, one implicit step each, "
+                                  "Jacobi-BiCGStab2 1e-10, one persistent launch",
+                      "cells": cells, "ms_per_batch": ms, "ms_all": times, "cell_steps_per_s": cells / (ms * 1e-3),
+                      "converged": sum(r["converged"] for r in reps), "iters_min": min(its), "iters_max": max(its),
+                      "iters_mean": statistics.mean(its), "tuning": tuning,
+                      "cpu_baseline": {"value_s_per_batch": cpu_s, "cores": O.num_threads(), "kind": "port",
+                                       "sample": f"{len(sample)} instances, scaled by cells"}}), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "gauss64":
+        return run_gauss64(args)
+    if args.workload == "hetero":
+        return run_hetero(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_dare(args)
 
 

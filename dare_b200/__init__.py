@@ -117,6 +117,7 @@ _SIGS = [
     ("dare_batch_num_cells", C.c_int64, [_P, C.c_int]),
     ("dare_batch_set_field", C.c_int, [_P, C.c_int, _P]),
     ("dare_batch_get_field", C.c_int, [_P, C.c_int, _P]),
+    ("dare_batch_zero_fields", C.c_int, [_P]),
     ("dare_batch_solve", C.c_int, [_P, _P, _P]),
     ("dare_batch_autotune", C.c_int, [_P, _P, C.POINTER(C.c_int)]),
     ("dare_batch_get_tuning", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -295,8 +296,11 @@ class Field:
             raise ValueError("field upload expects the ghosted layout")
         _check(lib().dare_field_upload(self.h, level, _ptr(a)), self.grid.ctx.h, "field_upload")
 
-    def download(self, level: int = 0) -> np.ndarray:
-        a = np.empty(self.grid.num_cells_ghosted, dtype=np.float64)
+    def download(self, level: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy a level to the host; `out` (e.g. pinned memory) is filled in place when given."""
+        a = np.empty(self.grid.num_cells_ghosted, dtype=np.float64) if out is None else out.reshape(-1)
+        if a.size != self.grid.num_cells_ghosted or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("field download expects a contiguous float64 ghosted buffer")
         _check(lib().dare_field_download(self.h, level, _ptr(a)), self.grid.ctx.h, "field_download")
         return a
 
@@ -509,6 +513,9 @@ class Batch:
         a = np.empty(self.num_cells(idx), dtype=np.float64)
         _check(lib().dare_batch_get_field(self.h, idx, _ptr(a)), self.ctx.h, "batch_get_field")
         return a
+
+    def zero_fields(self):
+        _check(lib().dare_batch_zero_fields(self.h), self.ctx.h, "batch_zero_fields")
 
     def solve(self, solver: "BiCGStab2", reports: bool = True):
         rep = (BatchReport * self.count)() if reports else None

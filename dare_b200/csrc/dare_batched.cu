@@ -600,6 +600,14 @@ int dare_batch_get_field(dare_batch* bt, int idx, double* host_phi) {
     return DARE_OK;
 }
 
+int dare_batch_zero_fields(dare_batch* bt) {
+    if (!bt) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = bt->ctx;
+    cudaSetDevice(ctx->device);
+    DARE_CUDA(ctx, cudaMemsetAsync(bt->arena, 0, sizeof(double) * (size_t)bt->total, ctx->stream));
+    return DARE_OK;
+}
+
 int dare_batch_solve(dare_batch* bt, const dare_solver_params* p, dare_batch_report* reports) {
     using namespace dare_gpu;
     if (!bt || !p) return DARE_ERR_BAD_ARG;

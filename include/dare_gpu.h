@@ -251,6 +251,8 @@ DARE_API int dare_batch_destroy(dare_batch* bt);
 DARE_API int64_t dare_batch_num_cells(const dare_batch* bt, int idx);
 DARE_API int dare_batch_set_field(dare_batch* bt, int idx, const double* host_phi);
 DARE_API int dare_batch_get_field(dare_batch* bt, int idx, double* host_phi);
+/* Set every instance's field to 0 on the device (phi_0 = 0 start). */
+DARE_API int dare_batch_zero_fields(dare_batch* bt);
 /* Solves every instance (p: tol, tol_relative, max_it; Jacobi, FP64). The
  * fields are replaced by the solutions; reports (host, count entries) may be NULL. */
 DARE_API int dare_batch_solve(dare_batch* bt, const dare_solver_params* p, dare_batch_report* reports);
