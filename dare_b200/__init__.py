@@ -124,6 +124,41 @@ _SIGS = [
 ]
 
 
+class UNetTrainParams(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("batch", C.c_int), ("steps", C.c_int), ("max_pairs_per_rhs", C.c_int), ("seed", C.c_uint64)]
+
+
+class UNetTrainReport(C.Structure):
+    _fields_ = [("pairs_added", C.c_int), ("pairs_total", C.c_int), ("plain_iters", C.c_int), ("steps", C.c_int),
+                ("loss_first", C.c_double), ("loss_last", C.c_double)]
+
+
+class LearnedParams(C.Structure):
+    _fields_ = [("iteration_budget", C.c_int), ("inner_max_it", C.c_int), ("inner_rel_tol", C.c_double),
+                ("max_refinements", C.c_int)]
+
+
+_SIGS += [
+    ("dare_unet_train_params_default", None, [C.POINTER(UNetTrainParams)]),
+    ("dare_learned_params_default", None, [C.POINTER(LearnedParams)]),
+    ("dare_unet_create", C.c_int, [_P, C.POINTER(C.c_int), C.c_uint64, C.POINTER(_P)]),
+    ("dare_unet_destroy", C.c_int, [_P]),
+    ("dare_unet_num_params", C.c_int64, [_P]),
+    ("dare_unet_get_weights", C.c_int, [_P, _P, C.c_int64]),
+    ("dare_unet_set_weights", C.c_int, [_P, _P, C.c_int64]),
+    ("dare_unet_apply", C.c_int, [_P, _P, _P]),
+    ("dare_unet_loss_grad", C.c_int, [_P, _P, _P, C.c_int, C.POINTER(C.c_double), _P]),
+    ("dare_unet_train_step", C.c_int, [_P, _P, _P, C.c_int, C.POINTER(UNetTrainParams), C.POINTER(C.c_double)]),
+    ("dare_unet_train_on_system", C.c_int, [_P, _P, C.c_double, C.POINTER(UNetTrainParams),
+                                            C.POINTER(UNetTrainReport)]),
+    ("dare_unet_stats", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("dare_unet_read_activation", C.c_int, [_P, C.c_int, _P, C.c_int64]),
+    ("dare_bicgstab2_learned", C.c_int, [_P, _P, C.POINTER(SolverParams), C.POINTER(LearnedParams),
+                                         C.POINTER(SolveReport)]),
+]
+
+
 class BatchInstance(C.Structure):
     _fields_ = [("n", C.c_int64 * 3), ("size", C.c_double * 3), ("D", C.c_double), ("dt", C.c_double),
                 ("bc_type", C.c_int * 6), ("bc_value", C.c_double * 6)]
@@ -532,3 +567,101 @@ class Batch:
         vec = (C.c_int * 8)()
         lib().dare_batch_get_tuning(self.h, C.byref(blk), vec)
         return {"block": blk.value, "cells_per_thread_by_size": list(vec)}
+
+
+class LearnedPreconditioner:
+    """The linear conv U-Net preconditioner N(u) = u + U(u) of the Jacobi-folded
+    system (dare_unet): 8 bias-free 3x3x3 convolutions over 4 levels, BF16
+    weights, FP32 tensor-core accumulation, trained on the GPU."""
+
+    LAYERS = (("enc0", 0, 1, 16), ("enc1", 1, 16, 32), ("enc2", 2, 32, 64), ("enc3", 3, 64, 64),
+              ("dec3", 3, 64, 64), ("dec2", 2, 64, 32), ("dec1", 1, 32, 16), ("dec0", 0, 16, 1))
+    ACTIVATIONS = (("S0", 0, 16), ("P1", 1, 16), ("S1", 1, 32), ("P2", 2, 32), ("S2", 2, 64), ("P3", 3, 64),
+                   ("E3", 3, 64))
+
+    def __init__(self, ctx: Context, n, seed: int = 0):
+        self.ctx = ctx
+        self.n = tuple(int(x) for x in n)
+        nn = (C.c_int * 3)(*self.n)
+        h = C.c_void_p()
+        _check(lib().dare_unet_create(ctx.h, nn, C.c_uint64(seed), C.byref(h)), ctx.h, "unet_create")
+        self.h = h
+        self.num_params = int(lib().dare_unet_num_params(h))
+        self.num_cells = self.n[0] * self.n[1] * self.n[2]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dare_unet_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def train_params(**kw) -> UNetTrainParams:
+        p = UNetTrainParams()
+        lib().dare_unet_train_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+    def get_weights(self) -> np.ndarray:
+        w = np.empty(self.num_params, dtype=np.float32)
+        _check(lib().dare_unet_get_weights(self.h, _ptr(w), self.num_params), self.ctx.h, "unet_get_weights")
+        return w
+
+    def set_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().dare_unet_set_weights(self.h, _ptr(w), w.size), self.ctx.h, "unet_set_weights")
+
+    def apply(self, u_ptr: int, z_ptr: int):
+        """z = N(u) for FP32 device vectors (raw pointers)."""
+        _check(lib().dare_unet_apply(self.h, u_ptr, z_ptr), self.ctx.h, "unet_apply")
+
+    def activation(self, which: int) -> np.ndarray:
+        _, lev, ch = self.ACTIVATIONS[which]
+        cells = int(np.prod([x >> lev for x in self.n]))
+        a = np.empty(cells * ch, dtype=np.float32)
+        _check(lib().dare_unet_read_activation(self.h, which, _ptr(a), a.size), self.ctx.h, "unet_read_activation")
+        return a.reshape(cells, ch)
+
+    def loss_grad(self, r_ptr: int, e_ptr: int, count: int, want_grad: bool = True):
+        loss = C.c_double()
+        g = np.empty(self.num_params, dtype=np.float32) if want_grad else None
+        _check(lib().dare_unet_loss_grad(self.h, r_ptr, e_ptr, count, C.byref(loss), _ptr(g)), self.ctx.h,
+               "unet_loss_grad")
+        return loss.value, g
+
+    def train_step(self, r_ptr: int, e_ptr: int, count: int, params: UNetTrainParams | None = None) -> float:
+        p = params or self.train_params()
+        loss = C.c_double()
+        _check(lib().dare_unet_train_step(self.h, r_ptr, e_ptr, count, C.byref(p), C.byref(loss)), self.ctx.h,
+               "unet_train_step")
+        return loss.value
+
+    def train_on_system(self, system: MatrixSystem, tol: float, params: UNetTrainParams | None = None) -> dict:
+        p = params or self.train_params()
+        rep = UNetTrainReport()
+        _check(lib().dare_unet_train_on_system(self.h, system.h, tol, C.byref(p), C.byref(rep)), self.ctx.h,
+               "unet_train_on_system")
+        return {name: getattr(rep, name) for name, _ in rep._fields_}
+
+    def stats(self) -> dict:
+        s, q = C.c_int64(), C.c_int64()
+        lib().dare_unet_stats(self.h, C.byref(s), C.byref(q))
+        return {"steps": s.value, "pairs_seen": q.value}
+
+    @staticmethod
+    def learned_params(**kw) -> LearnedParams:
+        p = LearnedParams()
+        lib().dare_learned_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+    def solve(self, system: MatrixSystem, solver: BiCGStab2, params: LearnedParams | None = None) -> dict:
+        """Learned-preconditioned mixed-precision BiCGStab2 with the automatic
+        fallback to the plain FP64 Jacobi-BiCGStab2."""
+        lp = params or self.learned_params()
+        rep = SolveReport()
+        _check(lib().dare_bicgstab2_learned(system.h, self.h, C.byref(solver.params), C.byref(lp), C.byref(rep)),
+               system.grid.ctx.h, "bicgstab2_learned")
+        solver.report = rep.as_dict()
+        return solver.report

@@ -36,6 +36,8 @@ SOURCES = {
     "dare_step.cu": [],
     "dare_noalloc.cu": [],
     "dare_batched.cu": [],
+    "dare_unet.cu": [],
+    "dare_learned.cu": [],
 }
 
 

@@ -41,6 +41,7 @@ void dare_solver_ws_free(dare_solver_ws* ws) {
     cudaFree(ws->st);
     if (ws->st_host) cudaFreeHost(ws->st_host);
     dare_mixed_ws_free(ws);
+    dare_learned_ws_free(ws->learned);
     delete ws;
 }
 

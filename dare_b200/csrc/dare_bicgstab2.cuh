@@ -163,7 +163,10 @@ struct dare_solver_ws {
     float* vec32 = nullptr;      // 12 * n (11 work vectors + the correction)
     double* r64 = nullptr;       // unused slot kept for layout stability
     dare_gpu::MarchCfg march32;
+    // learned-preconditioner solver (dare_learned.cu)
+    struct dare_learned_ws* learned = nullptr;
 };
 
 void dare_mixed_ws_free(dare_solver_ws* ws);
+void dare_learned_ws_free(struct dare_learned_ws* lw);
 int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_report* rep);

@@ -1,0 +1,1262 @@
+// dare_unet.cu -- the learned linear preconditioner N(u) = u + U(u) of the
+// Jacobi-folded system: network kernels, training, C ABI.
+//
+// Convolutions are implicit GEMMs on the tcgen05 tensor cores.  A level's
+// activations are zero-padded and channels-last ([padded cell][C] bf16), so
+// the 27 taps of a 3^3 kernel are constant shifts of the flattened padded
+// position.  One CTA owns 128 consecutive padded positions of a (j,k) plane
+// and marches along i: it keeps the input planes i-1, i, i+1 of its
+// positions (plus the one-row halo of the plane) in a 4-slot shared-memory
+// ring, so every input element is fetched from HBM about once per plane
+// pass, and issues for each output plane 27 x (Cin/16) MMAs of
+// M=128 x N x K=16 whose A operand is the staged plane at the tap's shift
+// (only the descriptor's start address changes) and whose B operand is the
+// packed weight tile of that tap.  The FP32 accumulator lives in TMEM,
+// double-buffered: the epilogue of plane i-1 (tcgen05.ld, bf16 store, or
+// the fused prolongation-add into the finer level, or the FP32 output
+// z = u + acc) and the prefetch of plane i+2 overlap the MMAs of plane i.
+//
+// Weight gradients run the same staging with the reduction over positions:
+// dW[t][co][ci] = sum_p dY[p][co] X[p + shift_t][ci] as an MMA with
+// M = co (128 rows, rows >= Cout are ignored), N = Cin of one tap, K = 16
+// positions, both operands MN-major straight from the staged planes; each
+// CTA accumulates its planes in TMEM and writes one partial per CTA, summed
+// in a fixed order afterwards (deterministic).  Data gradients are forward
+// convolutions with flipped, transposed weights.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "dare_bicgstab2.cuh"
+#include "dare_tc.cuh"
+#include "dare_unet.cuh"
+
+using namespace dare_gpu;
+using namespace dare_gpu::unet;
+using namespace dare_gpu::tc;
+
+namespace dare_gpu {
+namespace unet {
+
+constexpr size_t kMaxSmem = 232448;  // 227 KB of opt-in shared memory per CTA
+
+// ---------------------------------------------------------------------------
+// operand staging: one plane segment of `rows` padded positions starting at
+// flattened position Q0, as C/8 planes of 16-byte chunks with row pitch RP
+// (chunk (kc, q) at byte (kc * RP + q) * 16).  Positions outside the array
+// read zero.  IN_EMBED (C == 16) takes an FP32 vector over the internal
+// cells as channel 0 (rounded to bf16) and zero elsewhere.
+template <int C, int MODE>
+__device__ __forceinline__ void stage(uint8_t* slot, const bf16* __restrict__ in, const float* __restrict__ in32,
+                                      const Geom& g, int64_t Q0, int rows, int RP) {
+    if (MODE == IN_BF16) {
+        constexpr int KC = C / 8;
+        const int nent = rows * KC;
+        for (int idx = threadIdx.x; idx < nent; idx += kThreads) {
+            const int q = idx / KC, kc = idx - q * KC;
+            const int64_t Q = Q0 + q;
+            const bool v = Q >= 0 && Q < g.total;
+            cp16(slot + ((size_t)kc * RP + q) * 16, in + (v ? Q : 0) * C + kc * 8, v);
+        }
+    } else {
+        for (int q = threadIdx.x; q < rows; q += kThreads) {
+            const int64_t Q = Q0 + q;
+            float v = 0.f;
+            if (Q >= 0 && Q < g.total) {
+                const int I = (int)(Q / g.plane);
+                const int rem = (int)(Q - (int64_t)I * g.plane);
+                const int J = rem / g.W, K = rem - J * g.W;
+                if (I >= 1 && I <= g.n0 && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2)
+                    v = __ldg(in32 + ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1));
+            }
+            *reinterpret_cast<uint4*>(slot + (size_t)q * 16) = make_uint4(pack_bf16(v, 0.f), 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(slot + ((size_t)RP + q) * 16) = make_uint4(0u, 0u, 0u, 0u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// forward convolution
+struct FwdArgs {
+    Geom g;          // level of input and output
+    Geom fg;         // finer level (OUT_ADDUP)
+    const bf16* in;  // IN_BF16: [g.total][CIN]
+    const float* in32;
+    const bf16* w;   // packed [nz][27][CIN/8][NT][8]
+    int cout;        // channel count (stride) of out / fine
+    bf16* out;       // OUT_STORE: [g.total][cout]
+    bf16* fine;      // OUT_ADDUP: [fg.total][cout]
+    float* out32;    // OUT_F32: internal cells, channel 0 (+ res32)
+    const float* res32;
+    int ppc;
+    int* err;
+};
+
+template <int NT, int OUTM>
+__device__ __forceinline__ void fwd_epilogue(const FwdArgs& a, uint32_t tmem, int buf, int I, int P0, int co0) {
+    fence_after_sync();
+    const int warp = threadIdx.x >> 5;
+    uint32_t r[NT];
+#pragma unroll
+    for (int c = 0; c < NT; c += 16) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * NT + c, &r[c]);
+    tmem_wait_ld();
+#pragma unroll
+    for (int c = 0; c < NT; c++) reg_fence(r[c]);
+    const Geom& g = a.g;
+    const int pp = P0 + (int)threadIdx.x;
+    if (pp >= g.plane) return;
+    const int J = pp / g.W, K = pp - J * g.W;
+    if (J < 1 || J > g.n1 || K < 1 || K > g.n2) return;
+    if (OUTM == OUT_STORE) {
+        bf16* dst = a.out + ((int64_t)I * g.plane + pp) * a.cout + co0;
+#pragma unroll
+        for (int c = 0; c < NT; c += 8) {
+            uint4 q;
+            q.x = pack_bf16(__uint_as_float(r[c + 0]), __uint_as_float(r[c + 1]));
+            q.y = pack_bf16(__uint_as_float(r[c + 2]), __uint_as_float(r[c + 3]));
+            q.z = pack_bf16(__uint_as_float(r[c + 4]), __uint_as_float(r[c + 5]));
+            q.w = pack_bf16(__uint_as_float(r[c + 6]), __uint_as_float(r[c + 7]));
+            *reinterpret_cast<uint4*>(dst + c) = q;
+        }
+    } else if (OUTM == OUT_ADDUP) {
+        // nearest-neighbour prolongation of this coarse cell, added into its
+        // eight children on the finer level (the additive skip)
+        const Geom& f = a.fg;
+#pragma unroll 1
+        for (int ch = 0; ch < 8; ch++) {
+            const int fi = 2 * I - 1 + (ch >> 2), fj = 2 * J - 1 + ((ch >> 1) & 1), fk = 2 * K - 1 + (ch & 1);
+            bf16* dst = a.fine + (((int64_t)fi * (f.n1 + 2) + fj) * f.W + fk) * a.cout + co0;
+#pragma unroll
+            for (int c = 0; c < NT; c += 8) {
+                uint4 o = *reinterpret_cast<const uint4*>(dst + c);
+                uint4 q;
+                q.x = pack_bf16(bf16_lo(o.x) + __uint_as_float(r[c + 0]), bf16_hi(o.x) + __uint_as_float(r[c + 1]));
+                q.y = pack_bf16(bf16_lo(o.y) + __uint_as_float(r[c + 2]), bf16_hi(o.y) + __uint_as_float(r[c + 3]));
+                q.z = pack_bf16(bf16_lo(o.z) + __uint_as_float(r[c + 4]), bf16_hi(o.z) + __uint_as_float(r[c + 5]));
+                q.w = pack_bf16(bf16_lo(o.w) + __uint_as_float(r[c + 6]), bf16_hi(o.w) + __uint_as_float(r[c + 7]));
+                *reinterpret_cast<uint4*>(dst + c) = q;
+            }
+        }
+    } else {
+        const int64_t c = ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1);
+        a.out32[c] = (a.res32 ? a.res32[c] : 0.f) + __uint_as_float(r[0]);
+    }
+}
+
+template <int CIN, int NT, int INM, int OUTM>
+__global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int KC = CIN / 8;
+    constexpr uint32_t WB = kTaps * CIN * NT * 2;
+    constexpr uint32_t COLS = 2 * NT < 32 ? 32 : 2 * NT;
+    const Geom g = a.g;
+    const int tid = threadIdx.x;
+    const int rows = stage_rows(g);
+    const int RP = row_pitch(rows, CIN);
+    const uint32_t SB = (uint32_t)KC * RP * 16;
+    uint8_t* wsm = smem;
+    uint8_t* slots = smem + WB;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(slots + 4 * SB);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+
+    const int P0 = blockIdx.x * kTileM;
+    const int I0 = 1 + blockIdx.y * a.ppc;
+    if (I0 > g.n0) return;
+    const int I1 = min(g.n0, I0 + a.ppc - 1);
+
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        mbar_fence_init();
+    }
+    if (tid < 32) tmem_alloc(tslot, COLS);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    {
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(a.w) + (size_t)blockIdx.z * WB;
+        for (uint32_t o = tid * 16; o < WB; o += kThreads * 16) cp16(wsm + o, src + o, true);
+    }
+    const int64_t pbase = (int64_t)P0 - g.W - 1;
+    for (int I = I0 - 1; I <= I0 + 1; I++)
+        stage<CIN, INM>(slots + (I & 3) * SB, a.in, a.in32, g, (int64_t)I * g.plane + pbase, rows, RP);
+    cp_commit();
+
+    constexpr uint32_t idesc = idesc_bf16(kTileM, NT, 0, 0);
+    uint32_t phase = 0;
+    bool aborted = false;
+    for (int I = I0; I <= I1; I++) {
+        const int buf = (I - I0) & 1;
+        cp_wait_all();
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after_sync();
+            const uint32_t sl = smem_u32(slots), wa = smem_u32(wsm);
+#pragma unroll 1
+            for (int t = 0; t < kTaps; t++) {
+                const int di = t / 9 - 1, dj = (t / 3) % 3 - 1, dk = t % 3 - 1;
+                const uint32_t ab = sl + ((I + di) & 3) * SB + (uint32_t)((dj + 1) * g.W + (dk + 1)) * 16;
+                const uint32_t bb = wa + (uint32_t)t * KC * NT * 16;
+#pragma unroll
+                for (int s = 0; s < CIN / 16; s++)
+                    mma_bf16(tmem + buf * NT, smem_desc(ab + 2 * s * RP * 16, RP * 16, 128),
+                             smem_desc(bb + 2 * s * NT * 16, NT * 16, 128), idesc, (t | s) ? 1u : 0u);
+            }
+            mma_commit(smem_u32(&mbar[buf]));
+        }
+        if (I > I0) {
+            const int pb = buf ^ 1;
+            const bool ok = mbar_wait(&mbar[pb], (phase >> pb) & 1u, a.err, 1);
+            phase ^= 1u << pb;
+            if (__syncthreads_or(!ok)) {
+                aborted = true;
+                break;
+            }
+        }
+        if (I + 2 <= I1 + 1)
+            stage<CIN, INM>(slots + ((I + 2) & 3) * SB, a.in, a.in32, g, (int64_t)(I + 2) * g.plane + pbase, rows,
+                            RP);
+        cp_commit();
+        if (I > I0) fwd_epilogue<NT, OUTM>(a, tmem, buf ^ 1, I - 1, P0, blockIdx.z * NT);
+        fence_before_sync();
+    }
+    if (!aborted) {
+        const int lb = (I1 - I0) & 1;
+        const bool ok = mbar_wait(&mbar[lb], (phase >> lb) & 1u, a.err, 2);
+        if (!__syncthreads_or(!ok)) fwd_epilogue<NT, OUTM>(a, tmem, lb, I1, P0, blockIdx.z * NT);
+    }
+    cp_wait_all();
+    fence_before_sync();
+    __syncthreads();
+    if (tid < 32) {
+        fence_after_sync();
+        tmem_dealloc(tmem, COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient
+struct WgrArgs {
+    Geom g;
+    const bf16* x;     // input activations (IN_BF16) ...
+    const float* x32;  // ... or the FP32 vector (IN_EMBED)
+    const bf16* dy;    // output gradient (IN_BF16) ...
+    const float* dy32; // ... or the FP32 vector (IN_EMBED)
+    float* part;       // [cta][tpg][COUT][CIN]
+    int ppc, tpg;
+    uint32_t cols;
+    int* err;
+};
+
+template <int C>
+__host__ __device__ constexpr int dy_pitch() {
+    return kTileM + (C == 16 ? 4 : (C == 32 ? 2 : 1));
+}
+
+template <int CIN, int COUT, int XM, int YM>
+__global__ void __launch_bounds__(kThreads) k_conv_wgrad(WgrArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int KCX = CIN / 8, KCY = COUT / 8;
+    constexpr int RPD = dy_pitch<COUT>();
+    constexpr uint32_t DB = (uint32_t)KCY * RPD * 16;
+    const Geom g = a.g;
+    const int tid = threadIdx.x;
+    const int rows = stage_rows(g);
+    const int RP = row_pitch(rows, CIN);
+    const uint32_t SB = (uint32_t)KCX * RP * 16;
+    uint8_t* dys = smem;
+    uint8_t* xs = smem + 2 * DB;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(xs + 4 * SB);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+
+    const int P0 = blockIdx.x * kTileM;
+    const int I0 = 1 + blockIdx.y * a.ppc;
+    const int t0 = blockIdx.z * a.tpg, t1 = min(kTaps, t0 + a.tpg);
+    if (I0 > g.n0 || t0 >= kTaps) return;
+    const int I1 = min(g.n0, I0 + a.ppc - 1);
+
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        mbar_fence_init();
+    }
+    if (tid < 32) tmem_alloc(tslot, a.cols);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    const int64_t pbase = (int64_t)P0 - g.W - 1;
+    for (int I = I0 - 1; I <= I0 + 1; I++)
+        stage<CIN, XM>(xs + (I & 3) * SB, a.x, a.x32, g, (int64_t)I * g.plane + pbase, rows, RP);
+    stage<COUT, YM>(dys + (I0 & 1) * DB, a.dy, a.dy32, g, (int64_t)I0 * g.plane + P0, kTileM, RPD);
+    cp_commit();
+
+    constexpr uint32_t idesc = idesc_bf16(kTileM, CIN, 1, 1);
+    uint32_t phase = 0;
+    bool aborted = false;
+    for (int I = I0; I <= I1; I++) {
+        const int buf = (I - I0) & 1;
+        cp_wait_all();
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after_sync();
+            const uint32_t xa = smem_u32(xs), ya = smem_u32(dys) + (I & 1) * DB;
+#pragma unroll 1
+            for (int t = t0; t < t1; t++) {
+                const int di = t / 9 - 1, dj = (t / 3) % 3 - 1, dk = t % 3 - 1;
+                const uint32_t xb = xa + ((I + di) & 3) * SB + (uint32_t)((dj + 1) * g.W + (dk + 1)) * 16;
+                const uint32_t d = tmem + (uint32_t)(t - t0) * CIN;
+#pragma unroll
+                for (int s = 0; s < kTileM / 16; s++)
+                    mma_bf16(d, smem_desc(ya + s * 256, 128, RPD * 16), smem_desc(xb + s * 256, 128, RP * 16), idesc,
+                             (I == I0 && s == 0) ? 0u : 1u);
+            }
+            mma_commit(smem_u32(&mbar[buf]));
+        }
+        if (I > I0) {
+            const int pb = buf ^ 1;
+            const bool ok = mbar_wait(&mbar[pb], (phase >> pb) & 1u, a.err, 3);
+            phase ^= 1u << pb;
+            if (__syncthreads_or(!ok)) {
+                aborted = true;
+                break;
+            }
+        }
+        if (I + 2 <= I1 + 1)
+            stage<CIN, XM>(xs + ((I + 2) & 3) * SB, a.x, a.x32, g, (int64_t)(I + 2) * g.plane + pbase, rows, RP);
+        if (I + 1 <= I1)
+            stage<COUT, YM>(dys + ((I + 1) & 1) * DB, a.dy, a.dy32, g, (int64_t)(I + 1) * g.plane + P0, kTileM, RPD);
+        cp_commit();
+    }
+    if (!aborted) {
+        const int lb = (I1 - I0) & 1;
+        const bool ok = mbar_wait(&mbar[lb], (phase >> lb) & 1u, a.err, 4);
+        if (!__syncthreads_or(!ok)) {
+            fence_after_sync();
+            const int warp = tid >> 5, lane = tid & 31;
+            if (warp * 32 < COUT) {
+                const int co = warp * 32 + lane;
+                const int ncol = (t1 - t0) * CIN;
+                const size_t cta = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+                float* base = a.part + cta * (size_t)a.tpg * COUT * CIN;
+#pragma unroll 1
+                for (int col = 0; col < ncol; col += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + col, r);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 16; i++) reg_fence(r[i]);
+                    if (co < COUT) {
+                        const int tl = col / CIN, ci0 = col - tl * CIN;
+                        float4* d = reinterpret_cast<float4*>(base + ((size_t)tl * COUT + co) * CIN + ci0);
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            d[i] = make_float4(__uint_as_float(r[4 * i]), __uint_as_float(r[4 * i + 1]),
+                                               __uint_as_float(r[4 * i + 2]), __uint_as_float(r[4 * i + 3]));
+                    }
+                }
+            }
+        }
+    }
+    cp_wait_all();
+    fence_before_sync();
+    __syncthreads();
+    if (tid < 32) {
+        fence_after_sync();
+        tmem_dealloc(tmem, a.cols);
+    }
+}
+
+// grad[t][co][ci] += scale * sum over the CTAs of tap group t / tpg (fixed order)
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int nxy, int tpg, int CINK, int COUTK, int cin,
+                               int cout, float scale, float* __restrict__ grad) {
+    const int total = kTaps * cout * cin;
+    const size_t ps = (size_t)tpg * COUTK * CINK;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        const int ci = idx % cin, co = (idx / cin) % cout, t = idx / (cin * cout);
+        const int z = t / tpg, tl = t - z * tpg;
+        const float* p = part + (size_t)z * nxy * ps + ((size_t)tl * COUTK + co) * CINK + ci;
+        double s = 0.;
+        for (int b = 0; b < nxy; b++) s += (double)p[(size_t)b * ps];
+        grad[idx] += scale * (float)s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// level transfer: 2x2x2 restriction (scale 1/8 = average pool, 1 = the
+// transpose of nearest prolongation) and the transpose of the average pool
+// added into the finer level
+template <int C>
+__global__ void k_restrict(Geom f, Geom c, const bf16* __restrict__ fine, bf16* __restrict__ coarse, float scale) {
+    constexpr int KC = C / 8;
+    const int64_t total = (int64_t)c.n0 * c.n1 * c.n2 * KC;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int kc = (int)(idx % KC);
+        int64_t v = idx / KC;
+        const int k = (int)(v % c.n2);
+        v /= c.n2;
+        const int j = (int)(v % c.n1);
+        const int i = (int)(v / c.n1);
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int ch = 0; ch < 8; ch++) {
+            const int fi = 2 * i + 1 + (ch >> 2), fj = 2 * j + 1 + ((ch >> 1) & 1), fk = 2 * k + 1 + (ch & 1);
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(
+                fine + (((int64_t)fi * (f.n1 + 2) + fj) * f.W + fk) * C + kc * 8));
+            acc[0] += bf16_lo(q.x);
+            acc[1] += bf16_hi(q.x);
+            acc[2] += bf16_lo(q.y);
+            acc[3] += bf16_hi(q.y);
+            acc[4] += bf16_lo(q.z);
+            acc[5] += bf16_hi(q.z);
+            acc[6] += bf16_lo(q.w);
+            acc[7] += bf16_hi(q.w);
+        }
+        uint4 o;
+        o.x = pack_bf16(acc[0] * scale, acc[1] * scale);
+        o.y = pack_bf16(acc[2] * scale, acc[3] * scale);
+        o.z = pack_bf16(acc[4] * scale, acc[5] * scale);
+        o.w = pack_bf16(acc[6] * scale, acc[7] * scale);
+        *reinterpret_cast<uint4*>(coarse + (((int64_t)(i + 1) * (c.n1 + 2) + (j + 1)) * c.W + (k + 1)) * C + kc * 8) =
+            o;
+    }
+}
+
+template <int C>
+__global__ void k_prolong_add(Geom f, Geom c, const bf16* __restrict__ coarse, bf16* __restrict__ fine, float scale) {
+    constexpr int KC = C / 8;
+    const int64_t total = (int64_t)f.n0 * f.n1 * f.n2 * KC;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int kc = (int)(idx % KC);
+        int64_t v = idx / KC;
+        const int k = (int)(v % f.n2);
+        v /= f.n2;
+        const int j = (int)(v % f.n1);
+        const int i = (int)(v / f.n1);
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(
+            coarse + (((int64_t)(i / 2 + 1) * (c.n1 + 2) + (j / 2 + 1)) * c.W + (k / 2 + 1)) * C + kc * 8));
+        uint4* dst =
+            reinterpret_cast<uint4*>(fine + (((int64_t)(i + 1) * (f.n1 + 2) + (j + 1)) * f.W + (k + 1)) * C + kc * 8);
+        const uint4 o = *dst;
+        uint4 r;
+        r.x = pack_bf16(bf16_lo(o.x) + scale * bf16_lo(q.x), bf16_hi(o.x) + scale * bf16_hi(q.x));
+        r.y = pack_bf16(bf16_lo(o.y) + scale * bf16_lo(q.y), bf16_hi(o.y) + scale * bf16_hi(q.y));
+        r.z = pack_bf16(bf16_lo(o.z) + scale * bf16_lo(q.z), bf16_hi(o.z) + scale * bf16_hi(q.z));
+        r.w = pack_bf16(bf16_lo(o.w) + scale * bf16_lo(q.w), bf16_hi(o.w) + scale * bf16_hi(q.w));
+        *dst = r;
+    }
+}
+
+// padded bf16 activations -> FP32 [cell][C] over the internal cells
+__global__ void k_read_act(Geom g, int C, const bf16* __restrict__ a, float* __restrict__ out) {
+    const int64_t total = (int64_t)g.n0 * g.n1 * g.n2 * C;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int ch = (int)(idx % C);
+        int64_t v = idx / C;
+        const int k = (int)(v % g.n2);
+        v /= g.n2;
+        const int j = (int)(v % g.n1);
+        const int i = (int)(v / g.n1);
+        out[idx] = __bfloat162float(a[(((int64_t)(i + 1) * (g.n1 + 2) + (j + 1)) * g.W + (k + 1)) * C + ch]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// loss: w = scale / ||e||^2; g = 2 w (z - e); loss += w ||z - e||^2
+__global__ void __launch_bounds__(256) k_loss_grad(int64_t n, const float* __restrict__ z, const float* __restrict__ e,
+                                                   const float* __restrict__ en2, float scale, float* __restrict__ g,
+                                                   double* __restrict__ loss) {
+    __shared__ double sh[8];
+    const float w = scale / fmaxf(*en2, 1e-30f);
+    double acc = 0.;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const float d = z[c] - e[c];
+        g[c] = 2.f * w * d;
+        acc += (double)d * d;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sh[i];
+        atomicAdd(loss, s * (double)w);
+    }
+}
+
+__global__ void k_adam(int64_t n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float eps, float bc1, float bc2) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    }
+}
+
+// master weights [27][cout][cin] -> packed bf16 [nz][27][CINK/8][NT][8].
+// flip: the data-gradient convolution (input cout channels, output cin),
+// W'[t][o][i] = W[26 - t][i][o].
+__global__ void k_pack(const float* __restrict__ W, int cin, int cout, int CINK, int NT, int nz, int flip,
+                       bf16* __restrict__ out) {
+    const int KC = CINK / 8;
+    const int64_t total = (int64_t)nz * kTaps * KC * NT * 8;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = idx;
+        const int e = (int)(r % 8);
+        r /= 8;
+        const int n = (int)(r % NT);
+        r /= NT;
+        const int kc = (int)(r % KC);
+        r /= KC;
+        const int t = (int)(r % kTaps);
+        const int z = (int)(r / kTaps);
+        const int o = z * NT + n, i = kc * 8 + e;
+        float v = 0.f;
+        if (!flip) {
+            if (o < cout && i < cin) v = W[((int64_t)t * cout + o) * cin + i];
+        } else {
+            if (o < cin && i < cout) v = W[((int64_t)(kTaps - 1 - t) * cout + i) * cin + o];
+        }
+        out[idx] = __float2bfloat16_rn(v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pair generation: r = b - A x_k (FP32), e = diag_C (x* - x_k) (FP32),
+// acc += ||e||^2 (FP64, atomically)
+__global__ void __launch_bounds__(256) k_make_pair(GridDev g, const double* __restrict__ diag,
+                                                   const double* __restrict__ b, const double* __restrict__ xk,
+                                                   const double* __restrict__ xs, float* __restrict__ r,
+                                                   float* __restrict__ e, double* __restrict__ acc) {
+    __shared__ double sh[8];
+    const int64_t n = g.ncell, nyz = (int64_t)g.n[1] * g.n[2];
+    double s = 0.;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c / nyz), j = (int)((c / g.n[2]) % g.n[1]), k = (int)(c % g.n[2]);
+        int64_t nb[7];
+        neighbour_ordinals(g, i, j, k, c, nb);
+        double ax = 0.;
+#pragma unroll
+        for (int q = 0; q < 7; q++) ax += diag[q * n + c] * xk[nb[q]];
+        r[c] = (float)(b[c] - ax);
+        const float ev = (float)(diag[c] * (xs[c] - xk[c]));
+        e[c] = ev;
+        s += (double)ev * ev;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+        atomicAdd(acc, t);
+    }
+}
+
+__global__ void k_store_norm(const double* acc, float* out) { *out = (float)*acc; }
+
+__global__ void __launch_bounds__(256) k_sqnorm(int64_t n, const float* __restrict__ e, double* __restrict__ acc) {
+    __shared__ double sh[8];
+    double s = 0.;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+        s += (double)e[c] * e[c];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+        atomicAdd(acc, t);
+    }
+}
+
+// y = D x: the right-preconditioned solve iterates on y with x = D^-1 y and
+// takes its initial guess as y0 (BiCGStab2.inl:258-261 with the Jacobi
+// preconditioner), so a warm start at the physical x passes D x
+__global__ void k_warm(int64_t n, const double* __restrict__ diag, const double* __restrict__ x, double* __restrict__ y) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+        y[c] = diag[c] * x[c];
+}
+
+// ---------------------------------------------------------------------------
+// host side: launch configuration and dispatch
+static size_t fwd_smem(int cin, int nt, const Geom& g) {
+    const int RP = row_pitch(stage_rows(g), cin);
+    return (size_t)kTaps * cin * nt * 2 + 4 * (size_t)(cin / 8) * RP * 16 + 32;
+}
+
+static int dy_pitch_rt(int c) { return kTileM + (c == 16 ? 4 : (c == 32 ? 2 : 1)); }
+
+static size_t wgr_smem(int cin, int cout, const Geom& g) {
+    const int RP = row_pitch(stage_rows(g), cin);
+    const size_t DB = (size_t)(cout / 8) * dy_pitch_rt(cout) * 16;
+    const size_t body = 2 * DB + 4 * (size_t)(cin / 8) * RP * 16 + 32;
+    // the A operand (dY^T, 128 rows of which Cout are real) of the second dY
+    // slot reaches 16 row groups past its start: keep that inside the CTA
+    const size_t reach = DB + (size_t)(kTileM / 16) * 256 + 15 * (size_t)dy_pitch_rt(cout) * 16 + 256;
+    return std::max(body, reach + 32);
+}
+
+template <typename K>
+static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int* occ_out) {
+    DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    int occ = 0;
+    for (;;) {
+        DARE_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
+        // CTAs resident on one SM must never ask for more than its 512 TMEM columns
+        if (occ * cols <= 512 || smem + 4096 > kMaxSmem) break;
+        smem += 4096;
+    }
+    if (occ < 1 || occ * cols > 512) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: no launchable configuration");
+    *occ_out = occ;
+    return DARE_OK;
+}
+
+template <int CIN, int NT, int INM, int OUTM>
+static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const FwdArgs& a0) {
+    auto kern = k_conv_fwd<CIN, NT, INM, OUTM>;
+    if (!lc.ready) {
+        size_t smem = fwd_smem(CIN, NT, a0.g);
+        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
+        const uint32_t cols = 2 * NT < 32 ? 32 : 2 * NT;
+        int occ = 0, rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ))) return rc;
+        const int n0 = a0.g.n0;
+        const int64_t target = (int64_t)ctx->num_sms * occ * 2;
+        int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + (int64_t)a0.g.tiles * nz - 1) /
+                                                                            ((int64_t)a0.g.tiles * nz)));
+        int ppc = (n0 + chunks - 1) / chunks;
+        ppc = std::max(ppc, std::min(n0, 4));
+        lc.ppc = ppc;
+        lc.grid = dim3(a0.g.tiles, (n0 + ppc - 1) / ppc, nz);
+        lc.smem = smem;
+        lc.cols = cols;
+        lc.ready = true;
+    }
+    FwdArgs a = a0;
+    a.ppc = lc.ppc;
+    kern<<<lc.grid, kThreads, lc.smem, ctx->stream>>>(a);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+static int launch_fwd(dare_ctx* ctx, LaunchCfg& lc, int cin, int nt, int nz, int inm, int outm, const FwdArgs& a) {
+#define DARE_FWD(CI, N, IM, OM) \
+    if (cin == CI && nt == N && inm == IM && outm == OM) return launch_fwd_t<CI, N, IM, OM>(ctx, lc, nz, a);
+    DARE_FWD(16, 16, IN_EMBED, OUT_STORE)
+    DARE_FWD(16, 16, IN_BF16, OUT_STORE)
+    DARE_FWD(16, 32, IN_BF16, OUT_STORE)
+    DARE_FWD(32, 16, IN_BF16, OUT_STORE)
+    DARE_FWD(32, 32, IN_BF16, OUT_STORE)
+    DARE_FWD(64, 16, IN_BF16, OUT_STORE)
+    DARE_FWD(64, 32, IN_BF16, OUT_STORE)
+    DARE_FWD(32, 16, IN_BF16, OUT_ADDUP)
+    DARE_FWD(64, 16, IN_BF16, OUT_ADDUP)
+    DARE_FWD(64, 32, IN_BF16, OUT_ADDUP)
+    DARE_FWD(16, 16, IN_BF16, OUT_F32)
+#undef DARE_FWD
+    return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: no forward convolution kernel for this shape");
+}
+
+template <int CIN, int COUT, int XM, int YM>
+static int launch_wgr_t(dare_ctx* ctx, LaunchCfg& lc, WgrArgs a, size_t* part_need) {
+    auto kern = k_conv_wgrad<CIN, COUT, XM, YM>;
+    if (!lc.ready) {
+        size_t smem = wgr_smem(CIN, COUT, a.g);
+        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
+        const int tpg = std::min(kTaps, 256 / CIN);
+        uint32_t cols = 32;
+        while (cols < (uint32_t)(tpg * CIN)) cols <<= 1;
+        int occ = 0, rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ))) return rc;
+        const int groups = (kTaps + tpg - 1) / tpg;
+        const int n0 = a.g.n0;
+        const int64_t target = (int64_t)ctx->num_sms * occ * 2;
+        const int64_t per = (int64_t)a.g.tiles * groups;
+        int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + per - 1) / per));
+        const int ppc = (n0 + chunks - 1) / chunks;
+        lc.ppc = ppc;
+        lc.tpg = tpg;
+        lc.cols = cols;
+        lc.grid = dim3(a.g.tiles, (n0 + ppc - 1) / ppc, groups);
+        lc.smem = smem;
+        lc.ready = true;
+    }
+    *part_need = (size_t)lc.grid.x * lc.grid.y * lc.grid.z * lc.tpg * COUT * CIN;
+    if (!a.part) return DARE_OK;  // sizing pass
+    a.ppc = lc.ppc;
+    a.tpg = lc.tpg;
+    a.cols = lc.cols;
+    kern<<<lc.grid, kThreads, lc.smem, ctx->stream>>>(a);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+static int launch_wgr(dare_ctx* ctx, LaunchCfg& lc, int cin, int cout, int xm, int ym, const WgrArgs& a,
+                      size_t* part_need) {
+#define DARE_WGR(CI, CO, XM, YM) \
+    if (cin == CI && cout == CO && xm == XM && ym == YM) return launch_wgr_t<CI, CO, XM, YM>(ctx, lc, a, part_need);
+    DARE_WGR(16, 16, IN_EMBED, IN_BF16)
+    DARE_WGR(16, 32, IN_BF16, IN_BF16)
+    DARE_WGR(32, 64, IN_BF16, IN_BF16)
+    DARE_WGR(64, 64, IN_BF16, IN_BF16)
+    DARE_WGR(64, 32, IN_BF16, IN_BF16)
+    DARE_WGR(32, 16, IN_BF16, IN_BF16)
+    DARE_WGR(16, 16, IN_BF16, IN_EMBED)
+#undef DARE_WGR
+    return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: no weight-gradient kernel for this shape");
+}
+
+static int pick_nt(int cink, int coutk, const Geom& g) {
+    if (coutk % 32 == 0 && fwd_smem(cink, 32, g) <= kMaxSmem) return 32;
+    return 16;
+}
+
+static inline int eblocks(const dare_ctx* ctx, int64_t work) { return grid_blocks(ctx, work, 256, 8); }
+
+// ---- network passes ----------------------------------------------------------
+static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32, int outm, bf16* out, bf16* fine,
+                        float* out32, const float* res32) {
+    Layer& L = net->layer[l];
+    FwdArgs a{};
+    a.g = net->geo[L.level];
+    if (L.level > 0) a.fg = net->geo[L.level - 1];
+    a.in = in;
+    a.in32 = in32;
+    a.w = L.wf;
+    a.cout = L.coutk;
+    a.out = out;
+    a.fine = fine;
+    a.out32 = out32;
+    a.res32 = res32;
+    a.err = net->err;
+    return launch_fwd(net->ctx, L.fwd, L.cink, L.nt, L.coutk / L.nt, in32 ? IN_EMBED : IN_BF16, outm, a);
+}
+
+// data gradient of layer l: dX = conv(dY, W flipped and transposed)
+static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, bf16* dx) {
+    Layer& L = net->layer[l];
+    FwdArgs a{};
+    a.g = net->geo[L.level];
+    a.in = dy;
+    a.in32 = dy32;
+    a.w = L.wb;
+    a.cout = L.cink;
+    a.out = dx;
+    a.err = net->err;
+    return launch_fwd(net->ctx, L.bwd, L.coutk, L.ntb, L.cink / L.ntb, dy32 ? IN_EMBED : IN_BF16, OUT_STORE, a);
+}
+
+static int conv_wgrad(dare_unet* net, int l, const bf16* x, const float* x32, const bf16* dy, const float* dy32,
+                      float scale) {
+    Layer& L = net->layer[l];
+    dare_ctx* ctx = net->ctx;
+    WgrArgs a{};
+    a.g = net->geo[L.level];
+    a.x = x;
+    a.x32 = x32;
+    a.dy = dy;
+    a.dy32 = dy32;
+    a.err = net->err;
+    size_t need = 0;
+    int rc = launch_wgr(ctx, L.wgr, L.cink, L.coutk, x32 ? IN_EMBED : IN_BF16, dy32 ? IN_EMBED : IN_BF16, a, &need);
+    if (rc) return rc;
+    if (need > net->part_floats) {
+        cudaFree(net->part);
+        net->part = nullptr;
+        net->part_floats = 0;
+        DARE_CUDA(ctx, cudaMalloc(&net->part, need * sizeof(float)));
+        net->part_floats = need;
+    }
+    a.part = net->part;
+    if ((rc = launch_wgr(ctx, L.wgr, L.cink, L.coutk, x32 ? IN_EMBED : IN_BF16, dy32 ? IN_EMBED : IN_BF16, a, &need)))
+        return rc;
+    const int nxy = (int)(L.wgr.grid.x * L.wgr.grid.y);
+    k_wgrad_reduce<<<eblocks(ctx, kTaps * L.cin * L.cout), 256, 0, ctx->stream>>>(
+        net->part, nxy, L.wgr.tpg, L.cink, L.coutk, L.cin, L.cout, scale, net->grad + L.woff);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+template <int C>
+static int restrict_to(dare_unet* net, int fl, const bf16* fine, bf16* coarse, float scale) {
+    dare_ctx* ctx = net->ctx;
+    const Geom& c = net->geo[fl + 1];
+    k_restrict<C><<<eblocks(ctx, (int64_t)c.n0 * c.n1 * c.n2 * (C / 8)), 256, 0, ctx->stream>>>(net->geo[fl], c, fine,
+                                                                                                coarse, scale);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+template <int C>
+static int prolong_add(dare_unet* net, int fl, const bf16* coarse, bf16* fine, float scale) {
+    dare_ctx* ctx = net->ctx;
+    const Geom& f = net->geo[fl];
+    k_prolong_add<C><<<eblocks(ctx, (int64_t)f.n0 * f.n1 * f.n2 * (C / 8)), 256, 0, ctx->stream>>>(
+        f, net->geo[fl + 1], coarse, fine, scale);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+int apply(dare_unet* net, const float* u, float* z) {
+    int rc;
+    if ((rc = conv_forward(net, ENC0, nullptr, u, OUT_STORE, net->S0, nullptr, nullptr, nullptr))) return rc;
+    if ((rc = restrict_to<16>(net, 0, net->S0, net->P1, 0.125f))) return rc;
+    if ((rc = conv_forward(net, ENC1, net->P1, nullptr, OUT_STORE, net->S1, nullptr, nullptr, nullptr))) return rc;
+    if ((rc = restrict_to<32>(net, 1, net->S1, net->P2, 0.125f))) return rc;
+    if ((rc = conv_forward(net, ENC2, net->P2, nullptr, OUT_STORE, net->S2, nullptr, nullptr, nullptr))) return rc;
+    if ((rc = restrict_to<64>(net, 2, net->S2, net->P3, 0.125f))) return rc;
+    if ((rc = conv_forward(net, ENC3, net->P3, nullptr, OUT_STORE, net->E3, nullptr, nullptr, nullptr))) return rc;
+    if ((rc = conv_forward(net, DEC3, net->E3, nullptr, OUT_ADDUP, nullptr, net->S2, nullptr, nullptr))) return rc;
+    if ((rc = conv_forward(net, DEC2, net->S2, nullptr, OUT_ADDUP, nullptr, net->S1, nullptr, nullptr))) return rc;
+    if ((rc = conv_forward(net, DEC1, net->S1, nullptr, OUT_ADDUP, nullptr, net->S0, nullptr, nullptr))) return rc;
+    return conv_forward(net, DEC0, net->S0, nullptr, OUT_F32, nullptr, nullptr, z, u);
+}
+
+// Backward pass of the last apply() for input u and output gradient g;
+// adds scale * dL/dW to net->grad.
+static int backward(dare_unet* net, const float* u, const float* g, float scale) {
+    int rc;
+    if ((rc = conv_wgrad(net, DEC0, net->S0, nullptr, nullptr, g, scale))) return rc;
+    if ((rc = conv_dgrad(net, DEC0, nullptr, g, net->dS0))) return rc;
+    if ((rc = restrict_to<16>(net, 0, net->dS0, net->dD1, 1.f))) return rc;
+    if ((rc = conv_wgrad(net, DEC1, net->S1, nullptr, net->dD1, nullptr, scale))) return rc;
+    if ((rc = conv_dgrad(net, DEC1, net->dD1, nullptr, net->dS1))) return rc;
+    if ((rc = restrict_to<32>(net, 1, net->dS1, net->dD2, 1.f))) return rc;
+    if ((rc = conv_wgrad(net, DEC2, net->S2, nullptr, net->dD2, nullptr, scale))) return rc;
+    if ((rc = conv_dgrad(net, DEC2, net->dD2, nullptr, net->dS2))) return rc;
+    if ((rc = restrict_to<64>(net, 2, net->dS2, net->dD3, 1.f))) return rc;
+    if ((rc = conv_wgrad(net, DEC3, net->E3, nullptr, net->dD3, nullptr, scale))) return rc;
+    if ((rc = conv_dgrad(net, DEC3, net->dD3, nullptr, net->dE3))) return rc;
+    if ((rc = conv_wgrad(net, ENC3, net->P3, nullptr, net->dE3, nullptr, scale))) return rc;
+    if ((rc = conv_dgrad(net, ENC3, net->dE3, nullptr, net->dP3))) return rc;
+    if ((rc = prolong_add<64>(net, 2, net->dP3, net->dS2, 0.125f))) return rc;
+    if ((rc = conv_wgrad(net, ENC2, net->P2, nullptr, net->dS2, nullptr, scale))) return rc;
+    if ((rc = conv_dgrad(net, ENC2, net->dS2, nullptr, net->dP2))) return rc;
+    if ((rc = prolong_add<32>(net, 1, net->dP2, net->dS1, 0.125f))) return rc;
+    if ((rc = conv_wgrad(net, ENC1, net->P1, nullptr, net->dS1, nullptr, scale))) return rc;
+    if ((rc = conv_dgrad(net, ENC1, net->dS1, nullptr, net->dP1))) return rc;
+    if ((rc = prolong_add<16>(net, 0, net->dP1, net->dS0, 0.125f))) return rc;
+    return conv_wgrad(net, ENC0, nullptr, u, net->dS0, nullptr, scale);
+}
+
+static int pack_weights(dare_unet* net) {
+    dare_ctx* ctx = net->ctx;
+    for (int l = 0; l < kLayers; l++) {
+        Layer& L = net->layer[l];
+        const int nz = L.coutk / L.nt;
+        k_pack<<<eblocks(ctx, (int64_t)nz * kTaps * L.cink * L.nt), 256, 0, ctx->stream>>>(
+            net->w + L.woff, L.cin, L.cout, L.cink, L.nt, nz, 0, L.wf);
+        DARE_LAUNCHED(ctx);
+        if (l != ENC0) {
+            const int nzb = L.cink / L.ntb;
+            k_pack<<<eblocks(ctx, (int64_t)nzb * kTaps * L.coutk * L.ntb), 256, 0, ctx->stream>>>(
+                net->w + L.woff, L.cin, L.cout, L.coutk, L.ntb, nzb, 1, L.wb);
+            DARE_LAUNCHED(ctx);
+        }
+    }
+    return DARE_OK;
+}
+
+static int check_err(dare_unet* net) {
+    int e = 0;
+    DARE_CUDA(net->ctx, cudaMemcpyAsync(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost, net->ctx->stream));
+    DARE_CUDA(net->ctx, cudaStreamSynchronize(net->ctx->stream));
+    if (e) return set_error(net->ctx, DARE_ERR_CUDA, "unet: a tensor-core wait timed out (code " + std::to_string(e) + ")");
+    return DARE_OK;
+}
+
+// Mean loss and gradient over `count` pairs; grad is zeroed first.
+static int loss_grad(dare_unet* net, const float* const* r, const float* const* e, const float* const* en2, int count,
+                     double* loss) {
+    dare_ctx* ctx = net->ctx;
+    int rc;
+    DARE_CUDA(ctx, cudaMemsetAsync(net->grad, 0, net->nparam * sizeof(float), ctx->stream));
+    DARE_CUDA(ctx, cudaMemsetAsync(net->dscal, 0, sizeof(double), ctx->stream));
+    const float scale = 1.f / (float)count;
+    for (int b = 0; b < count; b++) {
+        if ((rc = apply(net, r[b], net->z))) return rc;
+        k_loss_grad<<<eblocks(ctx, net->ncell), 256, 0, ctx->stream>>>(net->ncell, net->z, e[b], en2[b], scale,
+                                                                       net->g, net->dscal);
+        DARE_LAUNCHED(ctx);
+        if ((rc = backward(net, r[b], net->g, 1.f))) return rc;
+    }
+    if (loss) {
+        DARE_CUDA(ctx, cudaMemcpyAsync(loss, net->dscal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    return check_err(net);
+}
+
+static int adam_step(dare_unet* net, const dare_unet_train_params* p) {
+    dare_ctx* ctx = net->ctx;
+    net->adam_t++;
+    const float bc1 = 1.f - powf(p->beta1, (float)net->adam_t);
+    const float bc2 = 1.f - powf(p->beta2, (float)net->adam_t);
+    k_adam<<<eblocks(ctx, net->nparam), 256, 0, ctx->stream>>>(net->nparam, net->w, net->grad, net->adam_m,
+                                                               net->adam_v, p->lr, p->beta1, p->beta2, p->eps, bc1, bc2);
+    DARE_LAUNCHED(ctx);
+    net->steps++;
+    return pack_weights(net);
+}
+
+// ||e||^2 of device pairs into out[b] (for the public loss calls)
+static int pair_norms(dare_unet* net, const float* e, int count, float* out) {
+    dare_ctx* ctx = net->ctx;
+    for (int b = 0; b < count; b++) {
+        DARE_CUDA(ctx, cudaMemsetAsync(net->dscal + 1, 0, sizeof(double), ctx->stream));
+        k_sqnorm<<<eblocks(ctx, net->ncell), 256, 0, ctx->stream>>>(net->ncell, e + (size_t)b * net->ncell,
+                                                                    net->dscal + 1);
+        DARE_LAUNCHED(ctx);
+        k_store_norm<<<1, 1, 0, ctx->stream>>>(net->dscal + 1, out + b);
+        DARE_LAUNCHED(ctx);
+    }
+    return DARE_OK;
+}
+
+}  // namespace unet
+}  // namespace dare_gpu
+
+// ===========================================================================
+// C ABI
+extern "C" {
+
+void dare_unet_train_params_default(dare_unet_train_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->lr = 1e-3f;
+    p->beta1 = 0.9f;
+    p->beta2 = 0.999f;
+    p->eps = 1e-8f;
+    p->batch = 4;
+    p->steps = 8;
+    p->max_pairs_per_rhs = 12;
+    p->seed = 1234;
+}
+
+static void unet_free(dare_unet* net) {
+    for (int l = 0; l < kLayers; l++) {
+        cudaFree(net->layer[l].wf);
+        cudaFree(net->layer[l].wb);
+    }
+    cudaFree(net->w);
+    cudaFree(net->grad);
+    cudaFree(net->adam_m);
+    cudaFree(net->adam_v);
+    cudaFree(net->act_block);
+    cudaFree(net->z);
+    cudaFree(net->g);
+    cudaFree(net->part);
+    cudaFree(net->dscal);
+    cudaFree(net->err);
+    cudaFree(net->ring_r);
+    cudaFree(net->ring_e);
+    cudaFree(net->ring_en);
+    cudaFree(net->sol);
+}
+
+int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** out) {
+    if (!ctx || !n || !out) return DARE_ERR_BAD_ARG;
+    *out = nullptr;
+    for (int d = 0; d < 3; d++)
+        if (n[d] < 8 || n[d] % 8 != 0)
+            return set_error(ctx, DARE_ERR_BAD_ARG, "dare_unet_create: every grid size must be a positive multiple of 8");
+    cudaSetDevice(ctx->device);
+    dare_unet* net = new dare_unet();
+    net->ctx = ctx;
+    for (int d = 0; d < 3; d++) net->n[d] = n[d];
+    net->ncell = (int64_t)n[0] * n[1] * n[2];
+    for (int l = 0; l < kLevels; l++) net->geo[l] = make_geom(n[0] >> l, n[1] >> l, n[2] >> l);
+    int64_t off = 0;
+    for (int l = 0; l < kLayers; l++) {
+        Layer& L = net->layer[l];
+        L.level = kDefs[l].level;
+        L.cin = kDefs[l].cin;
+        L.cout = kDefs[l].cout;
+        L.cink = std::max(L.cin, 16);
+        L.coutk = std::max(L.cout, 16);
+        const Geom& g = net->geo[L.level];
+        L.nt = pick_nt(L.cink, L.coutk, g);
+        L.ntb = pick_nt(L.coutk, L.cink, g);
+        if (fwd_smem(L.cink, L.nt, g) > kMaxSmem || fwd_smem(L.coutk, L.ntb, g) > kMaxSmem ||
+            wgr_smem(L.cink, L.coutk, g) > kMaxSmem) {
+            delete net;
+            return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_create: grid too wide for the staged convolutions");
+        }
+        L.woff = off;
+        L.nparam = (int64_t)kTaps * L.cin * L.cout;
+        off += L.nparam;
+    }
+    net->nparam = off;
+
+    // activations: one zeroed block, every buffer 256-byte aligned
+    const int64_t T[4] = {net->geo[0].total, net->geo[1].total, net->geo[2].total, net->geo[3].total};
+    struct Slot {
+        bf16** p;
+        int level, c;
+    } slots[] = {{&net->S0, 0, 16}, {&net->P1, 1, 16}, {&net->S1, 1, 32}, {&net->P2, 2, 32}, {&net->S2, 2, 64},
+                 {&net->P3, 3, 64}, {&net->E3, 3, 64}, {&net->dS0, 0, 16}, {&net->dD1, 1, 16}, {&net->dS1, 1, 32},
+                 {&net->dD2, 2, 32}, {&net->dS2, 2, 64}, {&net->dD3, 3, 64}, {&net->dE3, 3, 64}, {&net->dP3, 3, 64},
+                 {&net->dP2, 2, 32}, {&net->dP1, 1, 16}};
+    size_t bytes = 0;
+    std::vector<size_t> offs;
+    for (auto& s : slots) {
+        offs.push_back(bytes);
+        bytes += ((size_t)T[s.level] * s.c * sizeof(bf16) + 255) / 256 * 256;
+    }
+    cudaError_t e = cudaMalloc(&net->act_block, bytes);
+    if (e == cudaSuccess) e = cudaMemset(net->act_block, 0, bytes);
+    for (size_t i = 0; i < sizeof(slots) / sizeof(slots[0]) && e == cudaSuccess; i++)
+        *slots[i].p = reinterpret_cast<bf16*>(static_cast<uint8_t*>(net->act_block) + offs[i]);
+    const size_t pb = net->nparam * sizeof(float);
+    if (e == cudaSuccess) e = cudaMalloc(&net->w, pb);
+    if (e == cudaSuccess) e = cudaMalloc(&net->grad, pb);
+    if (e == cudaSuccess) e = cudaMalloc(&net->adam_m, pb);
+    if (e == cudaSuccess) e = cudaMalloc(&net->adam_v, pb);
+    if (e == cudaSuccess) e = cudaMemset(net->adam_m, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(net->adam_v, 0, pb);
+    if (e == cudaSuccess) e = cudaMalloc(&net->z, net->ncell * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(net->z, 0, net->ncell * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&net->g, net->ncell * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&net->dscal, 4 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&net->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(net->err, 0, sizeof(int));
+    for (int l = 0; l < kLayers && e == cudaSuccess; l++) {
+        Layer& L = net->layer[l];
+        e = cudaMalloc(&L.wf, (size_t)kTaps * L.cink * L.coutk * sizeof(bf16));
+        if (e == cudaSuccess && l != ENC0) e = cudaMalloc(&L.wb, (size_t)kTaps * L.cink * L.coutk * sizeof(bf16));
+    }
+    if (e != cudaSuccess) {
+        unet_free(net);
+        delete net;
+        return check_cuda(ctx, e, "dare_unet_create");
+    }
+    // initial weights: N(0, 1/(27 cin)) per layer (variance-preserving for a
+    // linear network); dec0 zero so that N = I before training
+    std::vector<float> h(net->nparam, 0.f);
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < kLayers; l++) {
+        const Layer& L = net->layer[l];
+        if (l == DEC0) continue;
+        std::normal_distribution<float> nd(0.f, 1.f / std::sqrt((float)(kTaps * L.cin)));
+        for (int64_t i = 0; i < L.nparam; i++) h[L.woff + i] = nd(rng);
+    }
+    net->rng = seed * 0x9E3779B97F4A7C15ull + 1;
+    int rc = dare_unet_set_weights(net, h.data(), net->nparam);
+    if (rc) {
+        unet_free(net);
+        delete net;
+        return rc;
+    }
+    *out = net;
+    return DARE_OK;
+}
+
+int dare_unet_destroy(dare_unet* net) {
+    if (!net) return DARE_OK;
+    cudaSetDevice(net->ctx->device);
+    unet_free(net);
+    delete net;
+    return DARE_OK;
+}
+
+int64_t dare_unet_num_params(const dare_unet* net) { return net ? net->nparam : 0; }
+
+int dare_unet_get_weights(dare_unet* net, float* host, int64_t count) {
+    if (!net || !host || count != net->nparam) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = net->ctx;
+    cudaSetDevice(ctx->device);
+    DARE_CUDA(ctx, cudaMemcpyAsync(host, net->w, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DARE_OK;
+}
+
+int dare_unet_set_weights(dare_unet* net, const float* host, int64_t count) {
+    if (!net || !host || count != net->nparam) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = net->ctx;
+    cudaSetDevice(ctx->device);
+    DARE_CUDA(ctx, cudaMemcpyAsync(net->w, host, count * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    int rc = pack_weights(net);
+    if (rc) return rc;
+    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DARE_OK;
+}
+
+int dare_unet_apply(dare_unet* net, const float* u, float* z) {
+    if (!net || !u || !z || u == z) return DARE_ERR_BAD_ARG;
+    cudaSetDevice(net->ctx->device);
+    int rc = apply(net, u, z);
+    if (rc) return rc;
+    return check_err(net);
+}
+
+int dare_unet_read_activation(dare_unet* net, int which, float* host, int64_t count) {
+    if (!net || !host || which < 0 || which > 6) return DARE_ERR_BAD_ARG;
+    static const int lev[7] = {0, 1, 1, 2, 2, 3, 3}, ch[7] = {16, 16, 32, 32, 64, 64, 64};
+    bf16* const buf[7] = {net->S0, net->P1, net->S1, net->P2, net->S2, net->P3, net->E3};
+    const Geom& g = net->geo[lev[which]];
+    const int64_t total = (int64_t)g.n0 * g.n1 * g.n2 * ch[which];
+    if (count != total) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = net->ctx;
+    cudaSetDevice(ctx->device);
+    float* d = nullptr;
+    DARE_CUDA(ctx, cudaMalloc(&d, total * sizeof(float)));
+    k_read_act<<<eblocks(ctx, total), 256, 0, ctx->stream>>>(g, ch[which], buf[which], d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, total * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "dare_unet_read_activation");
+    return DARE_OK;
+}
+
+int dare_unet_loss_grad(dare_unet* net, const float* r, const float* e, int count, double* loss, float* grad_host) {
+    if (!net || !r || !e || count < 1) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = net->ctx;
+    cudaSetDevice(ctx->device);
+    float* en2 = nullptr;
+    DARE_CUDA(ctx, cudaMalloc(&en2, count * sizeof(float)));
+    int rc = pair_norms(net, e, count, en2);
+    std::vector<const float*> rp(count), ep(count), np(count);
+    for (int b = 0; b < count; b++) {
+        rp[b] = r + (size_t)b * net->ncell;
+        ep[b] = e + (size_t)b * net->ncell;
+        np[b] = en2 + b;
+    }
+    double l = 0.;
+    if (!rc) rc = loss_grad(net, rp.data(), ep.data(), np.data(), count, &l);
+    if (!rc && grad_host) {
+        cudaError_t ce = cudaMemcpyAsync(grad_host, net->grad, net->nparam * sizeof(float), cudaMemcpyDeviceToHost,
+                                         ctx->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+        if (ce != cudaSuccess) rc = check_cuda(ctx, ce, "dare_unet_loss_grad");
+    }
+    cudaFree(en2);
+    if (loss) *loss = l;
+    return rc;
+}
+
+int dare_unet_train_step(dare_unet* net, const float* r, const float* e, int count, const dare_unet_train_params* p,
+                         double* loss) {
+    if (!net || !r || !e || !p || count < 1) return DARE_ERR_BAD_ARG;
+    int rc = dare_unet_loss_grad(net, r, e, count, loss, nullptr);
+    if (rc) return rc;
+    if ((rc = adam_step(net, p))) return rc;
+    DARE_CUDA(net->ctx, cudaStreamSynchronize(net->ctx->stream));
+    return DARE_OK;
+}
+
+int dare_unet_stats(const dare_unet* net, int64_t* steps, int64_t* pairs_seen) {
+    if (!net) return DARE_ERR_BAD_ARG;
+    if (steps) *steps = net->steps;
+    if (pairs_seen) *pairs_seen = net->pairs_seen;
+    return DARE_OK;
+}
+
+int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const dare_unet_train_params* p,
+                              dare_unet_train_report* rep) {
+    if (!net || !s || !p || !rep || p->batch < 1 || p->steps < 0) return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = net->ctx;
+    const GridDev& g = s->grid->dev;
+    if (g.dim != 3 || g.n[0] != net->n[0] || g.n[1] != net->n[1] || g.n[2] != net->n[2])
+        return set_error(ctx, DARE_ERR_BAD_ARG, "dare_unet_train_on_system: grid does not match the network");
+    cudaSetDevice(ctx->device);
+    std::memset(rep, 0, sizeof(*rep));
+    const int64_t n = net->ncell;
+    if (!net->ring_r) {
+        // ring of pairs: up to 256, at most ~4 GB
+        const size_t pair_bytes = (size_t)n * 2 * sizeof(float);
+        int cap = (int)std::min<size_t>(256, std::max<size_t>(8, ((size_t)4 << 30) / pair_bytes));
+        cudaError_t e = cudaMalloc(&net->ring_r, (size_t)cap * n * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&net->ring_e, (size_t)cap * n * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&net->ring_en, (size_t)cap * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&net->sol, (size_t)2 * n * sizeof(double));
+        if (e != cudaSuccess) return check_cuda(ctx, e, "dare_unet_train_on_system");
+        net->ring_cap = cap;
+    }
+    double* x0 = net->sol;
+    double* xs = net->sol + n;
+    const int eb = eblocks(ctx, n);
+    DARE_CUDA(ctx, cudaMemcpyAsync(x0, s->x, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+
+    // the plain solve to the tolerance, warm-started at x0
+    dare_solver_params sp;
+    dare_solver_params_default(&sp);
+    sp.tol = tol;
+    sp.tol_relative = 1;
+    sp.max_it = 1000;
+    sp.compute_true_residual = 0;
+    dare_solve_report sr;
+    k_warm<<<eb, 256, 0, ctx->stream>>>(n, s->diag, x0, s->x);
+    DARE_LAUNCHED(ctx);
+    int rc = dare_bicgstab2_fp64(s, &sp, &sr);
+    if (rc) return rc;
+    rep->plain_iters = sr.iters;
+    DARE_CUDA(ctx, cudaMemcpyAsync(xs, s->x, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+
+    // its iterates x_k, k = 0 .. K-1, as pairs
+    const int K = std::min(std::max(sr.iters, 1), p->max_pairs_per_rhs);
+    for (int k = 0; k < K; k++) {
+        const double* xk = x0;
+        if (k > 0) {
+            dare_solver_params q = sp;
+            q.tol = 0.;
+            q.tol_relative = 0;
+            q.max_it = k;
+            k_warm<<<eb, 256, 0, ctx->stream>>>(n, s->diag, x0, s->x);
+            DARE_LAUNCHED(ctx);
+            dare_solve_report qr;
+            if ((rc = dare_bicgstab2_fp64(s, &q, &qr))) return rc;
+            xk = s->x;
+        }
+        const int slot = net->ring_next;
+        DARE_CUDA(ctx, cudaMemsetAsync(net->dscal + 2, 0, sizeof(double), ctx->stream));
+        k_make_pair<<<eb, 256, 0, ctx->stream>>>(g, s->diag, s->rhs, xk, xs, net->ring_r + (size_t)slot * n,
+                                                 net->ring_e + (size_t)slot * n, net->dscal + 2);
+        DARE_LAUNCHED(ctx);
+        k_store_norm<<<1, 1, 0, ctx->stream>>>(net->dscal + 2, net->ring_en + slot);
+        DARE_LAUNCHED(ctx);
+        net->ring_next = (net->ring_next + 1) % net->ring_cap;
+        net->ring_size = std::min(net->ring_size + 1, net->ring_cap);
+        rep->pairs_added++;
+        net->pairs_seen++;
+    }
+    DARE_CUDA(ctx, cudaMemcpyAsync(s->x, xs, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+
+    // optimiser steps on minibatches drawn from the ring
+    std::mt19937_64 rng(p->seed ^ net->rng);
+    net->rng = net->rng * 6364136223846793005ull + 1442695040888963407ull;
+    std::vector<const float*> rp(p->batch), ep(p->batch), np(p->batch);
+    for (int st = 0; st < p->steps; st++) {
+        for (int b = 0; b < p->batch; b++) {
+            const int i = (int)(rng() % (uint64_t)net->ring_size);
+            rp[b] = net->ring_r + (size_t)i * n;
+            ep[b] = net->ring_e + (size_t)i * n;
+            np[b] = net->ring_en + i;
+        }
+        double l = 0.;
+        if ((rc = loss_grad(net, rp.data(), ep.data(), np.data(), p->batch, &l))) return rc;
+        if (st == 0) rep->loss_first = l;
+        rep->loss_last = l;
+        if ((rc = adam_step(net, p))) return rc;
+        rep->steps++;
+    }
+    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    rep->pairs_total = net->ring_size;
+    return DARE_OK;
+}
+
+}  // extern "C"

@@ -282,6 +282,91 @@ DARE_API int dare_residual_norm_noalloc(int dim, const int64_t n[3], const int p
                                         const double* x, const double* b, double* norm_out, void* stream,
                                         char* err, int err_len);
 
+/* ---- learned linear preconditioner ---------------------------------------------
+ * No counterpart in the reference: DaRe preconditions BiCGStab2 with Jacobi
+ * only (BiCGStab2.inl:258-261, 568-571).  This is the preconditioner of
+ * the Jacobi-folded system Ahat = A D^-1:
+ *     N(u) = u + U(u),
+ * U a bias-free, activation-free (so linear) convolutional U-Net on one 3D
+ * grid whose three sizes are multiples of 8: four levels of 16, 32, 64, 64
+ * channels, 3x3x3 kernels with zero padding, 2x2x2 average-pool restriction,
+ * nearest-neighbour prolongation added to the encoder output of the finer
+ * level (additive skip).  Eight convolutions: enc0 1->16, enc1 16->32,
+ * enc2 32->64, enc3 64->64, dec3 64->64, dec2 64->32, dec1 32->16,
+ * dec0 16->1.  Weights and activations are BF16, accumulation FP32 (tcgen05
+ * tensor memory).  Vectors are FP32 over the internal cells, ordinal
+ * (i*ny + j)*nz + k, in device memory.  Parameters are FP32 master weights,
+ * layer after layer, each [27][cout][cin] with tap t = (di+1)*9 + (dj+1)*3 +
+ * (dk+1) reading input cell (i+di, j+dj, k+dk). */
+typedef struct dare_unet dare_unet;
+
+typedef struct {
+    float lr;                /* Adam step size */
+    float beta1, beta2, eps; /* Adam moments */
+    int batch;               /* (residual, error) pairs per optimiser step */
+    int steps;               /* optimiser steps per dare_unet_train_on_system call */
+    int max_pairs_per_rhs;   /* solver iterates turned into pairs per call */
+    uint64_t seed;           /* minibatch sampling */
+} dare_unet_train_params;
+
+typedef struct {
+    int pairs_added;         /* pairs generated from the plain solver by this call */
+    int pairs_total;         /* pairs held in the training ring */
+    int plain_iters;         /* iterations of the plain solve to the tolerance */
+    int steps;               /* optimiser steps taken */
+    double loss_first;       /* mean relative squared error of the first / last step */
+    double loss_last;
+} dare_unet_train_report;
+
+typedef struct {
+    int iteration_budget;    /* learned inner iterations allowed in total before the
+                                automatic switch to the plain FP64 Jacobi-BiCGStab2 */
+    int inner_max_it;        /* per refinement */
+    double inner_rel_tol;    /* relative reduction of each inner solve */
+    int max_refinements;
+} dare_learned_params;
+
+DARE_API void dare_unet_train_params_default(dare_unet_train_params* p);
+DARE_API void dare_learned_params_default(dare_learned_params* p);
+/* Randomly initialised network (He-style scale, dec0 starts at zero so N = I). */
+DARE_API int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** out);
+DARE_API int dare_unet_destroy(dare_unet* net);
+DARE_API int64_t dare_unet_num_params(const dare_unet* net);
+DARE_API int dare_unet_get_weights(dare_unet* net, float* host, int64_t count);
+DARE_API int dare_unet_set_weights(dare_unet* net, const float* host, int64_t count);
+/* z = N(u) (device vectors, may not alias). */
+DARE_API int dare_unet_apply(dare_unet* net, const float* u, float* z);
+/* Loss over `count` pairs stored back to back (r[c*ncell..], e[c*ncell..]):
+ * mean over pairs of ||N(r) - e||^2 / ||e||^2; its gradient with respect to
+ * every parameter is written to grad_host (num_params floats, may be NULL). */
+DARE_API int dare_unet_loss_grad(dare_unet* net, const float* r, const float* e, int count, double* loss,
+                                 float* grad_host);
+/* One Adam step on the mean loss of `count` device pairs. */
+DARE_API int dare_unet_train_step(dare_unet* net, const float* r, const float* e, int count,
+                                  const dare_unet_train_params* p, double* loss);
+/* Solve the assembled system with the plain FP64 Jacobi-BiCGStab2 from its
+ * current x to ||b - A x|| <= tol ||b||, turn the solver's iterates x_k into pairs (r_k = b - A x_k,
+ * e_k = D (x* - x_k), D the diagonal), add them to the training ring and take
+ * p->steps optimiser steps on minibatches drawn from the ring.  On return the
+ * system holds the converged plain solution x*. */
+DARE_API int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const dare_unet_train_params* p,
+                                       dare_unet_train_report* rep);
+/* Number of optimiser steps and pairs seen since creation. */
+DARE_API int dare_unet_stats(const dare_unet* net, int64_t* steps, int64_t* pairs_seen);
+/* Internal activation `which` (0 S0, 1 P1, 2 S1, 3 P2, 4 S2, 5 P3, 6 E3) as
+ * FP32 [cell][channel] over the internal cells of its level. */
+DARE_API int dare_unet_read_activation(dare_unet* net, int which, float* host, int64_t count);
+
+/* Mixed-precision BiCGStab2 with the learned preconditioner: FP64 iterative
+ * refinement r = b - A x, an FP32 inner BiCGStab2 on Ahat N y = r with FP64
+ * dot products, x += D^-1 N y.  When the learned phase misses the stated
+ * iteration budget (or stops contracting) the plain FP64 Jacobi-BiCGStab2
+ * continues from the current iterate; rep->fallback_used reports that.  The
+ * final residual is the FP64 ||b - A x||_2.  p->tol / tol_relative set the
+ * stop test, p->max_it caps the fallback. */
+DARE_API int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare_solver_params* p,
+                                    const dare_learned_params* lp, dare_solve_report* rep);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,6 +112,12 @@ def lib():
         L.dor_bicgstab2.restype = C.c_int
         L.dor_num_threads.restype = C.c_int
         L.dor_set_threads.argtypes = [C.c_int]
+        L.dor_unet_num_params.restype = C.c_int64
+        L.dor_unet_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.dor_unet_forward.restype = C.c_int
+        L.dor_unet_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p]
+        L.dor_unet_loss_grad.restype = C.c_int
     return _lib
 
 
@@ -266,3 +272,62 @@ def num_threads() -> int:
 
 def set_threads(n: int) -> None:
     lib().dor_set_threads(n)
+
+
+# ---- learned linear preconditioner (dare_oracle_unet.c) ----------------------
+UNET_LAYERS = (("enc0", 0, 1, 16), ("enc1", 1, 16, 32), ("enc2", 2, 32, 64), ("enc3", 3, 64, 64),
+               ("dec3", 3, 64, 64), ("dec2", 2, 64, 32), ("dec1", 1, 32, 16), ("dec0", 0, 16, 1))
+UNET_ACTS = (("S0", 0, 16), ("P1", 1, 16), ("S1", 1, 32), ("P2", 2, 32), ("S2", 2, 64), ("P3", 3, 64),
+             ("E3", 3, 64))
+
+
+def unet_num_params() -> int:
+    return int(lib().dor_unet_num_params())
+
+
+def unet_layer_slices():
+    """name -> (slice into the flat parameter vector, (27, cout, cin))."""
+    out, off = {}, 0
+    for name, _, cin, cout in UNET_LAYERS:
+        m = 27 * cin * cout
+        out[name] = (slice(off, off + m), (27, cout, cin))
+        off += m
+    return out
+
+
+def unet_forward(n, w, u, bf16=True, with_acts=False):
+    """z = u + U(u) (float64); optionally the activations S0..E3 as a dict."""
+    n3 = np.ascontiguousarray(n, dtype=np.int32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    u = np.ascontiguousarray(u, dtype=np.float64).ravel()
+    z = np.empty_like(u)
+    acts = None
+    if with_acts:
+        cells = [int(np.prod([x >> l for x in n])) for l in range(4)]
+        acts = np.empty(sum(cells[l] * c for _, l, c in UNET_ACTS), dtype=np.float64)
+    rc = lib().dor_unet_forward(_ptr(n3), _ptr(w), _ptr(u), int(bf16), _ptr(z), _ptr(acts))
+    if rc:
+        raise ValueError("oracle unet: bad grid")
+    if not with_acts:
+        return z
+    res, off = {}, 0
+    for name, l, c in UNET_ACTS:
+        m = cells[l] * c
+        res[name] = acts[off:off + m].reshape(cells[l], c)
+        off += m
+    return z, res
+
+
+def unet_loss_grad(n, w, r, e, bf16=True, want_grad=True):
+    """Mean relative squared error over the pairs (rows of r, e) and its gradient."""
+    n3 = np.ascontiguousarray(n, dtype=np.int32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    e = np.ascontiguousarray(e, dtype=np.float64)
+    count = r.shape[0] if r.ndim == 2 else 1
+    loss = C.c_double(0.0)
+    grad = np.empty(unet_num_params(), dtype=np.float64) if want_grad else None
+    rc = lib().dor_unet_loss_grad(_ptr(n3), _ptr(w), _ptr(r), _ptr(e), count, int(bf16), C.byref(loss), _ptr(grad))
+    if rc:
+        raise ValueError("oracle unet: bad grid")
+    return loss.value, grad

@@ -1,0 +1,166 @@
+"""GPU parity of the learned preconditioner's tcgen05 kernels with the CPU
+oracle (forward activations, output, loss, every layer's weight gradient),
+on-GPU training, and the learned solver with its automatic fallback."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+# BF16 activations and weights, FP32 accumulation on both sides; the oracle
+# rounds at the same points in double arithmetic, so the gap is summation
+# order plus the occasional differently rounded bf16 value.
+FWD_TOL = 2e-2
+GRAD_TOL = 3e-2
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _weights(seed, n_params):
+    rng = np.random.default_rng(seed)
+    w = np.zeros(n_params, dtype=np.float32)
+    for name, (sl, (_, cout, cin)) in O.unet_layer_slices().items():
+        w[sl] = rng.normal(0.0, 1.0 / np.sqrt(27 * cin), sl.stop - sl.start)
+    return w
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import dare_b200 as D
+    return D.Context(0)
+
+
+@pytest.mark.parametrize("n", [(16, 24, 32), (8, 8, 8), (32, 16, 8)])
+def test_forward_matches_oracle(ctx, n):
+    import dare_b200 as D
+    torch = _torch()
+    net = D.LearnedPreconditioner(ctx, n, seed=3)
+    w = _weights(11, net.num_params)
+    net.set_weights(w)
+    N = int(np.prod(n))
+    g = torch.Generator().manual_seed(5)
+    u = torch.randn(N, generator=g, dtype=torch.float32).cuda()
+    z = torch.empty_like(u)
+    net.apply(u.data_ptr(), z.data_ptr())
+    torch.cuda.synchronize()
+    zo, acts = O.unet_forward(n, w, u.cpu().double().numpy(), bf16=True, with_acts=True)
+    errs = {}
+    for i, (name, _, _) in enumerate(O.UNET_ACTS):
+        errs[name] = rel_l2(net.activation(i), acts[name])
+    uu = u.cpu().double().numpy()
+    errs["U(u)"] = rel_l2(z.cpu().double().numpy() - uu, zo - uu)
+    print(n, errs)
+    assert all(e < FWD_TOL for e in errs.values()), errs
+
+
+def test_identity_at_initialisation(ctx):
+    # dec0 starts at zero: N = I exactly before any training
+    import dare_b200 as D
+    torch = _torch()
+    n = (16, 16, 16)
+    net = D.LearnedPreconditioner(ctx, n, seed=0)
+    u = torch.randn(int(np.prod(n)), dtype=torch.float32).cuda()
+    z = torch.empty_like(u)
+    net.apply(u.data_ptr(), z.data_ptr())
+    assert torch.equal(z, u)
+
+
+def test_gradients_match_oracle(ctx):
+    import dare_b200 as D
+    torch = _torch()
+    n = (16, 24, 32)
+    net = D.LearnedPreconditioner(ctx, n, seed=3)
+    w = _weights(12, net.num_params)
+    net.set_weights(w)
+    N = int(np.prod(n))
+    g = torch.Generator().manual_seed(9)
+    r = torch.randn(2, N, generator=g, dtype=torch.float32).cuda()
+    e = torch.randn(2, N, generator=g, dtype=torch.float32).cuda()
+    loss, grad = net.loss_grad(r.data_ptr(), e.data_ptr(), 2)
+    lo, go = O.unet_loss_grad(n, w, r.cpu().double().numpy(), e.cpu().double().numpy(), bf16=True)
+    errs = {"loss": abs(loss - lo) / lo}
+    for name, (sl, _) in O.unet_layer_slices().items():
+        errs[name] = rel_l2(grad[sl], go[sl])
+    print(errs)
+    assert all(v < GRAD_TOL for v in errs.values()), errs
+    # and the BF16 gradient is close to the exact (FP64, unrounded) one
+    _, gx = O.unet_loss_grad(n, w, r.cpu().double().numpy(), e.cpu().double().numpy(), bf16=False)
+    assert rel_l2(grad, gx) < 5e-2
+
+
+def test_train_step_reduces_loss(ctx):
+    import dare_b200 as D
+    torch = _torch()
+    n = (16, 16, 16)
+    net = D.LearnedPreconditioner(ctx, n, seed=4)
+    N = int(np.prod(n))
+    # target: a fixed smoothing of the input (a linear map the net can represent)
+    g = torch.Generator().manual_seed(2)
+    r = torch.randn(4, N, generator=g, dtype=torch.float32).cuda()
+    x = r.view(4, *n)
+    e = (x + 0.25 * (torch.roll(x, 1, 1) + torch.roll(x, -1, 1) + torch.roll(x, 1, 3) + torch.roll(x, -1, 3)))
+    e = e.reshape(4, N).contiguous()
+    p = net.train_params(lr=3e-3)
+    losses = [net.train_step(r.data_ptr(), e.data_ptr(), 4, p) for _ in range(60)]
+    print(losses[0], losses[-1])
+    assert losses[-1] < 0.5 * losses[0]
+    assert net.stats()["steps"] == 60
+
+
+def _operator(ctx, n, seed):
+    from dare_b200 import training
+    return training.Operator(ctx, training.sample_case(n, seed, "cuda:0"))
+
+
+def test_learned_solver_fallback_and_residual_judge(ctx):
+    import dare_b200 as D
+    n = 32
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=5)
+    op = _operator(ctx, n, 101)
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 500, "tol_relative": 1})
+    op.assemble()
+    plain = solver.solve(op.system)
+    x_plain = op.system.solution()
+    # a budget of one inner iteration cannot reach 1e-10: the plain solve takes over
+    op.assemble()
+    rep = net.solve(op.system, solver, net.learned_params(iteration_budget=1))
+    assert rep["fallback_used"] == 1 and rep["converged"] == 1
+    assert rep["true_res_abs"] <= rep["tol_abs"] * 1.0000001
+    # a normal budget: converged by the learned phase, judged by the FP64 residual
+    op.assemble()
+    rep = net.solve(op.system, solver)
+    print(plain, rep)
+    assert rep["converged"] == 1 and rep["fallback_used"] == 0
+    assert rep["true_res_abs"] <= rep["tol_abs"]
+    assert rel_l2(op.system.solution(), x_plain) < 1e-8
+
+
+def test_trained_network_gains_over_identity(ctx):
+    """Training on the plain solver's pairs lowers the iterations the learned
+    solver needs, against the same solver with N = I (the untrained net)."""
+    import dare_b200 as D
+    from dare_b200 import training
+    n = 32
+    ident = D.LearnedPreconditioner(ctx, (n, n, n), seed=6)
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=6)
+    p = net.train_params(steps=24, batch=4, lr=2e-3)
+    reps = training.train(net, ctx, n, operators=6, steps_per_operator=3, params=p, seed=1000)
+    first, last = reps[0]["loss_first"], np.mean([r["loss_last"] for r in reps[-3:]])
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 500, "tol_relative": 1})
+    its = {"identity": [], "trained": []}
+    for seed in (5001, 5002):
+        op = _operator(ctx, n, seed)
+        for name, m in (("identity", ident), ("trained", net)):
+            op.reset()
+            op.assemble()
+            r = m.solve(op.system, solver)
+            assert r["converged"] == 1 and r["true_res_abs"] <= r["tol_abs"]
+            its[name].append(r["inner_iters"])
+    print({"loss_first": first, "loss_last": last, "iters": its})
+    assert last < first
+    assert sum(its["trained"]) < sum(its["identity"])
