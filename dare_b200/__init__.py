@@ -154,6 +154,7 @@ _SIGS += [
                                             C.POINTER(UNetTrainReport)]),
     ("dare_unet_stats", C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("dare_unet_read_activation", C.c_int, [_P, C.c_int, _P, C.c_int64]),
+    ("dare_unet_launch_info", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_int64)]),
     ("dare_bicgstab2_learned", C.c_int, [_P, _P, C.POINTER(SolverParams), C.POINTER(LearnedParams),
                                          C.POINTER(SolveReport)]),
 ]
@@ -642,6 +643,15 @@ class LearnedPreconditioner:
         _check(lib().dare_unet_train_on_system(self.h, system.h, tol, C.byref(p), C.byref(rep)), self.ctx.h,
                "unet_train_on_system")
         return {name: getattr(rep, name) for name, _ in rep._fields_}
+
+    def launch_info(self, layer: int, kind: int = 0) -> dict | None:
+        """Launch shape of a convolution kernel (kind 0 forward, 1 data
+        gradient, 2 weight gradient) after its first launch."""
+        v = (C.c_int64 * 8)()
+        if lib().dare_unet_launch_info(self.h, layer, kind, v) != 0:
+            return None
+        keys = ("grid_x", "grid_y", "grid_z", "smem", "planes_per_cta", "taps_per_cta", "tmem_cols", "ctas_per_sm")
+        return dict(zip(keys, list(v)))
 
     def stats(self) -> dict:
         s, q = C.c_int64(), C.c_int64()

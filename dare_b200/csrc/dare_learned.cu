@@ -4,10 +4,24 @@
 //
 //   outer (FP64):  r = b - A x; stop when ||r||_2 <= tol_abs
 //   inner (FP32):  BiCGStab(2) on  Ahat N y = r,  Ahat = A D^-1 (unit
-//                  diagonal), N the U-Net, y0 = 0, FP64 dot products and
+//                  diagonal), N the U-Net, from zero, FP64 dot products and
 //                  scalar recurrences (the reference's steps 3-25,
-//                  BiCGStab2.inl:262-560, with the operator Ahat N)
-//   update (FP64): x += D^-1 N y
+//                  BiCGStab2.inl:262-560, with the operator Ahat N), in
+//                  flexible form (below)
+//   update (FP64): x += D^-1 d,  d the inner solution in the x variable
+//
+// Flexible form.  The network is linear in exact arithmetic but its BF16
+// activations make N(a + b) differ from N(a) + N(b) by a few 1e-3, so the
+// textbook right-preconditioned update (accumulate y, apply N once at the
+// end) would leave the recurrence residual inconsistent with the iterate at
+// that level.  Instead every iteration keeps the four network outputs it
+// computes, zu = N(u) (step 6), zr = N(r) (step 9), zv = N(v) (step 13),
+// zs = N(s) (step 18), and updates the x-variable correction directly,
+//     d += (a1 - a2 b1) zu + (a2 + w1) zr - w1 a2 zv + w2 zs,
+// the x-space image of the reference's y updates (steps 10 and 24) written
+// with exactly the vectors whose Ahat-images (v, s, w, t) entered the
+// residual recurrence (steps 8, 16, 25).  The recurrence residual is then
+// the residual of d up to FP32 rounding, however nonlinear N is.
 // The learned phase stops when its inner iterations exceed the iteration
 // budget or the refinement stops contracting; the plain FP64 solve then
 // continues from the current iterate.  The reported residual is always the
@@ -15,7 +29,9 @@
 //
 // One inner iteration is one CUDA graph: 4 network applications (11
 // tensor-core/level-transfer kernels each), 4 SpMV kernels with fused dot
-// products, 5 vector kernels.  Scalars live on the device; kernels after a
+// products, 5 vector kernels.  The inner solve may stop after its first
+// iteration (the reference's `k > 1` rule applies to its own solve, not to
+// this inner correction).  Scalars live on the device; kernels after a
 // breakdown see `done` and skip their work.
 #include <algorithm>
 #include <cmath>
@@ -34,13 +50,15 @@ enum : int { L_RUNNING = 0, L_CONVERGED = 1, L_MAXIT = 2, L_BREAKDOWN = 3, L_NAN
 
 struct LState {
     double rho0, alpha, beta, omega1, omega2, rnorm, rnorm0, tol;
+    double alpha1, beta1;  // alpha of step 7 and beta of step 11 (the flexible update)
     int k, max_it, done, status, step;
     unsigned int count;
 };
 
 struct Vecs {
-    float *rh, *r, *u, *v, *s, *w, *t, *y, *z, *rin;
+    float *rh, *r, *u, *v, *s, *w, *t, *d, *zu, *zr, *zv, *zs, *rin;
 };
+constexpr int kNumVecs = 13;
 
 }  // namespace learned
 }  // namespace dare_gpu
@@ -48,7 +66,7 @@ struct Vecs {
 struct dare_learned_ws {
     int64_t n = 0;
     float* ahat32 = nullptr;   // 6 n
-    float* vec = nullptr;      // 10 n
+    float* vec = nullptr;      // kNumVecs n
     double* partials = nullptr;
     double* scal = nullptr;    // [0] outer norms
     dare_gpu::learned::LState* st = nullptr;
@@ -123,7 +141,7 @@ __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, in
     GRID_LOOP(c, n) b[c] = (float)a[c];
 }
 
-// start of an inner solve: r = rh = rin, u = v = w = y = 0
+// start of an inner solve: r = rh = rin, u = v = w = d = 0
 __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, LState* st, double* partials, double rel_tol,
                                               int max_it) {
     double acc[1] = {0.};
@@ -134,7 +152,7 @@ __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, LState* st, do
         vs.u[c] = 0.f;
         vs.v[c] = 0.f;
         vs.w[c] = 0.f;
-        vs.y[c] = 0.f;
+        vs.d[c] = 0.f;
         acc[0] += (double)r * r;
     }
     double tot[1];
@@ -189,14 +207,15 @@ __global__ void k_upd_u(int64_t n, Vecs vs, const LState* st) {
     GRID_LOOP(c, n) vs.u[c] = vs.r[c] - beta * vs.u[c];
 }
 
-// out = Ahat z with <out, rh> (mode 0: gamma -> alpha, step 7/14;
+// out = Ahat z with <out, rh> (mode 0: gamma -> alpha, steps 7 and 14;
 // mode 1: rho1 -> beta, step 11)
-__global__ void __launch_bounds__(256) k_spmv_dot(GridDev g, const float* __restrict__ ah, Vecs vs, float* out,
-                                                  LState* st, double* partials, int mode, int step) {
+__global__ void __launch_bounds__(256) k_spmv_dot(GridDev g, const float* __restrict__ ah, Vecs vs,
+                                                  const float* __restrict__ z, float* out, LState* st,
+                                                  double* partials, int mode, int step) {
     if (st->done) return;
     double acc[1] = {0.};
     GRID_LOOP(c, g.ncell) {
-        const float v = ahat_apply(g, ah, vs.z, c);
+        const float v = ahat_apply(g, ah, z, c);
         out[c] = v;
         acc[0] += (double)v * vs.rh[c];
     }
@@ -206,21 +225,20 @@ __global__ void __launch_bounds__(256) k_spmv_dot(GridDev g, const float* __rest
         if (mode == 0) {
             if (tot[0] == 0.) return fail(st, step);
             st->alpha = st->rho0 / tot[0];
+            if (step == 7) st->alpha1 = st->alpha;
         } else {
             st->beta = st->alpha * tot[0] / st->rho0;
+            st->beta1 = st->beta;
             st->rho0 = tot[0];
         }
     }
 }
 
-// (8), (10): r -= alpha v; y += alpha u
-__global__ void k_upd_ry(int64_t n, Vecs vs, const LState* st) {
+// (8): r -= alpha v (the matching x update is folded into k_upd_final)
+__global__ void k_upd_r(int64_t n, Vecs vs, const LState* st) {
     if (st->done) return;
     const float alpha = (float)st->alpha;
-    GRID_LOOP(c, n) {
-        vs.r[c] -= alpha * vs.v[c];
-        vs.y[c] += alpha * vs.u[c];
-    }
+    GRID_LOOP(c, n) vs.r[c] -= alpha * vs.v[c];
 }
 
 // (12) v = s - beta v
@@ -248,7 +266,7 @@ __global__ void __launch_bounds__(256) k_spmv_omega(GridDev g, const float* __re
     if (st->done) return;
     double acc[5] = {0., 0., 0., 0., 0.};
     GRID_LOOP(c, g.ncell) {
-        const float t = ahat_apply(g, ah, vs.z, c);
+        const float t = ahat_apply(g, ah, vs.zs, c);
         vs.t[c] = t;
         const double r = vs.r[c], s = vs.s[c];
         acc[0] += r * s;
@@ -271,15 +289,17 @@ __global__ void __launch_bounds__(256) k_spmv_omega(GridDev g, const float* __re
     }
 }
 
-// (24), (25): y += w1 r + w2 s + alpha u; r -= w1 s + w2 t; u -= w1 v + w2 w;
-// convergence test on ||r||
+// (10), (24) in flexible form: d += (a1 - a2 b1) zu + (a2 + w1) zr - w1 a2 zv + w2 zs;
+// (25): r -= w1 s + w2 t; u -= w1 v + w2 w; convergence test on ||r||
 __global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, LState* st, double* partials) {
     if (st->done) return;
-    const float w1 = (float)st->omega1, w2 = (float)st->omega2, alpha = (float)st->alpha;
+    const double a1 = st->alpha1, a2 = st->alpha, b1 = st->beta1, om1 = st->omega1, om2 = st->omega2;
+    const float cu = (float)(a1 - a2 * b1), cr = (float)(a2 + om1), cv = (float)(-om1 * a2), cs = (float)om2;
+    const float w1 = (float)om1, w2 = (float)om2;
     double acc[1] = {0.};
     GRID_LOOP(c, n) {
         const float r = vs.r[c], s = vs.s[c];
-        vs.y[c] += w1 * r + w2 * s + alpha * vs.u[c];
+        vs.d[c] += cu * vs.zu[c] + cr * vs.zr[c] + cv * vs.zv[c] + cs * vs.zs[c];
         const float rn = r - w1 * s - w2 * vs.t[c];
         vs.r[c] = rn;
         vs.u[c] -= w1 * vs.v[c] + w2 * vs.w[c];
@@ -293,7 +313,7 @@ __global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, LState* s
         if (!(rn == rn)) {
             st->done = 1;
             st->status = L_NAN;
-        } else if (rn <= st->tol && st->k > 1) {
+        } else if (rn <= st->tol) {
             st->done = 1;
             st->status = L_CONVERGED;
         } else if (++st->k > st->max_it) {
@@ -323,22 +343,22 @@ static int launch_iteration(dare_ctx* ctx, dare_unet* net, const GridDev& g, con
     DARE_LAUNCHED(ctx);
     k_upd_u<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
-    if ((rc = unet::apply(net, vs.u, vs.z))) return rc;
-    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.v, st, partials, 0, 7);
+    if ((rc = unet::apply(net, vs.u, vs.zu))) return rc;
+    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.zu, vs.v, st, partials, 0, 7);
     DARE_LAUNCHED(ctx);
-    k_upd_ry<<<eb, 256, 0, s>>>(n, vs, st);
+    k_upd_r<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
-    if ((rc = unet::apply(net, vs.r, vs.z))) return rc;
-    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.s, st, partials, 1, 11);
+    if ((rc = unet::apply(net, vs.r, vs.zr))) return rc;
+    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.zr, vs.s, st, partials, 1, 11);
     DARE_LAUNCHED(ctx);
     k_upd_v<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
-    if ((rc = unet::apply(net, vs.v, vs.z))) return rc;
-    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.w, st, partials, 0, 14);
+    if ((rc = unet::apply(net, vs.v, vs.zv))) return rc;
+    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.zv, vs.w, st, partials, 0, 14);
     DARE_LAUNCHED(ctx);
     k_upd3<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
-    if ((rc = unet::apply(net, vs.s, vs.z))) return rc;
+    if ((rc = unet::apply(net, vs.s, vs.zs))) return rc;
     k_spmv_omega<<<eb, 256, 0, s>>>(g, ah, vs, st, partials);
     DARE_LAUNCHED(ctx);
     k_upd_final<<<eb, 256, 0, s>>>(n, vs, st, partials);
@@ -384,7 +404,7 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         if (!lw) return DARE_ERR_OOM;
         lw->n = n;
         cudaError_t e = cudaMalloc(&lw->ahat32, (size_t)n * 6 * sizeof(float));
-        if (e == cudaSuccess) e = cudaMalloc(&lw->vec, (size_t)n * 10 * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&lw->vec, (size_t)n * kNumVecs * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&lw->partials, (size_t)kMaxQ * kMaxBlocks * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&lw->scal, 4 * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&lw->st, sizeof(LState));
@@ -399,7 +419,10 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     dare_learned_ws* lw = ws->learned;
     const int eb = grid_blocks(ctx, n, 256, 8);
     float* V = lw->vec;
-    Vecs vs{V, V + n, V + 2 * n, V + 3 * n, V + 4 * n, V + 5 * n, V + 6 * n, V + 7 * n, V + 8 * n, V + 9 * n};
+    Vecs vs;
+    float** slots[kNumVecs] = {&vs.rh, &vs.r, &vs.u, &vs.v, &vs.s, &vs.w, &vs.t,
+                               &vs.d, &vs.zu, &vs.zr, &vs.zv, &vs.zs, &vs.rin};
+    for (int i = 0; i < kNumVecs; i++) *slots[i] = V + (size_t)i * n;
 
     // Ahat = A D^-1 (FP64 fold) and its FP32 copy
     if ((rc = launch_fold(ctx, g, ws->march, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
@@ -416,7 +439,7 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     if (!lw->graph || lw->graph_net != net) {
         if (lw->graph) cudaGraphExecDestroy(lw->graph);
         lw->graph = nullptr;
-        if ((rc = dare_gpu::unet::apply(net, vs.rin, vs.z))) return rc;  // sets the launch configurations
+        if ((rc = dare_gpu::unet::apply(net, vs.rin, vs.zs))) return rc;  // sets the launch configurations
         DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         cudaGraph_t graph = nullptr;
         DARE_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -467,9 +490,8 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         const LState st = *lw->st_host;
         inner_total += std::min(st.k, cap);
         if (st.status == L_NAN) break;
-        // x += D^-1 N y
-        if ((rc = dare_gpu::unet::apply(net, vs.y, vs.z))) return rc;
-        k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, vs.z, s->x);
+        // x += D^-1 d
+        k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, vs.d, s->x);
         DARE_LAUNCHED(ctx);
         refinements++;
     }

@@ -46,36 +46,60 @@ constexpr size_t kMaxSmem = 232448;  // 227 KB of opt-in shared memory per CTA
 // operand staging: one plane segment of `rows` padded positions starting at
 // flattened position Q0, as C/8 planes of 16-byte chunks with row pitch RP
 // (chunk (kc, q) at byte (kc * RP + q) * 16).  Positions outside the array
-// read zero.  IN_EMBED (C == 16) takes an FP32 vector over the internal
-// cells as channel 0 (rounded to bf16) and zero elsewhere.
+// and rows q >= valid_rows read zero.
+// IN_EMBED (C == 16) takes an FP32 vector over the internal cells as channel
+// 0 (rounded to bf16) and zero elsewhere: the slot's other channels are
+// zeroed once per kernel (stage_zero), the FP32 values land asynchronously
+// in a raw 4-byte-per-row buffer, and stage_finish (run by the issuing
+// thread after its cp.async wait) writes the bf16 channel-0 values.
 template <int C, int MODE>
-__device__ __forceinline__ void stage(uint8_t* slot, const bf16* __restrict__ in, const float* __restrict__ in32,
-                                      const Geom& g, int64_t Q0, int rows, int RP) {
+__device__ __forceinline__ void stage(uint8_t* slot, float* raw, const bf16* __restrict__ in,
+                                      const float* __restrict__ in32, const Geom& g, int64_t Q0, int rows, int RP,
+                                      int valid_rows) {
     if (MODE == IN_BF16) {
         constexpr int KC = C / 8;
         const int nent = rows * KC;
         for (int idx = threadIdx.x; idx < nent; idx += kThreads) {
             const int q = idx / KC, kc = idx - q * KC;
             const int64_t Q = Q0 + q;
-            const bool v = Q >= 0 && Q < g.total;
+            const bool v = Q >= 0 && Q < g.total && q < valid_rows;
             cp16(slot + ((size_t)kc * RP + q) * 16, in + (v ? Q : 0) * C + kc * 8, v);
         }
     } else {
         for (int q = threadIdx.x; q < rows; q += kThreads) {
             const int64_t Q = Q0 + q;
-            float v = 0.f;
-            if (Q >= 0 && Q < g.total) {
+            bool ok = false;
+            int64_t ci = 0;
+            if (Q >= 0 && Q < g.total && q < valid_rows) {
                 const int I = (int)(Q / g.plane);
                 const int rem = (int)(Q - (int64_t)I * g.plane);
                 const int J = rem / g.W, K = rem - J * g.W;
-                if (I >= 1 && I <= g.n0 && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2)
-                    v = __ldg(in32 + ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1));
+                ok = I >= 1 && I <= g.n0 && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2;
+                ci = ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1);
             }
-            *reinterpret_cast<uint4*>(slot + (size_t)q * 16) = make_uint4(pack_bf16(v, 0.f), 0u, 0u, 0u);
-            *reinterpret_cast<uint4*>(slot + ((size_t)RP + q) * 16) = make_uint4(0u, 0u, 0u, 0u);
+            if (ok)
+                cp4(raw + q, in32 + ci);
+            else
+                raw[q] = 0.f;
         }
     }
 }
+
+template <int MODE>
+__device__ __forceinline__ void stage_finish(uint8_t* slot, const float* raw, int rows) {
+    if (MODE == IN_EMBED) {
+        for (int q = threadIdx.x; q < rows; q += kThreads)
+            *reinterpret_cast<bf16*>(slot + (size_t)q * 16) = __float2bfloat16_rn(raw[q]);
+    }
+}
+
+__device__ __forceinline__ void stage_zero(uint8_t* p, uint32_t bytes) {
+    for (uint32_t o = threadIdx.x * 16; o < bytes; o += kThreads * 16)
+        *reinterpret_cast<uint4*>(p + o) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// raw FP32 staging bytes of one slot (IN_EMBED), 16-byte aligned
+__host__ __device__ inline uint32_t raw_bytes(int rows) { return (uint32_t)(((rows + 3) / 4) * 16); }
 
 // ---------------------------------------------------------------------------
 // forward convolution
@@ -123,20 +147,30 @@ __device__ __forceinline__ void fwd_epilogue(const FwdArgs& a, uint32_t tmem, in
     } else if (OUTM == OUT_ADDUP) {
         // nearest-neighbour prolongation of this coarse cell, added into its
         // eight children on the finer level (the additive skip)
+        // (the eight children's loads of one 8-channel chunk are issued together)
         const Geom& f = a.fg;
-#pragma unroll 1
-        for (int ch = 0; ch < 8; ch++) {
-            const int fi = 2 * I - 1 + (ch >> 2), fj = 2 * J - 1 + ((ch >> 1) & 1), fk = 2 * K - 1 + (ch & 1);
-            bf16* dst = a.fine + (((int64_t)fi * (f.n1 + 2) + fj) * f.W + fk) * a.cout + co0;
+        const int64_t fplane = (int64_t)(f.n1 + 2) * f.W;
+        bf16* base = a.fine + (((int64_t)(2 * I - 1) * (f.n1 + 2) + (2 * J - 1)) * f.W + (2 * K - 1)) * a.cout + co0;
 #pragma unroll
-            for (int c = 0; c < NT; c += 8) {
-                uint4 o = *reinterpret_cast<const uint4*>(dst + c);
+        for (int c = 0; c < NT; c += 8) {
+            uint4 o[8];
+#pragma unroll
+            for (int ch = 0; ch < 8; ch++)
+                o[ch] = *reinterpret_cast<const uint4*>(
+                    base + ((ch >> 2) * fplane + ((ch >> 1) & 1) * f.W + (ch & 1)) * a.cout + c);
+#pragma unroll
+            for (int ch = 0; ch < 8; ch++) {
                 uint4 q;
-                q.x = pack_bf16(bf16_lo(o.x) + __uint_as_float(r[c + 0]), bf16_hi(o.x) + __uint_as_float(r[c + 1]));
-                q.y = pack_bf16(bf16_lo(o.y) + __uint_as_float(r[c + 2]), bf16_hi(o.y) + __uint_as_float(r[c + 3]));
-                q.z = pack_bf16(bf16_lo(o.z) + __uint_as_float(r[c + 4]), bf16_hi(o.z) + __uint_as_float(r[c + 5]));
-                q.w = pack_bf16(bf16_lo(o.w) + __uint_as_float(r[c + 6]), bf16_hi(o.w) + __uint_as_float(r[c + 7]));
-                *reinterpret_cast<uint4*>(dst + c) = q;
+                q.x = pack_bf16(bf16_lo(o[ch].x) + __uint_as_float(r[c + 0]),
+                                bf16_hi(o[ch].x) + __uint_as_float(r[c + 1]));
+                q.y = pack_bf16(bf16_lo(o[ch].y) + __uint_as_float(r[c + 2]),
+                                bf16_hi(o[ch].y) + __uint_as_float(r[c + 3]));
+                q.z = pack_bf16(bf16_lo(o[ch].z) + __uint_as_float(r[c + 4]),
+                                bf16_hi(o[ch].z) + __uint_as_float(r[c + 5]));
+                q.w = pack_bf16(bf16_lo(o[ch].w) + __uint_as_float(r[c + 6]),
+                                bf16_hi(o[ch].w) + __uint_as_float(r[c + 7]));
+                *reinterpret_cast<uint4*>(base + ((ch >> 2) * fplane + ((ch >> 1) & 1) * f.W + (ch & 1)) * a.cout +
+                                          c) = q;
             }
         }
     } else {
@@ -156,9 +190,11 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
     const int rows = stage_rows(g);
     const int RP = row_pitch(rows, CIN);
     const uint32_t SB = (uint32_t)KC * RP * 16;
+    const uint32_t RB = INM == IN_EMBED ? raw_bytes(rows) : 0u;
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(slots + 4 * SB);
+    float* raw = reinterpret_cast<float*>(slots + 4 * SB);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(slots + 4 * SB + 4 * RB);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
 
     const int P0 = blockIdx.x * kTileM;
@@ -171,6 +207,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
         mbar_init(&mbar[1], 1);
         mbar_fence_init();
     }
+    if (INM == IN_EMBED) stage_zero(slots, 4 * SB);
     if (tid < 32) tmem_alloc(tslot, COLS);
     fence_before_sync();
     __syncthreads();
@@ -183,7 +220,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
     }
     const int64_t pbase = (int64_t)P0 - g.W - 1;
     for (int I = I0 - 1; I <= I0 + 1; I++)
-        stage<CIN, INM>(slots + (I & 3) * SB, a.in, a.in32, g, (int64_t)I * g.plane + pbase, rows, RP);
+        stage<CIN, INM>(slots + (I & 3) * SB, raw + (I & 3) * (RB / 4), a.in, a.in32, g,
+                        (int64_t)I * g.plane + pbase, rows, RP, rows);
     cp_commit();
 
     constexpr uint32_t idesc = idesc_bf16(kTileM, NT, 0, 0);
@@ -192,6 +230,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
     for (int I = I0; I <= I1; I++) {
         const int buf = (I - I0) & 1;
         cp_wait_all();
+        for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1; p++)
+            stage_finish<INM>(slots + (p & 3) * SB, raw + (p & 3) * (RB / 4), rows);
         fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
@@ -219,8 +259,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
             }
         }
         if (I + 2 <= I1 + 1)
-            stage<CIN, INM>(slots + ((I + 2) & 3) * SB, a.in, a.in32, g, (int64_t)(I + 2) * g.plane + pbase, rows,
-                            RP);
+            stage<CIN, INM>(slots + ((I + 2) & 3) * SB, raw + ((I + 2) & 3) * (RB / 4), a.in, a.in32, g,
+                            (int64_t)(I + 2) * g.plane + pbase, rows, RP, rows);
         cp_commit();
         if (I > I0) fwd_epilogue<NT, OUTM>(a, tmem, buf ^ 1, I - 1, P0, blockIdx.z * NT);
         fence_before_sync();
@@ -269,9 +309,13 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(WgrArgs a) {
     const int rows = stage_rows(g);
     const int RP = row_pitch(rows, CIN);
     const uint32_t SB = (uint32_t)KCX * RP * 16;
+    const uint32_t RBX = XM == IN_EMBED ? raw_bytes(rows) : 0u;
+    const uint32_t RBY = YM == IN_EMBED ? raw_bytes(kTileM) : 0u;
     uint8_t* dys = smem;
     uint8_t* xs = smem + 2 * DB;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(xs + 4 * SB);
+    float* xraw = reinterpret_cast<float*>(xs + 4 * SB);
+    float* yraw = reinterpret_cast<float*>(xs + 4 * SB + 4 * RBX);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(xs + 4 * SB + 4 * RBX + 2 * RBY);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
 
     const int P0 = blockIdx.x * kTileM;
@@ -285,6 +329,8 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(WgrArgs a) {
         mbar_init(&mbar[1], 1);
         mbar_fence_init();
     }
+    if (XM == IN_EMBED) stage_zero(xs, 4 * SB);
+    if (YM == IN_EMBED) stage_zero(dys, 2 * DB);
     if (tid < 32) tmem_alloc(tslot, a.cols);
     fence_before_sync();
     __syncthreads();
@@ -293,8 +339,14 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(WgrArgs a) {
 
     const int64_t pbase = (int64_t)P0 - g.W - 1;
     for (int I = I0 - 1; I <= I0 + 1; I++)
-        stage<CIN, XM>(xs + (I & 3) * SB, a.x, a.x32, g, (int64_t)I * g.plane + pbase, rows, RP);
-    stage<COUT, YM>(dys + (I0 & 1) * DB, a.dy, a.dy32, g, (int64_t)I0 * g.plane + P0, kTileM, RPD);
+        stage<CIN, XM>(xs + (I & 3) * SB, xraw + (I & 3) * (RBX / 4), a.x, a.x32, g, (int64_t)I * g.plane + pbase,
+                       rows, RP, rows);
+    // dY only at the tile's positions inside this plane: on coarse levels a
+    // 128-position tile runs past the plane's end into the next plane's rows,
+    // which that plane's own pass counts
+    const int yrows = min(kTileM, g.plane - P0);
+    stage<COUT, YM>(dys + (I0 & 1) * DB, yraw + (I0 & 1) * (RBY / 4), a.dy, a.dy32, g, (int64_t)I0 * g.plane + P0,
+                    kTileM, RPD, yrows);
     cp_commit();
 
     constexpr uint32_t idesc = idesc_bf16(kTileM, CIN, 1, 1);
@@ -303,6 +355,9 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(WgrArgs a) {
     for (int I = I0; I <= I1; I++) {
         const int buf = (I - I0) & 1;
         cp_wait_all();
+        for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1; p++)
+            stage_finish<XM>(xs + (p & 3) * SB, xraw + (p & 3) * (RBX / 4), rows);
+        stage_finish<YM>(dys + (I & 1) * DB, yraw + (I & 1) * (RBY / 4), kTileM);
         fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
@@ -330,9 +385,11 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(WgrArgs a) {
             }
         }
         if (I + 2 <= I1 + 1)
-            stage<CIN, XM>(xs + ((I + 2) & 3) * SB, a.x, a.x32, g, (int64_t)(I + 2) * g.plane + pbase, rows, RP);
+            stage<CIN, XM>(xs + ((I + 2) & 3) * SB, xraw + ((I + 2) & 3) * (RBX / 4), a.x, a.x32, g,
+                           (int64_t)(I + 2) * g.plane + pbase, rows, RP, rows);
         if (I + 1 <= I1)
-            stage<COUT, YM>(dys + ((I + 1) & 1) * DB, a.dy, a.dy32, g, (int64_t)(I + 1) * g.plane + P0, kTileM, RPD);
+            stage<COUT, YM>(dys + ((I + 1) & 1) * DB, yraw + ((I + 1) & 1) * (RBY / 4), a.dy, a.dy32, g,
+                            (int64_t)(I + 1) * g.plane + P0, kTileM, RPD, yrows);
         cp_commit();
     }
     if (!aborted) {
@@ -594,17 +651,21 @@ __global__ void k_warm(int64_t n, const double* __restrict__ diag, const double*
 
 // ---------------------------------------------------------------------------
 // host side: launch configuration and dispatch
-static size_t fwd_smem(int cin, int nt, const Geom& g) {
-    const int RP = row_pitch(stage_rows(g), cin);
-    return (size_t)kTaps * cin * nt * 2 + 4 * (size_t)(cin / 8) * RP * 16 + 32;
+static size_t fwd_smem(int cin, int nt, const Geom& g, bool embed) {
+    const int rows = stage_rows(g);
+    const int RP = row_pitch(rows, cin);
+    return (size_t)kTaps * cin * nt * 2 + 4 * (size_t)(cin / 8) * RP * 16 + (embed ? 4 * (size_t)raw_bytes(rows) : 0) +
+           32;
 }
 
 static int dy_pitch_rt(int c) { return kTileM + (c == 16 ? 4 : (c == 32 ? 2 : 1)); }
 
-static size_t wgr_smem(int cin, int cout, const Geom& g) {
-    const int RP = row_pitch(stage_rows(g), cin);
+static size_t wgr_smem(int cin, int cout, const Geom& g, bool xembed, bool yembed) {
+    const int rows = stage_rows(g);
+    const int RP = row_pitch(rows, cin);
     const size_t DB = (size_t)(cout / 8) * dy_pitch_rt(cout) * 16;
-    const size_t body = 2 * DB + 4 * (size_t)(cin / 8) * RP * 16 + 32;
+    const size_t body = 2 * DB + 4 * (size_t)(cin / 8) * RP * 16 + (xembed ? 4 * (size_t)raw_bytes(rows) : 0) +
+                        (yembed ? 2 * (size_t)raw_bytes(kTileM) : 0) + 32;
     // the A operand (dY^T, 128 rows of which Cout are real) of the second dY
     // slot reaches 16 row groups past its start: keep that inside the CTA
     const size_t reach = DB + (size_t)(kTileM / 16) * 256 + 15 * (size_t)dy_pitch_rt(cout) * 16 + 256;
@@ -614,6 +675,8 @@ static size_t wgr_smem(int cin, int cout, const Geom& g) {
 template <typename K>
 static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int* occ_out) {
     DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
     int occ = 0;
     for (;;) {
         DARE_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
@@ -630,18 +693,21 @@ template <int CIN, int NT, int INM, int OUTM>
 static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const FwdArgs& a0) {
     auto kern = k_conv_fwd<CIN, NT, INM, OUTM>;
     if (!lc.ready) {
-        size_t smem = fwd_smem(CIN, NT, a0.g);
+        size_t smem = fwd_smem(CIN, NT, a0.g, INM == IN_EMBED);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         const uint32_t cols = 2 * NT < 32 ? 32 : 2 * NT;
         int occ = 0, rc;
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ))) return rc;
+        // about four waves of CTAs; a CTA marches at least two planes (it
+        // stages two more than it computes)
         const int n0 = a0.g.n0;
-        const int64_t target = (int64_t)ctx->num_sms * occ * 2;
+        const int64_t target = (int64_t)ctx->num_sms * occ * 4;
         int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + (int64_t)a0.g.tiles * nz - 1) /
                                                                             ((int64_t)a0.g.tiles * nz)));
         int ppc = (n0 + chunks - 1) / chunks;
-        ppc = std::max(ppc, std::min(n0, 4));
+        ppc = std::max(ppc, std::min(n0, 2));
         lc.ppc = ppc;
+        lc.occ = occ;
         lc.grid = dim3(a0.g.tiles, (n0 + ppc - 1) / ppc, nz);
         lc.smem = smem;
         lc.cols = cols;
@@ -676,7 +742,7 @@ template <int CIN, int COUT, int XM, int YM>
 static int launch_wgr_t(dare_ctx* ctx, LaunchCfg& lc, WgrArgs a, size_t* part_need) {
     auto kern = k_conv_wgrad<CIN, COUT, XM, YM>;
     if (!lc.ready) {
-        size_t smem = wgr_smem(CIN, COUT, a.g);
+        size_t smem = wgr_smem(CIN, COUT, a.g, XM == IN_EMBED, YM == IN_EMBED);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         const int tpg = std::min(kTaps, 256 / CIN);
         uint32_t cols = 32;
@@ -692,6 +758,7 @@ static int launch_wgr_t(dare_ctx* ctx, LaunchCfg& lc, WgrArgs a, size_t* part_ne
         lc.ppc = ppc;
         lc.tpg = tpg;
         lc.cols = cols;
+        lc.occ = occ;
         lc.grid = dim3(a.g.tiles, (n0 + ppc - 1) / ppc, groups);
         lc.smem = smem;
         lc.ready = true;
@@ -722,7 +789,7 @@ static int launch_wgr(dare_ctx* ctx, LaunchCfg& lc, int cin, int cout, int xm, i
 }
 
 static int pick_nt(int cink, int coutk, const Geom& g) {
-    if (coutk % 32 == 0 && fwd_smem(cink, 32, g) <= kMaxSmem) return 32;
+    if (coutk % 32 == 0 && fwd_smem(cink, 32, g, false) <= kMaxSmem) return 32;
     return 16;
 }
 
@@ -937,7 +1004,7 @@ extern "C" {
 void dare_unet_train_params_default(dare_unet_train_params* p) {
     if (!p) return;
     std::memset(p, 0, sizeof(*p));
-    p->lr = 1e-3f;
+    p->lr = 2e-4f;
     p->beta1 = 0.9f;
     p->beta2 = 0.999f;
     p->eps = 1e-8f;
@@ -991,8 +1058,8 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         const Geom& g = net->geo[L.level];
         L.nt = pick_nt(L.cink, L.coutk, g);
         L.ntb = pick_nt(L.coutk, L.cink, g);
-        if (fwd_smem(L.cink, L.nt, g) > kMaxSmem || fwd_smem(L.coutk, L.ntb, g) > kMaxSmem ||
-            wgr_smem(L.cink, L.coutk, g) > kMaxSmem) {
+        if (fwd_smem(L.cink, L.nt, g, l == ENC0) > kMaxSmem || fwd_smem(L.coutk, L.ntb, g, l == DEC0) > kMaxSmem ||
+            wgr_smem(L.cink, L.coutk, g, l == ENC0, l == DEC0) > kMaxSmem) {
             delete net;
             return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_create: grid too wide for the staged convolutions");
         }
@@ -1156,6 +1223,17 @@ int dare_unet_train_step(dare_unet* net, const float* r, const float* e, int cou
     if (rc) return rc;
     if ((rc = adam_step(net, p))) return rc;
     DARE_CUDA(net->ctx, cudaStreamSynchronize(net->ctx->stream));
+    return DARE_OK;
+}
+
+int dare_unet_launch_info(const dare_unet* net, int layer, int kind, int64_t info[8]) {
+    if (!net || !info || layer < 0 || layer >= kLayers || kind < 0 || kind > 2) return DARE_ERR_BAD_ARG;
+    const Layer& L = net->layer[layer];
+    const LaunchCfg& c = kind == 0 ? L.fwd : (kind == 1 ? L.bwd : L.wgr);
+    if (!c.ready) return DARE_ERR_STATE;
+    const int64_t v[8] = {c.grid.x, c.grid.y, c.grid.z, (int64_t)c.smem, c.ppc, kind == 2 ? c.tpg : kTaps, c.cols,
+                          c.occ};
+    for (int i = 0; i < 8; i++) info[i] = v[i];
     return DARE_OK;
 }
 

@@ -67,6 +67,7 @@ struct LaunchCfg {
     int ppc = 1;   // planes per CTA
     int tpg = 27;  // taps per CTA (weight gradient)
     int cols = 32; // TMEM columns
+    int occ = 0;   // resident CTAs per SM
 };
 
 struct Layer {

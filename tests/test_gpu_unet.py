@@ -148,17 +148,20 @@ def test_trained_network_gains_over_identity(ctx):
     n = 32
     ident = D.LearnedPreconditioner(ctx, (n, n, n), seed=6)
     net = D.LearnedPreconditioner(ctx, (n, n, n), seed=6)
-    p = net.train_params(steps=24, batch=4, lr=2e-3)
+    p = net.train_params(steps=24, batch=4, lr=2e-4)
     reps = training.train(net, ctx, n, operators=6, steps_per_operator=3, params=p, seed=1000)
     first, last = reps[0]["loss_first"], np.mean([r["loss_last"] for r in reps[-3:]])
     solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 500, "tol_relative": 1})
+    # a deep inner reduction per refinement, so the inner solves are long
+    # enough for the preconditioner to show (each takes at least 2 iterations)
+    lp = net.learned_params(inner_rel_tol=1e-5)
     its = {"identity": [], "trained": []}
     for seed in (5001, 5002):
         op = _operator(ctx, n, seed)
         for name, m in (("identity", ident), ("trained", net)):
             op.reset()
             op.assemble()
-            r = m.solve(op.system, solver)
+            r = m.solve(op.system, solver, lp)
             assert r["converged"] == 1 and r["true_res_abs"] <= r["tol_abs"]
             its[name].append(r["inner_iters"])
     print({"loss_first": first, "loss_last": last, "iters": its})
