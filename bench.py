@@ -32,7 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-METRIC = "implicit steps/s (256^3 TVD convection-diffusion, Jacobi-BiCGStab2 to 1e-10)"
+METRIC = "implicit steps/s & time-to-1e-10 residual: learned vs plain BiCGStab2, 1 B200"
 UNIT = "steps/s"
 # Algorithmic bytes per cell and launch (FP64, each operand streamed once; the
 # SpMV inputs at the 6 neighbours come from cache).  See DESIGN.md.
@@ -57,10 +57,13 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["tvd", "gauss64", "hetero", "batched"], default="tvd",
+    ap.add_argument("--workload", choices=["tvd", "gauss64", "hetero", "batched", "unet"], default="tvd",
                     help="tvd: the headline 256^3 line; the others print their own measurement line")
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
+    ap.add_argument("--learn-operators", type=int, default=8,
+                    help="128^3 operators the preconditioner is trained on (4 implicit steps each)")
     return ap.parse_args(argv)
 
 
@@ -309,6 +312,10 @@ def run_dare(args):
                "sample": f"{len(times)} full implicit steps of the same {n}^3 workload from the same initial "
                          f"field (CPU oracle, OpenMP), iterations {citers}"}
 
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_comparison(D, ctx, system, field, asm, n, args)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -321,6 +328,8 @@ def run_dare(args):
                        "l2": "inputs larger than L2 (system ~3.6 GB per GPU)"},
             "time_to_residual_ms": ms / args.steps, "iterations_per_step": statistics.mean(iters),
             "cell_updates_per_s": value * n ** 3,
+            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e); learned-preconditioned solve in 'learned'",
+            "learned": learned,
             "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -328,6 +337,69 @@ def run_dare(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _timed_solve(ctx, system, field, asm, fn, reps=2):
+    """Assemble from the field and solve; the last of `reps` runs is reported
+    (the first captures graphs and sizes workspaces)."""
+    out = None
+    for _ in range(reps):
+        system.build(field, asm)
+        ctx.synchronize()
+        ctx.timer_start()
+        rep = fn()
+        ms = ctx.timer_stop()
+        out = {"ms": ms, "iters": rep["iters"], "inner_iters": rep["inner_iters"],
+               "refinements": rep["refinements"], "fallback_used": rep["fallback_used"],
+               "converged": rep["converged"], "res_rel": rep["true_res_abs"] / rep["b_norm"]}
+    return out
+
+
+def learned_comparison(D, ctx, system, field, asm, n, args):
+    """Time-to-1e-10 of one implicit step: plain FP64 Jacobi-BiCGStab2 against
+    the learned-preconditioned mixed-precision BiCGStab2.  The network is
+    trained here, on the GPU, on 128^3 operators of the training distribution
+    (constant or log-normal D, Pe in [1, 10], CFL 0.5), then evaluated on
+    held-out 128^3 operators and, with the same weights, on this workload."""
+    from dare_b200 import training
+    out = {}
+    t0 = time.perf_counter()
+    m = 128
+    net128 = D.LearnedPreconditioner(ctx, (m, m, m), seed=args.seed + 1)
+    reps = training.train(net128, ctx, m, operators=args.learn_operators, steps_per_operator=4,
+                          params=net128.train_params(steps=8, batch=4), seed=args.seed + 1000)
+    out["training"] = {"grid": f"{m}^3", "operators": args.learn_operators, "implicit_steps": len(reps),
+                       "pairs": sum(r["pairs_added"] for r in reps), "adam_steps": sum(r["steps"] for r in reps),
+                       "loss_first": reps[0]["loss_first"], "loss_last_mean4": float(np.mean([r["loss_last"]
+                                                                                             for r in reps[-4:]])),
+                       "wall_s": time.perf_counter() - t0}
+    plain = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    refine = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1},
+                         precision="FP32_REFINE")
+    ident128 = D.LearnedPreconditioner(ctx, (m, m, m), seed=args.seed + 1)
+    held = []
+    for seed in (args.seed + 9001, args.seed + 9002):
+        op = training.Operator(ctx, training.sample_case(m, seed, "cuda:0"))
+        row = {"peclet": op.case["peclet"], "heterogeneous_D": "cell_D" in op.case}
+        for name, fn in (("plain_fp64", lambda: plain.solve(op.system)),
+                         ("fp32_refine_jacobi", lambda: refine.solve(op.system)),
+                         ("learned_untrained", lambda: ident128.solve(op.system, plain)),
+                         ("learned", lambda: net128.solve(op.system, plain))):
+            row[name] = _timed_solve(ctx, op.system, op.field, op.asm, fn)
+        held.append(row)
+        del op
+    out["held_out_128"] = held
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=args.seed + 1)
+    net.set_weights(net128.get_weights())
+    res = {"grid": f"{n}^3 (this workload, weights trained at {m}^3)"}
+    for name, fn in (("plain_fp64", lambda: plain.solve(system)),
+                     ("fp32_refine_jacobi", lambda: refine.solve(system)),
+                     ("learned", lambda: net.solve(system, plain))):
+        res[name] = _timed_solve(ctx, system, field, asm, fn)
+    res["learned_speedup_vs_plain"] = res["plain_fp64"]["ms"] / res["learned"]["ms"]
+    out["bench_workload"] = res
+    out["target_3x_met"] = res["learned_speedup_vs_plain"] >= 3.0
+    return out
 
 
 # ----------------------------------------------------------------------------
@@ -437,6 +509,46 @@ def run_hetero(args):
     return 0
 
 
+def run_unet(args):
+    """The learned preconditioner's network alone: `--steps` timed applies of
+    N at n^3 (seeded random weights) after `--warmup` untimed ones, and one
+    training step (forward + backward + Adam, batch 4) when n <= 128."""
+    import torch
+
+    import dare_b200 as D
+    n = args.n
+    ctx = D.Context(0)
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=args.seed)
+    rng = np.random.default_rng(args.seed)
+    net.set_weights(rng.normal(0.0, 0.02, net.num_params).astype(np.float32))
+    gen = torch.Generator(device="cuda").manual_seed(args.seed)
+    u = torch.randn(n ** 3, device="cuda", generator=gen)
+    z = torch.empty_like(u)
+    for _ in range(max(1, args.warmup)):
+        net.apply(u.data_ptr(), z.data_ptr())
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        net.apply(u.data_ptr(), z.data_ptr())
+    ms = ctx.timer_stop() / args.steps
+    layers = D.LearnedPreconditioner.LAYERS
+    flops = sum(2 * 27 * cin * cout * (n >> lev) ** 3 for _, lev, cin, cout in layers)
+    out = {"workload": f"learned preconditioner apply z = u + U(u), {n}^3", "apply_ms": ms,
+           "cells_per_s": n ** 3 / (ms * 1e-3), "useful_tflops": flops / (ms * 1e-3) / 1e12,
+           "launch": {name: net.launch_info(i, 0) for i, (name, _, _, _) in enumerate(layers)}}
+    if n <= 128:
+        r = torch.randn(4, n ** 3, device="cuda", generator=gen)
+        e = torch.randn(4, n ** 3, device="cuda", generator=gen)
+        p = net.train_params()
+        net.train_step(r.data_ptr(), e.data_ptr(), 4, p)
+        ctx.synchronize()
+        ctx.timer_start()
+        net.train_step(r.data_ptr(), e.data_ptr(), 4, p)
+        out["train_step_batch4_ms"] = ctx.timer_stop()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_batched(args):
     """4096 independent diffusion boxes (sides 16-64), one implicit step each, one launch."""
     import dare_b200 as D
@@ -494,6 +606,8 @@ def main(argv=None):
         return run_gauss64(args)
     if args.workload == "hetero":
         return run_hetero(args)
+    if args.workload == "unet":
+        return run_unet(args)
     if args.workload == "batched":
         return run_batched(args)
     return run_dare(args)
