@@ -650,7 +650,7 @@ class LearnedPreconditioner:
         v = (C.c_int64 * 8)()
         if lib().dare_unet_launch_info(self.h, layer, kind, v) != 0:
             return None
-        keys = ("grid_x", "grid_y", "grid_z", "smem", "planes_per_cta", "taps_per_cta", "tmem_cols", "ctas_per_sm")
+        keys = ("grid_x", "grid_y", "grid_z", "smem", "planes_per_cta", "taps_or_ring", "tmem_cols", "ctas_per_sm")
         return dict(zip(keys, list(v)))
 
     def stats(self) -> dict:

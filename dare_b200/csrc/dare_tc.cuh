@@ -128,6 +128,12 @@ __device__ __forceinline__ void cp4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// An arrive on the mbarrier once every cp.async this thread issued so far has
+// landed (the pending count is raised first, so a regular arrive of the same
+// thread is still needed to count it).
+__device__ __forceinline__ void cp_mbar_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // ---- bf16 packing ------------------------------------------------------------

@@ -52,6 +52,42 @@ constexpr size_t kMaxSmem = 232448;  // 227 KB of opt-in shared memory per CTA
 // zeroed once per kernel (stage_zero), the FP32 values land asynchronously
 // in a raw 4-byte-per-row buffer, and stage_finish (run by the issuing
 // thread after its cp.async wait) writes the bf16 channel-0 values.
+// FP32 channel-0 rows q = first, first + stride, ... of a plane segment into
+// the raw buffer.  The padded coordinates of a row are stepped from the
+// previous one (one division per call, not per row).
+__device__ __forceinline__ void embed_rows(float* raw, const float* __restrict__ in32, const Geom& g, int64_t Q0,
+                                           int rows, int valid_rows, int first, int stride) {
+    const int Jn = g.n1 + 2;
+    int64_t Q = Q0 + first;
+    int I = 0, J = 0, K = 0;
+    bool have = false;
+    for (int q = first; q < rows; q += stride, Q += stride) {
+        if (!have && Q >= 0) {
+            I = (int)(Q / g.plane);
+            const int rem = (int)(Q - (int64_t)I * g.plane);
+            J = rem / g.W;
+            K = rem - J * g.W;
+            have = true;
+        }
+        const bool ok = have && Q < g.total && q < valid_rows && I >= 1 && I <= g.n0 && J >= 1 && J <= g.n1 &&
+                        K >= 1 && K <= g.n2;
+        if (ok)
+            cp4(raw + q, in32 + ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1));
+        else
+            raw[q] = 0.f;
+        if (have) {
+            K += stride;
+            while (K >= g.W) {
+                K -= g.W;
+                if (++J == Jn) {
+                    J = 0;
+                    ++I;
+                }
+            }
+        }
+    }
+}
+
 template <int C, int MODE>
 __device__ __forceinline__ void stage(uint8_t* slot, float* raw, const bf16* __restrict__ in,
                                       const float* __restrict__ in32, const Geom& g, int64_t Q0, int rows, int RP,
@@ -66,22 +102,7 @@ __device__ __forceinline__ void stage(uint8_t* slot, float* raw, const bf16* __r
             cp16(slot + ((size_t)kc * RP + q) * 16, in + (v ? Q : 0) * C + kc * 8, v);
         }
     } else {
-        for (int q = threadIdx.x; q < rows; q += kThreads) {
-            const int64_t Q = Q0 + q;
-            bool ok = false;
-            int64_t ci = 0;
-            if (Q >= 0 && Q < g.total && q < valid_rows) {
-                const int I = (int)(Q / g.plane);
-                const int rem = (int)(Q - (int64_t)I * g.plane);
-                const int J = rem / g.W, K = rem - J * g.W;
-                ok = I >= 1 && I <= g.n0 && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2;
-                ci = ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1);
-            }
-            if (ok)
-                cp4(raw + q, in32 + ci);
-            else
-                raw[q] = 0.f;
-        }
+        embed_rows(raw, in32, g, Q0, rows, valid_rows, threadIdx.x, kThreads);
     }
 }
 
@@ -93,9 +114,37 @@ __device__ __forceinline__ void stage_finish(uint8_t* slot, const float* raw, in
     }
 }
 
-__device__ __forceinline__ void stage_zero(uint8_t* p, uint32_t bytes) {
-    for (uint32_t o = threadIdx.x * 16; o < bytes; o += kThreads * 16)
+__device__ __forceinline__ void stage_zero(uint8_t* p, uint32_t bytes, int nthreads = kThreads) {
+    for (uint32_t o = threadIdx.x * 16; o < bytes; o += nthreads * 16)
         *reinterpret_cast<uint4*>(p + o) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// The same staging done by one warp (lane-strided), for the producer warp of
+// the warp-specialised forward kernel.
+template <int C, int MODE>
+__device__ __forceinline__ void stage_lanes(uint8_t* slot, float* raw, const bf16* __restrict__ in,
+                                            const float* __restrict__ in32, const Geom& g, int64_t Q0, int rows,
+                                            int RP, int lane) {
+    if (MODE == IN_BF16) {
+        constexpr int KC = C / 8;
+        const int nent = rows * KC;
+        for (int idx = lane; idx < nent; idx += 32) {
+            const int q = idx / KC, kc = idx - q * KC;
+            const int64_t Q = Q0 + q;
+            const bool v = Q >= 0 && Q < g.total;
+            cp16(slot + ((size_t)kc * RP + q) * 16, in + (v ? Q : 0) * C + kc * 8, v);
+        }
+    } else {
+        embed_rows(raw, in32, g, Q0, rows, rows, lane, 32);
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ void stage_finish_lanes(uint8_t* slot, const float* raw, int rows, int lane) {
+    if (MODE == IN_EMBED) {
+        for (int q = lane; q < rows; q += 32)
+            *reinterpret_cast<bf16*>(slot + (size_t)q * 16) = __float2bfloat16_rn(raw[q]);
+    }
 }
 
 // raw FP32 staging bytes of one slot (IN_EMBED), 16-byte aligned
@@ -115,21 +164,16 @@ struct FwdArgs {
     float* out32;    // OUT_F32: internal cells, channel 0 (+ res32)
     const float* res32;
     int ppc;
+    int slots;       // ring depth (shared-memory slots of staged planes)
     int* err;
 };
 
+// One output row (a padded position of plane I) from its NT accumulator
+// values: BF16 store, prolongation-add into the eight finer children, or the
+// FP32 output.  Ghost positions and positions past the plane are skipped.
 template <int NT, int OUTM>
-__device__ __forceinline__ void fwd_epilogue(const FwdArgs& a, uint32_t tmem, int buf, int I, int P0, int co0) {
-    fence_after_sync();
-    const int warp = threadIdx.x >> 5;
-    uint32_t r[NT];
-#pragma unroll
-    for (int c = 0; c < NT; c += 16) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * NT + c, &r[c]);
-    tmem_wait_ld();
-#pragma unroll
-    for (int c = 0; c < NT; c++) reg_fence(r[c]);
+__device__ __forceinline__ void fwd_store(const FwdArgs& a, const uint32_t* r, int I, int pp, int co0) {
     const Geom& g = a.g;
-    const int pp = P0 + (int)threadIdx.x;
     if (pp >= g.plane) return;
     const int J = pp / g.W, K = pp - J * g.W;
     if (J < 1 || J > g.n1 || K < 1 || K > g.n2) return;
@@ -146,8 +190,8 @@ __device__ __forceinline__ void fwd_epilogue(const FwdArgs& a, uint32_t tmem, in
         }
     } else if (OUTM == OUT_ADDUP) {
         // nearest-neighbour prolongation of this coarse cell, added into its
-        // eight children on the finer level (the additive skip)
-        // (the eight children's loads of one 8-channel chunk are issued together)
+        // eight children on the finer level (the additive skip); the eight
+        // children's loads of one 8-channel chunk are issued together
         const Geom& f = a.fg;
         const int64_t fplane = (int64_t)(f.n1 + 2) * f.W;
         bf16* base = a.fine + (((int64_t)(2 * I - 1) * (f.n1 + 2) + (2 * J - 1)) * f.W + (2 * K - 1)) * a.cout + co0;
@@ -179,101 +223,207 @@ __device__ __forceinline__ void fwd_epilogue(const FwdArgs& a, uint32_t tmem, in
     }
 }
 
-template <int CIN, int NT, int INM, int OUTM>
-__global__ void __launch_bounds__(kThreads) k_conv_fwd(FwdArgs a) {
+// Bounded mbarrier wait that also gives up when another role has aborted.
+__device__ __forceinline__ bool role_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                          int code) {
+    const uint32_t addr = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitLimit; it++) {
+        if (mbar_try_wait(addr, parity)) return true;
+        if ((it & 63) == 63 && *abort_flag) return false;
+    }
+    *abort_flag = 1;
+    if (err) atomicCAS(err, 0, code);
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Warp-specialised forward convolution.  Warps 0-3 drain the accumulator
+// (each its 32-lane TMEM quarter), warp 4 stages input planes, warp 5 (one
+// lane) issues the MMAs, warp 6 converts FP32 input rows to BF16 (FP32-input
+// layers only).  A CTA owns MT consecutive 128-position tiles of a
+// (j,k) plane and marches along i through planes I0..I1; input planes live in
+// a ring of `slots` shared-memory slots.  Barriers:
+//   full[s]   producer -> MMA   plane in slot s staged (32 producer arrivals,
+//                               each completed by the lane's cp.async copies)
+//   rawf[s]   producer -> converter, the same for the FP32 rows
+//   empty[s]  MMA -> producer   the last MMA reading slot s has completed
+//   accf[b]   MMA -> epilogue   accumulator b holds a finished plane
+//   acce[b]   epilogue -> MMA   accumulator b has been read (128 arrivals)
+// Every wait is bounded; a role that times out raises a shared abort flag
+// the others poll, and the MMA lane waits for its own MMAs before TMEM is
+// released.
+template <int CIN, int NT, int MT, int INM, int OUTM>
+__global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int KC = CIN / 8;
     constexpr uint32_t WB = kTaps * CIN * NT * 2;
-    constexpr uint32_t COLS = 2 * NT < 32 ? 32 : 2 * NT;
+    constexpr uint32_t ACOLS = MT * NT;  // columns of one accumulator buffer
+    constexpr uint32_t COLS = 2 * ACOLS <= 32 ? 32 : (2 * ACOLS <= 64 ? 64 : (2 * ACOLS <= 128 ? 128 : 256));
     const Geom g = a.g;
-    const int tid = threadIdx.x;
-    const int rows = stage_rows(g);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int S = a.slots;
+    const int rows = fwd_rows(g, MT);
     const int RP = row_pitch(rows, CIN);
     const uint32_t SB = (uint32_t)KC * RP * 16;
     const uint32_t RB = INM == IN_EMBED ? raw_bytes(rows) : 0u;
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
-    float* raw = reinterpret_cast<float*>(slots + 4 * SB);
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(slots + 4 * SB + 4 * RB);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+    float* raw = reinterpret_cast<float*>(slots + S * SB);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(slots + S * SB + S * RB);
+    uint64_t* full = bars;            // [kMaxSlots]
+    uint64_t* empty = bars + kMaxSlots;
+    uint64_t* accf = bars + 2 * kMaxSlots;
+    uint64_t* acce = accf + 2;
+    uint64_t* drain = acce + 2;
+    uint64_t* rawf = drain + 1;       // [kMaxSlots] producer -> converter (FP32 input)
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(rawf + kMaxSlots);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
-    const int P0 = blockIdx.x * kTileM;
+    const int P0 = blockIdx.x * (MT * kTileM);
     const int I0 = 1 + blockIdx.y * a.ppc;
     if (I0 > g.n0) return;
     const int I1 = min(g.n0, I0 + a.ppc - 1);
+    const int co0 = blockIdx.z * NT;
 
     if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], 32);
+            mbar_init(&empty[s], 1);
+            mbar_init(&rawf[s], 32);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], kEpiThreads);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
         mbar_fence_init();
     }
-    if (INM == IN_EMBED) stage_zero(slots, 4 * SB);
-    if (tid < 32) tmem_alloc(tslot, COLS);
+    if (INM == IN_EMBED) stage_zero(slots, S * SB, kFwdThreads);
+    if (warp == 0) tmem_alloc(tslot, COLS);
+    {
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(a.w) + (size_t)blockIdx.z * WB;
+        for (uint32_t o = tid * 16; o < WB; o += kFwdThreads * 16) cp16(wsm + o, src + o, true);
+        cp_commit();
+        cp_wait_all();
+    }
+    fence_proxy_async();
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = *tslot;
-
-    {
-        const uint8_t* src = reinterpret_cast<const uint8_t*>(a.w) + (size_t)blockIdx.z * WB;
-        for (uint32_t o = tid * 16; o < WB; o += kThreads * 16) cp16(wsm + o, src + o, true);
-    }
     const int64_t pbase = (int64_t)P0 - g.W - 1;
-    for (int I = I0 - 1; I <= I0 + 1; I++)
-        stage<CIN, INM>(slots + (I & 3) * SB, raw + (I & 3) * (RB / 4), a.in, a.in32, g,
-                        (int64_t)I * g.plane + pbase, rows, RP, rows);
-    cp_commit();
 
-    constexpr uint32_t idesc = idesc_bf16(kTileM, NT, 0, 0);
-    uint32_t phase = 0;
-    bool aborted = false;
-    for (int I = I0; I <= I1; I++) {
-        const int buf = (I - I0) & 1;
+    if (warp == 4) {
+        // ---- producer: planes I0-1 .. I1+1 into the ring; a plane is
+        // published by the completion of the lanes' own copies (BF16 slots)
+        // or handed to the converter warp (FP32 raw rows) ----
+        uint32_t eph = 0xFFu;  // parity of the next wait on empty[s] (fresh slots pass)
+        for (int p = I0 - 1; p <= I1 + 1; p++) {
+            const int sl = p % S;
+            if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 5)) break;
+            eph ^= 1u << sl;
+            stage_lanes<CIN, INM>(slots + sl * SB, raw + sl * (RB / 4), a.in, a.in32, g,
+                                  (int64_t)p * g.plane + pbase, rows, RP, lane);
+            uint64_t* bar = INM == IN_EMBED ? &rawf[sl] : &full[sl];
+            cp_mbar_arrive(bar);
+            mbar_arrive(bar);
+        }
         cp_wait_all();
-        for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1; p++)
-            stage_finish<INM>(slots + (p & 3) * SB, raw + (p & 3) * (RB / 4), rows);
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            fence_after_sync();
-            const uint32_t sl = smem_u32(slots), wa = smem_u32(wsm);
-#pragma unroll 1
-            for (int t = 0; t < kTaps; t++) {
-                const int di = t / 9 - 1, dj = (t / 3) % 3 - 1, dk = t % 3 - 1;
-                const uint32_t ab = sl + ((I + di) & 3) * SB + (uint32_t)((dj + 1) * g.W + (dk + 1)) * 16;
-                const uint32_t bb = wa + (uint32_t)t * KC * NT * 16;
+    } else if (warp == 6) {
+        // ---- converter (FP32 input only): raw FP32 rows -> BF16 channel 0 ----
+        if (INM == IN_EMBED) {
+            uint32_t rph = 0;
+            for (int p = I0 - 1; p <= I1 + 1; p++) {
+                const int sl = p % S;
+                if (!role_wait(&rawf[sl], (rph >> sl) & 1u, abort_flag, a.err, 10)) break;
+                rph ^= 1u << sl;
+                stage_finish_lanes<INM>(slots + sl * SB, raw + sl * (RB / 4), rows, lane);
+                fence_proxy_async();
+                mbar_arrive(&full[sl]);
+            }
+        }
+    } else if (warp == 5) {
+        // ---- MMA issue (one lane) ----
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(kTileM, NT, 0, 0);
+            const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
+            const uint64_t adesc = smem_desc(0, RP * 16, 128), bdesc = smem_desc(0, NT * 16, 128);
+            const uint32_t w16 = (uint32_t)g.W * 16, rp32 = (uint32_t)RP * 32;
+            uint32_t fph = 0, aph = 3u;
+            bool ok = true;
+            for (int I = I0; I <= I1 && ok; I++) {
+                const int buf = (I - I0) & 1;
+                for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1 && ok; p++) {
+                    const int sp = p % S;
+                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 6);
+                    fph ^= 1u << sp;
+                }
+                if (ok) ok = role_wait(&acce[buf], (aph >> buf) & 1u, abort_flag, a.err, 7);
+                aph ^= 1u << buf;
+                if (!ok) break;
+                fence_after_sync();
+                // descriptors = constant high bits | (start address >> 4); the
+                // 27 taps are unrolled so each start address is one add
+                const uint32_t sb[3] = {sl0 + (uint32_t)((I - 1) % S) * SB, sl0 + (uint32_t)(I % S) * SB,
+                                        sl0 + (uint32_t)((I + 1) % S) * SB};
 #pragma unroll
-                for (int s = 0; s < CIN / 16; s++)
-                    mma_bf16(tmem + buf * NT, smem_desc(ab + 2 * s * RP * 16, RP * 16, 128),
-                             smem_desc(bb + 2 * s * NT * 16, NT * 16, 128), idesc, (t | s) ? 1u : 0u);
+                for (int t = 0; t < kTaps; t++) {
+                    const int di = t / 9, dj = (t / 3) % 3, dk = t % 3;
+                    const uint32_t ab = sb[di] + dj * w16 + dk * 16;
+#pragma unroll
+                    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                        for (int s = 0; s < CIN / 16; s++)
+                            mma_bf16(tmem + buf * ACOLS + mt * NT,
+                                     adesc | (((ab + mt * kTileM * 16 + s * rp32) >> 4) & 0x3FFFu),
+                                     bdesc | (((wa + (uint32_t)((t * KC + 2 * s) * NT * 16)) >> 4) & 0x3FFFu), idesc,
+                                     (t | s) ? 1u : 0u);
+                }
+                mma_commit(smem_u32(&accf[buf]));
+                mma_commit(smem_u32(&empty[(I - 1) % S]));  // plane I-1 is not read again
             }
-            mma_commit(smem_u32(&mbar[buf]));
+            // every MMA of this CTA has completed before TMEM is released
+            mma_commit(smem_u32(drain));
+            mbar_wait(drain, 0, a.err, 8);
         }
-        if (I > I0) {
-            const int pb = buf ^ 1;
-            const bool ok = mbar_wait(&mbar[pb], (phase >> pb) & 1u, a.err, 1);
-            phase ^= 1u << pb;
-            if (__syncthreads_or(!ok)) {
-                aborted = true;
-                break;
-            }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warps 0-3, TMEM lanes 32*warp .. 32*warp+31 ----
+        uint32_t fph = 0;
+        for (int I = I0; I <= I1; I++) {
+            const int buf = (I - I0) & 1;
+            if (!role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 9)) break;
+            fph ^= 1u << buf;
+            fence_after_sync();
+            uint32_t r[MT][NT];
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                for (int c = 0; c < NT; c += 16)
+                    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * NT + c, &r[mt][c]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                for (int c = 0; c < NT; c++) reg_fence(r[mt][c]);
+            fence_before_sync();
+            mbar_arrive(&acce[buf]);
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++) fwd_store<NT, OUTM>(a, r[mt], I, P0 + mt * kTileM + tid, co0);
         }
-        if (I + 2 <= I1 + 1)
-            stage<CIN, INM>(slots + ((I + 2) & 3) * SB, raw + ((I + 2) & 3) * (RB / 4), a.in, a.in32, g,
-                            (int64_t)(I + 2) * g.plane + pbase, rows, RP, rows);
-        cp_commit();
-        if (I > I0) fwd_epilogue<NT, OUTM>(a, tmem, buf ^ 1, I - 1, P0, blockIdx.z * NT);
-        fence_before_sync();
     }
-    if (!aborted) {
-        const int lb = (I1 - I0) & 1;
-        const bool ok = mbar_wait(&mbar[lb], (phase >> lb) & 1u, a.err, 2);
-        if (!__syncthreads_or(!ok)) fwd_epilogue<NT, OUTM>(a, tmem, lb, I1, P0, blockIdx.z * NT);
-    }
-    cp_wait_all();
     fence_before_sync();
     __syncthreads();
-    if (tid < 32) {
+    if (warp == 0) {
         fence_after_sync();
         tmem_dealloc(tmem, COLS);
     }
@@ -651,11 +801,17 @@ __global__ void k_warm(int64_t n, const double* __restrict__ diag, const double*
 
 // ---------------------------------------------------------------------------
 // host side: launch configuration and dispatch
-static size_t fwd_smem(int cin, int nt, const Geom& g, bool embed) {
-    const int rows = stage_rows(g);
+static size_t fwd_smem(int cin, int nt, const Geom& g, bool embed, int mt, int slots) {
+    const int rows = fwd_rows(g, mt);
     const int RP = row_pitch(rows, cin);
-    return (size_t)kTaps * cin * nt * 2 + 4 * (size_t)(cin / 8) * RP * 16 + (embed ? 4 * (size_t)raw_bytes(rows) : 0) +
-           32;
+    return (size_t)kTaps * cin * nt * 2 + slots * (size_t)(cin / 8) * RP * 16 +
+           (embed ? slots * (size_t)raw_bytes(rows) : 0) + (3 * kMaxSlots + 5) * 8 + 16;
+}
+
+// two 128-position tiles per step on planes wider than two tiles, when a
+// 4-slot ring of the wider plane segments still fits
+static int pick_mt(const Geom& g, int cin, int nt, bool embed) {
+    return g.plane > 2 * kTileM && fwd_smem(cin, nt, g, embed, 2, 4) <= kMaxSmem ? 2 : 1;
 }
 
 static int dy_pitch_rt(int c) { return kTileM + (c == 16 ? 4 : (c == 32 ? 2 : 1)); }
@@ -673,13 +829,14 @@ static size_t wgr_smem(int cin, int cout, const Geom& g, bool xembed, bool yembe
 }
 
 template <typename K>
-static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int* occ_out) {
+static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int* occ_out,
+                         int threads = kThreads) {
     DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                         (int)cudaSharedmemCarveoutMaxShared));
     int occ = 0;
     for (;;) {
-        DARE_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
+        DARE_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem));
         // CTAs resident on one SM must never ask for more than its 512 TMEM columns
         if (occ * cols <= 512 || smem + 4096 > kMaxSmem) break;
         smem += 4096;
@@ -689,40 +846,50 @@ static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int
     return DARE_OK;
 }
 
-template <int CIN, int NT, int INM, int OUTM>
+template <int CIN, int NT, int MT, int INM, int OUTM>
 static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const FwdArgs& a0) {
-    auto kern = k_conv_fwd<CIN, NT, INM, OUTM>;
+    auto kern = k_conv_fwd<CIN, NT, MT, INM, OUTM>;
     if (!lc.ready) {
-        size_t smem = fwd_smem(CIN, NT, a0.g, INM == IN_EMBED);
+        // the deepest ring (4..8 staged planes) that fits
+        int slots = kMaxSlots;
+        while (slots > 4 && fwd_smem(CIN, NT, a0.g, INM == IN_EMBED, MT, slots) > kMaxSmem) slots--;
+        size_t smem = fwd_smem(CIN, NT, a0.g, INM == IN_EMBED, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
-        const uint32_t cols = 2 * NT < 32 ? 32 : 2 * NT;
+        const uint32_t acols = 2 * MT * NT;
+        const uint32_t cols = acols <= 32 ? 32 : (acols <= 64 ? 64 : (acols <= 128 ? 128 : 256));
         int occ = 0, rc;
-        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ))) return rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, kFwdThreads))) return rc;
         // about four waves of CTAs; a CTA marches at least two planes (it
         // stages two more than it computes)
         const int n0 = a0.g.n0;
+        const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
         const int64_t target = (int64_t)ctx->num_sms * occ * 4;
-        int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + (int64_t)a0.g.tiles * nz - 1) /
-                                                                            ((int64_t)a0.g.tiles * nz)));
+        int chunks = (int)std::min<int64_t>(
+            n0, std::max<int64_t>(1, (target + (int64_t)tiles * nz - 1) / ((int64_t)tiles * nz)));
         int ppc = (n0 + chunks - 1) / chunks;
         ppc = std::max(ppc, std::min(n0, 2));
         lc.ppc = ppc;
         lc.occ = occ;
-        lc.grid = dim3(a0.g.tiles, (n0 + ppc - 1) / ppc, nz);
+        lc.mt = MT;
+        lc.slots = slots;
+        lc.grid = dim3(tiles, (n0 + ppc - 1) / ppc, nz);
         lc.smem = smem;
         lc.cols = cols;
         lc.ready = true;
     }
     FwdArgs a = a0;
     a.ppc = lc.ppc;
-    kern<<<lc.grid, kThreads, lc.smem, ctx->stream>>>(a);
+    a.slots = lc.slots;
+    kern<<<lc.grid, kFwdThreads, lc.smem, ctx->stream>>>(a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
 
 static int launch_fwd(dare_ctx* ctx, LaunchCfg& lc, int cin, int nt, int nz, int inm, int outm, const FwdArgs& a) {
-#define DARE_FWD(CI, N, IM, OM) \
-    if (cin == CI && nt == N && inm == IM && outm == OM) return launch_fwd_t<CI, N, IM, OM>(ctx, lc, nz, a);
+    const int mt = pick_mt(a.g, cin, nt, inm == IN_EMBED);
+#define DARE_FWD(CI, N, IM, OM)                                                                       \
+    if (cin == CI && nt == N && inm == IM && outm == OM)                                              \
+        return mt == 2 ? launch_fwd_t<CI, N, 2, IM, OM>(ctx, lc, nz, a) : launch_fwd_t<CI, N, 1, IM, OM>(ctx, lc, nz, a);
     DARE_FWD(16, 16, IN_EMBED, OUT_STORE)
     DARE_FWD(16, 16, IN_BF16, OUT_STORE)
     DARE_FWD(16, 32, IN_BF16, OUT_STORE)
@@ -789,7 +956,7 @@ static int launch_wgr(dare_ctx* ctx, LaunchCfg& lc, int cin, int cout, int xm, i
 }
 
 static int pick_nt(int cink, int coutk, const Geom& g) {
-    if (coutk % 32 == 0 && fwd_smem(cink, 32, g, false) <= kMaxSmem) return 32;
+    if (coutk % 32 == 0 && fwd_smem(cink, 32, g, false, 1, 4) <= kMaxSmem) return 32;
     return 16;
 }
 
@@ -1058,7 +1225,8 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         const Geom& g = net->geo[L.level];
         L.nt = pick_nt(L.cink, L.coutk, g);
         L.ntb = pick_nt(L.coutk, L.cink, g);
-        if (fwd_smem(L.cink, L.nt, g, l == ENC0) > kMaxSmem || fwd_smem(L.coutk, L.ntb, g, l == DEC0) > kMaxSmem ||
+        if (fwd_smem(L.cink, L.nt, g, l == ENC0, 1, 4) > kMaxSmem ||
+            fwd_smem(L.coutk, L.ntb, g, l == DEC0, 1, 4) > kMaxSmem ||
             wgr_smem(L.cink, L.coutk, g, l == ENC0, l == DEC0) > kMaxSmem) {
             delete net;
             return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_create: grid too wide for the staged convolutions");
@@ -1231,7 +1399,7 @@ int dare_unet_launch_info(const dare_unet* net, int layer, int kind, int64_t inf
     const Layer& L = net->layer[layer];
     const LaunchCfg& c = kind == 0 ? L.fwd : (kind == 1 ? L.bwd : L.wgr);
     if (!c.ready) return DARE_ERR_STATE;
-    const int64_t v[8] = {c.grid.x, c.grid.y, c.grid.z, (int64_t)c.smem, c.ppc, kind == 2 ? c.tpg : kTaps, c.cols,
+    const int64_t v[8] = {c.grid.x, c.grid.y, c.grid.z, (int64_t)c.smem, c.ppc, kind == 2 ? c.tpg : c.slots, c.cols,
                           c.occ};
     for (int i = 0; i < 8; i++) info[i] = v[i];
     return DARE_OK;

@@ -16,6 +16,10 @@ constexpr int kLayers = 8;
 constexpr int kTaps = 27;
 constexpr int kThreads = 128;  // one CTA = 4 warps = the 128 TMEM lanes of an M=128 tile
 constexpr int kTileM = 128;    // output rows (padded positions) per MMA tile
+// warp-specialised forward convolution: 4 epilogue warps + producer + MMA + converter
+constexpr int kEpiThreads = 128;
+constexpr int kFwdThreads = 224;  // + a converter warp for FP32-input layers
+constexpr int kMaxSlots = 8;   // staged-plane ring depth limit
 
 // A level's activations live in a zero-padded, channels-last layout:
 // [(n0+2)][(n1+2)][(n2+2)][C] bf16, ghosts kept at zero, so every 3^3 tap is
@@ -43,6 +47,8 @@ inline Geom make_geom(int n0, int n1, int n2) {
 // The rows of one staged input plane: the 128 outputs plus a one-row and
 // one-cell halo on either side in the flattened (j,k) plane.
 __host__ __device__ inline int stage_rows(const Geom& g) { return kTileM + 2 * g.W + 2; }
+// ... and for MT consecutive tiles
+__host__ __device__ inline int fwd_rows(const Geom& g, int mt) { return mt * kTileM + 2 * g.W + 2; }
 // Row pitch of a staged plane: rounded to 8 rows, then offset so that the
 // 16-byte chunks of one row written by neighbouring threads fall into
 // different shared-memory banks.
@@ -68,6 +74,8 @@ struct LaunchCfg {
     int tpg = 27;  // taps per CTA (weight gradient)
     int cols = 32; // TMEM columns
     int occ = 0;   // resident CTAs per SM
+    int mt = 1;    // 128-position tiles per CTA step (forward)
+    int slots = 4; // staged-plane ring depth (forward)
 };
 
 struct Layer {

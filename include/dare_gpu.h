@@ -356,8 +356,8 @@ DARE_API int dare_unet_stats(const dare_unet* net, int64_t* steps, int64_t* pair
 /* Launch shape of a convolution kernel after its first launch: layer 0..7
  * (enc0..dec0 as above), kind 0 forward, 1 data gradient, 2 weight gradient;
  * info = {grid x, grid y, grid z, dynamic smem bytes, planes per CTA, taps
- * per CTA, TMEM columns, resident CTAs per SM}.  DARE_ERR_STATE before the
- * first launch. */
+ * per CTA (weight gradient) or staged-plane ring depth (the others), TMEM
+ * columns, resident CTAs per SM}.  DARE_ERR_STATE before the first launch. */
 DARE_API int dare_unet_launch_info(const dare_unet* net, int layer, int kind, int64_t info[8]);
 /* Internal activation `which` (0 S0, 1 P1, 2 S1, 3 P2, 4 S2, 5 P3, 6 E3) as
  * FP32 [cell][channel] over the internal cells of its level. */
