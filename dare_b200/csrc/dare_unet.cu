@@ -430,6 +430,408 @@ __global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// One-channel layers.  A tcgen05 MMA costs about the same whatever its N
+// (measured: ~150 cycles for M = 128, K = 16 and any N from 16 to 256), so
+// the 3^3 convolutions with a single input or output channel are re-cast so
+// that each MMA carries several taps:
+//   k_conv_in  (1 -> 16, FP32 input): "window" rows, row q of a staged plane
+//              holding x(q), x(q+1), ..., x(q+7) in BF16.  A K-chunk of 8 then
+//              covers the three dk taps of one (di, dj) (the other five
+//              weights are zero), and the A operand of taps (di, dj) is the
+//              window plane shifted by dj rows of the (j,k) plane: 6 MMAs per
+//              128 outputs instead of 27.
+//   k_conv_out (16 -> 1, FP32 output): the taps in N,
+//              Z[q][t] = sum_ci X[q][ci] W[t][ci] (one MMA per 128 input
+//              rows of a plane), Z staged from TMEM to shared memory, and
+//              every output row gathers its 27 terms, the accumulators of
+//              the three output planes an input plane feeds held in
+//              registers of the row's thread.
+
+struct InArgs {
+    Geom g;
+    const float* in32;  // FP32 vector over the internal cells
+    const bf16* w;      // [3 di][2 pairs][2 chunks][16 co][8]
+    bf16* out;          // [g.total][16]
+    int ppc, slots;
+    int* err;
+};
+
+constexpr int kInThreads = 224;  // 4 epilogue warps, producer, MMA, window builder
+
+__host__ __device__ inline int in_rows(const Geom& g, int mt) { return fwd_rows(g, mt); }
+// raw FP32 rows staged per plane (the windows reach 7 rows further)
+__host__ __device__ inline int in_raw_rows(const Geom& g, int mt) { return fwd_rows(g, mt) + 8; }
+
+// enc0 forward and dec0 data gradient: 1 -> 16 channels.
+template <int MT>
+__global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr uint32_t WB = 3 * 2 * 2 * 16 * 16;
+    constexpr uint32_t ACOLS = MT * 16;
+    constexpr uint32_t COLS = 2 * ACOLS <= 32 ? 32 : 64;
+    const Geom g = a.g;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int S = a.slots;
+    const int rows = in_rows(g, MT);
+    const int rraw = in_raw_rows(g, MT);
+    const uint32_t SB = (uint32_t)((rows + 7) / 8) * 8 * 16;   // window rows x 16 bytes
+    const uint32_t RB = raw_bytes(rraw);
+    uint8_t* wsm = smem;
+    uint8_t* win = smem + WB;                                   // [S][SB]
+    float* raw = reinterpret_cast<float*>(win + S * SB);        // [S][RB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(raw) + S * RB);
+    uint64_t* rawf = bars;
+    uint64_t* full = bars + kMaxSlots;
+    uint64_t* empty = bars + 2 * kMaxSlots;
+    uint64_t* accf = bars + 3 * kMaxSlots;
+    uint64_t* acce = accf + 2;
+    uint64_t* drain = acce + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+
+    const int P0 = blockIdx.x * (MT * kTileM);
+    const int I0 = 1 + blockIdx.y * a.ppc;
+    if (I0 > g.n0) return;
+    const int I1 = min(g.n0, I0 + a.ppc - 1);
+
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(&rawf[s], 32);
+            mbar_init(&full[s], 32);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], kEpiThreads);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        mbar_fence_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, COLS);
+    for (uint32_t o = tid * 16; o < WB; o += kInThreads * 16)
+        cp16(wsm + o, reinterpret_cast<const uint8_t*>(a.w) + o, true);
+    cp_commit();
+    cp_wait_all();
+    fence_proxy_async();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const int64_t pbase = (int64_t)P0 - g.W - 1;
+
+    if (warp == 4) {
+        // ---- producer: FP32 plane segments ----
+        uint32_t eph = 0xFFu;
+        for (int p = I0 - 1; p <= I1 + 1; p++) {
+            const int sl = p % S;
+            if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 11)) break;
+            eph ^= 1u << sl;
+            embed_rows(raw + sl * (RB / 4), a.in32, g, (int64_t)p * g.plane + pbase, rraw, rraw, lane, 32);
+            cp_mbar_arrive(&rawf[sl]);
+            mbar_arrive(&rawf[sl]);
+        }
+        cp_wait_all();
+    } else if (warp == 6) {
+        // ---- window builder: row q = bf16(x(q)), ..., bf16(x(q + 7)) ----
+        uint32_t rph = 0;
+        for (int p = I0 - 1; p <= I1 + 1; p++) {
+            const int sl = p % S;
+            if (!role_wait(&rawf[sl], (rph >> sl) & 1u, abort_flag, a.err, 12)) break;
+            rph ^= 1u << sl;
+            const float* x = raw + sl * (RB / 4);
+            uint8_t* wrow = win + sl * SB;
+            for (int q = lane; q < rows; q += 32)
+                *reinterpret_cast<uint4*>(wrow + (size_t)q * 16) =
+                    make_uint4(pack_bf16(x[q], x[q + 1]), pack_bf16(x[q + 2], x[q + 3]),
+                               pack_bf16(x[q + 4], x[q + 5]), pack_bf16(x[q + 6], x[q + 7]));
+            fence_proxy_async();
+            mbar_arrive(&full[sl]);
+        }
+    } else if (warp == 5) {
+        // ---- MMA: per di, taps (dj 0, dj 1) in one K = 16 MMA, dj 2 in a second ----
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(kTileM, 16, 0, 0);
+            const uint32_t w0 = smem_u32(win), wa = smem_u32(wsm);
+            const uint64_t adesc01 = smem_desc(0, (uint32_t)g.W * 16, 128);  // second chunk: dj + 1
+            const uint64_t adesc2 = smem_desc(0, 0, 128);                     // second chunk: the same rows
+            const uint64_t bdesc = smem_desc(0, 16 * 16, 128);
+            uint32_t fph = 0, eph = 3u;
+            bool ok = true;
+            for (int I = I0; I <= I1 && ok; I++) {
+                const int buf = (I - I0) & 1;
+                for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1 && ok; p++) {
+                    const int sp = p % S;
+                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 13);
+                    fph ^= 1u << sp;
+                }
+                if (ok) ok = role_wait(&acce[buf], (eph >> buf) & 1u, abort_flag, a.err, 14);
+                eph ^= 1u << buf;
+                if (!ok) break;
+                fence_after_sync();
+#pragma unroll
+                for (int di = 0; di < 3; di++) {
+                    const uint32_t pl = w0 + (uint32_t)((I - 1 + di) % S) * SB;
+#pragma unroll
+                    for (int mt = 0; mt < MT; mt++) {
+                        const uint32_t row0 = pl + (uint32_t)(mt * kTileM) * 16;
+                        mma_bf16(tmem + buf * ACOLS + mt * 16, adesc01 | ((row0 >> 4) & 0x3FFFu),
+                                 bdesc | (((wa + (uint32_t)((di * 2 + 0) * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc,
+                                 di ? 1u : 0u);
+                        mma_bf16(tmem + buf * ACOLS + mt * 16,
+                                 adesc2 | (((row0 + (uint32_t)g.W * 32) >> 4) & 0x3FFFu),
+                                 bdesc | (((wa + (uint32_t)((di * 2 + 1) * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc, 1u);
+                    }
+                }
+                mma_commit(smem_u32(&accf[buf]));
+                mma_commit(smem_u32(&empty[(I - 1) % S]));
+            }
+            mma_commit(smem_u32(drain));
+            mbar_wait(drain, 0, a.err, 16);
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: BF16 16-channel rows ----
+        FwdArgs fa{};
+        fa.g = g;
+        fa.cout = 16;
+        fa.out = a.out;
+        uint32_t fph = 0;
+        for (int I = I0; I <= I1; I++) {
+            const int buf = (I - I0) & 1;
+            if (!role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 17)) break;
+            fph ^= 1u << buf;
+            fence_after_sync();
+            uint32_t r[MT][16];
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++)
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * 16, r[mt]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                for (int c = 0; c < 16; c++) reg_fence(r[mt][c]);
+            fence_before_sync();
+            mbar_arrive(&acce[buf]);
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++) fwd_store<16, OUT_STORE>(fa, r[mt], I, P0 + mt * kTileM + tid, 0);
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        tmem_dealloc(tmem, COLS);
+    }
+}
+
+struct OutArgs {
+    Geom g;
+    const bf16* in;     // [g.total][16]
+    const bf16* w;      // [2][32][8]: chunk kc holds input channels 8kc..8kc+7 of each tap
+    float* out32;       // internal cells
+    const float* res32; // added to the output (may be null)
+    int ppc, slots;
+    int* err;
+};
+
+constexpr int kOutThreads = 192;  // 4 gather warps, producer, MMA
+constexpr int kZPitch = 27;       // floats per staged Z row (odd: conflict-free)
+
+// true in every epilogue thread if it is true in any (named barrier 1, the
+// 128 epilogue threads)
+__device__ __forceinline__ bool epi_any(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__host__ __device__ inline int out_mti(const Geom& g, int mt) { return (fwd_rows(g, mt) + kTileM - 1) / kTileM; }
+
+// dec0 forward: 16 -> 1 channel, z = res + conv.
+template <int MT>
+__global__ void __launch_bounds__(kOutThreads) k_conv_out(OutArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr uint32_t WB = 2 * 32 * 16;
+    constexpr int ORows = MT * kTileM;                  // output rows of the tile
+    const Geom g = a.g;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int S = a.slots;
+    const int rows = fwd_rows(g, MT);
+    const int MTI = out_mti(g, MT);                     // input M tiles per plane
+    const int RP = row_pitch(MTI * kTileM, 16);
+    const uint32_t SB = 2u * RP * 16;
+    const uint32_t ZC = (uint32_t)MTI * 32;             // TMEM columns of one plane's Z
+    const uint32_t COLS = ZC <= 32 ? 32 : (ZC <= 64 ? 64 : (ZC <= 128 ? 128 : (ZC <= 256 ? 256 : 512)));
+    uint8_t* wsm = smem;
+    uint8_t* slots = smem + WB;
+    float* zs = reinterpret_cast<float*>(slots + S * SB);  // [MTI * 128][kZPitch]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(zs + (size_t)MTI * kTileM * kZPitch + 2);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + kMaxSlots;
+    uint64_t* zf = bars + 2 * kMaxSlots;
+    uint64_t* ze = zf + 1;
+    uint64_t* drain = ze + 1;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+
+    const int P0 = blockIdx.x * ORows;
+    const int I0 = 1 + blockIdx.y * a.ppc;
+    if (I0 > g.n0) return;
+    const int I1 = min(g.n0, I0 + a.ppc - 1);
+
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], 32);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(zf, 1);
+        mbar_init(ze, kEpiThreads);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        mbar_fence_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, COLS);
+    for (uint32_t o = tid * 16; o < WB; o += kOutThreads * 16)
+        cp16(wsm + o, reinterpret_cast<const uint8_t*>(a.w) + o, true);
+    cp_commit();
+    cp_wait_all();
+    fence_proxy_async();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *tslot;
+    const int64_t pbase = (int64_t)P0 - g.W - 1;
+
+    if (warp == 4) {
+        // ---- producer: input planes I0-1 .. I1+1, MTI * 128 rows (zero past `rows`) ----
+        uint32_t eph = 0xFFu;
+        for (int p = I0 - 1; p <= I1 + 1; p++) {
+            const int sl = p % S;
+            if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 21)) break;
+            eph ^= 1u << sl;
+            const int64_t Q0 = (int64_t)p * g.plane + pbase;
+            for (int idx = lane; idx < MTI * kTileM * 2; idx += 32) {
+                const int q = idx >> 1, kc = idx & 1;
+                const int64_t Q = Q0 + q;
+                const bool v = q < rows && Q >= 0 && Q < g.total;
+                cp16(slots + sl * SB + ((size_t)kc * RP + q) * 16, a.in + (v ? Q : 0) * 16 + kc * 8, v);
+            }
+            cp_mbar_arrive(&full[sl]);
+            mbar_arrive(&full[sl]);
+        }
+        cp_wait_all();
+    } else if (warp == 5) {
+        // ---- MMA: Z of each input plane, MTI tiles of 128 rows x 32 taps ----
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(kTileM, 32, 0, 0);
+            const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
+            const uint64_t adesc = smem_desc(0, RP * 16, 128);
+            const uint64_t bd = smem_desc(wa, 32 * 16, 128);
+            uint32_t fph = 0, eph = 1u;
+            for (int p = I0 - 1; p <= I1 + 1; p++) {
+                const int sp = p % S;
+                if (!role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 22)) break;
+                fph ^= 1u << sp;
+                if (!role_wait(ze, eph, abort_flag, a.err, 23)) break;
+                eph ^= 1u;
+                fence_after_sync();
+                for (int mi = 0; mi < MTI; mi++)
+                    mma_bf16(tmem + mi * 32, adesc | (((sl0 + sp * SB + (uint32_t)mi * kTileM * 16) >> 4) & 0x3FFFu),
+                             bd, idesc, 0u);
+                mma_commit(smem_u32(zf));
+                mma_commit(smem_u32(&empty[sp]));  // each input plane is read once
+            }
+            mma_commit(smem_u32(drain));
+            mbar_wait(drain, 0, a.err, 24);
+        }
+        __syncwarp();
+    } else {
+        // ---- Z to shared memory, then every output row gathers its terms ----
+        // this thread's rows r = tid + 128 m of the output planes J - 1, J, J + 1
+        float am1[MT], a0[MT], ap1[MT];
+#pragma unroll
+        for (int m = 0; m < MT; m++) am1[m] = a0[m] = ap1[m] = 0.f;
+        uint32_t fph = 0;
+        for (int J = I0 - 1; J <= I1 + 1; J++) {
+            const bool ok = role_wait(zf, fph, abort_flag, a.err, 25);
+            if (epi_any(!ok)) break;  // the four warps leave together
+            fph ^= 1u;
+            fence_after_sync();
+            for (int mi = 0; mi < MTI; mi++) {
+                uint32_t z[32];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + mi * 32, z);
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + mi * 32 + 16, z + 16);
+                tmem_wait_ld();
+                float* zr = zs + (size_t)(mi * kTileM + tid) * kZPitch;
+#pragma unroll
+                for (int t = 0; t < kTaps; t++) {
+                    reg_fence(z[t]);
+                    zr[t] = __uint_as_float(z[t]);
+                }
+            }
+            fence_before_sync();
+            mbar_arrive(ze);
+            epi_sync();
+            // out[p] of plane J - di += Z[p + W + 1 + dj W + dk][t]  (rows of the segment)
+#pragma unroll
+            for (int m = 0; m < MT; m++) {
+                const int r = tid + m * kTileM;
+                float sum[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int dj = 0; dj < 3; dj++)
+#pragma unroll
+                    for (int dk = 0; dk < 3; dk++) {
+                        const float* zr = zs + (size_t)(r + dj * g.W + dk) * kZPitch + dj * 3 + dk;
+#pragma unroll
+                        for (int di = 0; di < 3; di++) sum[di] += zr[di * 9];
+                    }
+                // input plane J feeds output plane J - (di - 1)
+                ap1[m] += sum[0];
+                a0[m] += sum[1];
+                am1[m] += sum[2];
+            }
+            epi_sync();  // Z rows are overwritten by the next plane
+            // output plane J-1 has all its contributions (input planes J-2, J-1, J)
+            const int op = J - 1;
+            if (op >= I0 && op <= I1) {
+#pragma unroll
+                for (int m = 0; m < MT; m++) {
+                    const int pp = P0 + tid + m * kTileM;
+                    if (pp < g.plane) {
+                        const int Jr = pp / g.W, Kc = pp - Jr * g.W;
+                        if (Jr >= 1 && Jr <= g.n1 && Kc >= 1 && Kc <= g.n2) {
+                            const int64_t c = ((int64_t)(op - 1) * g.n1 + (Jr - 1)) * g.n2 + (Kc - 1);
+                            a.out32[c] = (a.res32 ? a.res32[c] : 0.f) + am1[m];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < MT; m++) {
+                am1[m] = a0[m];
+                a0[m] = ap1[m];
+                ap1[m] = 0.f;
+            }
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        tmem_dealloc(tmem, COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // weight gradient
 struct WgrArgs {
     Geom g;
@@ -742,6 +1144,32 @@ __global__ void k_pack(const float* __restrict__ W, int cin, int cout, int CINK,
     }
 }
 
+// One-channel-input weights for the window layout of k_conv_in:
+// out[di][pair][chunk][n][e] = W(t, n) with dj = 2 pair + chunk, dk = e,
+// t = 9 di + 3 dj + dk when dj < 3 and dk < 3, else 0; W(t, n) = W[t][n][0]
+// (enc0, cout 16, cin 1) or, flipped for the dec0 data gradient,
+// W[26 - t][0][n] (cout 1, cin 16).
+__global__ void k_pack_tapk(const float* __restrict__ W, int flip, bf16* __restrict__ out) {
+    for (int idx = threadIdx.x; idx < 3 * 2 * 2 * 16 * 8; idx += blockDim.x) {
+        const int e = idx & 7, n = (idx >> 3) & 15, chunk = (idx >> 7) & 1, pair = (idx >> 8) & 1, di = idx >> 9;
+        const int dj = 2 * pair + chunk, dk = e;
+        float v = 0.f;
+        if (dj < 3 && dk < 3) {
+            const int t = di * 9 + dj * 3 + dk;
+            v = flip ? W[(kTaps - 1 - t) * 16 + n] : W[t * 16 + n];
+        }
+        out[idx] = __float2bfloat16_rn(v);
+    }
+}
+
+// dec0 forward weights, taps along N: out[kc][t][e] = W[t][0][8 kc + e], t < 27.
+__global__ void k_pack_tapn(const float* __restrict__ W, bf16* __restrict__ out) {
+    for (int idx = threadIdx.x; idx < 2 * 32 * 8; idx += blockDim.x) {
+        const int e = idx & 7, t = (idx >> 3) & 31, kc = idx >> 8;
+        out[idx] = __float2bfloat16_rn(t < kTaps ? W[t * 16 + kc * 8 + e] : 0.f);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // pair generation: r = b - A x_k (FP32), e = diag_C (x* - x_k) (FP32),
 // acc += ||e||^2 (FP64, atomically)
@@ -955,6 +1383,106 @@ static int launch_wgr(dare_ctx* ctx, LaunchCfg& lc, int cin, int cout, int xm, i
     return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: no weight-gradient kernel for this shape");
 }
 
+static size_t in_smem(const Geom& g, int mt, int slots) {
+    const size_t sb = (size_t)((in_rows(g, mt) + 7) / 8) * 8 * 16;
+    return 3 * 2 * 2 * 16 * 16 + slots * sb + slots * (size_t)raw_bytes(in_raw_rows(g, mt)) +
+           (3 * kMaxSlots + 5) * 8 + 16;
+}
+
+static int in_tiles_mt(const Geom& g) { return g.plane > 2 * kTileM ? 2 : 1; }
+
+template <int MT>
+static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a0) {
+    auto kern = k_conv_in<MT>;
+    if (!lc.ready) {
+        int slots = kMaxSlots;
+        while (slots > 4 && in_smem(a0.g, MT, slots) > kMaxSmem) slots--;
+        size_t smem = in_smem(a0.g, MT, slots);
+        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
+        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
+        int occ = 0, rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, kInThreads))) return rc;
+        // (the launch checks above keep the ring at >= 4 planes: 3 in use + 1 loading)
+        const int n0 = a0.g.n0;
+        const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
+        const int64_t target = (int64_t)ctx->num_sms * occ * 4;
+        const int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + tiles - 1) / tiles));
+        const int ppc = std::max((n0 + chunks - 1) / chunks, std::min(n0, 2));
+        lc.ppc = ppc;
+        lc.occ = occ;
+        lc.mt = MT;
+        lc.slots = slots;
+        lc.grid = dim3(tiles, (n0 + ppc - 1) / ppc, 1);
+        lc.smem = smem;
+        lc.cols = cols;
+        lc.ready = true;
+    }
+    InArgs a = a0;
+    a.ppc = lc.ppc;
+    a.slots = lc.slots;
+    kern<<<lc.grid, kInThreads, lc.smem, ctx->stream>>>(a);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a) {
+    return in_tiles_mt(a.g) == 2 ? launch_in_t<2>(ctx, lc, a) : launch_in_t<1>(ctx, lc, a);
+}
+
+static size_t out_smem(const Geom& g, int mt, int slots) {
+    const int mti = out_mti(g, mt);
+    const int RP = row_pitch(mti * kTileM, 16);
+    return 2 * 32 * 16 + slots * (size_t)2 * RP * 16 + ((size_t)mti * kTileM * kZPitch + 2) * 4 +
+           (2 * kMaxSlots + 3) * 8 + 16;
+}
+
+// two output tiles per CTA step when the plane is wide and one plane's Z
+// (32 TMEM columns per 128 input rows) stays within 256 columns
+static int out_tiles_mt(const Geom& g) {
+    if (g.plane > 2 * kTileM && out_mti(g, 2) * 32 <= 256) return 2;
+    return 1;
+}
+
+template <int MT>
+static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
+    auto kern = k_conv_out<MT>;
+    if (!lc.ready) {
+        if (out_mti(a0.g, MT) * 32 > 512)
+            return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the one-channel output conv");
+        int slots = kMaxSlots;
+        while (slots > 2 && out_smem(a0.g, MT, slots) > kMaxSmem) slots--;
+        size_t smem = out_smem(a0.g, MT, slots);
+        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
+        const uint32_t zc = (uint32_t)out_mti(a0.g, MT) * 32;
+        const uint32_t cols = zc <= 32 ? 32 : (zc <= 64 ? 64 : (zc <= 128 ? 128 : (zc <= 256 ? 256 : 512)));
+        int occ = 0, rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, kOutThreads))) return rc;
+        const int n0 = a0.g.n0;
+        const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
+        const int64_t target = (int64_t)ctx->num_sms * occ * 4;
+        const int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + tiles - 1) / tiles));
+        const int ppc = std::max((n0 + chunks - 1) / chunks, std::min(n0, 2));
+        lc.ppc = ppc;
+        lc.occ = occ;
+        lc.mt = MT;
+        lc.slots = slots;
+        lc.grid = dim3(tiles, (n0 + ppc - 1) / ppc, 1);
+        lc.smem = smem;
+        lc.cols = cols;
+        lc.ready = true;
+    }
+    OutArgs a = a0;
+    a.ppc = lc.ppc;
+    a.slots = lc.slots;
+    kern<<<lc.grid, kOutThreads, lc.smem, ctx->stream>>>(a);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+static int launch_out(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a) {
+    return out_tiles_mt(a.g) == 2 ? launch_out_t<2>(ctx, lc, a) : launch_out_t<1>(ctx, lc, a);
+}
+
 static int pick_nt(int cink, int coutk, const Geom& g) {
     if (coutk % 32 == 0 && fwd_smem(cink, 32, g, false, 1, 4) <= kMaxSmem) return 32;
     return 16;
@@ -966,6 +1494,25 @@ static inline int eblocks(const dare_ctx* ctx, int64_t work) { return grid_block
 static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32, int outm, bf16* out, bf16* fine,
                         float* out32, const float* res32) {
     Layer& L = net->layer[l];
+    if (l == ENC0) {
+        InArgs a{};
+        a.g = net->geo[0];
+        a.in32 = in32;
+        a.w = L.wf;
+        a.out = out;
+        a.err = net->err;
+        return launch_in(net->ctx, L.fwd, a);
+    }
+    if (l == DEC0) {
+        OutArgs a{};
+        a.g = net->geo[0];
+        a.in = in;
+        a.w = L.wf;
+        a.out32 = out32;
+        a.res32 = res32;
+        a.err = net->err;
+        return launch_out(net->ctx, L.fwd, a);
+    }
     FwdArgs a{};
     a.g = net->geo[L.level];
     if (L.level > 0) a.fg = net->geo[L.level - 1];
@@ -984,6 +1531,15 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
 // data gradient of layer l: dX = conv(dY, W flipped and transposed)
 static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, bf16* dx) {
     Layer& L = net->layer[l];
+    if (l == DEC0) {
+        InArgs a{};
+        a.g = net->geo[0];
+        a.in32 = dy32;
+        a.w = L.wb;
+        a.out = dx;
+        a.err = net->err;
+        return launch_in(net->ctx, L.bwd, a);
+    }
     FwdArgs a{};
     a.g = net->geo[L.level];
     a.in = dy;
@@ -1090,7 +1646,13 @@ static int backward(dare_unet* net, const float* u, const float* g, float scale)
 
 static int pack_weights(dare_unet* net) {
     dare_ctx* ctx = net->ctx;
-    for (int l = 0; l < kLayers; l++) {
+    k_pack_tapk<<<1, 256, 0, ctx->stream>>>(net->w + net->layer[ENC0].woff, 0, net->layer[ENC0].wf);
+    DARE_LAUNCHED(ctx);
+    k_pack_tapn<<<1, 256, 0, ctx->stream>>>(net->w + net->layer[DEC0].woff, net->layer[DEC0].wf);
+    DARE_LAUNCHED(ctx);
+    k_pack_tapk<<<1, 256, 0, ctx->stream>>>(net->w + net->layer[DEC0].woff, 1, net->layer[DEC0].wb);
+    DARE_LAUNCHED(ctx);
+    for (int l = ENC1; l <= DEC1; l++) {
         Layer& L = net->layer[l];
         const int nz = L.coutk / L.nt;
         k_pack<<<eblocks(ctx, (int64_t)nz * kTaps * L.cink * L.nt), 256, 0, ctx->stream>>>(
@@ -1225,9 +1787,13 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         const Geom& g = net->geo[L.level];
         L.nt = pick_nt(L.cink, L.coutk, g);
         L.ntb = pick_nt(L.coutk, L.cink, g);
-        if (fwd_smem(L.cink, L.nt, g, l == ENC0, 1, 4) > kMaxSmem ||
-            fwd_smem(L.coutk, L.ntb, g, l == DEC0, 1, 4) > kMaxSmem ||
-            wgr_smem(L.cink, L.coutk, g, l == ENC0, l == DEC0) > kMaxSmem) {
+        const bool fits_fwd = l == ENC0   ? in_smem(g, 1, 4) <= kMaxSmem
+                              : l == DEC0 ? out_smem(g, 1, 2) <= kMaxSmem && out_mti(g, 1) * 32 <= 512
+                                          : fwd_smem(L.cink, L.nt, g, false, 1, 4) <= kMaxSmem;
+        const bool fits_bwd = l == ENC0   ? true
+                              : l == DEC0 ? in_smem(g, 1, 4) <= kMaxSmem
+                                          : fwd_smem(L.coutk, L.ntb, g, false, 1, 4) <= kMaxSmem;
+        if (!fits_fwd || !fits_bwd || wgr_smem(L.cink, L.coutk, g, l == ENC0, l == DEC0) > kMaxSmem) {
             delete net;
             return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_create: grid too wide for the staged convolutions");
         }
