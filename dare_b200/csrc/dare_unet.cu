@@ -23,6 +23,9 @@
 // CTA accumulates its planes in TMEM and writes one partial per CTA, summed
 // in a fixed order afterwards (deterministic).  Data gradients are forward
 // convolutions with flipped, transposed weights.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -246,22 +249,24 @@ __device__ __forceinline__ void cp_wait_group() {
 }
 
 // Warp-specialised forward convolution.  Warps 0-3 drain the accumulator
-// (each its 32-lane TMEM quarter), warp 4 stages input planes, warp 5 (one
-// lane) issues the MMAs, warp 6 converts FP32 input rows to BF16 (FP32-input
-// layers only).  A CTA owns MT consecutive 128-position tiles of a
-// (j,k) plane and marches along i through planes I0..I1; input planes live in
-// a ring of `slots` shared-memory slots.  Barriers:
-//   full[s]   producer -> MMA   plane in slot s staged (32 producer arrivals,
-//                               each completed by the lane's cp.async copies)
-//   rawf[s]   producer -> converter, the same for the FP32 rows
-//   empty[s]  MMA -> producer   the last MMA reading slot s has completed
-//   accf[b]   MMA -> epilogue   accumulator b holds a finished plane
+// (each its 32-lane TMEM quarter), one lane of warp 4 stages input planes with
+// TMA, one lane of each of warps 5 .. 5+MT-1 issues the MMAs of one M tile
+// (a single issuing thread cannot keep the tensor pipe busy with these short
+// MMAs; separate issuers with separate accumulators can).  A CTA owns MT consecutive
+// 128-position tiles of a (j,k) plane and marches along i through planes
+// I0..I1; input planes live in a ring of `slots` shared-memory slots, each
+// CIN/8 chunk planes of RP rows x 16 bytes, filled by CIN/8 x RP/32 TMA boxes
+// of 8 channels x 32 positions (rows outside the array read zero).
+// Barriers:
+//   full[s]   producer -> MMA   expect_tx + the boxes' bytes of slot s
+//   empty[s]  MMA -> producer   the last MMAs reading slot s have completed (MT commits)
+//   accf[b]   MMA -> epilogue   accumulator b holds a finished plane (MT commits)
 //   acce[b]   epilogue -> MMA   accumulator b has been read (128 arrivals)
 // Every wait is bounded; a role that times out raises a shared abort flag
 // the others poll, and the MMA lane waits for its own MMAs before TMEM is
 // released.
-template <int CIN, int NT, int MT, int INM, int OUTM>
-__global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
+template <int CIN, int NT, int MT, int OUTM>
+__global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_constant__ CUtensorMap tmap, FwdArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int KC = CIN / 8;
     constexpr uint32_t WB = kTaps * CIN * NT * 2;
@@ -271,20 +276,18 @@ __global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
     const int rows = fwd_rows(g, MT);
-    const int RP = row_pitch(rows, CIN);
+    const int NTL = box_count(rows), BR = box_height(rows);  // TMA boxes per chunk plane, rows per box
+    const int RP = NTL * BR;
     const uint32_t SB = (uint32_t)KC * RP * 16;
-    const uint32_t RB = INM == IN_EMBED ? raw_bytes(rows) : 0u;
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
-    float* raw = reinterpret_cast<float*>(slots + S * SB);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(slots + S * SB + S * RB);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(slots + S * SB);
     uint64_t* full = bars;            // [kMaxSlots]
     uint64_t* empty = bars + kMaxSlots;
     uint64_t* accf = bars + 2 * kMaxSlots;
     uint64_t* acce = accf + 2;
     uint64_t* drain = acce + 2;
-    uint64_t* rawf = drain + 1;       // [kMaxSlots] producer -> converter (FP32 input)
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(rawf + kMaxSlots);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
     const int P0 = blockIdx.x * (MT * kTileM);
@@ -295,23 +298,21 @@ __global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
 
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], 32);
-            mbar_init(&empty[s], 1);
-            mbar_init(&rawf[s], 32);
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], MT);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(&accf[b], 1);
+            mbar_init(&accf[b], MT);
             mbar_init(&acce[b], kEpiThreads);
         }
-        mbar_init(drain, 1);
+        mbar_init(drain, MT);
         *abort_flag = 0;
         mbar_fence_init();
     }
-    if (INM == IN_EMBED) stage_zero(slots, S * SB, kFwdThreads);
     if (warp == 0) tmem_alloc(tslot, COLS);
     {
         const uint8_t* src = reinterpret_cast<const uint8_t*>(a.w) + (size_t)blockIdx.z * WB;
-        for (uint32_t o = tid * 16; o < WB; o += kFwdThreads * 16) cp16(wsm + o, src + o, true);
+        for (uint32_t o = tid * 16; o < WB; o += fwd_threads(MT) * 16) cp16(wsm + o, src + o, true);
         cp_commit();
         cp_wait_all();
     }
@@ -320,39 +321,29 @@ __global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = *tslot;
-    const int64_t pbase = (int64_t)P0 - g.W - 1;
+    const int pbase = P0 - g.W - 1;
 
     if (warp == 4) {
-        // ---- producer: planes I0-1 .. I1+1 into the ring; a plane is
-        // published by the completion of the lanes' own copies (BF16 slots)
-        // or handed to the converter warp (FP32 raw rows) ----
-        uint32_t eph = 0xFFu;  // parity of the next wait on empty[s] (fresh slots pass)
-        for (int p = I0 - 1; p <= I1 + 1; p++) {
-            const int sl = p % S;
-            if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 5)) break;
-            eph ^= 1u << sl;
-            stage_lanes<CIN, INM>(slots + sl * SB, raw + sl * (RB / 4), a.in, a.in32, g,
-                                  (int64_t)p * g.plane + pbase, rows, RP, lane);
-            uint64_t* bar = INM == IN_EMBED ? &rawf[sl] : &full[sl];
-            cp_mbar_arrive(bar);
-            mbar_arrive(bar);
-        }
-        cp_wait_all();
-    } else if (warp == 6) {
-        // ---- converter (FP32 input only): raw FP32 rows -> BF16 channel 0 ----
-        if (INM == IN_EMBED) {
-            uint32_t rph = 0;
+        // ---- producer: planes I0-1 .. I1+1 into the ring by TMA ----
+        if (lane == 0) {
+            const uint32_t bytes = (uint32_t)KC * NTL * BR * 16;
+            uint32_t eph = 0xFFu;  // parity of the next wait on empty[s] (fresh slots pass)
             for (int p = I0 - 1; p <= I1 + 1; p++) {
                 const int sl = p % S;
-                if (!role_wait(&rawf[sl], (rph >> sl) & 1u, abort_flag, a.err, 10)) break;
-                rph ^= 1u << sl;
-                stage_finish_lanes<INM>(slots + sl * SB, raw + sl * (RB / 4), rows, lane);
-                fence_proxy_async();
-                mbar_arrive(&full[sl]);
+                if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 5)) break;
+                eph ^= 1u << sl;
+                mbar_arrive_expect_tx(&full[sl], bytes);
+                const int y0 = p * g.plane + pbase;
+                for (int kc = 0; kc < KC; kc++)
+                    for (int rt = 0; rt < NTL; rt++)
+                        tma_load_2d(slots + sl * SB + ((size_t)kc * RP + rt * BR) * 16, &tmap, kc * 8, y0 + rt * BR,
+                                    &full[sl]);
             }
         }
-    } else if (warp == 5) {
-        // ---- MMA issue (one lane) ----
+        __syncwarp();
+    } else if (warp >= 5) {
+        // ---- MMA issue: lane 0 of warp 5 + mt, M tile mt ----
+        const int mt = warp - 5;
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16(kTileM, NT, 0, 0);
             const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
@@ -378,20 +369,17 @@ __global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
 #pragma unroll
                 for (int t = 0; t < kTaps; t++) {
                     const int di = t / 9, dj = (t / 3) % 3, dk = t % 3;
-                    const uint32_t ab = sb[di] + dj * w16 + dk * 16;
+                    const uint32_t ab = sb[di] + dj * w16 + dk * 16 + (uint32_t)(mt * kTileM) * 16;
 #pragma unroll
-                    for (int mt = 0; mt < MT; mt++)
-#pragma unroll
-                        for (int s = 0; s < CIN / 16; s++)
-                            mma_bf16(tmem + buf * ACOLS + mt * NT,
-                                     adesc | (((ab + mt * kTileM * 16 + s * rp32) >> 4) & 0x3FFFu),
-                                     bdesc | (((wa + (uint32_t)((t * KC + 2 * s) * NT * 16)) >> 4) & 0x3FFFu), idesc,
-                                     (t | s) ? 1u : 0u);
+                    for (int s = 0; s < CIN / 16; s++)
+                        mma_bf16(tmem + buf * ACOLS + mt * NT, adesc | (((ab + s * rp32) >> 4) & 0x3FFFu),
+                                 bdesc | (((wa + (uint32_t)((t * KC + 2 * s) * NT * 16)) >> 4) & 0x3FFFu), idesc,
+                                 (t | s) ? 1u : 0u);
                 }
                 mma_commit(smem_u32(&accf[buf]));
                 mma_commit(smem_u32(&empty[(I - 1) % S]));  // plane I-1 is not read again
             }
-            // every MMA of this CTA has completed before TMEM is released
+            // every MMA of this CTA (all issuers) has completed before TMEM is released
             mma_commit(smem_u32(drain));
             mbar_wait(drain, 0, a.err, 8);
         }
@@ -449,22 +437,26 @@ __global__ void __launch_bounds__(kFwdThreads) k_conv_fwd(FwdArgs a) {
 
 struct InArgs {
     Geom g;
-    const float* in32;  // FP32 vector over the internal cells
+    const bf16* xpad;   // the input as BF16 over the padded cells (ghosts zero), g.total (+ slack) elements
     const bf16* w;      // [3 di][2 pairs][2 chunks][16 co][8]
     bf16* out;          // [g.total][16]
     int ppc, slots;
     int* err;
 };
 
-constexpr int kInThreads = 224;  // 4 epilogue warps, producer, MMA, window builder
+// 4 epilogue warps, one MMA warp per M tile, 2 window-builder warps, 1 producer warp
+__host__ __device__ constexpr int in_threads(int mt) { return (4 + mt + 2 + 1) * 32; }
+constexpr int kInBuilders = 64;
+constexpr int kPadSlack = 1024;  // elements past the padded input that a segment copy may read
 
 __host__ __device__ inline int in_rows(const Geom& g, int mt) { return fwd_rows(g, mt); }
-// raw FP32 rows staged per plane (the windows reach 7 rows further)
-__host__ __device__ inline int in_raw_rows(const Geom& g, int mt) { return fwd_rows(g, mt) + 8; }
+// BF16 elements staged per plane: the windows reach 7 rows further, the copy
+// starts up to 7 elements early (16-byte alignment) and is a multiple of 8
+__host__ __device__ inline int in_raw_elems(const Geom& g, int mt) { return (fwd_rows(g, mt) + 8 + 7 + 7) / 8 * 8; }
 
 // enc0 forward and dec0 data gradient: 1 -> 16 channels.
 template <int MT>
-__global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
+__global__ void __launch_bounds__(in_threads(MT)) k_conv_in(InArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr uint32_t WB = 3 * 2 * 2 * 16 * 16;
     constexpr uint32_t ACOLS = MT * 16;
@@ -473,12 +465,12 @@ __global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
     const int rows = in_rows(g, MT);
-    const int rraw = in_raw_rows(g, MT);
+    const int relems = in_raw_elems(g, MT);
     const uint32_t SB = (uint32_t)((rows + 7) / 8) * 8 * 16;   // window rows x 16 bytes
-    const uint32_t RB = raw_bytes(rraw);
+    const uint32_t RB = (uint32_t)relems * 2;
     uint8_t* wsm = smem;
     uint8_t* win = smem + WB;                                   // [S][SB]
-    float* raw = reinterpret_cast<float*>(win + S * SB);        // [S][RB]
+    bf16* raw = reinterpret_cast<bf16*>(win + S * SB);          // [S][relems]
     uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(raw) + S * RB);
     uint64_t* rawf = bars;
     uint64_t* full = bars + kMaxSlots;
@@ -496,20 +488,20 @@ __global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
 
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
-            mbar_init(&rawf[s], 32);
-            mbar_init(&full[s], 32);
-            mbar_init(&empty[s], 1);
+            mbar_init(&rawf[s], 1);
+            mbar_init(&full[s], kInBuilders);
+            mbar_init(&empty[s], MT);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(&accf[b], 1);
+            mbar_init(&accf[b], MT);
             mbar_init(&acce[b], kEpiThreads);
         }
-        mbar_init(drain, 1);
+        mbar_init(drain, MT);
         *abort_flag = 0;
         mbar_fence_init();
     }
     if (warp == 0) tmem_alloc(tslot, COLS);
-    for (uint32_t o = tid * 16; o < WB; o += kInThreads * 16)
+    for (uint32_t o = tid * 16; o < WB; o += in_threads(MT) * 16)
         cp16(wsm + o, reinterpret_cast<const uint8_t*>(a.w) + o, true);
     cp_commit();
     cp_wait_all();
@@ -520,36 +512,50 @@ __global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
     const uint32_t tmem = *tslot;
     const int64_t pbase = (int64_t)P0 - g.W - 1;
 
-    if (warp == 4) {
-        // ---- producer: FP32 plane segments ----
+    if (warp == 4 + MT + 2) {
+        // ---- producer: one bulk copy of each plane segment of the padded BF16
+        // input (all-ghost planes 0 and n0+1 are zero-filled instead) ----
         uint32_t eph = 0xFFu;
         for (int p = I0 - 1; p <= I1 + 1; p++) {
             const int sl = p % S;
             if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 11)) break;
             eph ^= 1u << sl;
-            embed_rows(raw + sl * (RB / 4), a.in32, g, (int64_t)p * g.plane + pbase, rraw, rraw, lane, 32);
-            cp_mbar_arrive(&rawf[sl]);
-            mbar_arrive(&rawf[sl]);
+            bf16* dst = raw + (size_t)sl * relems;
+            if (p == 0 || p == g.n0 + 1) {
+                for (int i = lane; i < relems / 8; i += 32)
+                    reinterpret_cast<uint4*>(dst)[i] = make_uint4(0u, 0u, 0u, 0u);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&rawf[sl]);
+            } else if (lane == 0) {
+                const int64_t Q0 = (int64_t)p * g.plane + pbase;  // > 0 for 1 <= p <= n0
+                const int64_t Qa = Q0 & ~(int64_t)7;
+                mbar_arrive_expect_tx(&rawf[sl], RB);
+                bulk_load(dst, a.xpad + Qa, RB, &rawf[sl]);
+            }
+            __syncwarp();
         }
-        cp_wait_all();
-    } else if (warp == 6) {
-        // ---- window builder: row q = bf16(x(q)), ..., bf16(x(q + 7)) ----
+    } else if (warp >= 4 + MT) {
+        // ---- window builders (2 warps): row q = x(q), ..., x(q + 7) ----
+        const int bt = tid - (4 + MT) * 32;
         uint32_t rph = 0;
         for (int p = I0 - 1; p <= I1 + 1; p++) {
             const int sl = p % S;
             if (!role_wait(&rawf[sl], (rph >> sl) & 1u, abort_flag, a.err, 12)) break;
             rph ^= 1u << sl;
-            const float* x = raw + sl * (RB / 4);
+            const int shift = (p == 0 || p == g.n0 + 1) ? 0 : (int)((((int64_t)p * g.plane + pbase)) & 7);
+            const uint16_t* x = reinterpret_cast<const uint16_t*>(raw + (size_t)sl * relems) + shift;
             uint8_t* wrow = win + sl * SB;
-            for (int q = lane; q < rows; q += 32)
+            for (int q = bt; q < rows; q += kInBuilders)
                 *reinterpret_cast<uint4*>(wrow + (size_t)q * 16) =
-                    make_uint4(pack_bf16(x[q], x[q + 1]), pack_bf16(x[q + 2], x[q + 3]),
-                               pack_bf16(x[q + 4], x[q + 5]), pack_bf16(x[q + 6], x[q + 7]));
+                    make_uint4(x[q] | ((uint32_t)x[q + 1] << 16), x[q + 2] | ((uint32_t)x[q + 3] << 16),
+                               x[q + 4] | ((uint32_t)x[q + 5] << 16), x[q + 6] | ((uint32_t)x[q + 7] << 16));
             fence_proxy_async();
             mbar_arrive(&full[sl]);
         }
-    } else if (warp == 5) {
-        // ---- MMA: per di, taps (dj 0, dj 1) in one K = 16 MMA, dj 2 in a second ----
+    } else if (warp >= 4) {
+        // ---- MMA: per di, taps (dj 0, dj 1) in one K = 16 MMA, dj 2 in a second;
+        // M tile mt = warp - 4 ----
+        const int mt = warp - 4;
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16(kTileM, 16, 0, 0);
             const uint32_t w0 = smem_u32(win), wa = smem_u32(wsm);
@@ -572,8 +578,7 @@ __global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
 #pragma unroll
                 for (int di = 0; di < 3; di++) {
                     const uint32_t pl = w0 + (uint32_t)((I - 1 + di) % S) * SB;
-#pragma unroll
-                    for (int mt = 0; mt < MT; mt++) {
+                    {
                         const uint32_t row0 = pl + (uint32_t)(mt * kTileM) * 16;
                         mma_bf16(tmem + buf * ACOLS + mt * 16, adesc01 | ((row0 >> 4) & 0x3FFFu),
                                  bdesc | (((wa + (uint32_t)((di * 2 + 0) * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc,
@@ -628,15 +633,20 @@ __global__ void __launch_bounds__(kInThreads) k_conv_in(InArgs a) {
 struct OutArgs {
     Geom g;
     const bf16* in;     // [g.total][16]
-    const bf16* w;      // [2][32][8]: chunk kc holds input channels 8kc..8kc+7 of each tap
+    const bf16* w;      // [9 (di,dj)][2 kc][16 n][8]: row n = dk < 3 holds W[(di,dj,dk)][0][8 kc ..]
     float* out32;       // internal cells
     const float* res32; // added to the output (may be null)
     int ppc, slots;
     int* err;
 };
 
-constexpr int kOutThreads = 192;  // 4 gather warps, producer, MMA
-constexpr int kZPitch = 27;       // floats per staged Z row (odd: conflict-free)
+// 4 epilogue warps, producer, one MMA warp per M tile
+__host__ __device__ constexpr int out_threads(int mt) { return (5 + mt) * 32; }
+constexpr int kOutStride = 126;   // outputs per 128-row M tile (the tile's first and last rows only feed neighbours)
+
+__host__ __device__ inline int out_rows(const Geom& g, int mt) { return (mt - 1) * kOutStride + kTileM + 2 * g.W; }
+
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 // true in every epilogue thread if it is true in any (named barrier 1, the
 // 128 epilogue threads)
@@ -652,55 +662,58 @@ __device__ __forceinline__ bool epi_any(bool v) {
         : "memory");
     return r != 0;
 }
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
-__host__ __device__ inline int out_mti(const Geom& g, int mt) { return (fwd_rows(g, mt) + kTileM - 1) / kTileM; }
-
-// dec0 forward: 16 -> 1 channel, z = res + conv.
+// dec0 forward: 16 -> 1 channel, z = res + conv.  The 9 (di, dj) shifts are
+// start addresses of the A operand (rows of a staged plane, as in
+// k_conv_fwd), the 3 dk taps are the N columns of the MMA (N = 16, 13 zero):
+//     D[q][dk] = sum_{di,dj} sum_ci X[q + (di-1, dj-1, 0)][ci] W[(di,dj,dk)][ci]
+// accumulates 9 MMAs in TMEM, and out[p] = D[p-1][0] + D[p][1] + D[p+1][2]:
+// 9 MMAs per 126 outputs instead of 27 per 128.
 template <int MT>
-__global__ void __launch_bounds__(kOutThreads) k_conv_out(OutArgs a) {
+__global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_constant__ CUtensorMap tmap, OutArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr uint32_t WB = 2 * 32 * 16;
-    constexpr int ORows = MT * kTileM;                  // output rows of the tile
+    constexpr uint32_t WB = 9 * 2 * 16 * 16;
+    constexpr uint32_t ACOLS = MT * 16;
+    constexpr uint32_t COLS = 2 * ACOLS <= 32 ? 32 : 64;
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
-    const int rows = fwd_rows(g, MT);
-    const int MTI = out_mti(g, MT);                     // input M tiles per plane
-    const int RP = row_pitch(MTI * kTileM, 16);
+    const int rows = out_rows(g, MT);
+    const int NTL = box_count(rows), BR = box_height(rows);
+    const int RP = NTL * BR;
     const uint32_t SB = 2u * RP * 16;
-    const uint32_t ZC = (uint32_t)MTI * 32;             // TMEM columns of one plane's Z
-    const uint32_t COLS = ZC <= 32 ? 32 : (ZC <= 64 ? 64 : (ZC <= 128 ? 128 : (ZC <= 256 ? 256 : 512)));
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
-    float* zs = reinterpret_cast<float*>(slots + S * SB);  // [MTI * 128][kZPitch]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(zs + (size_t)MTI * kTileM * kZPitch + 2);
+    float* dsm = reinterpret_cast<float*>(slots + S * SB);  // [2][MT][128][3]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(dsm + 2 * MT * kTileM * 3);
     uint64_t* full = bars;
     uint64_t* empty = bars + kMaxSlots;
-    uint64_t* zf = bars + 2 * kMaxSlots;
-    uint64_t* ze = zf + 1;
-    uint64_t* drain = ze + 1;
+    uint64_t* accf = bars + 2 * kMaxSlots;
+    uint64_t* acce = accf + 2;
+    uint64_t* drain = acce + 2;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
-    const int P0 = blockIdx.x * ORows;
+    const int P0 = blockIdx.x * (MT * kOutStride);
     const int I0 = 1 + blockIdx.y * a.ppc;
     if (I0 > g.n0) return;
     const int I1 = min(g.n0, I0 + a.ppc - 1);
 
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], 32);
-            mbar_init(&empty[s], 1);
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], MT);
         }
-        mbar_init(zf, 1);
-        mbar_init(ze, kEpiThreads);
-        mbar_init(drain, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&accf[b], MT);
+            mbar_init(&acce[b], kEpiThreads);
+        }
+        mbar_init(drain, MT);
         *abort_flag = 0;
         mbar_fence_init();
     }
     if (warp == 0) tmem_alloc(tslot, COLS);
-    for (uint32_t o = tid * 16; o < WB; o += kOutThreads * 16)
+    for (uint32_t o = tid * 16; o < WB; o += out_threads(MT) * 16)
         cp16(wsm + o, reinterpret_cast<const uint8_t*>(a.w) + o, true);
     cp_commit();
     cp_wait_all();
@@ -709,117 +722,102 @@ __global__ void __launch_bounds__(kOutThreads) k_conv_out(OutArgs a) {
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = *tslot;
-    const int64_t pbase = (int64_t)P0 - g.W - 1;
+    // segment row 0 is position P0 - 1 - W: D row m of tile mt (position
+    // P0 - 1 + 126 mt + m) reads segment rows 126 mt + m + dj W
+    const int pbase = P0 - 1 - g.W;
 
     if (warp == 4) {
-        // ---- producer: input planes I0-1 .. I1+1, MTI * 128 rows (zero past `rows`) ----
-        uint32_t eph = 0xFFu;
-        for (int p = I0 - 1; p <= I1 + 1; p++) {
-            const int sl = p % S;
-            if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 21)) break;
-            eph ^= 1u << sl;
-            const int64_t Q0 = (int64_t)p * g.plane + pbase;
-            for (int idx = lane; idx < MTI * kTileM * 2; idx += 32) {
-                const int q = idx >> 1, kc = idx & 1;
-                const int64_t Q = Q0 + q;
-                const bool v = q < rows && Q >= 0 && Q < g.total;
-                cp16(slots + sl * SB + ((size_t)kc * RP + q) * 16, a.in + (v ? Q : 0) * 16 + kc * 8, v);
-            }
-            cp_mbar_arrive(&full[sl]);
-            mbar_arrive(&full[sl]);
-        }
-        cp_wait_all();
-    } else if (warp == 5) {
-        // ---- MMA: Z of each input plane, MTI tiles of 128 rows x 32 taps ----
+        // ---- producer: TMA boxes of 8 channels x 32 positions ----
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_bf16(kTileM, 32, 0, 0);
-            const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
-            const uint64_t adesc = smem_desc(0, RP * 16, 128);
-            const uint64_t bd = smem_desc(wa, 32 * 16, 128);
-            uint32_t fph = 0, eph = 1u;
+            const uint32_t bytes = 2u * NTL * BR * 16;
+            uint32_t eph = 0xFFu;
             for (int p = I0 - 1; p <= I1 + 1; p++) {
-                const int sp = p % S;
-                if (!role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 22)) break;
-                fph ^= 1u << sp;
-                if (!role_wait(ze, eph, abort_flag, a.err, 23)) break;
-                eph ^= 1u;
+                const int sl = p % S;
+                if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 21)) break;
+                eph ^= 1u << sl;
+                mbar_arrive_expect_tx(&full[sl], bytes);
+                const int y0 = p * g.plane + pbase;
+                for (int kc = 0; kc < 2; kc++)
+                    for (int rt = 0; rt < NTL; rt++)
+                        tma_load_2d(slots + sl * SB + ((size_t)kc * RP + rt * BR) * 16, &tmap, kc * 8, y0 + rt * BR,
+                                    &full[sl]);
+            }
+        }
+        __syncwarp();
+    } else if (warp >= 5) {
+        // ---- MMA: 9 (di, dj) shifts per output plane, M tile mt = warp - 5 ----
+        const int mt = warp - 5;
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(kTileM, 16, 0, 0);
+            const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
+            const uint64_t adesc = smem_desc(0, RP * 16, 128), bdesc = smem_desc(0, 16 * 16, 128);
+            const uint32_t w16 = (uint32_t)g.W * 16;
+            uint32_t fph = 0, aph = 3u;
+            bool ok = true;
+            for (int I = I0; I <= I1 && ok; I++) {
+                const int buf = (I - I0) & 1;
+                for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1 && ok; p++) {
+                    const int sp = p % S;
+                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 22);
+                    fph ^= 1u << sp;
+                }
+                if (ok) ok = role_wait(&acce[buf], (aph >> buf) & 1u, abort_flag, a.err, 23);
+                aph ^= 1u << buf;
+                if (!ok) break;
                 fence_after_sync();
-                for (int mi = 0; mi < MTI; mi++)
-                    mma_bf16(tmem + mi * 32, adesc | (((sl0 + sp * SB + (uint32_t)mi * kTileM * 16) >> 4) & 0x3FFFu),
-                             bd, idesc, 0u);
-                mma_commit(smem_u32(zf));
-                mma_commit(smem_u32(&empty[sp]));  // each input plane is read once
+                const uint32_t sb[3] = {sl0 + (uint32_t)((I - 1) % S) * SB, sl0 + (uint32_t)(I % S) * SB,
+                                        sl0 + (uint32_t)((I + 1) % S) * SB};
+#pragma unroll
+                for (int g9 = 0; g9 < 9; g9++) {
+                    const int di = g9 / 3, dj = g9 % 3;
+                    mma_bf16(tmem + buf * ACOLS + mt * 16,
+                             adesc | (((sb[di] + dj * w16 + (uint32_t)(mt * kOutStride) * 16) >> 4) & 0x3FFFu),
+                             bdesc | (((wa + (uint32_t)(g9 * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc, g9 ? 1u : 0u);
+                }
+                mma_commit(smem_u32(&accf[buf]));
+                mma_commit(smem_u32(&empty[(I - 1) % S]));
             }
             mma_commit(smem_u32(drain));
             mbar_wait(drain, 0, a.err, 24);
         }
         __syncwarp();
     } else {
-        // ---- Z to shared memory, then every output row gathers its terms ----
-        // this thread's rows r = tid + 128 m of the output planes J - 1, J, J + 1
-        float am1[MT], a0[MT], ap1[MT];
-#pragma unroll
-        for (int m = 0; m < MT; m++) am1[m] = a0[m] = ap1[m] = 0.f;
+        // ---- epilogue: D columns 0..2 to shared memory, out[p] = D[p-1][0] + D[p][1] + D[p+1][2] ----
         uint32_t fph = 0;
-        for (int J = I0 - 1; J <= I1 + 1; J++) {
-            const bool ok = role_wait(zf, fph, abort_flag, a.err, 25);
+        for (int I = I0; I <= I1; I++) {
+            const int buf = (I - I0) & 1;
+            const bool ok = role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 25);
             if (epi_any(!ok)) break;  // the four warps leave together
-            fph ^= 1u;
+            fph ^= 1u << buf;
             fence_after_sync();
-            for (int mi = 0; mi < MTI; mi++) {
-                uint32_t z[32];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + mi * 32, z);
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + mi * 32 + 16, z + 16);
-                tmem_wait_ld();
-                float* zr = zs + (size_t)(mi * kTileM + tid) * kZPitch;
+            float* d = dsm + buf * MT * kTileM * 3;
 #pragma unroll
-                for (int t = 0; t < kTaps; t++) {
-                    reg_fence(z[t]);
-                    zr[t] = __uint_as_float(z[t]);
+            for (int mt = 0; mt < MT; mt++) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * 16, r);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    reg_fence(r[c]);
+                    d[(mt * kTileM + tid) * 3 + c] = __uint_as_float(r[c]);
                 }
             }
             fence_before_sync();
-            mbar_arrive(ze);
-            epi_sync();
-            // out[p] of plane J - di += Z[p + W + 1 + dj W + dk][t]  (rows of the segment)
+            mbar_arrive(&acce[buf]);
+            epi_sync();  // d[] complete (double-buffered: the next plane writes the other half)
 #pragma unroll
-            for (int m = 0; m < MT; m++) {
-                const int r = tid + m * kTileM;
-                float sum[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-                for (int dj = 0; dj < 3; dj++)
-#pragma unroll
-                    for (int dk = 0; dk < 3; dk++) {
-                        const float* zr = zs + (size_t)(r + dj * g.W + dk) * kZPitch + dj * 3 + dk;
-#pragma unroll
-                        for (int di = 0; di < 3; di++) sum[di] += zr[di * 9];
-                    }
-                // input plane J feeds output plane J - (di - 1)
-                ap1[m] += sum[0];
-                a0[m] += sum[1];
-                am1[m] += sum[2];
-            }
-            epi_sync();  // Z rows are overwritten by the next plane
-            // output plane J-1 has all its contributions (input planes J-2, J-1, J)
-            const int op = J - 1;
-            if (op >= I0 && op <= I1) {
-#pragma unroll
-                for (int m = 0; m < MT; m++) {
-                    const int pp = P0 + tid + m * kTileM;
-                    if (pp < g.plane) {
-                        const int Jr = pp / g.W, Kc = pp - Jr * g.W;
-                        if (Jr >= 1 && Jr <= g.n1 && Kc >= 1 && Kc <= g.n2) {
-                            const int64_t c = ((int64_t)(op - 1) * g.n1 + (Jr - 1)) * g.n2 + (Kc - 1);
-                            a.out32[c] = (a.res32 ? a.res32[c] : 0.f) + am1[m];
-                        }
+            for (int mt = 0; mt < MT; mt++) {
+                if (tid >= kOutStride) continue;
+                const float* dm = d + (mt * kTileM + tid) * 3;
+                const float v = dm[0] + dm[3 + 1] + dm[6 + 2];
+                const int pp = P0 + mt * kOutStride + tid;
+                if (pp < g.plane) {
+                    const int Jr = pp / g.W, Kc = pp - Jr * g.W;
+                    if (Jr >= 1 && Jr <= g.n1 && Kc >= 1 && Kc <= g.n2) {
+                        const int64_t c = ((int64_t)(I - 1) * g.n1 + (Jr - 1)) * g.n2 + (Kc - 1);
+                        a.out32[c] = (a.res32 ? a.res32[c] : 0.f) + v;
                     }
                 }
-            }
-#pragma unroll
-            for (int m = 0; m < MT; m++) {
-                am1[m] = a0[m];
-                a0[m] = ap1[m];
-                ap1[m] = 0.f;
             }
         }
     }
@@ -1065,6 +1063,19 @@ __global__ void k_prolong_add(Geom f, Geom c, const bf16* __restrict__ coarse, b
     }
 }
 
+// FP32 vector over the internal cells -> BF16 one-channel array over the
+// padded cells (the ghost entries are never written and stay zero).  One
+// block row per (i, j) line of cells.
+__global__ void k_embed(Geom g, const float* __restrict__ in32, bf16* __restrict__ xpad) {
+    const int lines = g.n0 * g.n1;
+    for (int line = blockIdx.x; line < lines; line += gridDim.x) {
+        const int i = line / g.n1, j = line - (line / g.n1) * g.n1;
+        const float* src = in32 + (int64_t)line * g.n2;
+        bf16* dst = xpad + ((int64_t)(i + 1) * (g.n1 + 2) + (j + 1)) * g.W + 1;
+        for (int k = threadIdx.x; k < g.n2; k += blockDim.x) dst[k] = __float2bfloat16_rn(src[k]);
+    }
+}
+
 // padded bf16 activations -> FP32 [cell][C] over the internal cells
 __global__ void k_read_act(Geom g, int C, const bf16* __restrict__ a, float* __restrict__ out) {
     const int64_t total = (int64_t)g.n0 * g.n1 * g.n2 * C;
@@ -1162,11 +1173,12 @@ __global__ void k_pack_tapk(const float* __restrict__ W, int flip, bf16* __restr
     }
 }
 
-// dec0 forward weights, taps along N: out[kc][t][e] = W[t][0][8 kc + e], t < 27.
+// dec0 forward weights, dk along N: out[g][kc][n][e] = W[t][0][8 kc + e] with
+// t = 3 g + n for the (di, dj) group g and n = dk < 3, else 0.
 __global__ void k_pack_tapn(const float* __restrict__ W, bf16* __restrict__ out) {
-    for (int idx = threadIdx.x; idx < 2 * 32 * 8; idx += blockDim.x) {
-        const int e = idx & 7, t = (idx >> 3) & 31, kc = idx >> 8;
-        out[idx] = __float2bfloat16_rn(t < kTaps ? W[t * 16 + kc * 8 + e] : 0.f);
+    for (int idx = threadIdx.x; idx < 9 * 2 * 16 * 8; idx += blockDim.x) {
+        const int e = idx & 7, n = (idx >> 3) & 15, kc = (idx >> 7) & 1, g9 = idx >> 8;
+        out[idx] = __float2bfloat16_rn(n < 3 ? W[(g9 * 3 + n) * 16 + kc * 8 + e] : 0.f);
     }
 }
 
@@ -1229,17 +1241,41 @@ __global__ void k_warm(int64_t n, const double* __restrict__ diag, const double*
 
 // ---------------------------------------------------------------------------
 // host side: launch configuration and dispatch
-static size_t fwd_smem(int cin, int nt, const Geom& g, bool embed, int mt, int slots) {
+static size_t fwd_smem(int cin, int nt, const Geom& g, int mt, int slots) {
     const int rows = fwd_rows(g, mt);
-    const int RP = row_pitch(rows, cin);
-    return (size_t)kTaps * cin * nt * 2 + slots * (size_t)(cin / 8) * RP * 16 +
-           (embed ? slots * (size_t)raw_bytes(rows) : 0) + (3 * kMaxSlots + 5) * 8 + 16;
+    const int RP = box_count(rows) * box_height(rows);
+    return (size_t)kTaps * cin * nt * 2 + slots * (size_t)(cin / 8) * RP * 16 + (2 * kMaxSlots + 5) * 8 + 16;
 }
 
 // two 128-position tiles per step on planes wider than two tiles, when a
 // 4-slot ring of the wider plane segments still fits
-static int pick_mt(const Geom& g, int cin, int nt, bool embed) {
-    return g.plane > 2 * kTileM && fwd_smem(cin, nt, g, embed, 2, 4) <= kMaxSmem ? 2 : 1;
+static int pick_mt(const Geom& g, int cin, int nt) {
+    return g.plane > 2 * kTileM && fwd_smem(cin, nt, g, 2, 4) <= kMaxSmem ? 2 : 1;
+}
+
+// TMA map of a padded channels-last activation [total][C] (bf16): boxes of 8
+// channels x `box_rows` positions, rows outside the array read zero
+static int act_map(dare_ctx* ctx, CUtensorMap* m, const bf16* base, int C, int64_t total, int box_rows) {
+    const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)total};
+    const cuuint64_t strides[1] = {(cuuint64_t)C * sizeof(bf16)};
+    const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+    const cuuint32_t es[2] = {1, 1};
+    // the driver's encoder, looked up through the runtime (no link-time
+    // dependency on the driver library)
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return set_error(ctx, DARE_ERR_CUDA, "unet: cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, es,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ctx, DARE_ERR_CUDA, "unet: cuTensorMapEncodeTiled failed");
+    return DARE_OK;
 }
 
 static int dy_pitch_rt(int c) { return kTileM + (c == 16 ? 4 : (c == 32 ? 2 : 1)); }
@@ -1274,19 +1310,19 @@ static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int
     return DARE_OK;
 }
 
-template <int CIN, int NT, int MT, int INM, int OUTM>
-static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const FwdArgs& a0) {
-    auto kern = k_conv_fwd<CIN, NT, MT, INM, OUTM>;
+template <int CIN, int NT, int MT, int OUTM>
+static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap& tmap, const FwdArgs& a0) {
+    auto kern = k_conv_fwd<CIN, NT, MT, OUTM>;
     if (!lc.ready) {
         // the deepest ring (4..8 staged planes) that fits
         int slots = kMaxSlots;
-        while (slots > 4 && fwd_smem(CIN, NT, a0.g, INM == IN_EMBED, MT, slots) > kMaxSmem) slots--;
-        size_t smem = fwd_smem(CIN, NT, a0.g, INM == IN_EMBED, MT, slots);
+        while (slots > 4 && fwd_smem(CIN, NT, a0.g, MT, slots) > kMaxSmem) slots--;
+        size_t smem = fwd_smem(CIN, NT, a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         const uint32_t acols = 2 * MT * NT;
         const uint32_t cols = acols <= 32 ? 32 : (acols <= 64 ? 64 : (acols <= 128 ? 128 : 256));
         int occ = 0, rc;
-        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, kFwdThreads))) return rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, fwd_threads(MT)))) return rc;
         // about four waves of CTAs; a CTA marches at least two planes (it
         // stages two more than it computes)
         const int n0 = a0.g.n0;
@@ -1308,27 +1344,29 @@ static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const FwdArgs& a0)
     FwdArgs a = a0;
     a.ppc = lc.ppc;
     a.slots = lc.slots;
-    kern<<<lc.grid, kFwdThreads, lc.smem, ctx->stream>>>(a);
+    kern<<<lc.grid, fwd_threads(MT), lc.smem, ctx->stream>>>(tmap, a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
 
-static int launch_fwd(dare_ctx* ctx, LaunchCfg& lc, int cin, int nt, int nz, int inm, int outm, const FwdArgs& a) {
-    const int mt = pick_mt(a.g, cin, nt, inm == IN_EMBED);
-#define DARE_FWD(CI, N, IM, OM)                                                                       \
-    if (cin == CI && nt == N && inm == IM && outm == OM)                                              \
-        return mt == 2 ? launch_fwd_t<CI, N, 2, IM, OM>(ctx, lc, nz, a) : launch_fwd_t<CI, N, 1, IM, OM>(ctx, lc, nz, a);
-    DARE_FWD(16, 16, IN_EMBED, OUT_STORE)
-    DARE_FWD(16, 16, IN_BF16, OUT_STORE)
-    DARE_FWD(16, 32, IN_BF16, OUT_STORE)
-    DARE_FWD(32, 16, IN_BF16, OUT_STORE)
-    DARE_FWD(32, 32, IN_BF16, OUT_STORE)
-    DARE_FWD(64, 16, IN_BF16, OUT_STORE)
-    DARE_FWD(64, 32, IN_BF16, OUT_STORE)
-    DARE_FWD(32, 16, IN_BF16, OUT_ADDUP)
-    DARE_FWD(64, 16, IN_BF16, OUT_ADDUP)
-    DARE_FWD(64, 32, IN_BF16, OUT_ADDUP)
-    DARE_FWD(16, 16, IN_BF16, OUT_F32)
+// BF16 input `a.in` with `cin` channels
+static int launch_fwd(dare_ctx* ctx, LaunchCfg& lc, int cin, int nt, int nz, int outm, const FwdArgs& a) {
+    const int mt = pick_mt(a.g, cin, nt);
+    CUtensorMap tmap;
+    int rc = act_map(ctx, &tmap, a.in, cin, a.g.total, box_height(fwd_rows(a.g, mt)));
+    if (rc) return rc;
+#define DARE_FWD(CI, N, OM)                                                                       \
+    if (cin == CI && nt == N && outm == OM)                                                       \
+        return mt == 2 ? launch_fwd_t<CI, N, 2, OM>(ctx, lc, nz, tmap, a) : launch_fwd_t<CI, N, 1, OM>(ctx, lc, nz, tmap, a);
+    DARE_FWD(16, 16, OUT_STORE)
+    DARE_FWD(16, 32, OUT_STORE)
+    DARE_FWD(32, 16, OUT_STORE)
+    DARE_FWD(32, 32, OUT_STORE)
+    DARE_FWD(64, 16, OUT_STORE)
+    DARE_FWD(64, 32, OUT_STORE)
+    DARE_FWD(32, 16, OUT_ADDUP)
+    DARE_FWD(64, 16, OUT_ADDUP)
+    DARE_FWD(64, 32, OUT_ADDUP)
 #undef DARE_FWD
     return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: no forward convolution kernel for this shape");
 }
@@ -1385,8 +1423,7 @@ static int launch_wgr(dare_ctx* ctx, LaunchCfg& lc, int cin, int cout, int xm, i
 
 static size_t in_smem(const Geom& g, int mt, int slots) {
     const size_t sb = (size_t)((in_rows(g, mt) + 7) / 8) * 8 * 16;
-    return 3 * 2 * 2 * 16 * 16 + slots * sb + slots * (size_t)raw_bytes(in_raw_rows(g, mt)) +
-           (3 * kMaxSlots + 5) * 8 + 16;
+    return 3 * 2 * 2 * 16 * 16 + slots * sb + slots * (size_t)in_raw_elems(g, mt) * 2 + (3 * kMaxSlots + 5) * 8 + 16;
 }
 
 static int in_tiles_mt(const Geom& g) { return g.plane > 2 * kTileM ? 2 : 1; }
@@ -1401,7 +1438,7 @@ static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a0) {
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
         int occ = 0, rc;
-        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, kInThreads))) return rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, in_threads(MT)))) return rc;
         // (the launch checks above keep the ring at >= 4 planes: 3 in use + 1 loading)
         const int n0 = a0.g.n0;
         const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
@@ -1420,45 +1457,45 @@ static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a0) {
     InArgs a = a0;
     a.ppc = lc.ppc;
     a.slots = lc.slots;
-    kern<<<lc.grid, kInThreads, lc.smem, ctx->stream>>>(a);
+    kern<<<lc.grid, in_threads(MT), lc.smem, ctx->stream>>>(a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
 
-static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a) {
+// in32 (FP32 over the internal cells) is first written into the padded BF16
+// array x0, which the kernel then stages plane by plane with bulk copies.
+static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a, const float* in32) {
+    const Geom& g = a.g;
+    k_embed<<<(int)std::min<int64_t>((int64_t)g.n0 * g.n1, (int64_t)ctx->num_sms * 16), 128, 0, ctx->stream>>>(
+        g, in32, const_cast<bf16*>(a.xpad));
+    DARE_LAUNCHED(ctx);
     return in_tiles_mt(a.g) == 2 ? launch_in_t<2>(ctx, lc, a) : launch_in_t<1>(ctx, lc, a);
 }
 
 static size_t out_smem(const Geom& g, int mt, int slots) {
-    const int mti = out_mti(g, mt);
-    const int RP = row_pitch(mti * kTileM, 16);
-    return 2 * 32 * 16 + slots * (size_t)2 * RP * 16 + ((size_t)mti * kTileM * kZPitch + 2) * 4 +
-           (2 * kMaxSlots + 3) * 8 + 16;
+    const int rows = out_rows(g, mt);
+    const int RP = box_count(rows) * box_height(rows);
+    return 9 * 2 * 16 * 16 + slots * (size_t)2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 + (2 * kMaxSlots + 5) * 8 +
+           16;
 }
 
-// two output tiles per CTA step when the plane is wide and one plane's Z
-// (32 TMEM columns per 128 input rows) stays within 256 columns
 static int out_tiles_mt(const Geom& g) {
-    if (g.plane > 2 * kTileM && out_mti(g, 2) * 32 <= 256) return 2;
-    return 1;
+    return g.plane > 2 * kOutStride && out_smem(g, 2, 4) <= kMaxSmem ? 2 : 1;
 }
 
 template <int MT>
 static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     auto kern = k_conv_out<MT>;
     if (!lc.ready) {
-        if (out_mti(a0.g, MT) * 32 > 512)
-            return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the one-channel output conv");
         int slots = kMaxSlots;
-        while (slots > 2 && out_smem(a0.g, MT, slots) > kMaxSmem) slots--;
+        while (slots > 4 && out_smem(a0.g, MT, slots) > kMaxSmem) slots--;
         size_t smem = out_smem(a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
-        const uint32_t zc = (uint32_t)out_mti(a0.g, MT) * 32;
-        const uint32_t cols = zc <= 32 ? 32 : (zc <= 64 ? 64 : (zc <= 128 ? 128 : (zc <= 256 ? 256 : 512)));
+        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
         int occ = 0, rc;
-        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, kOutThreads))) return rc;
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, out_threads(MT)))) return rc;
         const int n0 = a0.g.n0;
-        const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
+        const int tiles = (a0.g.plane + MT * kOutStride - 1) / (MT * kOutStride);
         const int64_t target = (int64_t)ctx->num_sms * occ * 4;
         const int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + tiles - 1) / tiles));
         const int ppc = std::max((n0 + chunks - 1) / chunks, std::min(n0, 2));
@@ -1474,7 +1511,10 @@ static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     OutArgs a = a0;
     a.ppc = lc.ppc;
     a.slots = lc.slots;
-    kern<<<lc.grid, kOutThreads, lc.smem, ctx->stream>>>(a);
+    CUtensorMap tmap;
+    int rc = act_map(ctx, &tmap, a.in, 16, a.g.total, box_height(out_rows(a.g, MT)));
+    if (rc) return rc;
+    kern<<<lc.grid, out_threads(MT), lc.smem, ctx->stream>>>(tmap, a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
@@ -1484,7 +1524,7 @@ static int launch_out(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a) {
 }
 
 static int pick_nt(int cink, int coutk, const Geom& g) {
-    if (coutk % 32 == 0 && fwd_smem(cink, 32, g, false, 1, 4) <= kMaxSmem) return 32;
+    if (coutk % 32 == 0 && fwd_smem(cink, 32, g, 1, 4) <= kMaxSmem) return 32;
     return 16;
 }
 
@@ -1497,11 +1537,11 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
     if (l == ENC0) {
         InArgs a{};
         a.g = net->geo[0];
-        a.in32 = in32;
+        a.xpad = net->X0;
         a.w = L.wf;
         a.out = out;
         a.err = net->err;
-        return launch_in(net->ctx, L.fwd, a);
+        return launch_in(net->ctx, L.fwd, a, in32);
     }
     if (l == DEC0) {
         OutArgs a{};
@@ -1525,7 +1565,7 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
     a.out32 = out32;
     a.res32 = res32;
     a.err = net->err;
-    return launch_fwd(net->ctx, L.fwd, L.cink, L.nt, L.coutk / L.nt, in32 ? IN_EMBED : IN_BF16, outm, a);
+    return launch_fwd(net->ctx, L.fwd, L.cink, L.nt, L.coutk / L.nt, outm, a);
 }
 
 // data gradient of layer l: dX = conv(dY, W flipped and transposed)
@@ -1534,11 +1574,11 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
     if (l == DEC0) {
         InArgs a{};
         a.g = net->geo[0];
-        a.in32 = dy32;
+        a.xpad = net->X0;
         a.w = L.wb;
         a.out = dx;
         a.err = net->err;
-        return launch_in(net->ctx, L.bwd, a);
+        return launch_in(net->ctx, L.bwd, a, dy32);
     }
     FwdArgs a{};
     a.g = net->geo[L.level];
@@ -1548,7 +1588,7 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
     a.cout = L.cink;
     a.out = dx;
     a.err = net->err;
-    return launch_fwd(net->ctx, L.bwd, L.coutk, L.ntb, L.cink / L.ntb, dy32 ? IN_EMBED : IN_BF16, OUT_STORE, a);
+    return launch_fwd(net->ctx, L.bwd, L.coutk, L.ntb, L.cink / L.ntb, OUT_STORE, a);
 }
 
 static int conv_wgrad(dare_unet* net, int l, const bf16* x, const float* x32, const bf16* dy, const float* dy32,
@@ -1788,11 +1828,11 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         L.nt = pick_nt(L.cink, L.coutk, g);
         L.ntb = pick_nt(L.coutk, L.cink, g);
         const bool fits_fwd = l == ENC0   ? in_smem(g, 1, 4) <= kMaxSmem
-                              : l == DEC0 ? out_smem(g, 1, 2) <= kMaxSmem && out_mti(g, 1) * 32 <= 512
-                                          : fwd_smem(L.cink, L.nt, g, false, 1, 4) <= kMaxSmem;
+                              : l == DEC0 ? out_smem(g, 1, 4) <= kMaxSmem
+                                          : fwd_smem(L.cink, L.nt, g, 1, 4) <= kMaxSmem;
         const bool fits_bwd = l == ENC0   ? true
                               : l == DEC0 ? in_smem(g, 1, 4) <= kMaxSmem
-                                          : fwd_smem(L.coutk, L.ntb, g, false, 1, 4) <= kMaxSmem;
+                                          : fwd_smem(L.coutk, L.ntb, g, 1, 4) <= kMaxSmem;
         if (!fits_fwd || !fits_bwd || wgr_smem(L.cink, L.coutk, g, l == ENC0, l == DEC0) > kMaxSmem) {
             delete net;
             return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_create: grid too wide for the staged convolutions");
@@ -1807,8 +1847,8 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     const int64_t T[4] = {net->geo[0].total, net->geo[1].total, net->geo[2].total, net->geo[3].total};
     struct Slot {
         bf16** p;
-        int level, c;
-    } slots[] = {{&net->S0, 0, 16}, {&net->P1, 1, 16}, {&net->S1, 1, 32}, {&net->P2, 2, 32}, {&net->S2, 2, 64},
+        int level, c, extra;
+    } slots[] = {{&net->X0, 0, 1, kPadSlack}, {&net->S0, 0, 16}, {&net->P1, 1, 16}, {&net->S1, 1, 32}, {&net->P2, 2, 32}, {&net->S2, 2, 64},
                  {&net->P3, 3, 64}, {&net->E3, 3, 64}, {&net->dS0, 0, 16}, {&net->dD1, 1, 16}, {&net->dS1, 1, 32},
                  {&net->dD2, 2, 32}, {&net->dS2, 2, 64}, {&net->dD3, 3, 64}, {&net->dE3, 3, 64}, {&net->dP3, 3, 64},
                  {&net->dP2, 2, 32}, {&net->dP1, 1, 16}};
@@ -1816,7 +1856,7 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     std::vector<size_t> offs;
     for (auto& s : slots) {
         offs.push_back(bytes);
-        bytes += ((size_t)T[s.level] * s.c * sizeof(bf16) + 255) / 256 * 256;
+        bytes += (((size_t)T[s.level] * s.c + s.extra) * sizeof(bf16) + 255) / 256 * 256;
     }
     cudaError_t e = cudaMalloc(&net->act_block, bytes);
     if (e == cudaSuccess) e = cudaMemset(net->act_block, 0, bytes);

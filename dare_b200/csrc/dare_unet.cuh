@@ -16,10 +16,18 @@ constexpr int kLayers = 8;
 constexpr int kTaps = 27;
 constexpr int kThreads = 128;  // one CTA = 4 warps = the 128 TMEM lanes of an M=128 tile
 constexpr int kTileM = 128;    // output rows (padded positions) per MMA tile
-// warp-specialised forward convolution: 4 epilogue warps + producer + MMA + converter
+// warp-specialised forward convolution: 4 epilogue warps + producer + one MMA warp per M tile
 constexpr int kEpiThreads = 128;
-constexpr int kFwdThreads = 224;  // + a converter warp for FP32-input layers
+__host__ __device__ constexpr int fwd_threads(int mt) { return (5 + mt) * 32; }
 constexpr int kMaxSlots = 8;   // staged-plane ring depth limit
+// A staged plane segment of `rows` positions is loaded as box_count(rows)
+// TMA boxes of box_height(rows) positions (at most 256, a multiple of 8)
+// per 8-channel chunk.
+__host__ __device__ inline int box_count(int rows) { return (rows + 255) / 256; }
+__host__ __device__ inline int box_height(int rows) {
+    const int nb = box_count(rows);
+    return ((rows + nb - 1) / nb + 7) / 8 * 8;
+}
 
 // A level's activations live in a zero-padded, channels-last layout:
 // [(n0+2)][(n1+2)][(n2+2)][C] bf16, ghosts kept at zero, so every 3^3 tap is
@@ -124,6 +132,7 @@ struct dare_unet {
     dare_gpu::unet::bf16* dP3 = nullptr;
     dare_gpu::unet::bf16* dP2 = nullptr;
     dare_gpu::unet::bf16* dP1 = nullptr;
+    dare_gpu::unet::bf16* X0 = nullptr;   // k_conv_in input: a FP32 vector as BF16 over the padded level-0 cells
     void* act_block = nullptr;            // one allocation for all of the above
     float* z = nullptr;                   // forward output during training
     float* g = nullptr;                   // dL/dz
