@@ -158,73 +158,15 @@ __host__ __device__ inline uint32_t raw_bytes(int rows) { return (uint32_t)(((ro
 struct FwdArgs {
     Geom g;          // level of input and output
     Geom fg;         // finer level (OUT_ADDUP)
-    const bf16* in;  // IN_BF16: [g.total][CIN]
-    const float* in32;
-    const bf16* w;   // packed [nz][27][CIN/8][NT][8]
+    const bf16* in;  // [g.total][CIN]
+    const bf16* w;   // packed [nz][9 (di,dj)][CIN/8][3 dk][NT][8]
     int cout;        // channel count (stride) of out / fine
     bf16* out;       // OUT_STORE: [g.total][cout]
     bf16* fine;      // OUT_ADDUP: [fg.total][cout]
-    float* out32;    // OUT_F32: internal cells, channel 0 (+ res32)
-    const float* res32;
     int ppc;
     int slots;       // ring depth (shared-memory slots of staged planes)
     int* err;
 };
-
-// One output row (a padded position of plane I) from its NT accumulator
-// values: BF16 store, prolongation-add into the eight finer children, or the
-// FP32 output.  Ghost positions and positions past the plane are skipped.
-template <int NT, int OUTM>
-__device__ __forceinline__ void fwd_store(const FwdArgs& a, const uint32_t* r, int I, int pp, int co0) {
-    const Geom& g = a.g;
-    if (pp >= g.plane) return;
-    const int J = pp / g.W, K = pp - J * g.W;
-    if (J < 1 || J > g.n1 || K < 1 || K > g.n2) return;
-    if (OUTM == OUT_STORE) {
-        bf16* dst = a.out + ((int64_t)I * g.plane + pp) * a.cout + co0;
-#pragma unroll
-        for (int c = 0; c < NT; c += 8) {
-            uint4 q;
-            q.x = pack_bf16(__uint_as_float(r[c + 0]), __uint_as_float(r[c + 1]));
-            q.y = pack_bf16(__uint_as_float(r[c + 2]), __uint_as_float(r[c + 3]));
-            q.z = pack_bf16(__uint_as_float(r[c + 4]), __uint_as_float(r[c + 5]));
-            q.w = pack_bf16(__uint_as_float(r[c + 6]), __uint_as_float(r[c + 7]));
-            *reinterpret_cast<uint4*>(dst + c) = q;
-        }
-    } else if (OUTM == OUT_ADDUP) {
-        // nearest-neighbour prolongation of this coarse cell, added into its
-        // eight children on the finer level (the additive skip); the eight
-        // children's loads of one 8-channel chunk are issued together
-        const Geom& f = a.fg;
-        const int64_t fplane = (int64_t)(f.n1 + 2) * f.W;
-        bf16* base = a.fine + (((int64_t)(2 * I - 1) * (f.n1 + 2) + (2 * J - 1)) * f.W + (2 * K - 1)) * a.cout + co0;
-#pragma unroll
-        for (int c = 0; c < NT; c += 8) {
-            uint4 o[8];
-#pragma unroll
-            for (int ch = 0; ch < 8; ch++)
-                o[ch] = *reinterpret_cast<const uint4*>(
-                    base + ((ch >> 2) * fplane + ((ch >> 1) & 1) * f.W + (ch & 1)) * a.cout + c);
-#pragma unroll
-            for (int ch = 0; ch < 8; ch++) {
-                uint4 q;
-                q.x = pack_bf16(bf16_lo(o[ch].x) + __uint_as_float(r[c + 0]),
-                                bf16_hi(o[ch].x) + __uint_as_float(r[c + 1]));
-                q.y = pack_bf16(bf16_lo(o[ch].y) + __uint_as_float(r[c + 2]),
-                                bf16_hi(o[ch].y) + __uint_as_float(r[c + 3]));
-                q.z = pack_bf16(bf16_lo(o[ch].z) + __uint_as_float(r[c + 4]),
-                                bf16_hi(o[ch].z) + __uint_as_float(r[c + 5]));
-                q.w = pack_bf16(bf16_lo(o[ch].w) + __uint_as_float(r[c + 6]),
-                                bf16_hi(o[ch].w) + __uint_as_float(r[c + 7]));
-                *reinterpret_cast<uint4*>(base + ((ch >> 2) * fplane + ((ch >> 1) & 1) * f.W + (ch & 1)) * a.cout +
-                                          c) = q;
-            }
-        }
-    } else {
-        const int64_t c = ((int64_t)(I - 1) * g.n1 + (J - 1)) * g.n2 + (K - 1);
-        a.out32[c] = (a.res32 ? a.res32[c] : 0.f) + __uint_as_float(r[0]);
-    }
-}
 
 // Bounded mbarrier wait that also gives up when another role has aborted.
 __device__ __forceinline__ bool role_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
@@ -248,15 +190,44 @@ __device__ __forceinline__ void cp_wait_group() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Warp-specialised forward convolution.  Warps 0-3 drain the accumulator
-// (each its 32-lane TMEM quarter), one lane of warp 4 stages input planes with
-// TMA, one lane of each of warps 5 .. 5+MT-1 issues the MMAs of one M tile
-// (a single issuing thread cannot keep the tensor pipe busy with these short
-// MMAs; separate issuers with separate accumulators can).  A CTA owns MT consecutive
-// 128-position tiles of a (j,k) plane and marches along i through planes
-// I0..I1; input planes live in a ring of `slots` shared-memory slots, each
-// CIN/8 chunk planes of RP rows x 16 bytes, filled by CIN/8 x RP/32 TMA boxes
-// of 8 channels x 32 positions (rows outside the array read zero).
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// true in every epilogue thread if it is true in any (named barrier 1, the
+// 128 epilogue threads)
+__device__ __forceinline__ bool epi_any(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+
+// Offset (in cells) of child ch = 4 a + 2 b + c of a coarse cell from its
+// first child on the finer level f: (+a planes, +b rows, +c cells).
+__device__ __forceinline__ int64_t child_off(const Geom& f, int64_t fplane, int ch) {
+    return (ch >> 2) * fplane + ((ch >> 1) & 1) * f.W + (ch & 1);
+}
+
+// Warp-specialised forward convolution with the three dk taps of a (di, dj)
+// in the N dimension of one MMA: D[m][dk NT + co] = sum_{di,dj,ci}
+// X[m + (di, dj)][ci] W[(di,dj,dk)][co][ci] over CIN/16 K steps per (di, dj),
+// i.e. 9 x CIN/16 MMAs of N = 3 NT per 128-row tile (an MMA of M = 128, K = 16
+// costs about the same for every N up to ~64, so this is ~3x fewer tensor
+// cycles than one MMA per tap), and out(m) = D[m-1][dk 0] + D[m][dk 1] +
+// D[m+1][dk 2] for m = 1 .. 126 (warp shuffles; the rows at a warp's edge
+// come through shared memory).
+// Roles: warps 0-3 drain the accumulators (each its 32-lane TMEM quarter),
+// one lane of warp 4 stages input planes with TMA, one lane of each of warps
+// 5 .. 5+MT-1 issues the MMAs of one M tile.  A CTA owns MT overlapping M
+// tiles (126 outputs each) of a (j,k) plane and marches along i through
+// planes I0..I1; input planes live in a ring of `slots` shared-memory slots,
+// each CIN/8 chunk planes of RP rows x 16 bytes filled by TMA boxes of
+// 8 channels x BR positions (rows outside the array read zero).
 // Barriers:
 //   full[s]   producer -> MMA   expect_tx + the boxes' bytes of slot s
 //   empty[s]  MMA -> producer   the last MMAs reading slot s have completed (MT commits)
@@ -264,25 +235,33 @@ __device__ __forceinline__ void cp_wait_group() {
 //   acce[b]   epilogue -> MMA   accumulator b has been read (128 arrivals)
 // Every wait is bounded; a role that times out raises a shared abort flag
 // the others poll, and the MMA lane waits for its own MMAs before TMEM is
-// released.
+// released.  OUT_ADDUP (nearest-neighbour prolongation added into the eight
+// children on the finer level) loads the children of plane I+1 while plane
+// I+1's MMAs run.
 template <int CIN, int NT, int MT, int OUTM>
 __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_constant__ CUtensorMap tmap, FwdArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int KC = CIN / 8;
+    constexpr int N3 = 3 * NT;
     constexpr uint32_t WB = kTaps * CIN * NT * 2;
-    constexpr uint32_t ACOLS = MT * NT;  // columns of one accumulator buffer
-    constexpr uint32_t COLS = 2 * ACOLS <= 32 ? 32 : (2 * ACOLS <= 64 ? 64 : (2 * ACOLS <= 128 ? 128 : 256));
+    constexpr uint32_t AST = N3 <= 64 ? 64 : 128;  // TMEM columns of one tile's accumulator
+    constexpr uint32_t ACOLS = MT * AST;           // ... of one buffer (two buffers)
+    constexpr uint32_t COLS = 2 * ACOLS <= 128 ? 128 : (2 * ACOLS <= 256 ? 256 : 512);
+    static_assert(2 * ACOLS <= 512, "accumulators exceed TMEM");
+    static_assert(OUTM == OUT_STORE || OUTM == OUT_ADDUP, "forward epilogue");
+    constexpr int XN = MT * 4 * 2 * NT;  // exchange floats per buffer
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
-    const int rows = fwd_rows(g, MT);
+    const int rows = strip_rows(g, MT);
     const int NTL = box_count(rows), BR = box_height(rows);  // TMA boxes per chunk plane, rows per box
     const int RP = NTL * BR;
     const uint32_t SB = (uint32_t)KC * RP * 16;
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(slots + S * SB);
-    uint64_t* full = bars;            // [kMaxSlots]
+    float* exch = reinterpret_cast<float*>(slots + S * SB);  // [2][MT][4 warps][2][NT]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(exch + 2 * XN);
+    uint64_t* full = bars;  // [kMaxSlots]
     uint64_t* empty = bars + kMaxSlots;
     uint64_t* accf = bars + 2 * kMaxSlots;
     uint64_t* acce = accf + 2;
@@ -290,7 +269,7 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
-    const int P0 = blockIdx.x * (MT * kTileM);
+    const int P0 = blockIdx.x * (MT * kOutStride);
     const int I0 = 1 + blockIdx.y * a.ppc;
     if (I0 > g.n0) return;
     const int I1 = min(g.n0, I0 + a.ppc - 1);
@@ -321,7 +300,9 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = *tslot;
-    const int pbase = P0 - g.W - 1;
+    // slot row 0 is position P0 - 1 - W; D row m of tile mt (position
+    // P0 - 1 + 126 mt + m) reads slot rows 126 mt + m + dj W
+    const int pbase = P0 - 1 - g.W;
 
     if (warp == 4) {
         // ---- producer: planes I0-1 .. I1+1 into the ring by TMA ----
@@ -345,9 +326,9 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
         // ---- MMA issue: lane 0 of warp 5 + mt, M tile mt ----
         const int mt = warp - 5;
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_bf16(kTileM, NT, 0, 0);
+            constexpr uint32_t idesc = idesc_bf16(kTileM, N3, 0, 0);
             const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
-            const uint64_t adesc = smem_desc(0, RP * 16, 128), bdesc = smem_desc(0, NT * 16, 128);
+            const uint64_t adesc = smem_desc(0, RP * 16, 128), bdesc = smem_desc(0, N3 * 16, 128);
             const uint32_t w16 = (uint32_t)g.W * 16, rp32 = (uint32_t)RP * 32;
             uint32_t fph = 0, aph = 3u;
             bool ok = true;
@@ -362,19 +343,18 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
                 aph ^= 1u << buf;
                 if (!ok) break;
                 fence_after_sync();
-                // descriptors = constant high bits | (start address >> 4); the
-                // 27 taps are unrolled so each start address is one add
+                // descriptors = constant high bits | (start address >> 4)
                 const uint32_t sb[3] = {sl0 + (uint32_t)((I - 1) % S) * SB, sl0 + (uint32_t)(I % S) * SB,
                                         sl0 + (uint32_t)((I + 1) % S) * SB};
 #pragma unroll
-                for (int t = 0; t < kTaps; t++) {
-                    const int di = t / 9, dj = (t / 3) % 3, dk = t % 3;
-                    const uint32_t ab = sb[di] + dj * w16 + dk * 16 + (uint32_t)(mt * kTileM) * 16;
+                for (int g9 = 0; g9 < 9; g9++) {
+                    const int di = g9 / 3, dj = g9 % 3;
+                    const uint32_t ab = sb[di] + dj * w16 + (uint32_t)(mt * kOutStride) * 16;
 #pragma unroll
                     for (int s = 0; s < CIN / 16; s++)
-                        mma_bf16(tmem + buf * ACOLS + mt * NT, adesc | (((ab + s * rp32) >> 4) & 0x3FFFu),
-                                 bdesc | (((wa + (uint32_t)((t * KC + 2 * s) * NT * 16)) >> 4) & 0x3FFFu), idesc,
-                                 (t | s) ? 1u : 0u);
+                        mma_bf16(tmem + buf * ACOLS + mt * AST, adesc | (((ab + s * rp32) >> 4) & 0x3FFFu),
+                                 bdesc | (((wa + (uint32_t)((g9 * KC + 2 * s) * N3 * 16)) >> 4) & 0x3FFFu), idesc,
+                                 (g9 | s) ? 1u : 0u);
                 }
                 mma_commit(smem_u32(&accf[buf]));
                 mma_commit(smem_u32(&empty[(I - 1) % S]));  // plane I-1 is not read again
@@ -385,28 +365,123 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warps 0-3, TMEM lanes 32*warp .. 32*warp+31 ----
+        // ---- epilogue: warps 0-3; thread tid drains D row tid of every tile ----
+        int pos[MT];  // in-plane output position of this thread's row, -1 if none
+        int64_t fofs[MT];
+        const Geom& f = a.fg;
+        const int64_t fplane = (int64_t)(f.n1 + 2) * f.W;
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) {
+            const int pp = P0 + mt * kOutStride + tid - 1;
+            const int J = pp / g.W, K = pp - J * g.W;
+            const bool ok = tid >= 1 && tid <= kOutStride && pp < g.plane && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2;
+            pos[mt] = ok ? pp : -1;
+            fofs[mt] = (int64_t)(2 * J - 1) * f.W + (2 * K - 1);  // first child, without the plane term (ADDUP)
+        }
+        // ADDUP: the children of the next plane are loaded ahead when their
+        // registers fit (MT x NT <= 32), else just before their update
+        constexpr bool kPre = OUTM == OUT_ADDUP && MT * NT <= 32;
+        uint4 pre[kPre ? MT : 1][NT / 8][8];
+        auto fetch = [&](int I, int mt, uint4(&o)[NT / 8][8]) {
+            const bf16* base = a.fine + ((int64_t)(2 * I - 1) * fplane + fofs[mt]) * a.cout + co0;
+#pragma unroll
+            for (int c8 = 0; c8 < NT / 8; c8++)
+#pragma unroll
+                for (int ch = 0; ch < 8; ch++)
+                    o[c8][ch] = *reinterpret_cast<const uint4*>(base + child_off(f, fplane, ch) * a.cout + c8 * 8);
+        };
+        if constexpr (kPre) {
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++)
+                if (pos[mt] >= 0) fetch(I0, mt, pre[mt]);
+        }
         uint32_t fph = 0;
         for (int I = I0; I <= I1; I++) {
             const int buf = (I - I0) & 1;
-            if (!role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 9)) break;
+            const bool ok = role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 9);
+            if (epi_any(!ok)) break;  // the four warps leave together
             fph ^= 1u << buf;
             fence_after_sync();
-            uint32_t r[MT][NT];
+            float acc[MT][NT];
+            float* ex = exch + buf * XN;
 #pragma unroll
             for (int mt = 0; mt < MT; mt++)
 #pragma unroll
-                for (int c = 0; c < NT; c += 16)
-                    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * NT + c, &r[mt][c]);
-            tmem_wait_ld();
+                for (int c = 0; c < NT; c += 16) {
+                    uint32_t r0[16], r1[16], r2[16];
+                    const uint32_t t0 = tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * AST + c;
+                    tmem_ld16(t0, r0);
+                    tmem_ld16(t0 + NT, r1);
+                    tmem_ld16(t0 + 2 * NT, r2);
+                    tmem_wait_ld();
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++)
+                    for (int i = 0; i < 16; i++) {
+                        reg_fence(r0[i]);
+                        reg_fence(r1[i]);
+                        reg_fence(r2[i]);
+                        const float v0 = __shfl_up_sync(0xFFFFFFFFu, __uint_as_float(r0[i]), 1);
+                        const float v2 = __shfl_down_sync(0xFFFFFFFFu, __uint_as_float(r2[i]), 1);
+                        acc[mt][c + i] = (lane == 0 ? 0.f : v0) + __uint_as_float(r1[i]) + (lane == 31 ? 0.f : v2);
+                    }
+                    // the rows at the warp's edges feed the neighbouring warps
+                    if (lane == 31) {
+                        float4* e = reinterpret_cast<float4*>(ex + ((mt * 4 + warp) * 2 + 0) * NT + c);
 #pragma unroll
-                for (int c = 0; c < NT; c++) reg_fence(r[mt][c]);
+                        for (int i = 0; i < 4; i++)
+                            e[i] = make_float4(__uint_as_float(r0[4 * i]), __uint_as_float(r0[4 * i + 1]),
+                                               __uint_as_float(r0[4 * i + 2]), __uint_as_float(r0[4 * i + 3]));
+                    } else if (lane == 0) {
+                        float4* e = reinterpret_cast<float4*>(ex + ((mt * 4 + warp) * 2 + 1) * NT + c);
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            e[i] = make_float4(__uint_as_float(r2[4 * i]), __uint_as_float(r2[4 * i + 1]),
+                                               __uint_as_float(r2[4 * i + 2]), __uint_as_float(r2[4 * i + 3]));
+                    }
+                }
             fence_before_sync();
             mbar_arrive(&acce[buf]);
+            epi_sync();  // the edge rows are in `ex` (double-buffered: the next plane writes the other half)
+            if ((lane == 0 && warp > 0) || (lane == 31 && warp < 3)) {
+                const int src = lane == 0 ? ((warp - 1) * 2 + 0) : ((warp + 1) * 2 + 1);
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++) fwd_store<NT, OUTM>(a, r[mt], I, P0 + mt * kTileM + tid, co0);
+                for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                    for (int c = 0; c < NT; c++) acc[mt][c] += ex[(mt * 4 * 2 + src) * NT + c];
+            }
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++) {
+                if (pos[mt] < 0) continue;
+                if constexpr (OUTM == OUT_STORE) {
+                    bf16* dst = a.out + ((int64_t)I * g.plane + pos[mt]) * a.cout + co0;
+#pragma unroll
+                    for (int c = 0; c < NT; c += 8)
+                        *reinterpret_cast<uint4*>(dst + c) =
+                            make_uint4(pack_bf16(acc[mt][c + 0], acc[mt][c + 1]), pack_bf16(acc[mt][c + 2], acc[mt][c + 3]),
+                                       pack_bf16(acc[mt][c + 4], acc[mt][c + 5]), pack_bf16(acc[mt][c + 6], acc[mt][c + 7]));
+                } else {
+                    if constexpr (!kPre) fetch(I, mt, pre[0]);
+                    bf16* base = a.fine + ((int64_t)(2 * I - 1) * fplane + fofs[mt]) * a.cout + co0;
+#pragma unroll
+                    for (int c8 = 0; c8 < NT / 8; c8++)
+#pragma unroll
+                        for (int ch = 0; ch < 8; ch++) {
+                            const uint4 o = pre[kPre ? mt : 0][c8][ch];
+                            const float* v = &acc[mt][c8 * 8];
+                            *reinterpret_cast<uint4*>(base + child_off(f, fplane, ch) * a.cout + c8 * 8) =
+                                make_uint4(pack_bf16(bf16_lo(o.x) + v[0], bf16_hi(o.x) + v[1]),
+                                           pack_bf16(bf16_lo(o.y) + v[2], bf16_hi(o.y) + v[3]),
+                                           pack_bf16(bf16_lo(o.z) + v[4], bf16_hi(o.z) + v[5]),
+                                           pack_bf16(bf16_lo(o.w) + v[6], bf16_hi(o.w) + v[7]));
+                        }
+                }
+            }
+            if constexpr (kPre) {
+                if (I < I1) {
+#pragma unroll
+                    for (int mt = 0; mt < MT; mt++)
+                        if (pos[mt] >= 0) fetch(I + 1, mt, pre[mt]);
+                }
+            }
         }
     }
     fence_before_sync();
@@ -597,10 +672,13 @@ __global__ void __launch_bounds__(in_threads(MT)) k_conv_in(InArgs a) {
         __syncwarp();
     } else {
         // ---- epilogue: BF16 16-channel rows ----
-        FwdArgs fa{};
-        fa.g = g;
-        fa.cout = 16;
-        fa.out = a.out;
+        int pos[MT];  // in-plane output position of this thread's row, -1 if none
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) {
+            const int pp = P0 + mt * kTileM + tid;
+            const int J = pp / g.W, K = pp - J * g.W;
+            pos[mt] = pp < g.plane && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2 ? pp : -1;
+        }
         uint32_t fph = 0;
         for (int I = I0; I <= I1; I++) {
             const int buf = (I - I0) & 1;
@@ -619,7 +697,15 @@ __global__ void __launch_bounds__(in_threads(MT)) k_conv_in(InArgs a) {
             fence_before_sync();
             mbar_arrive(&acce[buf]);
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++) fwd_store<16, OUT_STORE>(fa, r[mt], I, P0 + mt * kTileM + tid, 0);
+            for (int mt = 0; mt < MT; mt++) {
+                if (pos[mt] < 0) continue;
+                uint4* dst = reinterpret_cast<uint4*>(a.out + ((int64_t)I * g.plane + pos[mt]) * 16);
+                const float* v = reinterpret_cast<const float*>(r[mt]);
+                dst[0] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                                    pack_bf16(v[6], v[7]));
+                dst[1] = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]),
+                                    pack_bf16(v[14], v[15]));
+            }
         }
     }
     fence_before_sync();
@@ -642,26 +728,6 @@ struct OutArgs {
 
 // 4 epilogue warps, producer, one MMA warp per M tile
 __host__ __device__ constexpr int out_threads(int mt) { return (5 + mt) * 32; }
-constexpr int kOutStride = 126;   // outputs per 128-row M tile (the tile's first and last rows only feed neighbours)
-
-__host__ __device__ inline int out_rows(const Geom& g, int mt) { return (mt - 1) * kOutStride + kTileM + 2 * g.W; }
-
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-
-// true in every epilogue thread if it is true in any (named barrier 1, the
-// 128 epilogue threads)
-__device__ __forceinline__ bool epi_any(bool v) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, 1, 128, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(r)
-        : "r"((uint32_t)v)
-        : "memory");
-    return r != 0;
-}
 
 // dec0 forward: 16 -> 1 channel, z = res + conv.  The 9 (di, dj) shifts are
 // start addresses of the A operand (rows of a staged plane, as in
@@ -678,7 +744,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_const
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
-    const int rows = out_rows(g, MT);
+    const int rows = strip_rows(g, MT);
     const int NTL = box_count(rows), BR = box_height(rows);
     const int RP = NTL * BR;
     const uint32_t SB = 2u * RP * 16;
@@ -783,6 +849,24 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_const
         __syncwarp();
     } else {
         // ---- epilogue: D columns 0..2 to shared memory, out[p] = D[p-1][0] + D[p][1] + D[p+1][2] ----
+        int cof[MT];  // cell of this thread's output within a plane of internal cells, -1 if none
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) {
+            const int pp = P0 + mt * kOutStride + tid;
+            const int Jr = pp / g.W, Kc = pp - Jr * g.W;
+            cof[mt] = tid < kOutStride && pp < g.plane && Jr >= 1 && Jr <= g.n1 && Kc >= 1 && Kc <= g.n2
+                          ? (Jr - 1) * g.n2 + (Kc - 1)
+                          : -1;
+        }
+        const int64_t cplane = (int64_t)g.n1 * g.n2;
+        // the residual term of plane I is loaded while plane I's MMAs run
+        float res[MT];
+        auto fetch = [&](int I) {
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++)
+                res[mt] = a.res32 && cof[mt] >= 0 ? a.res32[(int64_t)(I - 1) * cplane + cof[mt]] : 0.f;
+        };
+        fetch(I0);
         uint32_t fph = 0;
         for (int I = I0; I <= I1; I++) {
             const int buf = (I - I0) & 1;
@@ -807,18 +891,11 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_const
             epi_sync();  // d[] complete (double-buffered: the next plane writes the other half)
 #pragma unroll
             for (int mt = 0; mt < MT; mt++) {
-                if (tid >= kOutStride) continue;
+                if (cof[mt] < 0) continue;
                 const float* dm = d + (mt * kTileM + tid) * 3;
-                const float v = dm[0] + dm[3 + 1] + dm[6 + 2];
-                const int pp = P0 + mt * kOutStride + tid;
-                if (pp < g.plane) {
-                    const int Jr = pp / g.W, Kc = pp - Jr * g.W;
-                    if (Jr >= 1 && Jr <= g.n1 && Kc >= 1 && Kc <= g.n2) {
-                        const int64_t c = ((int64_t)(I - 1) * g.n1 + (Jr - 1)) * g.n2 + (Kc - 1);
-                        a.out32[c] = (a.res32 ? a.res32[c] : 0.f) + v;
-                    }
-                }
+                a.out32[(int64_t)(I - 1) * cplane + cof[mt]] = res[mt] + (dm[0] + dm[3 + 1] + dm[6 + 2]);
             }
+            if (I < I1) fetch(I + 1);
         }
     }
     fence_before_sync();
@@ -1126,7 +1203,8 @@ __global__ void k_adam(int64_t n, float* __restrict__ w, const float* __restrict
     }
 }
 
-// master weights [27][cout][cin] -> packed bf16 [nz][27][CINK/8][NT][8].
+// master weights [27][cout][cin] -> packed bf16 [nz][9 (di,dj)][CINK/8][3 dk][NT][8]
+// (the B operand of k_conv_fwd: for one (di, dj) and K chunk, N rows dk NT + n).
 // flip: the data-gradient convolution (input cout channels, output cin),
 // W'[t][o][i] = W[26 - t][i][o].
 __global__ void k_pack(const float* __restrict__ W, int cin, int cout, int CINK, int NT, int nz, int flip,
@@ -1140,10 +1218,13 @@ __global__ void k_pack(const float* __restrict__ W, int cin, int cout, int CINK,
         r /= 8;
         const int n = (int)(r % NT);
         r /= NT;
+        const int dk = (int)(r % 3);
+        r /= 3;
         const int kc = (int)(r % KC);
         r /= KC;
-        const int t = (int)(r % kTaps);
-        const int z = (int)(r / kTaps);
+        const int g9 = (int)(r % 9);
+        const int z = (int)(r / 9);
+        const int t = 3 * g9 + dk;
         const int o = z * NT + n, i = kc * 8 + e;
         float v = 0.f;
         if (!flip) {
@@ -1242,15 +1323,36 @@ __global__ void k_warm(int64_t n, const double* __restrict__ diag, const double*
 // ---------------------------------------------------------------------------
 // host side: launch configuration and dispatch
 static size_t fwd_smem(int cin, int nt, const Geom& g, int mt, int slots) {
-    const int rows = fwd_rows(g, mt);
+    const int rows = strip_rows(g, mt);
     const int RP = box_count(rows) * box_height(rows);
-    return (size_t)kTaps * cin * nt * 2 + slots * (size_t)(cin / 8) * RP * 16 + (2 * kMaxSlots + 5) * 8 + 16;
+    return (size_t)kTaps * cin * nt * 2 + slots * (size_t)(cin / 8) * RP * 16 + 2 * (size_t)mt * 4 * 2 * nt * 4 +
+           (2 * kMaxSlots + 5) * 8 + 16;
 }
 
-// two 128-position tiles per step on planes wider than two tiles, when a
-// 4-slot ring of the wider plane segments still fits
+// two M tiles per step on planes wider than two tiles, when a 4-slot ring of
+// the wider plane segments still fits
 static int pick_mt(const Geom& g, int cin, int nt) {
-    return g.plane > 2 * kTileM && fwd_smem(cin, nt, g, 2, 4) <= kMaxSmem ? 2 : 1;
+    return g.plane > 2 * kOutStride && fwd_smem(cin, nt, g, 2, 4) <= kMaxSmem ? 2 : 1;
+}
+
+// Planes per CTA of a plane-marching grid with `units` CTAs per chunk of
+// planes: the choice that minimises the modelled time waves x (planes + 3)
+// (a CTA stages two planes more than it computes, plus its set-up), waves =
+// ceil(units x chunks / resident CTAs).
+static int pick_ppc(int n0, int64_t units, int64_t resident) {
+    int best = n0;
+    int64_t best_cost = INT64_MAX;
+    for (int chunks = 1; chunks <= n0; chunks++) {
+        const int ppc = (n0 + chunks - 1) / chunks;
+        if ((n0 + ppc - 1) / ppc != chunks) continue;
+        const int64_t waves = (units * chunks + resident - 1) / resident;
+        const int64_t cost = waves * (ppc + 3);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = ppc;
+        }
+    }
+    return best;
 }
 
 // TMA map of a padded channels-last activation [total][C] (bf16): boxes of 8
@@ -1319,19 +1421,13 @@ static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap&
         while (slots > 4 && fwd_smem(CIN, NT, a0.g, MT, slots) > kMaxSmem) slots--;
         size_t smem = fwd_smem(CIN, NT, a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
-        const uint32_t acols = 2 * MT * NT;
-        const uint32_t cols = acols <= 32 ? 32 : (acols <= 64 ? 64 : (acols <= 128 ? 128 : 256));
+        const uint32_t acols = 2 * MT * (3 * NT <= 64 ? 64 : 128);
+        const uint32_t cols = acols <= 128 ? 128 : (acols <= 256 ? 256 : 512);
         int occ = 0, rc;
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, fwd_threads(MT)))) return rc;
-        // about four waves of CTAs; a CTA marches at least two planes (it
-        // stages two more than it computes)
         const int n0 = a0.g.n0;
-        const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
-        const int64_t target = (int64_t)ctx->num_sms * occ * 4;
-        int chunks = (int)std::min<int64_t>(
-            n0, std::max<int64_t>(1, (target + (int64_t)tiles * nz - 1) / ((int64_t)tiles * nz)));
-        int ppc = (n0 + chunks - 1) / chunks;
-        ppc = std::max(ppc, std::min(n0, 2));
+        const int tiles = (a0.g.plane + MT * kOutStride - 1) / (MT * kOutStride);
+        const int ppc = pick_ppc(n0, (int64_t)tiles * nz, (int64_t)ctx->num_sms * occ);
         lc.ppc = ppc;
         lc.occ = occ;
         lc.mt = MT;
@@ -1353,7 +1449,7 @@ static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap&
 static int launch_fwd(dare_ctx* ctx, LaunchCfg& lc, int cin, int nt, int nz, int outm, const FwdArgs& a) {
     const int mt = pick_mt(a.g, cin, nt);
     CUtensorMap tmap;
-    int rc = act_map(ctx, &tmap, a.in, cin, a.g.total, box_height(fwd_rows(a.g, mt)));
+    int rc = act_map(ctx, &tmap, a.in, cin, a.g.total, box_height(strip_rows(a.g, mt)));
     if (rc) return rc;
 #define DARE_FWD(CI, N, OM)                                                                       \
     if (cin == CI && nt == N && outm == OM)                                                       \
@@ -1442,9 +1538,7 @@ static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a0) {
         // (the launch checks above keep the ring at >= 4 planes: 3 in use + 1 loading)
         const int n0 = a0.g.n0;
         const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
-        const int64_t target = (int64_t)ctx->num_sms * occ * 4;
-        const int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + tiles - 1) / tiles));
-        const int ppc = std::max((n0 + chunks - 1) / chunks, std::min(n0, 2));
+        const int ppc = pick_ppc(n0, tiles, (int64_t)ctx->num_sms * occ);
         lc.ppc = ppc;
         lc.occ = occ;
         lc.mt = MT;
@@ -1473,7 +1567,7 @@ static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a, const float*
 }
 
 static size_t out_smem(const Geom& g, int mt, int slots) {
-    const int rows = out_rows(g, mt);
+    const int rows = strip_rows(g, mt);
     const int RP = box_count(rows) * box_height(rows);
     return 9 * 2 * 16 * 16 + slots * (size_t)2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 + (2 * kMaxSlots + 5) * 8 +
            16;
@@ -1496,9 +1590,7 @@ static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, out_threads(MT)))) return rc;
         const int n0 = a0.g.n0;
         const int tiles = (a0.g.plane + MT * kOutStride - 1) / (MT * kOutStride);
-        const int64_t target = (int64_t)ctx->num_sms * occ * 4;
-        const int chunks = (int)std::min<int64_t>(n0, std::max<int64_t>(1, (target + tiles - 1) / tiles));
-        const int ppc = std::max((n0 + chunks - 1) / chunks, std::min(n0, 2));
+        const int ppc = pick_ppc(n0, tiles, (int64_t)ctx->num_sms * occ);
         lc.ppc = ppc;
         lc.occ = occ;
         lc.mt = MT;
@@ -1512,7 +1604,7 @@ static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     a.ppc = lc.ppc;
     a.slots = lc.slots;
     CUtensorMap tmap;
-    int rc = act_map(ctx, &tmap, a.in, 16, a.g.total, box_height(out_rows(a.g, MT)));
+    int rc = act_map(ctx, &tmap, a.in, 16, a.g.total, box_height(strip_rows(a.g, MT)));
     if (rc) return rc;
     kern<<<lc.grid, out_threads(MT), lc.smem, ctx->stream>>>(tmap, a);
     DARE_LAUNCHED(ctx);
@@ -1557,13 +1649,10 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
     a.g = net->geo[L.level];
     if (L.level > 0) a.fg = net->geo[L.level - 1];
     a.in = in;
-    a.in32 = in32;
     a.w = L.wf;
     a.cout = L.coutk;
     a.out = out;
     a.fine = fine;
-    a.out32 = out32;
-    a.res32 = res32;
     a.err = net->err;
     return launch_fwd(net->ctx, L.fwd, L.cink, L.nt, L.coutk / L.nt, outm, a);
 }
@@ -1583,7 +1672,6 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
     FwdArgs a{};
     a.g = net->geo[L.level];
     a.in = dy;
-    a.in32 = dy32;
     a.w = L.wb;
     a.cout = L.cink;
     a.out = dx;

@@ -57,6 +57,13 @@ inline Geom make_geom(int n0, int n1, int n2) {
 __host__ __device__ inline int stage_rows(const Geom& g) { return kTileM + 2 * g.W + 2; }
 // ... and for MT consecutive tiles
 __host__ __device__ inline int fwd_rows(const Geom& g, int mt) { return mt * kTileM + 2 * g.W + 2; }
+// Kernels with the three dk taps in the MMA's N dimension: D row m of a
+// 128-row M tile is position P - 1 + m, and out(P + m - 1) = D[m-1][dk 0] +
+// D[m][dk 1] + D[m+1][dk 2] for m = 1 .. 126, so M tiles overlap by two rows.
+constexpr int kOutStride = 126;
+// rows staged per input plane for MT such tiles: the (j) halo of W rows on
+// either side, no (k) halo
+__host__ __device__ inline int strip_rows(const Geom& g, int mt) { return (mt - 1) * kOutStride + kTileM + 2 * g.W; }
 // Row pitch of a staged plane: rounded to 8 rows, then offset so that the
 // 16-byte chunks of one row written by neighbouring threads fall into
 // different shared-memory banks.
