@@ -76,6 +76,26 @@ def _random_case(kind, seed=0):
             faces.append(np.concatenate([f, f[tuple(first)]], axis=d))
         c["face_D"] = faces
         return c
+    if kind.startswith("tiles3d"):
+        # several 31 x 8 (k, j) assembly tiles and plane runs; quantised phi
+        # (equal neighbours: r = +-inf and 0/0 in the limiters), face
+        # velocities with exact zeros, heterogeneous face D, mixed boundaries
+        n = (23, 19, 70) if kind == "tiles3d" else (9, 17, 65)
+        periodic = (1, 0, 0) if kind == "tiles3d" else (1, 1, 1)
+        phi = rng.integers(0, 4, size=tuple(x + 4 for x in n)) / 4.0
+        fv, fd = [], []
+        for d in range(3):
+            shape = tuple(x + (1 if e == d else 0) for e, x in enumerate(n))
+            v = rng.normal(size=shape)
+            v[rng.random(shape) < 0.05] = 0.0
+            fv.append(v)
+            fd.append(10.0 ** rng.uniform(-4, -2, size=shape))
+        c = {"n": n, "size": (1.0, 0.7, 2.0), "periodic": periodic, "dt": 0.03, "D": None, "phi0": phi,
+             "phi_old": rng.random(phi.shape), "face_vel": fv, "face_D": fd,
+             "limiter": "VANLEER" if kind == "tiles3d" else "VANALBADA"}
+        if kind == "tiles3d":
+            c["bc"] = {3: (1, 0.5), 4: (2, 0.0), 5: (2, 0.0), 6: (1, -1.0)}
+        return c
     if kind == "mixed3d":
         n = (5, 7, 9)
         phi = rng.random(tuple(x + 4 for x in n)) - 0.5
@@ -95,7 +115,7 @@ def _random_case(kind, seed=0):
 
 
 ASM_CASES = ["diffusion3d", "tvd3d-VANLEER", "tvd3d-CDS", "tvd3d-UPWIND", "tvd3d-MINMOD", "tvd3d-VANALBADA",
-             "facediff3d", "mixed3d", "tvd2d", "tvd1d"]
+             "facediff3d", "mixed3d", "tiles3d", "tiles3d-periodic", "tvd2d", "tvd1d"]
 
 
 @pytest.mark.parametrize("kind", ASM_CASES)
