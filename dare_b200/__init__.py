@@ -31,6 +31,9 @@ LIB_PATH = os.path.join(HERE, "libdare_gpu.so")
 CENTER, WEST, EAST, SOUTH, NORTH, BOTTOM, TOP = range(7)
 BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN = 0, 1, 2
 LIMITER = {"CDS": 0, "UPWIND": 1, "VANALBADA": 2, "MINMOD": 3, "VANLEER": 4}
+# time schemes of the div(...) terms (Equations/TimeDiscretizationSchemes.h)
+SCHEME = {"EULER_BACKWARD": 0, "EULER_FORWARD": 1, "CRANK_NICHOLSON": 2, "ADAMS_BASHFORTH": 3,
+          "ADAMS_MOULTON": 4}
 PREC_NONE, PREC_JACOBI = 0, 1
 PRECISION_FP64, PRECISION_FP32_REFINE = 0, 1
 SOLVE_STATUS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "nan"}
@@ -46,7 +49,7 @@ class GridInfo(C.Structure):
 class AssemblyDesc(C.Structure):
     _fields_ = [("dt", C.c_double), ("diffusion", C.c_int), ("D", C.c_double), ("face_D", C.c_void_p * 3),
                 ("convection", C.c_int), ("limiter", C.c_int), ("vel", C.c_double * 3),
-                ("face_vel", C.c_void_p * 3)]
+                ("face_vel", C.c_void_p * 3), ("scheme", C.c_int)]
 
 
 class SolverParams(C.Structure):
@@ -378,6 +381,7 @@ class Assembly:
     vel: tuple | None = None           # constant velocity
     face_vel: tuple | None = None      # 3 device pointers (int) or DeviceArray
     limiter: str = "VANLEER"
+    scheme: str = "EULER_BACKWARD"     # time scheme of the div(...) terms (SCHEME)
 
     def to_c(self) -> AssemblyDesc:
         a = AssemblyDesc()
@@ -398,6 +402,7 @@ class Assembly:
             for d, v in enumerate(self.vel):
                 a.vel[d] = float(v)
         a.limiter = LIMITER[self.limiter]
+        a.scheme = SCHEME[self.scheme]
         return a
 
 

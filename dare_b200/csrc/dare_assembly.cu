@@ -31,7 +31,24 @@ struct AsmParams {
     double bc_value[6];
     double tt;      // (V * 1) / dt, the DDT weight (evaluated once on the host: same IEEE result)
     double dn[3];   // 1 / dx per dimension (Gradient_Cartesian.inl:30-34)
+    int scheme;     // DARE_SCHEME_* of the div(...) terms
+    int nexp;       // its explicit levels T
+    double w[3];    // its weights w[0..T] (TimeDiscretizationSchemes.h:29-76)
 };
+
+// Weights of the Divergence time schemes (TimeDiscretizationSchemes.h:29-76);
+// returns the number of explicit levels, -1 for an unknown scheme.
+static int scheme_weights(int scheme, double w[3]) {
+    w[0] = w[1] = w[2] = 0.;
+    switch (scheme) {
+    case DARE_SCHEME_EULER_BACKWARD: w[0] = 1.; return 0;
+    case DARE_SCHEME_EULER_FORWARD: w[1] = 1.; return 1;
+    case DARE_SCHEME_CRANK_NICHOLSON: w[0] = 0.5; w[1] = 0.5; return 1;
+    case DARE_SCHEME_ADAMS_BASHFORTH: w[1] = 1.5; w[2] = -0.5; return 2;
+    case DARE_SCHEME_ADAMS_MOULTON: w[0] = 5. / 12.; w[1] = 8. / 12.; w[2] = -1. / 12.; return 2;
+    default: return -1;
+    }
+}
 
 __device__ __forceinline__ double limiter_value(int kind, double r) {
     switch (kind) {
@@ -209,10 +226,15 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             double sc[7];
             apply_divergence<DIM>(g, nb, cf, sc);
 #pragma unroll
-            for (int p = 0; p < 7; p++) sc[p] *= 1.;
+            for (int p = 0; p < 7; p++) sc[p] *= a.w[0];           // s_c *= weight[0]
             double srhs = g.area[0] * (rr[DARE_EAST] - rr[DARE_WEST]);
             if (DIM > 1) srhs += g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
             if (DIM > 2) srhs += g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
+            for (int t = 1; t <= a.nexp; t++) {                // explicit levels (copies of level 0)
+                srhs += a.w[t] * g.area[0] * (rr[DARE_EAST] - rr[DARE_WEST]);
+                if (DIM > 1) srhs += a.w[t] * g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
+                if (DIM > 2) srhs += a.w[t] * g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
+            }
 #pragma unroll
             for (int p = 0; p < 7; p++) coef[p] += sc[p];       // MatrixBlock::Add
             rhs += srhs;
@@ -245,6 +267,8 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             }
             double sc[7];
             apply_divergence<DIM>(g, nb, cf, sc);
+#pragma unroll
+            for (int p = 0; p < 7; p++) sc[p] *= a.w[0];           // s_c *= weight[0]
 #pragma unroll
             for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
             rhs += -1. * 0.;
@@ -428,9 +452,18 @@ __global__ void __launch_bounds__(256, 3) k_assemble3(GridDev g, AsmParams a, co
             }
             double sc[7];
             apply_divergence<3>(g, nb, cf, sc);
+            if (a.scheme != DARE_SCHEME_EULER_BACKWARD) {     // s_c *= weight[0] (1: identity)
+#pragma unroll
+                for (int p = 0; p < 7; p++) sc[p] *= a.w[0];
+            }
             double srhs = g.area[0] * (rr[DARE_EAST] - rr[DARE_WEST]);
             srhs += g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
             srhs += g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
+            for (int t = 1; t <= a.nexp; t++) {                // explicit levels (copies of level 0)
+                srhs += a.w[t] * g.area[0] * (rr[DARE_EAST] - rr[DARE_WEST]);
+                srhs += a.w[t] * g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
+                srhs += a.w[t] * g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
+            }
 #pragma unroll
             for (int p = 0; p < 7; p++) coef[p] += sc[p];       // MatrixBlock::Add
             rhs += srhs;
@@ -466,6 +499,10 @@ __global__ void __launch_bounds__(256, 3) k_assemble3(GridDev g, AsmParams a, co
             }
             double sc[7];
             apply_divergence<3>(g, nb, cf, sc);
+            if (a.scheme != DARE_SCHEME_EULER_BACKWARD) {     // s_c *= weight[0] (1: identity)
+#pragma unroll
+                for (int p = 0; p < 7; p++) sc[p] *= a.w[0];
+            }
 #pragma unroll
             for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
             rhs += -1. * 0.;
@@ -534,6 +571,9 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
         a.bc_value[f] = s->bc_value[f];
     }
     a.tt = a.dt > 0. ? (g.volume * 1.) / a.dt : 0.;
+    a.scheme = desc->scheme;
+    a.nexp = scheme_weights(desc->scheme, a.w);
+    if (a.nexp < 0) return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: unknown time scheme");
     for (int d = 0; d < 3; d++) a.dn[d] = 1. / g.dx[d];
     for (int d = 0; d < g.dim; d++) {
         if (a.diffusion == 2 && !a.face_D[d]) return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: face_D missing");

@@ -58,6 +58,18 @@ extern "C" {
 #define DARE_LIMITER_MINMOD 3
 #define DARE_LIMITER_VANLEER 4
 
+/* ---- time schemes of the Divergence operators ------------------------------
+ * Equations/TimeDiscretizationSchemes.h:29-76, weights w[0..T]: the implicit
+ * coefficients of div(...) are scaled by w[0], and each explicit level t >= 1
+ * adds w[t] * A * (rhs_E - rhs_W + ...) of the operator's face stencil
+ * (Grid/Cartesian/Divergence_Cartesian.inl:186-205; the levels are copies of
+ * the level-0 stencil, :61-62).  DDT keeps its implicit weights (1, 1). */
+#define DARE_SCHEME_EULER_BACKWARD 0  /* (1) */
+#define DARE_SCHEME_EULER_FORWARD 1   /* (0, 1) */
+#define DARE_SCHEME_CRANK_NICHOLSON 2 /* (0.5, 0.5) */
+#define DARE_SCHEME_ADAMS_BASHFORTH 3 /* (0, 1.5, -0.5) */
+#define DARE_SCHEME_ADAMS_MOULTON 4   /* (5/12, 8/12, -1/12) */
+
 /* ---- preconditioners (right, TrilinosSolver.inl:84-85) --------------------- */
 #define DARE_PREC_NONE 0
 #define DARE_PREC_JACOBI 1
@@ -107,6 +119,7 @@ typedef struct {
     int limiter;                     /* DARE_LIMITER_* */
     double vel[3];
     const double* face_vel[3];
+    int scheme;                      /* DARE_SCHEME_*, time scheme of both div(...) terms */
 } dare_assembly_desc;
 
 typedef struct {

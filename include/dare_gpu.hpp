@@ -147,6 +147,15 @@ private:
 enum class Limiter { CDS = DARE_LIMITER_CDS, UPWIND = DARE_LIMITER_UPWIND, VANALBADA = DARE_LIMITER_VANALBADA,
                      MINMOD = DARE_LIMITER_MINMOD, VANLEER = DARE_LIMITER_VANLEER };
 
+// Time discretisation of the div(...) terms (Equations/TimeDiscretizationSchemes.h).
+enum class TimeScheme : int {
+    EULER_BACKWARD = DARE_SCHEME_EULER_BACKWARD,
+    EULER_FORWARD = DARE_SCHEME_EULER_FORWARD,
+    CRANK_NICHOLSON = DARE_SCHEME_CRANK_NICHOLSON,
+    ADAMS_BASHFORTH = DARE_SCHEME_ADAMS_BASHFORTH,
+    ADAMS_MOULTON = DARE_SCHEME_ADAMS_MOULTON
+};
+
 // The fused per-cell functor: mb = ddt(field); mb += div(TVD(vel) * field);
 // mb -= div(D, grad(mb)); then the boundary folding of Trilinos::SetBC.
 struct Assembly {
@@ -158,6 +167,7 @@ struct Assembly {
     std::array<double, 3> velocity{0., 0., 0.};
     const double* face_velocity[3] = {nullptr, nullptr, nullptr};  // device face arrays (optional)
     Limiter limiter = Limiter::VANLEER;
+    TimeScheme scheme = TimeScheme::EULER_BACKWARD;
 
     dare_assembly_desc Desc() const {
         dare_assembly_desc d{};
@@ -166,6 +176,7 @@ struct Assembly {
         d.D = D;
         d.convection = face_velocity[0] ? 2 : (convection ? 1 : 0);
         d.limiter = (int)limiter;
+        d.scheme = (int)scheme;
         for (int i = 0; i < 3; i++) {
             d.face_D[i] = face_D[i];
             d.face_vel[i] = face_velocity[i];

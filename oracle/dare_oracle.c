@@ -228,6 +228,21 @@ static int64_t upper_face(const dor_grid* g, int d, int64_t i) {
     return (g->periodic[d] && i + 1 == g->n[d]) ? 0 : i + 1;
 }
 
+int dor_scheme_weights(int scheme, double w[3]) {
+    /* TimeDiscretizationSchemes.h: EULER_BACKWARD :29-36 (1), EULER_FORWARD
+     * :38-45 (0, 1), CRANK_NICHOLSON :47-54 (0.5, 0.5), ADAMS_BASHFORT :56-65
+     * (0, 1.5, -0.5), ADAMS_MOULTON :67-76 (5/12, 8/12, -1/12) */
+    w[0] = w[1] = w[2] = 0.;
+    switch (scheme) {
+    case DOR_SCHEME_EULER_BACKWARD: w[0] = 1.; return 0;
+    case DOR_SCHEME_EULER_FORWARD: w[0] = 0.; w[1] = 1.; return 1;
+    case DOR_SCHEME_CRANK_NICHOLSON: w[0] = 0.5; w[1] = 0.5; return 1;
+    case DOR_SCHEME_ADAMS_BASHFORTH: w[0] = 0.; w[1] = 1.5; w[2] = -0.5; return 2;
+    case DOR_SCHEME_ADAMS_MOULTON: w[0] = 5. / 12.; w[1] = 8. / 12.; w[2] = -1. / 12.; return 2;
+    default: return -1;
+    }
+}
+
 /* One cell of the composed user functor
  *     mb  = ddt(field);                      DDT.inl:39-81, Set  MatrixBlock_Cartesian.inl:480-497
  *     mb += div(TVD(vel) * field);           TVD_Cartesian.inl:185-261, Divergence_Cartesian.inl:139-207
@@ -250,6 +265,8 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
     const int64_t lstride[3] = {gn[1] * gn[2], gn[2], 1};
     uint8_t mask = 1;
     for (int d = 0; d < dim; d++) mask |= (uint8_t)((1u << (2 * d + 1)) | (1u << (2 * d + 2)));
+    double w[3];
+    const int T = dor_scheme_weights(a->scheme, w);
     for (int p = 0; p < 7; p++) coef[p] = 0.;
     double rhs = 0.;
 
@@ -264,7 +281,7 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
     }
 
     /* Convection: TVD<Cartesian,SC,Limiter>::operator* then Divergence with
-     * EULER_BACKWARD (weight 1), then MatrixBlock::Add. */
+     * the scheme's weights (EULER_BACKWARD: weight 1), then MatrixBlock::Add. */
     if (a->convection) {
         double nb[7], cc[7], rr[7];
         for (int p = 0; p < 7; p++) nb[p] = cc[p] = rr[p] = 0.;
@@ -326,10 +343,17 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
             sc[DOR_B] = -A[2] * nb[DOR_B];
             sc[DOR_C] -= A[2] * cc[DOR_B];
         }
-        for (int p = 0; p < 7; p++) sc[p] *= 1.;  /* s_c *= weight[0] */
+        for (int p = 0; p < 7; p++) sc[p] *= w[0];  /* s_c *= weight[0] */
         srhs = A[0] * (rr[DOR_E] - rr[DOR_W]);
         if (dim > 1) srhs += A[1] * (rr[DOR_N] - rr[DOR_S]);
         if (dim > 2) srhs += A[2] * (rr[DOR_T] - rr[DOR_B]);
+        /* explicit levels: copies of the level-0 face stencil (f[t] = f[0],
+         * Divergence_Cartesian.inl:61-62), weighted (:196-205) */
+        for (int t = 1; t <= T; t++) {
+            srhs += w[t] * A[0] * (rr[DOR_E] - rr[DOR_W]);
+            if (dim > 1) srhs += w[t] * A[1] * (rr[DOR_N] - rr[DOR_S]);
+            if (dim > 2) srhs += w[t] * A[2] * (rr[DOR_T] - rr[DOR_B]);
+        }
         /* MatrixBlock::Add: MatrixBlock_Cartesian.inl:527-546 */
         for (int p = 0; p < 7; p++) coef[p] += sc[p];
         rhs += srhs;
@@ -377,7 +401,9 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
             sc[DOR_B] = -A[2] * nb[DOR_B];
             sc[DOR_C] -= A[2] * cc[DOR_B];
         }
-        /* the gradient stencil carries no rhs: the diffusion rhs is +0 */
+        for (int p = 0; p < 7; p++) sc[p] *= w[0];  /* s_c *= weight[0] */
+        /* the gradient stencil carries no rhs: the diffusion rhs, explicit
+         * levels included, is +0 */
         for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
         rhs += -1. * 0.;
     }
@@ -410,6 +436,8 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
 int dor_assemble(const dor_assembly* a, const double* phi_conv, const double* phi_old,
                  double* diag, double* rhs, uint8_t* mask) {
     const dor_grid* g = &a->grid;
+    double w[3];
+    if (dor_scheme_weights(a->scheme, w) < 0) return -1;
     for (int d = 0; d < g->dim; d++) {
         if (g->n[d] <= g->num_ghost) return -1;
         if (!g->periodic[d]) {

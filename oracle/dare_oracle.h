@@ -57,7 +57,17 @@ typedef struct {
     const double* face_vel[3];  /* same face layout as face_D */
     int bc_type[6];             /* faces W,E,S,N,B,T */
     double bc_value[6];
+    int scheme;                 /* time scheme of the Divergence operators: DOR_SCHEME_* */
 } dor_assembly;
+
+/* Time discretisation of the Divergence operators (TimeDiscretizationSchemes.h:29-76):
+ * weights w[0..T]; the implicit coefficients are scaled by w[0] and every
+ * explicit level t >= 1 adds w[t] * A * (rhs_E - rhs_W) ... of its face
+ * stencil (Divergence_Cartesian.inl:186-205). */
+enum { DOR_SCHEME_EULER_BACKWARD = 0, DOR_SCHEME_EULER_FORWARD = 1, DOR_SCHEME_CRANK_NICHOLSON = 2,
+       DOR_SCHEME_ADAMS_BASHFORTH = 3, DOR_SCHEME_ADAMS_MOULTON = 4 };
+/* Number of explicit levels T and the weights w[0..T]; -1 for an unknown scheme. */
+int dor_scheme_weights(int scheme, double w[3]);
 
 typedef struct {
     double tol;        /* absolute tolerance on ||r||_2 (stop criterion RNORM) */

@@ -22,6 +22,9 @@ LIB_PATH = os.path.join(HERE, "libdare_oracle.so")
 C_, W, E, S, N, B, T = range(7)
 BC_NONE, BC_DIRICHLET, BC_NEUMANN = 0, 1, 2
 LIM_CDS, LIM_UPWIND, LIM_VANALBADA, LIM_MINMOD, LIM_VANLEER = range(5)
+# time schemes of the Divergence operators (TimeDiscretizationSchemes.h:29-76)
+(SCHEME_EULER_BACKWARD, SCHEME_EULER_FORWARD, SCHEME_CRANK_NICHOLSON, SCHEME_ADAMS_BASHFORTH,
+ SCHEME_ADAMS_MOULTON) = range(5)
 PREC_NONE, PREC_JACOBI = 0, 1
 
 
@@ -48,6 +51,7 @@ class Assembly(C.Structure):
         ("face_vel", C.c_void_p * 3),
         ("bc_type", C.c_int * 6),
         ("bc_value", C.c_double * 6),
+        ("scheme", C.c_int),
     ]
 
 
@@ -180,8 +184,9 @@ class AssemblyDesc:
     """Python-side description mirroring ``dor_assembly``; keeps arrays alive."""
 
     def __init__(self, grid: Grid, dt=0.0, D=None, face_D=None, vel=None, face_vel=None,
-                 limiter=LIM_VANLEER, bc=None):
+                 limiter=LIM_VANLEER, bc=None, scheme=SCHEME_EULER_BACKWARD):
         self.grid = grid
+        self.scheme = scheme
         self.dt = dt
         self.D = D
         self.face_D = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
@@ -212,6 +217,7 @@ class AssemblyDesc:
             for d in range(len(self.vel)):
                 a.vel[d] = float(self.vel[d])
         a.limiter = self.limiter
+        a.scheme = self.scheme
         for face, (kind, value) in self.bc.items():
             a.bc_type[face - 1] = kind
             a.bc_value[face - 1] = value

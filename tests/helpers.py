@@ -17,8 +17,11 @@ def oracle_assembly(og, case, face_D=None):
            "VANLEER": O.LIM_VANLEER}[case.get("limiter", "VANLEER")]
     fv = case.get("face_vel")
     fv = None if fv is None else [np.ascontiguousarray(np.asarray(a), dtype=np.float64) for a in fv]
+    scheme = {"EULER_BACKWARD": O.SCHEME_EULER_BACKWARD, "EULER_FORWARD": O.SCHEME_EULER_FORWARD,
+              "CRANK_NICHOLSON": O.SCHEME_CRANK_NICHOLSON, "ADAMS_BASHFORTH": O.SCHEME_ADAMS_BASHFORTH,
+              "ADAMS_MOULTON": O.SCHEME_ADAMS_MOULTON}[case.get("scheme", "EULER_BACKWARD")]
     return O.AssemblyDesc(og, dt=case.get("dt", 0.0), D=case.get("D"), face_D=face_D, vel=case.get("vel"),
-                          face_vel=fv, limiter=lim, bc=bc)
+                          face_vel=fv, limiter=lim, bc=bc, scheme=scheme)
 
 
 def oracle_timeloop(case, steps, precond=O.PREC_JACOBI, face_D=None, max_it=5000):

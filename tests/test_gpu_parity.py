@@ -47,7 +47,8 @@ def _gpu_case(ctx, case):
         keep += fd
         face_D = tuple(fd)
     asm = D.Assembly(dt=case.get("dt", 0.0), D=case.get("D"), face_D=face_D, vel=case.get("vel"),
-                     face_vel=face_vel, limiter=case.get("limiter", "VANLEER"))
+                     face_vel=face_vel, limiter=case.get("limiter", "VANLEER"),
+                     scheme=case.get("scheme", "EULER_BACKWARD"))
     return g, f, s, asm, keep, dim
 
 
@@ -96,6 +97,15 @@ def _random_case(kind, seed=0):
         if kind == "tiles3d":
             c["bc"] = {3: (1, 0.5), 4: (2, 0.0), 5: (2, 0.0), 6: (1, -1.0)}
         return c
+    if kind.startswith("scheme3d"):
+        # the Divergence time schemes on the 3-D kernel (several tiles)
+        c = _random_case("tiles3d", seed)
+        c["scheme"] = kind.split("-")[1]
+        return c
+    if kind.startswith("scheme2d"):
+        c = _random_case("tvd2d", seed)
+        c["scheme"] = kind.split("-")[1]
+        return c
     if kind == "mixed3d":
         n = (5, 7, 9)
         phi = rng.random(tuple(x + 4 for x in n)) - 0.5
@@ -115,7 +125,9 @@ def _random_case(kind, seed=0):
 
 
 ASM_CASES = ["diffusion3d", "tvd3d-VANLEER", "tvd3d-CDS", "tvd3d-UPWIND", "tvd3d-MINMOD", "tvd3d-VANALBADA",
-             "facediff3d", "mixed3d", "tiles3d", "tiles3d-periodic", "tvd2d", "tvd1d"]
+             "facediff3d", "mixed3d", "tiles3d", "tiles3d-periodic", "tvd2d", "tvd1d",
+             "scheme3d-EULER_FORWARD", "scheme3d-CRANK_NICHOLSON", "scheme3d-ADAMS_BASHFORTH",
+             "scheme3d-ADAMS_MOULTON", "scheme2d-CRANK_NICHOLSON", "scheme2d-ADAMS_MOULTON"]
 
 
 @pytest.mark.parametrize("kind", ASM_CASES)
@@ -214,12 +226,14 @@ def _gpu_timeloop(ctx, case, steps, precond="JACOBI"):
     return hist, iters, g
 
 
-@pytest.mark.parametrize("kind", ["gaussian", "tvd"])
+@pytest.mark.parametrize("kind", ["gaussian", "tvd", "tvd-CRANK_NICHOLSON", "tvd-ADAMS_MOULTON"])
 def test_timeloop_matches_oracle(ctx, kind):
     if kind == "gaussian":
         case = W.gaussian_diffusion(n=20, steps=3)
     else:
         case = W.tvd_convection_diffusion(n=24, steps=3)
+        if "-" in kind:
+            case["scheme"] = kind.split("-")[1]
     hist, iters, g = _gpu_timeloop(ctx, case, 3)
     ohist, oiters = oracle_timeloop(case, 3)
     for a, b in zip(hist, ohist):
