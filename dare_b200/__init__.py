@@ -96,6 +96,11 @@ _SIGS = [
     ("dare_field_device_ptr", _P, [_P, C.c_int]),
     ("dare_field_exchange_halo", C.c_int, [_P]),
     ("dare_field_copy_to_old", C.c_int, [_P]),
+    ("dare_vtk_write", C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(C.c_char_p), C.c_int, C.c_char_p, C.c_char_p,
+                                 C.c_int, C.c_double]),
+    ("dare_vtk_write_host", C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int,
+                                      C.POINTER(C.c_void_p), C.POINTER(C.c_char_p), C.c_int, C.c_char_p,
+                                      C.c_char_p, C.c_int, C.c_double]),
     ("dare_system_create", C.c_int, [_P, C.POINTER(_P)]),
     ("dare_system_destroy", C.c_int, [_P]),
     ("dare_system_set_bc", C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
@@ -503,6 +508,34 @@ def timestep(system: MatrixSystem, field: Field, assembly: Assembly, solver: BiC
            system.grid.ctx.h, "timestep")
     solver.report = rep.as_dict()
     return solver.report
+
+
+def write_vtk(fields, names, base_path: str, grid_name: str, step: int, time: float = -1.0, level: int = 0):
+    """io::VTKWriter(exman, time, step).Write(base_path, &vec...) for fields of one
+    grid: <base_path>/<grid_name>_<step>.pvts plus its piece in the subdirectory
+    <grid_name>_<step>/ (the ghosted grid, one Float64 cell array per field)."""
+    fields = list(fields)
+    names = [str(n) for n in names]
+    if len(fields) != len(names) or not fields:
+        raise ValueError("write_vtk: one name per field")
+    hs = (_P * len(fields))(*[f.h for f in fields])
+    ns = (C.c_char_p * len(names))(*[n.encode() for n in names])
+    ctx = fields[0].grid.ctx.h
+    _check(lib().dare_vtk_write(hs, level, ns, len(fields), base_path.encode(), grid_name.encode(), step, time),
+           ctx, "vtk_write")
+
+
+def write_vtk_host(n, size, num_ghost: int, arrays, names, base_path: str, grid_name: str, step: int,
+                   time: float = -1.0):
+    """The same writer from host arrays over the ghosted grid (no GPU involved)."""
+    dim = len(n)
+    n3 = (C.c_int64 * 3)(*(list(n) + [1] * (3 - dim)))
+    s3 = (C.c_double * 3)(*(list(size) + [1.0] * (3 - dim)))
+    arrays = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in arrays]
+    ps = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    ns = (C.c_char_p * len(names))(*[str(x).encode() for x in names])
+    _check(lib().dare_vtk_write_host(dim, n3, s3, num_ghost, ps, ns, len(arrays), base_path.encode(),
+                                     grid_name.encode(), step, time), None, "vtk_write_host")
 
 
 def face_average(grid: Grid, cell_D_ptr: int, face_ptrs) -> None:

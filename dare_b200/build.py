@@ -38,6 +38,7 @@ SOURCES = {
     "dare_batched.cu": [],
     "dare_unet.cu": [],
     "dare_learned.cu": [],
+    "dare_vtk.cu": [],
 }
 
 

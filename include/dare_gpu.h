@@ -190,6 +190,21 @@ DARE_API int dare_field_exchange_halo(dare_field* f);
 /* Field::CopyDataVectorsToOldTimeStep (Field.inl:88-93) */
 DARE_API int dare_field_copy_to_old(dare_field* f);
 
+/* ---- field output: io::VTKWriter<Cartesian<Dim>>(exman, time, step).Write(base_path, &vec...)
+ *      (IO/VTKWriter.h:73-160, IO/VTKWriter.inl:34-86) for one grid on one rank.
+ *      Writes <base_path>/<grid_name>_<step>.pvts and the piece
+ *      <base_path>/<grid_name>_<step>/<grid_name>_<step>_0.vts: the ghosted grid
+ *      (Grid/Cartesian/VTKOptions_Cartesian.h:146-323), one Float64 cell array per
+ *      field named names[f], "TimeValue" when time >= 0.  base_path and the
+ *      subdirectory are created when missing (one level each). */
+DARE_API int dare_vtk_write(dare_field* const* fields, int level, const char* const* names, int count,
+                            const char* base_path, const char* grid_name, int step, double time);
+/* The same from host arrays over the ghosted grid (num_ghost layers on each
+ * active side, the grid's numbering with the last dimension fastest); needs no GPU. */
+DARE_API int dare_vtk_write_host(int dim, const int64_t n[3], const double size[3], int num_ghost,
+                                 const double* const* data, const char* const* names, int count,
+                                 const char* base_path, const char* grid_name, int step, double time);
+
 /* ---- linear system: the structured 7-diagonal form of Trilinos<SC>'s A, x, B
  *      (MatrixSystem/Trilinos.h:51-314) -------------------------------------- */
 DARE_API int dare_system_create(dare_grid* g, dare_system** out);

@@ -405,3 +405,23 @@ def test_profiling_mode_same_result(ctx):
     for a, b in zip(hist_a, hist_b):
         np.testing.assert_array_equal(a, b)
     assert stats["assemble"][1] == 2 and stats["assemble"][0] > 0
+
+
+def test_vtk_writer_device_matches_host(ctx, tmp_path):
+    """dare_vtk_write (device fields) writes the same bytes as the host-array
+    writer tested in tests/test_vtk_writer.py."""
+    n, size = (9, 6, 7), (1.0, 0.6, 1.4)
+    g = D.Grid(ctx, n, size, 2, (1, 0, 1))
+    rng = np.random.default_rng(11)
+    shape = tuple(x + 4 for x in n)
+    a, b = rng.normal(size=shape).reshape(-1), rng.normal(size=shape).reshape(-1)
+    f1, f2 = D.Field(g, 2), D.Field(g, 2)
+    f1.upload(a, 0)
+    f1.upload(b, 1)
+    f2.upload(b, 0)
+    D.write_vtk([f1, f2], ["phi", "other"], str(tmp_path / "dev"), "Cartesian3D", 7, time=1.5, level=0)
+    D.write_vtk([f1], ["phi_old"], str(tmp_path / "dev"), "Old", 7, level=1)
+    D.write_vtk_host(n, size, 2, [a, b], ["phi", "other"], str(tmp_path / "host"), "Cartesian3D", 7, time=1.5)
+    D.write_vtk_host(n, size, 2, [b], ["phi_old"], str(tmp_path / "host"), "Old", 7)
+    for rel in ("Cartesian3D_7.pvts", "Cartesian3D_7/Cartesian3D_7_0.vts", "Old_7.pvts", "Old_7/Old_7_0.vts"):
+        assert (tmp_path / "dev" / rel).read_bytes() == (tmp_path / "host" / rel).read_bytes(), rel
