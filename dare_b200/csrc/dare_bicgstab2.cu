@@ -55,9 +55,16 @@ MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem) {
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     int tk = n2 > 16 ? 32 : n2 > 8 ? 16 : n2 > 4 ? 8 : n2 > 2 ? 4 : 1;
     int tj = 256 / tk;
+    if (n2 % 2 == 0 && n2 >= 32) {
+        // two cells per thread: 16 x 8 threads on 32 x 8 cells (the same
+        // tile and shared memory as one cell per thread, half the threads)
+        m.cpt = 2;
+        tk = 16;
+        tj = 8;
+    }
     while (tj > 1 && tj / 2 >= n1) tj /= 2;
     m.block = dim3(tk, tj, 1);
-    m.tiles_x = (n2 + tk - 1) / tk;
+    m.tiles_x = (n2 + tk * m.cpt - 1) / (tk * m.cpt);
     m.tiles_y = (n1 + tj - 1) / tj;
     const int64_t tiles = (int64_t)m.tiles_x * m.tiles_y;
     // Longest plane run that still leaves ~4 items per resident block (the
@@ -69,7 +76,7 @@ MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem) {
     if (planes > n0) planes = n0;
     m.planes = planes;
     m.nitems = (int)(tiles * ((n0 + planes - 1) / planes));
-    m.smem = 2 * (size_t)(tk + 2) * (tj + 2) * elem;
+    m.smem = 2 * (size_t)(tk * m.cpt + 2) * (tj + 2) * elem;
     return m;
 }
 

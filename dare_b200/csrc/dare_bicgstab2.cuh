@@ -48,6 +48,7 @@ struct MarchCfg {
     int planes = 1;
     int nitems = 1;
     size_t smem = 0;
+    int cpt = 1;      // cells per thread along k (2: paired 16-byte copies, needs an even n2)
 };
 
 // ---- deterministic grid reduction -----------------------------------------

@@ -360,24 +360,50 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Shared-memory bytes of one marching block for functor K.
+// Shared-memory elements of one stage of a marching block for functor K: a
+// tile of tw x tj cells (tw = threads in x times cells per thread), operand
+// rows padded by ic columns on each side (the halo column sits at ic - 1 and
+// ic + tw), plus the per-cell streams.
 template <class K>
-__host__ __device__ constexpr size_t march_stage_elems(int tk, int tj) {
-    return (size_t)K::NZ * (tk + 2) * (tj + 2) + (size_t)K::NP * tk * tj;
+__host__ __device__ constexpr size_t march_stage_elems(int tw, int tj, int ic) {
+    return (size_t)K::NZ * (tw + 2 * ic) * (tj + 2) + (size_t)K::NP * tw * tj;
 }
 template <class K>
 inline size_t march_smem_bytes(const MarchCfg& m) {
-    return 3 * march_stage_elems<K>(m.block.x, m.block.y) * sizeof(typename K::type);
+    const int ic = m.cpt == 2 ? 2 : 1;
+    return 3 * march_stage_elems<K>(m.block.x * m.cpt, m.block.y, ic) * sizeof(typename K::type);
+}
+
+// two consecutive elements of shared memory in one load (16-byte aligned for
+// double, 8-byte for float)
+template <typename T>
+struct Pair {
+    T x, y;
+};
+template <typename T>
+__device__ __forceinline__ Pair<T> ld_pair(const T* p) {
+    if constexpr (sizeof(T) == 8) {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        return Pair<T>{(T)v.x, (T)v.y};
+    } else {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        return Pair<T>{(T)v.x, (T)v.y};
+    }
 }
 
 // ---------------------------------------------------------------------------
-// the persistent plane-marching kernel
+// the persistent plane-marching kernel.  CPT cells per thread along k: with
+// CPT = 2 (even n2) every staged row segment of a thread is one 16-byte copy
+// (8 bytes for FP32), halving the per-cell copies, index arithmetic and
+// barrier waits; the operand rows are padded so those copies stay aligned.
 // ---------------------------------------------------------------------------
-template <class K>
+template <class K, int CPT = 1>
 __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* st, double* partials, MarchCfg m) {
     using T = typename K::type;
     constexpr int NZ = K::NZ, NP = K::NP;
     constexpr int QA = K::Q > 0 ? K::Q : 1;
+    constexpr int IC = CPT == 2 ? 2 : 1;        // first interior column of a staged operand row
+    constexpr int CB = CPT * (int)sizeof(T);    // bytes of one thread's row segment
     if (K::kCheckDone && st->done) return;
     K k = kern;
     k.load(st);
@@ -385,9 +411,11 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
     T* smem = reinterpret_cast<T*>(smem_raw);
     __shared__ int s_item;
     const int TK = blockDim.x, TJ = blockDim.y;
-    const int W = TK + 2, H = TJ + 2;
+    const int TW = TK * CPT;                    // tile width in cells
+    const int W = TW + 2 * IC, H = TJ + 2;
     const int ZT = W * H;                       // one staged operand tile
-    const int STAGE = NZ * ZT + NP * TK * TJ;   // elements per stage
+    const int NCT = TW * TJ;                    // cells of the tile
+    const int STAGE = NZ * ZT + NP * NCT;       // elements per stage
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = tx + TK * ty;
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
@@ -403,10 +431,11 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
         if (item >= m.nitems) break;
         const int tile_id = item % tiles;
         const int chunk = item / tiles;
-        const int kk = (tile_id % m.tiles_x) * TK + tx;
+        const int kk = (tile_id % m.tiles_x) * TW + CPT * tx;   // this thread's first cell
         const int jj = (tile_id / m.tiles_x) * TJ + ty;
         const int i0 = chunk * m.planes;
         const int i1 = min(i0 + m.planes, n0);
+        // (n2 is even when CPT = 2, so a thread's cells are both inside or both outside)
         const bool inside = jj < n1 && kk < n2;
         const bool edge = jj <= n1 && kk <= n2;   // the first row / column past the grid is read as halo
         const bool hS = inside && ty == 0, hN = inside && ty == TJ - 1;
@@ -435,7 +464,7 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
         const int64_t o_s = hS ? jk_offset(jj - 1, kk) : -1;
         const int64_t o_n = hN ? jk_offset(jj + 1, kk) : -1;
         const int64_t o_b = hB ? jk_offset(jj, kk - 1) : -1;
-        const int64_t o_t = hT ? jk_offset(jj, kk + 1) : -1;
+        const int64_t o_t = hT ? jk_offset(jj, kk + CPT) : -1;
         const int64_t o_own = inside ? (int64_t)jj * n2 + kk : 0;
 
         // Stage plane p into ring slot `slot`: operand inputs with halo, and
@@ -452,22 +481,24 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
                 pp -= n0;
             }
             const int64_t base = (int64_t)pp * plane;
+            const int col = IC + CPT * tx;
 #pragma unroll
             for (int z = 0; z < NZ; z++) {
                 const T* src = k.zs[z];
                 T* zt = sb + z * ZT;
-                cp_async<sizeof(T)>(zt + (ty + 1) * W + tx + 1, src + base + (o_c < 0 ? 0 : o_c), pv && o_c >= 0);
-                if (hS) cp_async<sizeof(T)>(zt + tx + 1, src + base + (o_s < 0 ? 0 : o_s), pv && o_s >= 0);
-                if (hN) cp_async<sizeof(T)>(zt + (TJ + 1) * W + tx + 1, src + base + (o_n < 0 ? 0 : o_n),
-                                            pv && o_n >= 0);
-                if (hB) cp_async<sizeof(T)>(zt + (ty + 1) * W, src + base + (o_b < 0 ? 0 : o_b), pv && o_b >= 0);
-                if (hT) cp_async<sizeof(T)>(zt + (ty + 1) * W + TK + 1, src + base + (o_t < 0 ? 0 : o_t),
-                                            pv && o_t >= 0);
+                cp_async<CB>(zt + (ty + 1) * W + col, src + base + (o_c < 0 ? 0 : o_c), pv && o_c >= 0);
+                if (hS) cp_async<CB>(zt + col, src + base + (o_s < 0 ? 0 : o_s), pv && o_s >= 0);
+                if (hN) cp_async<CB>(zt + (TJ + 1) * W + col, src + base + (o_n < 0 ? 0 : o_n), pv && o_n >= 0);
+                if (hB)
+                    cp_async<sizeof(T)>(zt + (ty + 1) * W + IC - 1, src + base + (o_b < 0 ? 0 : o_b), pv && o_b >= 0);
+                if (hT)
+                    cp_async<sizeof(T)>(zt + (ty + 1) * W + IC + TW, src + base + (o_t < 0 ? 0 : o_t),
+                                        pv && o_t >= 0);
             }
             if (full && inside) {
-                T* pt = sb + NZ * ZT + tid;
+                T* pt = sb + NZ * ZT + ty * TW + CPT * tx;
 #pragma unroll
-                for (int q = 0; q < NP; q++) cp_async<sizeof(T)>(pt + q * TK * TJ, k.ps[q] + base + o_own, true);
+                for (int q = 0; q < NP; q++) cp_async<CB>(pt + q * NCT, k.ps[q] + base + o_own, true);
             }
         };
         auto slot_of = [&](int p) { return (p - i0 + 1) % 3; };
@@ -489,7 +520,10 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
         cp_async_commit();
         cp_async_wait<2>();
         __syncthreads();
-        T zprev = inside ? zval(smem + (size_t)slot_of(i0 - 1) * STAGE, ty + 1, tx + 1) : T(0);
+        T zprev[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; c++)
+            zprev[c] = inside ? zval(smem + (size_t)slot_of(i0 - 1) * STAGE, ty + 1, IC + CPT * tx + c) : T(0);
         __syncthreads();
         for (int i = i0; i < i1; i++) {
             if (i + 2 <= i1) stage(i + 2, slot_of(i + 2), i + 2 < i1);   // reuses the slot of plane i-1
@@ -499,14 +533,48 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
             const T* sb = smem + (size_t)slot_of(i) * STAGE;
             const T* sn = smem + (size_t)slot_of(i + 1) * STAGE;
             if (inside) {
-                const T zcur = zval(sb, ty + 1, tx + 1);
-                const T z7[7] = {zcur, zprev, zval(sn, ty + 1, tx + 1), zval(sb, ty, tx + 1), zval(sb, ty + 2, tx + 1),
-                                 zval(sb, ty + 1, tx), zval(sb, ty + 1, tx + 2)};
-                T pv[NP];
+                if constexpr (CPT == 1) {
+                    const int col = IC + tx;
+                    const T zcur = zval(sb, ty + 1, col);
+                    const T z7[7] = {zcur, zprev[0], zval(sn, ty + 1, col), zval(sb, ty, col), zval(sb, ty + 2, col),
+                                     zval(sb, ty + 1, col - 1), zval(sb, ty + 1, col + 1)};
+                    T pv[NP];
 #pragma unroll
-                for (int q = 0; q < NP; q++) pv[q] = sb[NZ * ZT + q * TK * TJ + tid];
-                k.center((int64_t)i * plane + o_own, z7, pv, acc);
-                zprev = zcur;
+                    for (int q = 0; q < NP; q++) pv[q] = sb[NZ * ZT + q * NCT + tid];
+                    k.center((int64_t)i * plane + o_own, z7, pv, acc);
+                    zprev[0] = zcur;
+                } else {
+                    // the thread's two cells as one 16-byte (8-byte for FP32)
+                    // shared-memory load per row: consecutive threads read
+                    // consecutive pairs, without bank conflicts
+                    const int col = IC + 2 * tx;
+                    auto zpair = [&](const T* b, int row, T& z0, T& z1) {
+                        const Pair<T> a = ld_pair(b + row * W + col);
+                        Pair<T> c2{T(0), T(0)};
+                        if constexpr (NZ > 1) c2 = ld_pair(b + ZT + row * W + col);
+                        z0 = k.zc(a.x, c2.x);
+                        z1 = k.zc(a.y, c2.y);
+                    };
+                    T zc0, zc1, zn0, zn1, zs0, zs1, zt0, zt1;
+                    zpair(sb, ty + 1, zc0, zc1);
+                    zpair(sn, ty + 1, zn0, zn1);
+                    zpair(sb, ty, zs0, zs1);
+                    zpair(sb, ty + 2, zt0, zt1);
+                    const T zw = zval(sb, ty + 1, col - 1), ze = zval(sb, ty + 1, col + 2);
+                    T pv0[NP], pv1[NP];
+#pragma unroll
+                    for (int q = 0; q < NP; q++) {
+                        const Pair<T> pq = ld_pair(sb + NZ * ZT + q * NCT + ty * TW + 2 * tx);
+                        pv0[q] = pq.x;
+                        pv1[q] = pq.y;
+                    }
+                    const T z70[7] = {zc0, zprev[0], zn0, zs0, zt0, zw, zc1};
+                    k.center((int64_t)i * plane + o_own, z70, pv0, acc);
+                    const T z71[7] = {zc1, zprev[1], zn1, zs1, zt1, zc0, ze};
+                    k.center((int64_t)i * plane + o_own + 1, z71, pv1, acc);
+                    zprev[0] = zc0;
+                    zprev[1] = zc1;
+                }
             }
             __syncthreads();                    // slot of plane i is free for plane i+3
         }
@@ -528,25 +596,41 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
     }
 }
 
-template <class K>
-inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
-                        double* partials) {
-    if (m.nitems > kMaxBlocks) return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
+template <class K, int CPT>
+inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
+                          double* partials) {
     const size_t smem = march_smem_bytes<K>(m);
     static int per_sm = 0;
     static size_t per_sm_smem = 0;
     if (per_sm == 0 || per_sm_smem != smem) {
         if (smem > 48 * 1024)
-            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K>, m.block.x * m.block.y, smem);
+            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K, CPT>, m.block.x * m.block.y, smem);
         if (per_sm < 1) per_sm = 1;
         per_sm_smem = smem;
     }
     int blocks = per_sm * ctx->num_sms;
     if (blocks > m.nitems) blocks = m.nitems;
-    k_march<K><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, m);
+    k_march<K, CPT><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, m);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
+}
+
+// Two cells per thread pays off for the functors with few per-cell streams
+// (steps 1 and 3: 256^3 step times 0.291 -> 0.257 ms and 0.289 -> 0.253 ms);
+// with nine streams and five dot products (steps 2 and 4) the halved warp
+// count per SM no longer hides the arithmetic (0.34 -> 0.45 ms), so those run
+// one cell per thread on the same 32 x 8 tiles.
+template <class K>
+inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
+                        double* partials) {
+    if (m.nitems > kMaxBlocks) return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
+    if (m.cpt == 2 && K::NP <= 7) return launch_march_t<K, 2>(ctx, g, m, kern, st, partials);
+    if (m.cpt == 1) return launch_march_t<K, 1>(ctx, g, m, kern, st, partials);
+    MarchCfg m1 = m;   // the same tiles, one cell per thread
+    m1.cpt = 1;
+    m1.block = dim3(m.block.x * m.cpt, m.block.y, 1);
+    return launch_march_t<K, 1>(ctx, g, m1, kern, st, partials);
 }
 
 // K5: (24) x = x + w1 r + w2 s + alpha u; (25) r = r - w1 s - w2 t; ||r||;
