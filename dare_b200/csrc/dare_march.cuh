@@ -423,116 +423,136 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
     const int64_t plane = (int64_t)n1 * n2;
     const int tiles = m.tiles_x * m.tiles_y;
 
-    for (;;) {
-        if (tid == 0) s_item = (int)atomicAdd(&st->queue, 1u);
-        __syncthreads();
-        const int item = s_item;
-        __syncthreads();
-        if (item >= m.nitems) break;
+    // Geometry of one work item for this thread.
+    struct Geo {
+        int i0, i1;
+        bool inside, hS, hN, hB, hT;
+        int64_t o_c, o_s, o_n, o_b, o_t, o_own;
+    };
+    // in-plane position (j, kx) -> wrapped offset, or -1 when outside (zero)
+    auto jk_offset = [&](int j, int kx) -> int64_t {
+        if (j < 0) {
+            if (!p1) return -1;
+            j += n1;
+        } else if (j >= n1) {
+            if (!p1) return -1;
+            j -= n1;
+        }
+        if (kx < 0) {
+            if (!p2) return -1;
+            kx += n2;
+        } else if (kx >= n2) {
+            if (!p2) return -1;
+            kx -= n2;
+        }
+        if ((unsigned)j >= (unsigned)n1 || (unsigned)kx >= (unsigned)n2) return -1;
+        return (int64_t)j * n2 + kx;
+    };
+    auto geometry = [&](int item) {
+        Geo G;
         const int tile_id = item % tiles;
         const int chunk = item / tiles;
         const int kk = (tile_id % m.tiles_x) * TW + CPT * tx;   // this thread's first cell
         const int jj = (tile_id / m.tiles_x) * TJ + ty;
-        const int i0 = chunk * m.planes;
-        const int i1 = min(i0 + m.planes, n0);
+        G.i0 = chunk * m.planes;
+        G.i1 = min(G.i0 + m.planes, n0);
         // (n2 is even when CPT = 2, so a thread's cells are both inside or both outside)
-        const bool inside = jj < n1 && kk < n2;
+        G.inside = jj < n1 && kk < n2;
         const bool edge = jj <= n1 && kk <= n2;   // the first row / column past the grid is read as halo
-        const bool hS = inside && ty == 0, hN = inside && ty == TJ - 1;
-        const bool hB = inside && tx == 0, hT = inside && tx == TK - 1;
-
-        // in-plane position (j, kx) -> wrapped offset, or -1 when outside (zero)
-        auto jk_offset = [&](int j, int kx) -> int64_t {
-            if (j < 0) {
-                if (!p1) return -1;
-                j += n1;
-            } else if (j >= n1) {
-                if (!p1) return -1;
-                j -= n1;
-            }
-            if (kx < 0) {
-                if (!p2) return -1;
-                kx += n2;
-            } else if (kx >= n2) {
-                if (!p2) return -1;
-                kx -= n2;
-            }
-            if ((unsigned)j >= (unsigned)n1 || (unsigned)kx >= (unsigned)n2) return -1;
-            return (int64_t)j * n2 + kx;
-        };
-        const int64_t o_c = edge ? jk_offset(jj, kk) : -1;
-        const int64_t o_s = hS ? jk_offset(jj - 1, kk) : -1;
-        const int64_t o_n = hN ? jk_offset(jj + 1, kk) : -1;
-        const int64_t o_b = hB ? jk_offset(jj, kk - 1) : -1;
-        const int64_t o_t = hT ? jk_offset(jj, kk + CPT) : -1;
-        const int64_t o_own = inside ? (int64_t)jj * n2 + kk : 0;
-
-        // Stage plane p into ring slot `slot`: operand inputs with halo, and
-        // (when `full`) the per-cell streams.  Out-of-range planes are zeros.
-        auto stage = [&](int p, int slot, bool full) {
-            T* sb = smem + (size_t)slot * STAGE;
-            bool pv = true;
-            int pp = p;
-            if (pp < 0) {
-                pv = p0;
-                pp += n0;
-            } else if (pp >= n0) {
-                pv = p0;
-                pp -= n0;
-            }
-            const int64_t base = (int64_t)pp * plane;
-            const int col = IC + CPT * tx;
+        G.hS = G.inside && ty == 0;
+        G.hN = G.inside && ty == TJ - 1;
+        G.hB = G.inside && tx == 0;
+        G.hT = G.inside && tx == TK - 1;
+        G.o_c = edge ? jk_offset(jj, kk) : -1;
+        G.o_s = G.hS ? jk_offset(jj - 1, kk) : -1;
+        G.o_n = G.hN ? jk_offset(jj + 1, kk) : -1;
+        G.o_b = G.hB ? jk_offset(jj, kk - 1) : -1;
+        G.o_t = G.hT ? jk_offset(jj, kk + CPT) : -1;
+        G.o_own = G.inside ? (int64_t)jj * n2 + kk : 0;
+        return G;
+    };
+    auto slot_of = [&](const Geo& G, int p) { return (p - G.i0 + 1) % 3; };
+    // Stage plane p into its ring slot: operand inputs with halo, and (when
+    // `full`) the per-cell streams.  Out-of-range planes are zeros.
+    auto stage = [&](const Geo& G, int p, bool full) {
+        T* sb = smem + (size_t)slot_of(G, p) * STAGE;
+        bool pv = true;
+        int pp = p;
+        if (pp < 0) {
+            pv = p0;
+            pp += n0;
+        } else if (pp >= n0) {
+            pv = p0;
+            pp -= n0;
+        }
+        const int64_t base = (int64_t)pp * plane;
+        const int col = IC + CPT * tx;
 #pragma unroll
-            for (int z = 0; z < NZ; z++) {
-                const T* src = k.zs[z];
-                T* zt = sb + z * ZT;
-                cp_async<CB>(zt + (ty + 1) * W + col, src + base + (o_c < 0 ? 0 : o_c), pv && o_c >= 0);
-                if (hS) cp_async<CB>(zt + col, src + base + (o_s < 0 ? 0 : o_s), pv && o_s >= 0);
-                if (hN) cp_async<CB>(zt + (TJ + 1) * W + col, src + base + (o_n < 0 ? 0 : o_n), pv && o_n >= 0);
-                if (hB)
-                    cp_async<sizeof(T)>(zt + (ty + 1) * W + IC - 1, src + base + (o_b < 0 ? 0 : o_b), pv && o_b >= 0);
-                if (hT)
-                    cp_async<sizeof(T)>(zt + (ty + 1) * W + IC + TW, src + base + (o_t < 0 ? 0 : o_t),
-                                        pv && o_t >= 0);
-            }
-            if (full && inside) {
-                T* pt = sb + NZ * ZT + ty * TW + CPT * tx;
+        for (int z = 0; z < NZ; z++) {
+            const T* src = k.zs[z];
+            T* zt = sb + z * ZT;
+            cp_async<CB>(zt + (ty + 1) * W + col, src + base + (G.o_c < 0 ? 0 : G.o_c), pv && G.o_c >= 0);
+            if (G.hS) cp_async<CB>(zt + col, src + base + (G.o_s < 0 ? 0 : G.o_s), pv && G.o_s >= 0);
+            if (G.hN)
+                cp_async<CB>(zt + (TJ + 1) * W + col, src + base + (G.o_n < 0 ? 0 : G.o_n), pv && G.o_n >= 0);
+            if (G.hB)
+                cp_async<sizeof(T)>(zt + (ty + 1) * W + IC - 1, src + base + (G.o_b < 0 ? 0 : G.o_b),
+                                    pv && G.o_b >= 0);
+            if (G.hT)
+                cp_async<sizeof(T)>(zt + (ty + 1) * W + IC + TW, src + base + (G.o_t < 0 ? 0 : G.o_t),
+                                    pv && G.o_t >= 0);
+        }
+        if (full && G.inside) {
+            T* pt = sb + NZ * ZT + ty * TW + CPT * tx;
 #pragma unroll
-                for (int q = 0; q < NP; q++) cp_async<CB>(pt + q * NCT, k.ps[q] + base + o_own, true);
-            }
-        };
-        auto slot_of = [&](int p) { return (p - i0 + 1) % 3; };
-        auto zval = [&](const T* sb, int row, int col) -> T {
-            const T a = sb[row * W + col];
-            const T b = NZ > 1 ? sb[ZT + row * W + col] : T(0);
-            return k.zc(a, b);
-        };
+            for (int q = 0; q < NP; q++) cp_async<CB>(pt + q * NCT, k.ps[q] + base + G.o_own, true);
+        }
+    };
+    // prologue of an item: planes i0-1 (operand only), i0, i0+1
+    auto prologue = [&](const Geo& G) {
+        stage(G, G.i0 - 1, false);
+        cp_async_commit();
+        stage(G, G.i0, true);
+        cp_async_commit();
+        stage(G, G.i0 + 1, G.i0 + 1 < G.i1);
+        cp_async_commit();
+    };
+    auto zval = [&](const T* sb, int row, int col) -> T {
+        const T a = sb[row * W + col];
+        const T b = NZ > 1 ? sb[ZT + row * W + col] : T(0);
+        return k.zc(a, b);
+    };
 
+    // Items come from the queue one ahead: the next index is fetched when an
+    // item starts, and the next item's prologue copies are issued before the
+    // current item's reduction, so the queue atomic, the reduction and the
+    // first planes' DRAM latency overlap.
+    __shared__ int s_next;
+    if (tid == 0) s_item = (int)atomicAdd(&st->queue, 1u);
+    __syncthreads();
+    int item = s_item;
+    Geo G = geometry(item < m.nitems ? item : 0);
+    if (item < m.nitems) prologue(G);
+    while (item < m.nitems) {
+        if (tid == 0) s_next = (int)atomicAdd(&st->queue, 1u);
         double acc[QA];
 #pragma unroll
         for (int q = 0; q < QA; q++) acc[q] = 0.;
-        // prologue: planes i0-1 (operand only), i0, i0+1
-        stage(i0 - 1, slot_of(i0 - 1), false);
-        cp_async_commit();
-        stage(i0, slot_of(i0), true);
-        cp_async_commit();
-        stage(i0 + 1, slot_of(i0 + 1), i0 + 1 < i1);
-        cp_async_commit();
         cp_async_wait<2>();
         __syncthreads();
         T zprev[CPT];
 #pragma unroll
         for (int c = 0; c < CPT; c++)
-            zprev[c] = inside ? zval(smem + (size_t)slot_of(i0 - 1) * STAGE, ty + 1, IC + CPT * tx + c) : T(0);
+            zprev[c] = G.inside ? zval(smem + (size_t)slot_of(G, G.i0 - 1) * STAGE, ty + 1, IC + CPT * tx + c) : T(0);
         __syncthreads();
-        for (int i = i0; i < i1; i++) {
-            if (i + 2 <= i1) stage(i + 2, slot_of(i + 2), i + 2 < i1);   // reuses the slot of plane i-1
+        for (int i = G.i0; i < G.i1; i++) {
+            if (i + 2 <= G.i1) stage(G, i + 2, i + 2 < G.i1);   // reuses the slot of plane i-1
             cp_async_commit();
             cp_async_wait<1>();                 // planes i and i+1 have landed
             __syncthreads();
-            const T* sb = smem + (size_t)slot_of(i) * STAGE;
-            const T* sn = smem + (size_t)slot_of(i + 1) * STAGE;
-            if (inside) {
+            const T* sb = smem + (size_t)slot_of(G, i) * STAGE;
+            const T* sn = smem + (size_t)slot_of(G, i + 1) * STAGE;
+            if (G.inside) {
                 if constexpr (CPT == 1) {
                     const int col = IC + tx;
                     const T zcur = zval(sb, ty + 1, col);
@@ -541,7 +561,7 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
                     T pv[NP];
 #pragma unroll
                     for (int q = 0; q < NP; q++) pv[q] = sb[NZ * ZT + q * NCT + tid];
-                    k.center((int64_t)i * plane + o_own, z7, pv, acc);
+                    k.center((int64_t)i * plane + G.o_own, z7, pv, acc);
                     zprev[0] = zcur;
                 } else {
                     // the thread's two cells as one 16-byte (8-byte for FP32)
@@ -569,9 +589,9 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
                         pv1[q] = pq.y;
                     }
                     const T z70[7] = {zc0, zprev[0], zn0, zs0, zt0, zw, zc1};
-                    k.center((int64_t)i * plane + o_own, z70, pv0, acc);
+                    k.center((int64_t)i * plane + G.o_own, z70, pv0, acc);
                     const T z71[7] = {zc1, zprev[1], zn1, zs1, zt1, zc0, ze};
-                    k.center((int64_t)i * plane + o_own + 1, z71, pv1, acc);
+                    k.center((int64_t)i * plane + G.o_own + 1, z71, pv1, acc);
                     zprev[0] = zc0;
                     zprev[1] = zc1;
                 }
@@ -579,12 +599,21 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
             __syncthreads();                    // slot of plane i is free for plane i+3
         }
         cp_async_wait<0>();
+        const int next = s_next;                // written before this item's barriers
+        Geo GN = G;
+        if (next < m.nitems) {
+            GN = geometry(next);
+            prologue(GN);                       // every plane of this item has been read
+        }
         if constexpr (K::Q > 0) {
             double tot[K::Q];
             if (item_reduce<K::Q>(acc, partials, item, m.nitems, &st->count, tot) && tid == 0) k.done(st, tot);
         }
-        __syncthreads();
+        __syncthreads();                        // s_next is rewritten at the next item's start
+        item = next;
+        G = GN;
     }
+    cp_async_wait<0>();
     // the last block out resets the queue for the next launch
     if (tid == 0) {
         const unsigned prev = atomicAdd(&st->exitc, 1u);
