@@ -1400,9 +1400,19 @@ static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int
     DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     DARE_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                         (int)cudaSharedmemCarveoutMaxShared));
+    // Resident CTAs per SM from the kernel's registers, threads and shared
+    // memory (the runtime's occupancy query answers 1 for these kernels,
+    // while the hardware keeps as many as the resources allow).
+    cudaFuncAttributes fa;
+    DARE_CUDA(ctx, cudaFuncGetAttributes(&fa, kern));
+    const int warps = (threads + 31) / 32;
+    const int regs_warp = ((fa.numRegs + 7) / 8) * 8 * 32;
+    const int by_regs = 65536 / (warps * ((regs_warp + 255) / 256) * 256);
+    const int by_threads = 2048 / (warps * 32);
     int occ = 0;
     for (;;) {
-        DARE_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem));
+        const int by_smem = (int)(233472 / (smem + fa.sharedSizeBytes + 1024));
+        occ = std::min(std::min(by_regs, by_threads), std::min(by_smem, 32));
         // CTAs resident on one SM must never ask for more than its 512 TMEM columns
         if (occ * cols <= 512 || smem + 4096 > kMaxSmem) break;
         smem += 4096;
@@ -1416,13 +1426,11 @@ template <int CIN, int NT, int MT, int OUTM>
 static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap& tmap, const FwdArgs& a0) {
     auto kern = k_conv_fwd<CIN, NT, MT, OUTM>;
     if (!lc.ready) {
-        // the deepest ring (4..8 staged planes) that fits
-        int slots = kMaxSlots;
-        while (slots > 4 && fwd_smem(CIN, NT, a0.g, MT, slots) > kMaxSmem) slots--;
-        size_t smem = fwd_smem(CIN, NT, a0.g, MT, slots);
-        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         const uint32_t acols = 2 * MT * (3 * NT <= 64 ? 64 : 128);
         const uint32_t cols = acols <= 128 ? 128 : (acols <= 256 ? 256 : 512);
+        const int slots = pick_slots([&](int sl) { return fwd_smem(CIN, NT, a0.g, MT, sl); }, cols);
+        size_t smem = fwd_smem(CIN, NT, a0.g, MT, slots);
+        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         int occ = 0, rc;
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, fwd_threads(MT)))) return rc;
         const int n0 = a0.g.n0;
@@ -1517,6 +1525,26 @@ static int launch_wgr(dare_ctx* ctx, LaunchCfg& lc, int cin, int cout, int xm, i
     return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: no weight-gradient kernel for this shape");
 }
 
+// Ring depth (4..8 staged planes) of a plane-marching kernel: the deepest ring
+// among those that give the most resident CTAs per SM (shared memory of the
+// SM, 228 KB, with 1 KB reserved per CTA; TMEM columns), so that short rings
+// buy a second or third CTA where one deep ring would fill the SM.
+template <typename SmemFn>
+static int pick_slots(SmemFn smem_of, uint32_t cols) {
+    constexpr size_t kSmemPerSM = 233472;
+    int best = 0, best_occ = 0;
+    for (int slots = 4; slots <= kMaxSlots; slots++) {
+        const size_t smem = smem_of(slots);
+        if (smem > kMaxSmem) break;
+        const int occ = (int)std::min<size_t>(kSmemPerSM / (smem + 1024), 512 / cols);
+        if (occ >= best_occ) {
+            best_occ = occ;
+            best = slots;
+        }
+    }
+    return best > 0 ? best : 4;
+}
+
 static size_t in_smem(const Geom& g, int mt, int slots) {
     const size_t sb = (size_t)((in_rows(g, mt) + 7) / 8) * 8 * 16;
     return 3 * 2 * 2 * 16 * 16 + slots * sb + slots * (size_t)in_raw_elems(g, mt) * 2 + (3 * kMaxSlots + 5) * 8 + 16;
@@ -1528,11 +1556,10 @@ template <int MT>
 static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a0) {
     auto kern = k_conv_in<MT>;
     if (!lc.ready) {
-        int slots = kMaxSlots;
-        while (slots > 4 && in_smem(a0.g, MT, slots) > kMaxSmem) slots--;
+        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
+        const int slots = pick_slots([&](int sl) { return in_smem(a0.g, MT, sl); }, cols);
         size_t smem = in_smem(a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
-        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
         int occ = 0, rc;
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, in_threads(MT)))) return rc;
         // (the launch checks above keep the ring at >= 4 planes: 3 in use + 1 loading)
@@ -1581,11 +1608,10 @@ template <int MT>
 static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     auto kern = k_conv_out<MT>;
     if (!lc.ready) {
-        int slots = kMaxSlots;
-        while (slots > 4 && out_smem(a0.g, MT, slots) > kMaxSmem) slots--;
+        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
+        const int slots = pick_slots([&](int sl) { return out_smem(a0.g, MT, sl); }, cols);
         size_t smem = out_smem(a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
-        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
         int occ = 0, rc;
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, out_threads(MT)))) return rc;
         const int n0 = a0.g.n0;
