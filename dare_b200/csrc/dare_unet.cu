@@ -23,8 +23,6 @@
 // CTA accumulates its planes in TMEM and writes one partial per CTA, summed
 // in a fixed order afterwards (deterministic).  Data gradients are forward
 // convolutions with flipped, transposed weights.
-#include <cuda.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -102,7 +100,7 @@ __device__ __forceinline__ void stage(uint8_t* slot, float* raw, const bf16* __r
             const int q = idx / KC, kc = idx - q * KC;
             const int64_t Q = Q0 + q;
             const bool v = Q >= 0 && Q < g.total && q < valid_rows;
-            cp16(slot + ((size_t)kc * RP + q) * 16, in + (v ? Q : 0) * C + kc * 8, v);
+            cp16(slot + ((size_t)kc * RP + q) * 16, in + act_off(g.total, v ? Q : 0, kc), v);
         }
     } else {
         embed_rows(raw, in32, g, Q0, rows, valid_rows, threadIdx.x, kThreads);
@@ -135,7 +133,7 @@ __device__ __forceinline__ void stage_lanes(uint8_t* slot, float* raw, const bf1
             const int q = idx / KC, kc = idx - q * KC;
             const int64_t Q = Q0 + q;
             const bool v = Q >= 0 && Q < g.total;
-            cp16(slot + ((size_t)kc * RP + q) * 16, in + (v ? Q : 0) * C + kc * 8, v);
+            cp16(slot + ((size_t)kc * RP + q) * 16, in + act_off(g.total, v ? Q : 0, kc), v);
         }
     } else {
         embed_rows(raw, in32, g, Q0, rows, rows, lane, 32);
@@ -239,7 +237,7 @@ __device__ __forceinline__ int64_t child_off(const Geom& f, int64_t fplane, int 
 // children on the finer level) loads the children of plane I+1 while plane
 // I+1's MMAs run.
 template <int CIN, int NT, int MT, int OUTM>
-__global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_constant__ CUtensorMap tmap, FwdArgs a) {
+__global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int KC = CIN / 8;
     constexpr int N3 = 3 * NT;
@@ -253,9 +251,7 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
-    const int rows = strip_rows(g, MT);
-    const int NTL = box_count(rows), BR = box_height(rows);  // TMA boxes per chunk plane, rows per box
-    const int RP = NTL * BR;
+    const int RP = round8(strip_rows(g, MT));  // staged rows per chunk plane
     const uint32_t SB = (uint32_t)KC * RP * 16;
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
@@ -305,20 +301,20 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
     const int pbase = P0 - 1 - g.W;
 
     if (warp == 4) {
-        // ---- producer: planes I0-1 .. I1+1 into the ring by TMA ----
+        // ---- producer: planes I0-1 .. I1+1 into the ring, one bulk copy per
+        // chunk plane segment ----
         if (lane == 0) {
-            const uint32_t bytes = (uint32_t)KC * NTL * BR * 16;
+            const uint32_t bytes = (uint32_t)KC * RP * 16;
             uint32_t eph = 0xFFu;  // parity of the next wait on empty[s] (fresh slots pass)
             for (int p = I0 - 1; p <= I1 + 1; p++) {
                 const int sl = p % S;
                 if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 5)) break;
                 eph ^= 1u << sl;
                 mbar_arrive_expect_tx(&full[sl], bytes);
-                const int y0 = p * g.plane + pbase;
+                const int64_t y0 = (int64_t)p * g.plane + pbase;
                 for (int kc = 0; kc < KC; kc++)
-                    for (int rt = 0; rt < NTL; rt++)
-                        tma_load_2d(slots + sl * SB + ((size_t)kc * RP + rt * BR) * 16, &tmap, kc * 8, y0 + rt * BR,
-                                    &full[sl]);
+                    bulk_load(slots + sl * SB + (size_t)kc * RP * 16, a.in + act_off(g.total, y0, kc),
+                              (uint32_t)RP * 16, &full[sl]);
             }
         }
         __syncwarp();
@@ -383,12 +379,13 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
         constexpr bool kPre = OUTM == OUT_ADDUP && MT * NT <= 32;
         uint4 pre[kPre ? MT : 1][NT / 8][8];
         auto fetch = [&](int I, int mt, uint4(&o)[NT / 8][8]) {
-            const bf16* base = a.fine + ((int64_t)(2 * I - 1) * fplane + fofs[mt]) * a.cout + co0;
+            const int64_t Q = (int64_t)(2 * I - 1) * fplane + fofs[mt];
 #pragma unroll
             for (int c8 = 0; c8 < NT / 8; c8++)
 #pragma unroll
                 for (int ch = 0; ch < 8; ch++)
-                    o[c8][ch] = *reinterpret_cast<const uint4*>(base + child_off(f, fplane, ch) * a.cout + c8 * 8);
+                    o[c8][ch] = *reinterpret_cast<const uint4*>(
+                        a.fine + act_off(f.total, Q + child_off(f, fplane, ch), co0 / 8 + c8));
         };
         if constexpr (kPre) {
 #pragma unroll
@@ -452,22 +449,23 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(const __grid_const
             for (int mt = 0; mt < MT; mt++) {
                 if (pos[mt] < 0) continue;
                 if constexpr (OUTM == OUT_STORE) {
-                    bf16* dst = a.out + ((int64_t)I * g.plane + pos[mt]) * a.cout + co0;
+                    const int64_t Q = (int64_t)I * g.plane + pos[mt];
 #pragma unroll
                     for (int c = 0; c < NT; c += 8)
-                        *reinterpret_cast<uint4*>(dst + c) =
+                        *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, (co0 + c) / 8)) =
                             make_uint4(pack_bf16(acc[mt][c + 0], acc[mt][c + 1]), pack_bf16(acc[mt][c + 2], acc[mt][c + 3]),
                                        pack_bf16(acc[mt][c + 4], acc[mt][c + 5]), pack_bf16(acc[mt][c + 6], acc[mt][c + 7]));
                 } else {
                     if constexpr (!kPre) fetch(I, mt, pre[0]);
-                    bf16* base = a.fine + ((int64_t)(2 * I - 1) * fplane + fofs[mt]) * a.cout + co0;
+                    const int64_t Q = (int64_t)(2 * I - 1) * fplane + fofs[mt];
 #pragma unroll
                     for (int c8 = 0; c8 < NT / 8; c8++)
 #pragma unroll
                         for (int ch = 0; ch < 8; ch++) {
                             const uint4 o = pre[kPre ? mt : 0][c8][ch];
                             const float* v = &acc[mt][c8 * 8];
-                            *reinterpret_cast<uint4*>(base + child_off(f, fplane, ch) * a.cout + c8 * 8) =
+                            *reinterpret_cast<uint4*>(a.fine + act_off(f.total, Q + child_off(f, fplane, ch),
+                                                                       co0 / 8 + c8)) =
                                 make_uint4(pack_bf16(bf16_lo(o.x) + v[0], bf16_hi(o.x) + v[1]),
                                            pack_bf16(bf16_lo(o.y) + v[2], bf16_hi(o.y) + v[3]),
                                            pack_bf16(bf16_lo(o.z) + v[4], bf16_hi(o.z) + v[5]),
@@ -699,12 +697,14 @@ __global__ void __launch_bounds__(in_threads(MT)) k_conv_in(InArgs a) {
 #pragma unroll
             for (int mt = 0; mt < MT; mt++) {
                 if (pos[mt] < 0) continue;
-                uint4* dst = reinterpret_cast<uint4*>(a.out + ((int64_t)I * g.plane + pos[mt]) * 16);
+                const int64_t Q = (int64_t)I * g.plane + pos[mt];
                 const float* v = reinterpret_cast<const float*>(r[mt]);
-                dst[0] = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
-                                    pack_bf16(v[6], v[7]));
-                dst[1] = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]),
-                                    pack_bf16(v[14], v[15]));
+                *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, 0)) =
+                    make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                               pack_bf16(v[6], v[7]));
+                *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, 1)) =
+                    make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]),
+                               pack_bf16(v[14], v[15]));
             }
         }
     }
@@ -736,7 +736,7 @@ __host__ __device__ constexpr int out_threads(int mt) { return (5 + mt) * 32; }
 // accumulates 9 MMAs in TMEM, and out[p] = D[p-1][0] + D[p][1] + D[p+1][2]:
 // 9 MMAs per 126 outputs instead of 27 per 128.
 template <int MT>
-__global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_constant__ CUtensorMap tmap, OutArgs a) {
+__global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr uint32_t WB = 9 * 2 * 16 * 16;
     constexpr uint32_t ACOLS = MT * 16;
@@ -744,9 +744,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_const
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
-    const int rows = strip_rows(g, MT);
-    const int NTL = box_count(rows), BR = box_height(rows);
-    const int RP = NTL * BR;
+    const int RP = round8(strip_rows(g, MT));  // staged rows per chunk plane
     const uint32_t SB = 2u * RP * 16;
     uint8_t* wsm = smem;
     uint8_t* slots = smem + WB;
@@ -793,20 +791,19 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(const __grid_const
     const int pbase = P0 - 1 - g.W;
 
     if (warp == 4) {
-        // ---- producer: TMA boxes of 8 channels x 32 positions ----
+        // ---- producer: one bulk copy per chunk plane segment ----
         if (lane == 0) {
-            const uint32_t bytes = 2u * NTL * BR * 16;
+            const uint32_t bytes = 2u * RP * 16;
             uint32_t eph = 0xFFu;
             for (int p = I0 - 1; p <= I1 + 1; p++) {
                 const int sl = p % S;
                 if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 21)) break;
                 eph ^= 1u << sl;
                 mbar_arrive_expect_tx(&full[sl], bytes);
-                const int y0 = p * g.plane + pbase;
+                const int64_t y0 = (int64_t)p * g.plane + pbase;
                 for (int kc = 0; kc < 2; kc++)
-                    for (int rt = 0; rt < NTL; rt++)
-                        tma_load_2d(slots + sl * SB + ((size_t)kc * RP + rt * BR) * 16, &tmap, kc * 8, y0 + rt * BR,
-                                    &full[sl]);
+                    bulk_load(slots + sl * SB + (size_t)kc * RP * 16, a.in + act_off(g.total, y0, kc),
+                              (uint32_t)RP * 16, &full[sl]);
             }
         }
         __syncwarp();
@@ -1094,7 +1091,7 @@ __global__ void k_restrict(Geom f, Geom c, const bf16* __restrict__ fine, bf16* 
         for (int ch = 0; ch < 8; ch++) {
             const int fi = 2 * i + 1 + (ch >> 2), fj = 2 * j + 1 + ((ch >> 1) & 1), fk = 2 * k + 1 + (ch & 1);
             const uint4 q = __ldg(reinterpret_cast<const uint4*>(
-                fine + (((int64_t)fi * (f.n1 + 2) + fj) * f.W + fk) * C + kc * 8));
+                fine + act_off(f.total, ((int64_t)fi * (f.n1 + 2) + fj) * f.W + fk, kc)));
             acc[0] += bf16_lo(q.x);
             acc[1] += bf16_hi(q.x);
             acc[2] += bf16_lo(q.y);
@@ -1109,7 +1106,7 @@ __global__ void k_restrict(Geom f, Geom c, const bf16* __restrict__ fine, bf16* 
         o.y = pack_bf16(acc[2] * scale, acc[3] * scale);
         o.z = pack_bf16(acc[4] * scale, acc[5] * scale);
         o.w = pack_bf16(acc[6] * scale, acc[7] * scale);
-        *reinterpret_cast<uint4*>(coarse + (((int64_t)(i + 1) * (c.n1 + 2) + (j + 1)) * c.W + (k + 1)) * C + kc * 8) =
+        *reinterpret_cast<uint4*>(coarse + act_off(c.total, ((int64_t)(i + 1) * (c.n1 + 2) + (j + 1)) * c.W + (k + 1), kc)) =
             o;
     }
 }
@@ -1127,9 +1124,9 @@ __global__ void k_prolong_add(Geom f, Geom c, const bf16* __restrict__ coarse, b
         const int j = (int)(v % f.n1);
         const int i = (int)(v / f.n1);
         const uint4 q = __ldg(reinterpret_cast<const uint4*>(
-            coarse + (((int64_t)(i / 2 + 1) * (c.n1 + 2) + (j / 2 + 1)) * c.W + (k / 2 + 1)) * C + kc * 8));
-        uint4* dst =
-            reinterpret_cast<uint4*>(fine + (((int64_t)(i + 1) * (f.n1 + 2) + (j + 1)) * f.W + (k + 1)) * C + kc * 8);
+            coarse + act_off(c.total, ((int64_t)(i / 2 + 1) * (c.n1 + 2) + (j / 2 + 1)) * c.W + (k / 2 + 1), kc)));
+        uint4* dst = reinterpret_cast<uint4*>(
+            fine + act_off(f.total, ((int64_t)(i + 1) * (f.n1 + 2) + (j + 1)) * f.W + (k + 1), kc));
         const uint4 o = *dst;
         uint4 r;
         r.x = pack_bf16(bf16_lo(o.x) + scale * bf16_lo(q.x), bf16_hi(o.x) + scale * bf16_hi(q.x));
@@ -1164,7 +1161,8 @@ __global__ void k_read_act(Geom g, int C, const bf16* __restrict__ a, float* __r
         v /= g.n2;
         const int j = (int)(v % g.n1);
         const int i = (int)(v / g.n1);
-        out[idx] = __bfloat162float(a[(((int64_t)(i + 1) * (g.n1 + 2) + (j + 1)) * g.W + (k + 1)) * C + ch]);
+        out[idx] = __bfloat162float(
+            a[act_off(g.total, ((int64_t)(i + 1) * (g.n1 + 2) + (j + 1)) * g.W + (k + 1), ch / 8) + ch % 8]);
     }
 }
 
@@ -1323,8 +1321,7 @@ __global__ void k_warm(int64_t n, const double* __restrict__ diag, const double*
 // ---------------------------------------------------------------------------
 // host side: launch configuration and dispatch
 static size_t fwd_smem(int cin, int nt, const Geom& g, int mt, int slots) {
-    const int rows = strip_rows(g, mt);
-    const int RP = box_count(rows) * box_height(rows);
+    const int RP = round8(strip_rows(g, mt));
     return (size_t)kTaps * cin * nt * 2 + slots * (size_t)(cin / 8) * RP * 16 + 2 * (size_t)mt * 4 * 2 * nt * 4 +
            (2 * kMaxSlots + 5) * 8 + 16;
 }
@@ -1353,31 +1350,6 @@ static int pick_ppc(int n0, int64_t units, int64_t resident) {
         }
     }
     return best;
-}
-
-// TMA map of a padded channels-last activation [total][C] (bf16): boxes of 8
-// channels x `box_rows` positions, rows outside the array read zero
-static int act_map(dare_ctx* ctx, CUtensorMap* m, const bf16* base, int C, int64_t total, int box_rows) {
-    const cuuint64_t dims[2] = {(cuuint64_t)C, (cuuint64_t)total};
-    const cuuint64_t strides[1] = {(cuuint64_t)C * sizeof(bf16)};
-    const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
-    const cuuint32_t es[2] = {1, 1};
-    // the driver's encoder, looked up through the runtime (no link-time
-    // dependency on the driver library)
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return set_error(ctx, DARE_ERR_CUDA, "unet: cuTensorMapEncodeTiled is not available");
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
-    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dims, strides, box, es,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return set_error(ctx, DARE_ERR_CUDA, "unet: cuTensorMapEncodeTiled failed");
-    return DARE_OK;
 }
 
 static int dy_pitch_rt(int c) { return kTileM + (c == 16 ? 4 : (c == 32 ? 2 : 1)); }
@@ -1423,7 +1395,7 @@ static int occupancy_fit(dare_ctx* ctx, K kern, size_t& smem, uint32_t cols, int
 }
 
 template <int CIN, int NT, int MT, int OUTM>
-static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap& tmap, const FwdArgs& a0) {
+static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const FwdArgs& a0) {
     auto kern = k_conv_fwd<CIN, NT, MT, OUTM>;
     if (!lc.ready) {
         const uint32_t acols = 2 * MT * (3 * NT <= 64 ? 64 : 128);
@@ -1448,7 +1420,7 @@ static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap&
     FwdArgs a = a0;
     a.ppc = lc.ppc;
     a.slots = lc.slots;
-    kern<<<lc.grid, fwd_threads(MT), lc.smem, ctx->stream>>>(tmap, a);
+    kern<<<lc.grid, fwd_threads(MT), lc.smem, ctx->stream>>>(a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
@@ -1456,12 +1428,9 @@ static int launch_fwd_t(dare_ctx* ctx, LaunchCfg& lc, int nz, const CUtensorMap&
 // BF16 input `a.in` with `cin` channels
 static int launch_fwd(dare_ctx* ctx, LaunchCfg& lc, int cin, int nt, int nz, int outm, const FwdArgs& a) {
     const int mt = pick_mt(a.g, cin, nt);
-    CUtensorMap tmap;
-    int rc = act_map(ctx, &tmap, a.in, cin, a.g.total, box_height(strip_rows(a.g, mt)));
-    if (rc) return rc;
 #define DARE_FWD(CI, N, OM)                                                                       \
     if (cin == CI && nt == N && outm == OM)                                                       \
-        return mt == 2 ? launch_fwd_t<CI, N, 2, OM>(ctx, lc, nz, tmap, a) : launch_fwd_t<CI, N, 1, OM>(ctx, lc, nz, tmap, a);
+        return mt == 2 ? launch_fwd_t<CI, N, 2, OM>(ctx, lc, nz, a) : launch_fwd_t<CI, N, 1, OM>(ctx, lc, nz, a);
     DARE_FWD(16, 16, OUT_STORE)
     DARE_FWD(16, 32, OUT_STORE)
     DARE_FWD(32, 16, OUT_STORE)
@@ -1594,8 +1563,7 @@ static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a, const float*
 }
 
 static size_t out_smem(const Geom& g, int mt, int slots) {
-    const int rows = strip_rows(g, mt);
-    const int RP = box_count(rows) * box_height(rows);
+    const int RP = round8(strip_rows(g, mt));
     return 9 * 2 * 16 * 16 + slots * (size_t)2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 + (2 * kMaxSlots + 5) * 8 +
            16;
 }
@@ -1629,10 +1597,7 @@ static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     OutArgs a = a0;
     a.ppc = lc.ppc;
     a.slots = lc.slots;
-    CUtensorMap tmap;
-    int rc = act_map(ctx, &tmap, a.in, 16, a.g.total, box_height(strip_rows(a.g, MT)));
-    if (rc) return rc;
-    kern<<<lc.grid, out_threads(MT), lc.smem, ctx->stream>>>(tmap, a);
+    kern<<<lc.grid, out_threads(MT), lc.smem, ctx->stream>>>(a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
@@ -1972,6 +1937,7 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         offs.push_back(bytes);
         bytes += (((size_t)T[s.level] * s.c + s.extra) * sizeof(bf16) + 255) / 256 * 256;
     }
+    bytes += (size_t)kActSlackRows * 16;  // rows a staged segment may read past the last array
     cudaError_t e = cudaMalloc(&net->act_block, bytes);
     if (e == cudaSuccess) e = cudaMemset(net->act_block, 0, bytes);
     for (size_t i = 0; i < sizeof(slots) / sizeof(slots[0]) && e == cudaSuccess; i++)

@@ -20,18 +20,22 @@ constexpr int kTileM = 128;    // output rows (padded positions) per MMA tile
 constexpr int kEpiThreads = 128;
 __host__ __device__ constexpr int fwd_threads(int mt) { return (5 + mt) * 32; }
 constexpr int kMaxSlots = 8;   // staged-plane ring depth limit
-// A staged plane segment of `rows` positions is loaded as box_count(rows)
-// TMA boxes of box_height(rows) positions (at most 256, a multiple of 8)
-// per 8-channel chunk.
-__host__ __device__ inline int box_count(int rows) { return (rows + 255) / 256; }
-__host__ __device__ inline int box_height(int rows) {
-    const int nb = box_count(rows);
-    return ((rows + nb - 1) / nb + 7) / 8 * 8;
-}
+// Rows of a staged plane segment, rounded to the 8-row core-matrix groups.
+__host__ __device__ inline int round8(int rows) { return (rows + 7) / 8 * 8; }
 
-// A level's activations live in a zero-padded, channels-last layout:
-// [(n0+2)][(n1+2)][(n2+2)][C] bf16, ghosts kept at zero, so every 3^3 tap is
-// a constant shift of the flattened padded position.
+// A level's activations live zero-padded, [(n0+2)][(n1+2)][(n2+2)] positions
+// with ghosts kept at zero, so every 3^3 tap is a constant shift of the
+// flattened padded position, and chunk-planar: the 8-channel chunk kc of
+// position Q is 16 contiguous bytes at element act_off(total, Q, kc).  A plane
+// segment of one chunk is then one contiguous run, staged by one bulk copy
+// straight into the K-major operand layout of the MMAs (core matrices of
+// 8 positions x 16 bytes).
+__host__ __device__ inline int64_t act_off(int64_t total, int64_t Q, int kc) { return ((int64_t)kc * total + Q) * 8; }
+// Rows past either end of a chunk plane that a staged segment may read (they
+// feed only outputs that are not stored); the activation block keeps this
+// many spare rows after its last array.
+constexpr int64_t kActSlackRows = 8192;
+
 struct Geom {
     int n0, n1, n2;   // internal cells
     int W;            // n2 + 2 (row length)
