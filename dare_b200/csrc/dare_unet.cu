@@ -1111,29 +1111,29 @@ __global__ void k_restrict(Geom f, Geom c, const bf16* __restrict__ fine, bf16* 
     }
 }
 
+// fine += scale * (nearest prolongation of coarse), one block per (chunk,
+// i, j) line of fine cells, its threads along k
 template <int C>
 __global__ void k_prolong_add(Geom f, Geom c, const bf16* __restrict__ coarse, bf16* __restrict__ fine, float scale) {
     constexpr int KC = C / 8;
-    const int64_t total = (int64_t)f.n0 * f.n1 * f.n2 * KC;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int kc = (int)(idx % KC);
-        int64_t v = idx / KC;
-        const int k = (int)(v % f.n2);
-        v /= f.n2;
-        const int j = (int)(v % f.n1);
-        const int i = (int)(v / f.n1);
-        const uint4 q = __ldg(reinterpret_cast<const uint4*>(
-            coarse + act_off(c.total, ((int64_t)(i / 2 + 1) * (c.n1 + 2) + (j / 2 + 1)) * c.W + (k / 2 + 1), kc)));
-        uint4* dst = reinterpret_cast<uint4*>(
-            fine + act_off(f.total, ((int64_t)(i + 1) * (f.n1 + 2) + (j + 1)) * f.W + (k + 1), kc));
-        const uint4 o = *dst;
-        uint4 r;
-        r.x = pack_bf16(bf16_lo(o.x) + scale * bf16_lo(q.x), bf16_hi(o.x) + scale * bf16_hi(q.x));
-        r.y = pack_bf16(bf16_lo(o.y) + scale * bf16_lo(q.y), bf16_hi(o.y) + scale * bf16_hi(q.y));
-        r.z = pack_bf16(bf16_lo(o.z) + scale * bf16_lo(q.z), bf16_hi(o.z) + scale * bf16_hi(q.z));
-        r.w = pack_bf16(bf16_lo(o.w) + scale * bf16_lo(q.w), bf16_hi(o.w) + scale * bf16_hi(q.w));
-        *dst = r;
+    const int lines = f.n0 * f.n1;
+    for (int line = blockIdx.x; line < lines * KC; line += gridDim.x) {
+        const int kc = line / lines;
+        const int ij = line - kc * lines;
+        const int i = ij / f.n1, j = ij - (ij / f.n1) * f.n1;
+        const int64_t fq = ((int64_t)(i + 1) * (f.n1 + 2) + (j + 1)) * f.W + 1;
+        const int64_t cq = ((int64_t)(i / 2 + 1) * (c.n1 + 2) + (j / 2 + 1)) * c.W + 1;
+        for (int k = threadIdx.x; k < f.n2; k += blockDim.x) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(coarse + act_off(c.total, cq + k / 2, kc)));
+            uint4* dst = reinterpret_cast<uint4*>(fine + act_off(f.total, fq + k, kc));
+            const uint4 o = *dst;
+            uint4 r;
+            r.x = pack_bf16(bf16_lo(o.x) + scale * bf16_lo(q.x), bf16_hi(o.x) + scale * bf16_hi(q.x));
+            r.y = pack_bf16(bf16_lo(o.y) + scale * bf16_lo(q.y), bf16_hi(o.y) + scale * bf16_hi(q.y));
+            r.z = pack_bf16(bf16_lo(o.z) + scale * bf16_lo(q.z), bf16_hi(o.z) + scale * bf16_hi(q.z));
+            r.w = pack_bf16(bf16_lo(o.w) + scale * bf16_lo(q.w), bf16_hi(o.w) + scale * bf16_hi(q.w));
+            *dst = r;
+        }
     }
 }
 
@@ -1715,7 +1715,8 @@ template <int C>
 static int prolong_add(dare_unet* net, int fl, const bf16* coarse, bf16* fine, float scale) {
     dare_ctx* ctx = net->ctx;
     const Geom& f = net->geo[fl];
-    k_prolong_add<C><<<eblocks(ctx, (int64_t)f.n0 * f.n1 * f.n2 * (C / 8)), 256, 0, ctx->stream>>>(
+    const int64_t lines = (int64_t)f.n0 * f.n1 * (C / 8);
+    k_prolong_add<C><<<(int)std::min<int64_t>(lines, (int64_t)ctx->num_sms * 16), 128, 0, ctx->stream>>>(
         f, net->geo[fl + 1], coarse, fine, scale);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
@@ -1732,7 +1733,11 @@ int apply(dare_unet* net, const float* u, float* z) {
     if ((rc = conv_forward(net, ENC3, net->P3, nullptr, OUT_STORE, net->E3, nullptr, nullptr, nullptr))) return rc;
     if ((rc = conv_forward(net, DEC3, net->E3, nullptr, OUT_ADDUP, nullptr, net->S2, nullptr, nullptr))) return rc;
     if ((rc = conv_forward(net, DEC2, net->S2, nullptr, OUT_ADDUP, nullptr, net->S1, nullptr, nullptr))) return rc;
-    if ((rc = conv_forward(net, DEC1, net->S1, nullptr, OUT_ADDUP, nullptr, net->S0, nullptr, nullptr))) return rc;
+    // dec1 stores its level-1 output (into dD1, free during the forward pass)
+    // and a streaming pass adds its prolongation into S0: that read-modify-
+    // write of S0 inside the convolution's epilogue was latency-bound
+    if ((rc = conv_forward(net, DEC1, net->S1, nullptr, OUT_STORE, net->dD1, nullptr, nullptr, nullptr))) return rc;
+    if ((rc = prolong_add<16>(net, 0, net->dD1, net->S0, 1.f))) return rc;
     return conv_forward(net, DEC0, net->S0, nullptr, OUT_F32, nullptr, nullptr, z, u);
 }
 

@@ -227,6 +227,7 @@ static void net_forward(Net* N, const double* u, int bf, double* z) {
     conv(&L[2], N->S2, 64, N->Wl[5], 32, t);               /* dec2 */
     prolong_add(&L[1], &L[2], t, 32, 1.0, N->S1, bf);
     conv(&L[1], N->S1, 32, N->Wl[6], 16, t);               /* dec1 */
+    round_all(t, L[1].cells * 16, bf);                     /* stored at level 1, then added */
     prolong_add(&L[0], &L[1], t, 16, 1.0, N->S0, bf);
     conv(&L[0], N->S0, 16, N->Wl[7], 1, t);                /* dec0 */
     for (int64_t c = 0; c < L[0].cells; c++) z[c] = bf ? (double)((float)u[c] + (float)t[c]) : u[c] + t[c];
