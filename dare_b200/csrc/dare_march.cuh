@@ -157,6 +157,7 @@ struct FInit {
     using type = T;
     static constexpr int Q = 2, NZ = 1, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const T* zs[2];   // x
     const T* ps[NP];  // coefficients, b
     T *r, *rh, *u, *v, *w;
@@ -182,6 +183,7 @@ struct FStep1 {
     using type = T;
     static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
+    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
     const T* zs[2];   // r, u
     const T* ps[NP];  // coefficients, r_hat_0
     T *u_out, *v;
@@ -203,6 +205,7 @@ struct FStep2 {
     using type = T;
     static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 3;
     static constexpr bool kCheckDone = true;
+    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const T* zs[2];   // v, r
     const T* ps[NP];  // coefficients, r_hat_0, u, x
     T *r_out, *s, *x;
@@ -225,6 +228,7 @@ struct FStep3 {
     using type = T;
     static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
+    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
     const T* zs[2];   // s, v
     const T* ps[NP];  // coefficients, r_hat_0
     T *v_out, *w;
@@ -247,6 +251,7 @@ struct FStep4 {
     using type = T;
     static constexpr int Q = 5, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 3;
     static constexpr bool kCheckDone = true;
+    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const T* zs[2];   // w, s
     const T* ps[NP];  // coefficients, r, u, v
     T *u, *r, *s_out, *t;
@@ -280,6 +285,7 @@ struct FResidual {
     using type = T;
     static constexpr int Q = 1, NZ = 1, NP = 8;
     static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const T* zs[2];   // x
     const T* ps[NP];  // 7 coefficients, b
     double* out;
@@ -297,6 +303,7 @@ struct FFold {
     using type = double;
     static constexpr int Q = 0, NZ = 1, NP = 6;
     static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const double* zs[2];   // invd
     const double* ps[NP];  // the 6 off-diagonals of A
     double* ahat;
@@ -645,16 +652,16 @@ inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, co
     return DARE_OK;
 }
 
-// Two cells per thread pays off for the functors with few per-cell streams
-// (steps 1 and 3: 256^3 step times 0.291 -> 0.257 ms and 0.289 -> 0.253 ms);
-// with nine streams and five dot products (steps 2 and 4) the halved warp
-// count per SM no longer hides the arithmetic (0.34 -> 0.45 ms), so those run
-// one cell per thread on the same 32 x 8 tiles.
+// Two cells per thread (K::kPairs) pays off for steps 1 and 3 (256^3: 0.291
+// -> 0.257 ms and 0.289 -> 0.253 ms); with nine streams and five dot products
+// (steps 2 and 4), or many outputs per cell (init, fold), the halved warp
+// count per SM no longer hides the work (step 2: 0.34 -> 0.45 ms, init: 0.29
+// -> 0.38 ms), so those run one cell per thread on the same 32 x 8 tiles.
 template <class K>
 inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
                         double* partials) {
     if (m.nitems > kMaxBlocks) return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
-    if (m.cpt == 2 && K::NP <= 7) return launch_march_t<K, 2>(ctx, g, m, kern, st, partials);
+    if (m.cpt == 2 && K::kPairs) return launch_march_t<K, 2>(ctx, g, m, kern, st, partials);
     if (m.cpt == 1) return launch_march_t<K, 1>(ctx, g, m, kern, st, partials);
     MarchCfg m1 = m;   // the same tiles, one cell per thread
     m1.cpt = 1;

@@ -63,6 +63,7 @@ struct FRefResidual {
     using type = double;
     static constexpr int Q = 1, NZ = 1, NP = 8;
     static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;
     const double* zs[2];   // x
     const double* ps[NP];  // 7 coefficients, b
     float* r32;
