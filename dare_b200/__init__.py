@@ -90,6 +90,10 @@ _SIGS = [
     ("dare_grid_destroy", C.c_int, [_P]),
     ("dare_grid_get_info", C.c_int, [_P, C.POINTER(GridInfo)]),
     ("dare_field_create", C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    ("dare_field_create_n", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P)]),
+    ("dare_field_num_components", C.c_int, [_P]),
+    ("dare_system_create_n", C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    ("dare_system_num_components", C.c_int, [_P]),
     ("dare_field_destroy", C.c_int, [_P]),
     ("dare_field_upload", C.c_int, [_P, C.c_int, _P]),
     ("dare_field_download", C.c_int, [_P, C.c_int, _P]),
@@ -320,14 +324,17 @@ class Grid:
 
 
 class Field:
-    """Time levels of ghosted grid vectors on the device (Data::Field)."""
+    """Time levels of ghosted grid vectors on the device (Data::Field<Grid,SC,N>).
 
-    def __init__(self, grid: Grid, num_levels: int = 2):
+    Host arrays interleave the components: ghosted[cell * N + c]."""
+
+    def __init__(self, grid: Grid, num_levels: int = 2, components: int = 1):
         self.grid = grid
         h = C.c_void_p()
-        _check(lib().dare_field_create(grid.h, num_levels, C.byref(h)), grid.ctx.h, "field_create")
+        _check(lib().dare_field_create_n(grid.h, num_levels, components, C.byref(h)), grid.ctx.h, "field_create")
         self.h = h
         self.num_levels = num_levels
+        self.components = components
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -336,14 +343,15 @@ class Field:
 
     def upload(self, values: np.ndarray, level: int = 0):
         a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
-        if a.size != self.grid.num_cells_ghosted:
+        if a.size != self.grid.num_cells_ghosted * self.components:
             raise ValueError("field upload expects the ghosted layout")
         _check(lib().dare_field_upload(self.h, level, _ptr(a)), self.grid.ctx.h, "field_upload")
 
     def download(self, level: int = 0, out: np.ndarray | None = None) -> np.ndarray:
         """Copy a level to the host; `out` (e.g. pinned memory) is filled in place when given."""
-        a = np.empty(self.grid.num_cells_ghosted, dtype=np.float64) if out is None else out.reshape(-1)
-        if a.size != self.grid.num_cells_ghosted or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        size = self.grid.num_cells_ghosted * self.components
+        a = np.empty(size, dtype=np.float64) if out is None else out.reshape(-1)
+        if a.size != size or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
             raise ValueError("field download expects a contiguous float64 ghosted buffer")
         _check(lib().dare_field_download(self.h, level, _ptr(a)), self.grid.ctx.h, "field_download")
         return a
@@ -412,13 +420,16 @@ class Assembly:
 
 
 class MatrixSystem:
-    """Structured 7-diagonal system A x = B (Matrix::Trilinos<SC>)."""
+    """Structured 7-diagonal system A x = B (Matrix::Trilinos<SC>); with N
+    components one stencil per component, rows and columns cell * N + c."""
 
-    def __init__(self, grid: Grid):
+    def __init__(self, grid: Grid, components: int = 1):
         self.grid = grid
         h = C.c_void_p()
-        _check(lib().dare_system_create(grid.h, C.byref(h)), grid.ctx.h, "system_create")
+        _check(lib().dare_system_create_n(grid.h, components, C.byref(h)), grid.ctx.h, "system_create")
         self.h = h
+        self.components = components
+        self.rows = grid.num_cells * components
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -440,14 +451,14 @@ class MatrixSystem:
         _check(lib().dare_system_set_coefficients(self.h, _ptr(d), _ptr(r), _ptr(x)), self.grid.ctx.h, "set_coef")
 
     def coefficients(self):
-        n = self.grid.num_cells
+        n = self.rows
         diag = np.empty((7, n), dtype=np.float64)
         rhs = np.empty(n, dtype=np.float64)
         _check(lib().dare_system_get_coefficients(self.h, _ptr(diag), _ptr(rhs)), self.grid.ctx.h, "get_coef")
         return diag, rhs
 
     def solution(self) -> np.ndarray:
-        x = np.empty(self.grid.num_cells, dtype=np.float64)
+        x = np.empty(self.rows, dtype=np.float64)
         _check(lib().dare_system_get_solution(self.h, _ptr(x)), self.grid.ctx.h, "get_solution")
         return x
 
@@ -459,7 +470,7 @@ class MatrixSystem:
 
     def export_csr(self):
         nnz = int(lib().dare_system_csr_nnz(self.h))
-        n = self.grid.num_cells
+        n = self.rows
         rowptr = np.empty(n + 1, dtype=np.int64)
         cols = np.empty(nnz, dtype=np.int64)
         vals = np.empty(nnz, dtype=np.float64)

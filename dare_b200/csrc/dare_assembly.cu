@@ -31,6 +31,7 @@ struct AsmParams {
     double bc_value[6];
     double tt;      // (V * 1) / dt, the DDT weight (evaluated once on the host: same IEEE result)
     double dn[3];   // 1 / dx per dimension (Gradient_Cartesian.inl:30-34)
+    int64_t dstride; // elements between two coefficient slots (cells x field components)
     int scheme;     // DARE_SCHEME_* of the div(...) terms
     int nexp;       // its explicit levels T
     double w[3];    // its weights w[0..T] (TimeDiscretizationSchemes.h:29-76)
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
     const int i0 = blockIdx.z * planes;
     const int i1 = min(i0 + planes, n0);
     if (i0 >= i1) return;
-    const int64_t n = g.ncell;
+    const int64_t n = a.dstride;
     const int64_t S0 = (int64_t)g.gn[1] * g.gn[2], S1 = g.gn[2];
     const int64_t nplane = (int64_t)n1 * n2;
     const int64_t jk = (int64_t)jj * n2 + kk;
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble3(GridDev g, AsmParams a, co
     const int jl = min(jj, n1 - 1);
     const int kl = min(kk, n2 - 1);
     const int kf = max(kl, 0);
-    const int64_t n = g.ncell;
+    const int64_t n = a.dstride;
     const int64_t S0 = (int64_t)g.gn[1] * g.gn[2], S1 = g.gn[2];
     const int64_t nplane = (int64_t)n1 * n2;
     const int64_t jk = (int64_t)jl * n2 + kf;
@@ -571,6 +572,7 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
         a.bc_value[f] = s->bc_value[f];
     }
     a.tt = a.dt > 0. ? (g.volume * 1.) / a.dt : 0.;
+    a.dstride = s->sdev.ncell;
     a.scheme = desc->scheme;
     a.nexp = scheme_weights(desc->scheme, a.w);
     if (a.nexp < 0) return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: unknown time scheme");
@@ -623,30 +625,48 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
             }
         }
         const dim3 grid3(gx3, gy3, (unsigned)((n0 + best - 1) / best)), block3(32, kAsmJ, 1);
-        switch (a.limiter) {
-#define DARE_ASM3(L)                                                                                     \
-    case L:                                                                                              \
-        k_assemble3<L><<<grid3, block3, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x, best); \
+        // one launch per field component (its field values, its rows)
+        for (int c = 0; c < s->ncomp; c++) {
+            const double* pc = phi + (size_t)c * g.ncell_ghosted;
+            const double* po = phi_old + (size_t)c * g.ncell_ghosted;
+            double* dc = s->diag + (size_t)c * g.ncell;
+            double* rc = s->rhs + (size_t)c * g.ncell;
+            double* xc = s->x + (size_t)c * g.ncell;
+            switch (a.limiter) {
+#define DARE_ASM3(L)                                                                  \
+    case L:                                                                           \
+        k_assemble3<L><<<grid3, block3, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, best); \
         break;
-            DARE_ASM3(DARE_LIMITER_CDS)
-            DARE_ASM3(DARE_LIMITER_UPWIND)
-            DARE_ASM3(DARE_LIMITER_VANALBADA)
-            DARE_ASM3(DARE_LIMITER_MINMOD)
-            DARE_ASM3(DARE_LIMITER_VANLEER)
+                DARE_ASM3(DARE_LIMITER_CDS)
+                DARE_ASM3(DARE_LIMITER_UPWIND)
+                DARE_ASM3(DARE_LIMITER_VANALBADA)
+                DARE_ASM3(DARE_LIMITER_MINMOD)
+                DARE_ASM3(DARE_LIMITER_VANLEER)
 #undef DARE_ASM3
+            }
+            DARE_LAUNCHED(ctx);
         }
-    } else if (g.dim == 2)
-        k_assemble<2><<<grid, block, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x, planes);
-    else
-        k_assemble<1><<<grid, block, 0, ctx->stream>>>(g, a, phi, phi_old, s->diag, s->rhs, s->x, planes);
-    DARE_LAUNCHED(ctx);
+        return DARE_OK;
+    }
+    for (int c = 0; c < s->ncomp; c++) {
+        const double* pc = phi + (size_t)c * g.ncell_ghosted;
+        const double* po = phi_old + (size_t)c * g.ncell_ghosted;
+        double* dc = s->diag + (size_t)c * g.ncell;
+        double* rc = s->rhs + (size_t)c * g.ncell;
+        double* xc = s->x + (size_t)c * g.ncell;
+        if (g.dim == 2)
+            k_assemble<2><<<grid, block, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, planes);
+        else
+            k_assemble<1><<<grid, block, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, planes);
+        DARE_LAUNCHED(ctx);
+    }
     return DARE_OK;
 }
 
 }  // namespace dare_gpu
 
 extern "C" int dare_assemble(dare_system* s, const dare_assembly_desc* desc, dare_field* field) {
-    if (!s || !desc || !field || field->grid != s->grid) return DARE_ERR_BAD_ARG;
+    if (!s || !desc || !field || field->grid != s->grid || field->ncomp != s->ncomp) return DARE_ERR_BAD_ARG;
     cudaSetDevice(s->grid->ctx->device);
     const double* phi = field->level[0];
     const double* phi_old = field->num_levels > 1 ? field->level[1] : field->level[0];

@@ -69,20 +69,23 @@ MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem) {
     const int64_t tiles = (int64_t)m.tiles_x * m.tiles_y;
     // Longest plane run that still leaves ~4 items per resident block (the
     // dynamic queue then ends with a short tail); each run re-reads 2 planes.
+    // With several field components (stacked along i) runs stay inside one.
+    const int nc = g.ncomp, n0c = n0 / nc;
     const int64_t want = (int64_t)ctx->num_sms * 3 * 4;
     int planes = 32;
-    while (planes > 4 && tiles * ((n0 + planes - 1) / planes) < want) planes /= 2;
-    while (tiles * ((n0 + planes - 1) / planes) > kMaxBlocks && planes < n0) planes *= 2;
-    if (planes > n0) planes = n0;
+    while (planes > 4 && tiles * nc * ((n0c + planes - 1) / planes) < want) planes /= 2;
+    while (tiles * nc * ((n0c + planes - 1) / planes) > kMaxBlocks && planes < n0c) planes *= 2;
+    if (planes > n0c) planes = n0c;
     m.planes = planes;
-    m.nitems = (int)(tiles * ((n0 + planes - 1) / planes));
+    m.cpc = (n0c + planes - 1) / planes;
+    m.nitems = (int)(tiles * nc * m.cpc);
     m.smem = 2 * (size_t)(tk * m.cpt + 2) * (tj + 2) * elem;
     return m;
 }
 
 int ensure_solver_ws(dare_system* s) {
     dare_ctx* ctx = s->grid->ctx;
-    const int64_t n = s->grid->dev.ncell;
+    const int64_t n = s->sdev.ncell;   // all field components
     if (s->ws && s->ws->n == n) return DARE_OK;
     dare_solver_ws_free(s->ws);
     s->ws = nullptr;
@@ -100,7 +103,7 @@ int ensure_solver_ws(dare_system* s) {
         dare_solver_ws_free(ws);
         return check_cuda(ctx, e, "bicgstab2 workspace");
     }
-    ws->march = march_config(ctx, s->grid->dev, sizeof(double));
+    ws->march = march_config(ctx, s->sdev, sizeof(double));
     ws->stream_blocks = grid_blocks(ctx, n, 256, 8);
     s->ws = ws;
     return DARE_OK;
@@ -339,7 +342,7 @@ template int run_iterations<float, true>(dare_ctx*, const GridDev&, const MarchC
 int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_report* rep) {
     using namespace dare_gpu;
     dare_ctx* ctx = s->grid->ctx;
-    const GridDev& g = s->grid->dev;
+    const GridDev& g = s->sdev;   // components stacked along i
     int rc = ensure_solver_ws(s);
     if (rc) return rc;
     dare_solver_ws* ws = s->ws;

@@ -49,6 +49,7 @@ struct MarchCfg {
     int nitems = 1;
     size_t smem = 0;
     int cpt = 1;      // cells per thread along k (2: paired 16-byte copies, needs an even n2)
+    int cpc = 1;      // plane runs per field component (items: tiles x cpc x components)
 };
 
 // ---- deterministic grid reduction -----------------------------------------

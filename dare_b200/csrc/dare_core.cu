@@ -250,15 +250,21 @@ int dare_grid_get_info(const dare_grid* g, dare_grid_info* info) {
 }
 
 int dare_field_create(dare_grid* g, int num_levels, dare_field** out) {
-    if (!g || !out || num_levels < 1 || num_levels > 8) return DARE_ERR_BAD_ARG;
+    return dare_field_create_n(g, num_levels, 1, out);
+}
+
+int dare_field_create_n(dare_grid* g, int num_levels, int num_components, dare_field** out) {
+    if (!g || !out || num_levels < 1 || num_levels > 8 || num_components < 1 || num_components > 64)
+        return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = g->ctx;
     *out = nullptr;
     dare_field* f = new (std::nothrow) dare_field();
     if (!f) return DARE_ERR_OOM;
     f->grid = g;
     f->num_levels = num_levels;
+    f->ncomp = num_components;
     cudaSetDevice(ctx->device);
-    const size_t bytes = (size_t)g->dev.ncell_ghosted * sizeof(double);
+    const size_t bytes = (size_t)g->dev.ncell_ghosted * num_components * sizeof(double);
     for (int l = 0; l < num_levels; l++) {
         cudaError_t e = cudaMalloc(&f->level[l], bytes);
         if (e == cudaSuccess) e = cudaMemsetAsync(f->level[l], 0, bytes, ctx->stream);
@@ -280,23 +286,58 @@ int dare_field_destroy(dare_field* f) {
     return DARE_OK;
 }
 
+// The host side of a field or system uses the reference's interleaved order
+// (GridVector.inl:68-71: data[cell * N + c]); the device keeps each component
+// contiguous.  These convert between the two through a host buffer.
+static void interleave(const double* comp_major, int64_t n, int ncomp, double* inter) {
+    for (int64_t i = 0; i < n; i++)
+        for (int c = 0; c < ncomp; c++) inter[i * ncomp + c] = comp_major[(int64_t)c * n + i];
+}
+static void deinterleave(const double* inter, int64_t n, int ncomp, double* comp_major) {
+    for (int c = 0; c < ncomp; c++)
+        for (int64_t i = 0; i < n; i++) comp_major[(int64_t)c * n + i] = inter[i * ncomp + c];
+}
+
+static int upload_interleaved(dare_ctx* ctx, double* dev, const double* host, int64_t n, int ncomp) {
+    if (ncomp == 1) {
+        DARE_CUDA(ctx, cudaMemcpyAsync(dev, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        std::vector<double> t((size_t)n * ncomp);
+        deinterleave(host, n, ncomp, t.data());
+        DARE_CUDA(ctx, cudaMemcpyAsync(dev, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return DARE_OK;
+}
+
+static int download_interleaved(dare_ctx* ctx, double* host, const double* dev, int64_t n, int ncomp) {
+    if (ncomp == 1) {
+        DARE_CUDA(ctx, cudaMemcpyAsync(host, dev, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::vector<double> t((size_t)n * ncomp);
+        DARE_CUDA(ctx, cudaMemcpyAsync(t.data(), dev, t.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        interleave(t.data(), n, ncomp, host);
+    }
+    return DARE_OK;
+}
+
 int dare_field_upload(dare_field* f, int level, const double* host) {
     if (!f || !host || level < 0 || level >= f->num_levels) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = f->grid->ctx;
-    DARE_CUDA(ctx, cudaMemcpyAsync(f->level[level], host, (size_t)f->grid->dev.ncell_ghosted * sizeof(double),
-                                   cudaMemcpyHostToDevice, ctx->stream));
+    int rc = upload_interleaved(ctx, f->level[level], host, f->grid->dev.ncell_ghosted, f->ncomp);
+    if (rc) return rc;
     DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return DARE_OK;
 }
 
 int dare_field_download(dare_field* f, int level, double* host) {
     if (!f || !host || level < 0 || level >= f->num_levels) return DARE_ERR_BAD_ARG;
-    dare_ctx* ctx = f->grid->ctx;
-    DARE_CUDA(ctx, cudaMemcpyAsync(host, f->level[level], (size_t)f->grid->dev.ncell_ghosted * sizeof(double),
-                                   cudaMemcpyDeviceToHost, ctx->stream));
-    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return DARE_OK;
+    return download_interleaved(f->grid->ctx, host, f->level[level], f->grid->dev.ncell_ghosted, f->ncomp);
 }
+
+int dare_field_num_components(const dare_field* f) { return f ? f->ncomp : DARE_ERR_BAD_ARG; }
 
 double* dare_field_device_ptr(dare_field* f, int level) {
     if (!f || level < 0 || level >= f->num_levels) return nullptr;
@@ -305,27 +346,41 @@ double* dare_field_device_ptr(dare_field* f, int level) {
 
 int dare_field_exchange_halo(dare_field* f) {
     if (!f) return DARE_ERR_BAD_ARG;
-    return launch_halo(f->grid->ctx, f->grid->dev, f->level[0]);
+    for (int c = 0; c < f->ncomp; c++) {
+        const int rc = launch_halo(f->grid->ctx, f->grid->dev, f->level[0] + (size_t)c * f->grid->dev.ncell_ghosted);
+        if (rc) return rc;
+    }
+    return DARE_OK;
 }
 
 int dare_field_copy_to_old(dare_field* f) {
     if (!f) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = f->grid->ctx;
-    const size_t bytes = (size_t)f->grid->dev.ncell_ghosted * sizeof(double);
+    const size_t bytes = (size_t)f->grid->dev.ncell_ghosted * f->ncomp * sizeof(double);
     for (int n = f->num_levels - 1; n > 0; n--)
         DARE_CUDA(ctx, cudaMemcpyAsync(f->level[n], f->level[n - 1], bytes, cudaMemcpyDeviceToDevice, ctx->stream));
     return DARE_OK;
 }
 
-int dare_system_create(dare_grid* g, dare_system** out) {
-    if (!g || !out) return DARE_ERR_BAD_ARG;
+int dare_system_create(dare_grid* g, dare_system** out) { return dare_system_create_n(g, 1, out); }
+
+int dare_system_create_n(dare_grid* g, int num_components, dare_system** out) {
+    if (!g || !out || num_components < 1 || num_components > 64) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = g->ctx;
     *out = nullptr;
+    if ((int64_t)g->dev.n[0] * num_components >= ((int64_t)1 << 30) ||
+        g->dev.ncell_ghosted * num_components >= ((int64_t)1 << 31))
+        return set_error(ctx, DARE_ERR_BAD_ARG, "dare_system_create: too many cells x components");
     dare_system* s = new (std::nothrow) dare_system();
     if (!s) return DARE_ERR_OOM;
     s->grid = g;
+    s->ncomp = num_components;
+    s->sdev = g->dev;
+    s->sdev.ncomp = num_components;
+    s->sdev.n[0] = g->dev.n[0] * num_components;
+    s->sdev.ncell = g->dev.ncell * num_components;
     cudaSetDevice(ctx->device);
-    const size_t n = (size_t)g->dev.ncell;
+    const size_t n = (size_t)s->sdev.ncell;
     cudaError_t e = cudaMalloc(&s->diag, n * kSlots * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&s->rhs, n * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&s->x, n * sizeof(double));
@@ -378,10 +433,14 @@ int dare_system_set_bc(dare_system* s, int face, int type, double value) {
 int dare_system_set_coefficients(dare_system* s, const double* diag7, const double* rhs, const double* x0) {
     if (!s) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = s->grid->ctx;
-    const size_t n = (size_t)s->grid->dev.ncell;
-    if (diag7) DARE_CUDA(ctx, cudaMemcpyAsync(s->diag, diag7, n * kSlots * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if (rhs) DARE_CUDA(ctx, cudaMemcpyAsync(s->rhs, rhs, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if (x0) DARE_CUDA(ctx, cudaMemcpyAsync(s->x, x0, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const int64_t n = s->grid->dev.ncell;
+    const int nc = s->ncomp;
+    int rc;
+    if (diag7)
+        for (int q = 0; q < kSlots; q++)
+            if ((rc = upload_interleaved(ctx, s->diag + (size_t)q * n * nc, diag7 + (size_t)q * n * nc, n, nc))) return rc;
+    if (rhs && (rc = upload_interleaved(ctx, s->rhs, rhs, n, nc))) return rc;
+    if (x0 && (rc = upload_interleaved(ctx, s->x, x0, n, nc))) return rc;
     DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return DARE_OK;
 }
@@ -389,9 +448,14 @@ int dare_system_set_coefficients(dare_system* s, const double* diag7, const doub
 int dare_system_get_coefficients(dare_system* s, double* diag7, double* rhs) {
     if (!s) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = s->grid->ctx;
-    const size_t n = (size_t)s->grid->dev.ncell;
-    if (diag7) DARE_CUDA(ctx, cudaMemcpyAsync(diag7, s->diag, n * kSlots * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    if (rhs) DARE_CUDA(ctx, cudaMemcpyAsync(rhs, s->rhs, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    const int64_t n = s->grid->dev.ncell;
+    const int nc = s->ncomp;
+    int rc;
+    if (diag7)
+        for (int q = 0; q < kSlots; q++)
+            if ((rc = download_interleaved(ctx, diag7 + (size_t)q * n * nc, s->diag + (size_t)q * n * nc, n, nc)))
+                return rc;
+    if (rhs && (rc = download_interleaved(ctx, rhs, s->rhs, n, nc))) return rc;
     DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return DARE_OK;
 }
@@ -402,15 +466,14 @@ int dare_system_set_initial_guess(dare_system* s, const double* x0) {
 
 int dare_system_get_solution(dare_system* s, double* x) {
     if (!s || !x) return DARE_ERR_BAD_ARG;
-    dare_ctx* ctx = s->grid->ctx;
-    DARE_CUDA(ctx, cudaMemcpyAsync(x, s->x, (size_t)s->grid->dev.ncell * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return DARE_OK;
+    return download_interleaved(s->grid->ctx, x, s->x, s->grid->dev.ncell, s->ncomp);
 }
+
+int dare_system_num_components(const dare_system* s) { return s ? s->ncomp : DARE_ERR_BAD_ARG; }
 
 double* dare_system_device_ptr(dare_system* s, int which) {
     if (!s) return nullptr;
-    if (which >= 0 && which < kSlots) return s->diag + (size_t)which * s->grid->dev.ncell;
+    if (which >= 0 && which < kSlots) return s->diag + (size_t)which * s->sdev.ncell;
     if (which == 7) return s->rhs;
     if (which == 8) return s->x;
     return nullptr;
@@ -439,13 +502,14 @@ int64_t dare_system_csr_nnz(dare_system* s) {
     for (int i = 0; i < g.n[0]; i++)
         for (int j = 0; j < g.n[1]; j++)
             for (int k = 0; k < g.n[2]; k++) nnz += __builtin_popcount(row_mask(g, i, j, k));
-    return nnz;
+    return nnz * s->ncomp;
 }
 
 int dare_system_export_csr(dare_system* s, int64_t* rowptr, int64_t* cols, double* vals) {
     if (!s || !rowptr || !cols || !vals) return DARE_ERR_BAD_ARG;
     const GridDev& g = s->grid->dev;
-    std::vector<double> diag((size_t)g.ncell * kSlots);
+    const int nc = s->ncomp;
+    std::vector<double> diag((size_t)g.ncell * nc * kSlots);   // interleaved rows: cell * N + c
     int rc = dare_system_get_coefficients(s, diag.data(), nullptr);
     if (rc) return rc;
     static const int emit_order[7] = {DARE_WEST, DARE_SOUTH, DARE_BOTTOM, DARE_CENTER, DARE_TOP, DARE_NORTH, DARE_EAST};
@@ -454,18 +518,22 @@ int dare_system_export_csr(dare_system* s, int64_t* rowptr, int64_t* cols, doubl
     for (int i = 0; i < g.n[0]; i++)
         for (int j = 0; j < g.n[1]; j++)
             for (int k = 0; k < g.n[2]; k++) {
-                const int64_t c = ((int64_t)i * g.n[1] + j) * g.n[2] + k;
+                const int64_t cell = ((int64_t)i * g.n[1] + j) * g.n[2] + k;
                 const unsigned m = row_mask(g, i, j, k);
                 int64_t nb[7];
-                neighbour_ordinals(g, i, j, k, c, nb);
+                neighbour_ordinals(g, i, j, k, cell, nb);
+                // MatrixBlock::Finalize per component: column = neighbour * N + c
+                // (MatrixBlock_Cartesian.inl:127-240), rows cell * N + c
+                for (int comp = 0; comp < nc; comp++) {
+                const int64_t c = cell * nc + comp;
                 int64_t rc_[7];
                 double rv[7];
                 int cnt = 0;
                 for (int e = 0; e < 7; e++) {
                     const int p = emit_order[e];
                     if (!(m & (1u << p))) continue;
-                    rc_[cnt] = nb[p];
-                    rv[cnt] = diag[(size_t)p * g.ncell + c];
+                    rc_[cnt] = nb[p] * nc + comp;
+                    rv[cnt] = diag[(size_t)p * g.ncell * nc + c];
                     cnt++;
                 }
                 for (int a = 1; a < cnt; a++) {        // sort by column
@@ -486,13 +554,19 @@ int dare_system_export_csr(dare_system* s, int64_t* rowptr, int64_t* cols, doubl
                     pos++;
                 }
                 rowptr[c + 1] = pos;
+                }
             }
     return DARE_OK;
 }
 
 int dare_system_copy_to(dare_system* s, dare_field* f) {
-    if (!s || !f || f->grid != s->grid) return DARE_ERR_BAD_ARG;
-    return launch_scatter(s->grid->ctx, s->grid->dev, s->x, f->level[0]);
+    if (!s || !f || f->grid != s->grid || f->ncomp != s->ncomp) return DARE_ERR_BAD_ARG;
+    const GridDev& g = s->grid->dev;
+    for (int c = 0; c < s->ncomp; c++) {
+        const int rc = launch_scatter(s->grid->ctx, g, s->x + (size_t)c * g.ncell, f->level[0] + (size_t)c * g.ncell_ghosted);
+        if (rc) return rc;
+    }
+    return DARE_OK;
 }
 
 int dare_face_average(dare_grid* gr, const double* cell_D, double* face_D[3]) {

@@ -32,6 +32,10 @@ struct GridDev {             // passed by value to kernels
     double dx[3];
     double volume;
     double area[3];
+    // Solver view of a system with several field components: the components
+    // are stacked along i (n[0] = ncomp x the grid's n0, ncell likewise), each
+    // component's planes wrapping among themselves on a periodic x.
+    int ncomp = 1;
 };
 
 }  // namespace dare_gpu
@@ -74,6 +78,7 @@ struct dare_grid {
 struct dare_field {
     dare_grid* grid = nullptr;
     int num_levels = 0;
+    int ncomp = 1;                // components, stored component-major: level[l][c * ncell_ghosted + cell]
     double* level[8] = {nullptr};
 };
 
@@ -82,10 +87,12 @@ void dare_solver_ws_free(dare_solver_ws* ws);
 
 struct dare_system {
     dare_grid* grid = nullptr;
+    int ncomp = 1;               // field components (block-diagonal, one 7-point stencil each)
+    dare_gpu::GridDev sdev{};    // the solver's view: components stacked along i
     int bc_type[6] = {0, 0, 0, 0, 0, 0};
     double bc_value[6] = {0, 0, 0, 0, 0, 0};
-    double* diag = nullptr;   // 7 * ncell
-    double* rhs = nullptr;
+    double* diag = nullptr;   // [7][ncomp][ncell], component-major within a slot
+    double* rhs = nullptr;    // [ncomp][ncell]
     double* x = nullptr;
     dare_solver_ws* ws = nullptr;
 };

@@ -390,6 +390,8 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     dare_ctx* ctx = s->grid->ctx;
     const GridDev& g = s->grid->dev;
     if (net->ctx != ctx) return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: network on another context");
+    if (s->ncomp != 1)
+        return set_error(ctx, DARE_ERR_UNSUPPORTED, "bicgstab2_learned: the network preconditions one field component");
     if (g.dim != 3 || g.n[0] != net->n[0] || g.n[1] != net->n[1] || g.n[2] != net->n[2])
         return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: grid does not match the network");
     if (lp->iteration_budget < 1 || lp->inner_max_it < 1 || !(lp->inner_rel_tol > 0.))

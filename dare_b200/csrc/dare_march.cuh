@@ -426,6 +426,7 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = tx + TK * ty;
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int n0c = n0 / g.ncomp;               // planes of one field component
     const int p0 = g.periodic[0], p1 = g.periodic[1], p2 = g.periodic[2];
     const int64_t plane = (int64_t)n1 * n2;
     const int tiles = m.tiles_x * m.tiles_y;
@@ -433,6 +434,7 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
     // Geometry of one work item for this thread.
     struct Geo {
         int i0, i1;
+        int cb;        // first stacked plane of this item's component
         bool inside, hS, hN, hB, hT;
         int64_t o_c, o_s, o_n, o_b, o_t, o_own;
     };
@@ -461,8 +463,11 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
         const int chunk = item / tiles;
         const int kk = (tile_id % m.tiles_x) * TW + CPT * tx;   // this thread's first cell
         const int jj = (tile_id / m.tiles_x) * TJ + ty;
-        G.i0 = chunk * m.planes;
-        G.i1 = min(G.i0 + m.planes, n0);
+        // runs of planes never cross from one field component to the next
+        const int comp = g.ncomp > 1 ? chunk / m.cpc : 0;
+        G.cb = comp * n0c;
+        G.i0 = G.cb + (chunk - comp * m.cpc) * m.planes;
+        G.i1 = min(G.i0 + m.planes, G.cb + n0c);
         // (n2 is even when CPT = 2, so a thread's cells are both inside or both outside)
         G.inside = jj < n1 && kk < n2;
         const bool edge = jj <= n1 && kk <= n2;   // the first row / column past the grid is read as halo
@@ -484,15 +489,15 @@ __global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* s
     auto stage = [&](const Geo& G, int p, bool full) {
         T* sb = smem + (size_t)slot_of(G, p) * STAGE;
         bool pv = true;
-        int pp = p;
+        int pp = p - G.cb;   // plane within the component, wrapped on a periodic x
         if (pp < 0) {
             pv = p0;
-            pp += n0;
-        } else if (pp >= n0) {
+            pp += n0c;
+        } else if (pp >= n0c) {
             pv = p0;
-            pp -= n0;
+            pp -= n0c;
         }
-        const int64_t base = (int64_t)pp * plane;
+        const int64_t base = (int64_t)(G.cb + pp) * plane;
         const int col = IC + CPT * tx;
 #pragma unroll
         for (int z = 0; z < NZ; z++) {

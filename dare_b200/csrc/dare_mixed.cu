@@ -91,7 +91,7 @@ static int read_scalar(dare_ctx* ctx, const double* dptr, double* out) {
 int dare_bicgstab2_refine(dare_system* s, const dare_solver_params* p, dare_solve_report* rep) {
     using namespace dare_gpu;
     dare_ctx* ctx = s->grid->ctx;
-    const GridDev& g = s->grid->dev;
+    const GridDev& g = s->sdev;   // components stacked along i
     if (p->precond != DARE_PREC_JACOBI)
         return set_error(ctx, DARE_ERR_UNSUPPORTED, "FP32 refinement is built for the Jacobi-folded operator");
     int rc = ensure_solver_ws(s);

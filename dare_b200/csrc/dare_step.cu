@@ -20,7 +20,7 @@ extern "C" {
 
 int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc, const dare_solver_params* p,
                   dare_solve_report* rep) {
-    if (!s || !f || !desc || !p || !rep || f->grid != s->grid) return DARE_ERR_BAD_ARG;
+    if (!s || !f || !desc || !p || !rep || f->grid != s->grid || f->ncomp != s->ncomp) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = s->grid->ctx;
     cudaSetDevice(ctx->device);
     const double* phi = f->level[0];
@@ -41,9 +41,9 @@ int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
             cudaGetLastError();
         }
     }
-    rc = launch_scatter(ctx, s->grid->dev, s->x, f->level[0]);       // Trilinos::CopyTo
+    rc = dare_system_copy_to(s, f);                                   // Trilinos::CopyTo
     if (rc) return rc;
-    rc = launch_halo(ctx, s->grid->dev, f->level[0]);                // Field::ExchangeHaloCells
+    rc = dare_field_exchange_halo(f);                                 // Field::ExchangeHaloCells
     if (rc) return rc;
     return dare_field_copy_to_old(f);                                // CopyDataVectorsToOldTimeStep
 }

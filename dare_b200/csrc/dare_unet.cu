@@ -2110,6 +2110,8 @@ int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const 
     const GridDev& g = s->grid->dev;
     if (g.dim != 3 || g.n[0] != net->n[0] || g.n[1] != net->n[1] || g.n[2] != net->n[2])
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_unet_train_on_system: grid does not match the network");
+    if (s->ncomp != 1)
+        return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_train_on_system: one field component only");
     cudaSetDevice(ctx->device);
     std::memset(rep, 0, sizeof(*rep));
     const int64_t n = net->ncell;

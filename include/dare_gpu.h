@@ -181,6 +181,11 @@ DARE_API int dare_grid_get_info(const dare_grid* g, dare_grid_info* info);
 /* ---- field: Field<Grid,SC,1> time levels of ghosted GridVectors
  *      Data/Field.h:47-138, Data/GridVector.h:42-251 (level 0 = new, 1 = old) */
 DARE_API int dare_field_create(dare_grid* g, int num_levels, dare_field** out);
+/* Field<Grid,SC,N> with N = num_components (1..64): host arrays of upload and
+ * download interleave the components, ghosted[cell * N + c]
+ * (Data/GridVector.inl:68-71); halo exchange and copy-to-old act on every component. */
+DARE_API int dare_field_create_n(dare_grid* g, int num_levels, int num_components, dare_field** out);
+DARE_API int dare_field_num_components(const dare_field* f);
 DARE_API int dare_field_destroy(dare_field* f);
 DARE_API int dare_field_upload(dare_field* f, int level, const double* host_ghosted);
 DARE_API int dare_field_download(dare_field* f, int level, double* host_ghosted);
@@ -208,6 +213,16 @@ DARE_API int dare_vtk_write_host(int dim, const int64_t n[3], const double size[
 /* ---- linear system: the structured 7-diagonal form of Trilinos<SC>'s A, x, B
  *      (MatrixSystem/Trilinos.h:51-314) -------------------------------------- */
 DARE_API int dare_system_create(dare_grid* g, dare_system** out);
+/* MatrixBlock<Cartesian<Dim>,GO,SC,N>: one 7-point stencil per component, no
+ * coupling between components (Grid/Cartesian/MatrixBlock_Cartesian.h); rows
+ * and columns interleave the components, row = cell * N + c, column =
+ * neighbour * N + c (MatrixBlock_Cartesian.inl:127-240), in the host arrays of
+ * set/get_coefficients ([7][ncell * N]), the initial guess, the solution and
+ * the CSR export.  Assembly applies the descriptor to each component of an
+ * N-component field; one BiCGStab2 iteration runs on all components together
+ * (the reference solves the whole row map). */
+DARE_API int dare_system_create_n(dare_grid* g, int num_components, dare_system** out);
+DARE_API int dare_system_num_components(const dare_system* s);
 DARE_API int dare_system_destroy(dare_system* s);
 /* face: DARE_WEST..DARE_TOP; non-periodic faces need DIRICHLET or NEUMANN */
 DARE_API int dare_system_set_bc(dare_system* s, int face, int type, double value);

@@ -110,8 +110,9 @@ private:
 // Field: time levels of ghosted GridVectors on the device (level 0 = new).
 class Field {
 public:
-    Field(Cartesian& grid, int num_timesteps = 2) : grid_(&grid) {
-        check(dare_field_create(grid.get(), num_timesteps, &h_), ctx(), "dare_field_create");
+    // num_components: Field<Grid,SC,N>; host arrays interleave them (cell * N + c)
+    Field(Cartesian& grid, int num_timesteps = 2, int num_components = 1) : grid_(&grid) {
+        check(dare_field_create_n(grid.get(), num_timesteps, num_components, &h_), ctx(), "dare_field_create");
     }
     ~Field() {
         if (h_) dare_field_destroy(h_);
@@ -121,17 +122,19 @@ public:
     dare_field* get() const { return h_; }
     Cartesian& GetGrid() const { return *grid_; }
 
+    int GetNumComponents() const { return dare_field_num_components(h_); }
     void Upload(const std::vector<double>& ghosted, int level = 0) {
-        if ((int64_t)ghosted.size() != grid_->GetNumberLocalCells()) throw Error("Field::Upload: size", DARE_ERR_BAD_ARG);
+        if ((int64_t)ghosted.size() != grid_->GetNumberLocalCells() * GetNumComponents())
+            throw Error("Field::Upload: size", DARE_ERR_BAD_ARG);
         check(dare_field_upload(h_, level, ghosted.data()), ctx(), "dare_field_upload");
     }
     std::vector<double> Download(int level = 0) const {
-        std::vector<double> v((size_t)grid_->GetNumberLocalCells());
+        std::vector<double> v((size_t)(grid_->GetNumberLocalCells() * GetNumComponents()));
         check(dare_field_download(h_, level, v.data()), ctx(), "dare_field_download");
         return v;
     }
     void SetValues(double value, int level = 0) {
-        Upload(std::vector<double>((size_t)grid_->GetNumberLocalCells(), value), level);
+        Upload(std::vector<double>((size_t)(grid_->GetNumberLocalCells() * GetNumComponents()), value), level);
     }
     // Field::ExchangeHaloCells (Field.inl:100-103)
     void ExchangeHaloCells() { check(dare_field_exchange_halo(h_), ctx(), "exchange_halo"); }
@@ -189,8 +192,9 @@ struct Assembly {
 // Matrix::Trilinos<SC>: A, x, B of the structured system on the device.
 class Trilinos {
 public:
-    explicit Trilinos(Cartesian& grid) : grid_(&grid) {
-        check(dare_system_create(grid.get(), &h_), ctx(), "dare_system_create");
+    // num_components: one 7-point stencil per component, rows cell * N + c
+    explicit Trilinos(Cartesian& grid, int num_components = 1) : grid_(&grid) {
+        check(dare_system_create_n(grid.get(), num_components, &h_), ctx(), "dare_system_create");
     }
     ~Trilinos() {
         if (h_) dare_system_destroy(h_);
@@ -208,12 +212,14 @@ public:
         dare_assembly_desc d = functor.Desc();
         check(dare_assemble(h_, &d, field.get()), ctx(), "dare_assemble");
     }
-    // Host-built MatrixBlocks: SoA diag[7][cells] (slots CENTER..TOP), rhs, x0
+    // Host-built MatrixBlocks: SoA diag[7][cells * N] (slots CENTER..TOP, rows
+    // cell * N + c), rhs, x0
     void SetBlocks(const std::vector<double>& diag7, const std::vector<double>& rhs, const std::vector<double>& x0) {
         check(dare_system_set_coefficients(h_, diag7.data(), rhs.data(), x0.data()), ctx(), "set_coefficients");
     }
+    int GetNumComponents() const { return dare_system_num_components(h_); }
     std::vector<double> GetX() const {
-        std::vector<double> x((size_t)grid_->GetNumberLocalCellsInternal());
+        std::vector<double> x((size_t)(grid_->GetNumberLocalCellsInternal() * GetNumComponents()));
         check(dare_system_get_solution(h_, x.data()), ctx(), "get_solution");
         return x;
     }
@@ -222,7 +228,7 @@ public:
     // CSR rows sorted by column, as Trilinos::PrintRow shows them
     void ExportCSR(std::vector<int64_t>& rowptr, std::vector<int64_t>& cols, std::vector<double>& vals) {
         const int64_t nnz = dare_system_csr_nnz(h_);
-        rowptr.resize((size_t)grid_->GetNumberLocalCellsInternal() + 1);
+        rowptr.resize((size_t)(grid_->GetNumberLocalCellsInternal() * GetNumComponents()) + 1);
         cols.resize((size_t)nnz);
         vals.resize((size_t)nnz);
         check(dare_system_export_csr(h_, rowptr.data(), cols.data(), vals.data()), ctx(), "export_csr");

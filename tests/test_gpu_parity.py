@@ -425,3 +425,116 @@ def test_vtk_writer_device_matches_host(ctx, tmp_path):
     D.write_vtk_host(n, size, 2, [b], ["phi_old"], str(tmp_path / "host"), "Old", 7)
     for rel in ("Cartesian3D_7.pvts", "Cartesian3D_7/Cartesian3D_7_0.vts", "Old_7.pvts", "Old_7/Old_7_0.vts"):
         assert (tmp_path / "dev" / rel).read_bytes() == (tmp_path / "host" / rel).read_bytes(), rel
+
+
+# ---- several field components (Field<Grid,SC,N>, MatrixBlock<...,N>) ----------
+def _interleave_csr(csrs):
+    """Rows cell * N + c and columns neighbour * N + c from one CSR per component
+    (MatrixBlock_Cartesian.inl:127-240: no coupling between components)."""
+    N = len(csrs)
+    rp0 = csrs[0][0]
+    ncell = rp0.size - 1
+    rows, cols, vals = [], [], []
+    for cell in range(ncell):
+        for c, (rp, co, va) in enumerate(csrs):
+            a, b = rp[cell], rp[cell + 1]
+            rows.append(b - a)
+            cols.append(co[a:b] * N + c)
+            vals.append(va[a:b])
+    rowptr = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
+    return rowptr, np.concatenate(cols).astype(np.int64), np.concatenate(vals)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_multicomponent_linear_profiles(ctx, dim):
+    """test_integration_Cartesian_Trilinos.cpp (N = 3 components, SolveScalar
+    variants): every component its own Dirichlet values; rows cell * 3 + c."""
+    n = [20 + d for d in range(dim)]
+    bvals = [(0.0, 1.0), (1.0, 0.0), (-1.0, 2.0)]
+    parts = [profile_functor_diag(dim, n, w, e) for w, e in bvals]
+    N = len(parts)
+    ncell = int(np.prod(n))
+    diag = np.stack([p[0] for p in parts], axis=-1).reshape(7, ncell * N)
+    rhs = np.stack([p[1] for p in parts], axis=-1).reshape(-1)
+    x0 = np.stack([p[2] for p in parts], axis=-1).reshape(-1)
+    g = D.Grid(ctx, n, [1.0 + d for d in range(dim)], 2, None)
+    s = D.MatrixSystem(g, components=N)
+    s.set_coefficients(diag, rhs, x0)
+    d2, r2 = s.coefficients()
+    np.testing.assert_array_equal(d2, diag)
+    np.testing.assert_array_equal(r2, rhs)
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-14, "Maximum Iterations": 5000}, precond="JACOBI").solve(s)
+    assert rep["converged"], rep
+    x = s.solution().reshape(ncell, N)
+    nn = n + [1] * (3 - dim)
+    i = np.repeat(np.arange(nn[0]), nn[1] * nn[2])
+    for c, (w, e) in enumerate(bvals):
+        assert np.max(np.abs(x[:, c] - (w + (e - w) * (i + 0.5) / nn[0]))) < 1e-8
+    # the exported pattern interleaves the components, and the oracle's
+    # BiCGStab2 on that matrix gives the same solution
+    rp, cols, vals = _interleave_csr([diag_to_csr(dim, n, p[0]) for p in parts])
+    grp, gcols, gvals = s.export_csr()
+    np.testing.assert_array_equal(grp, rp)
+    np.testing.assert_array_equal(gcols, cols)
+    np.testing.assert_array_equal(gvals, vals)
+    ox, info = O.bicgstab2(rp, cols, vals, rhs, x0, 1e-14, 5000, O.PREC_JACOBI)
+    assert rel_l2(x.reshape(-1), ox) < SOL_TOL
+    assert abs(rep["iters"] - info["iters"]) <= max(2, info["iters"] // 10)
+
+
+@pytest.mark.parametrize("periodic", [(1, 1, 1), (0, 1, 0)])
+def test_multicomponent_assembly_and_timeloop(ctx, periodic):
+    """Two components of one convected scalar pair: the descriptor applies to
+    each component's values (bit-exact), one BiCGStab2 runs on both (runs of
+    planes and the periodic x wrap stay inside a component)."""
+    case = _random_case("tiles3d", 5)
+    n = case["n"]
+    case["periodic"] = periodic
+    case["bc"] = {} if periodic[0] else {1: (1, 0.3), 2: (2, 0.0), 5: (2, 0.0), 6: (1, -0.5)}
+    rng = np.random.default_rng(9)
+    shape = tuple(x + 4 for x in n)
+    comps = [rng.random(shape), 0.5 + 0.25 * rng.random(shape)]
+    old = [rng.random(shape), rng.random(shape)]
+    N = len(comps)
+    inter = lambda arrs: np.stack([a.reshape(-1) for a in arrs], axis=-1).reshape(-1)
+    g = D.Grid(ctx, n, case["size"], 2, periodic)
+    f = D.Field(g, 2, components=N)
+    f.upload(inter(comps), 0)
+    f.upload(inter(old), 1)
+    np.testing.assert_array_equal(f.download(0), inter(comps))
+    s = D.MatrixSystem(g, components=N)
+    for face, (kind, val) in case["bc"].items():
+        s.set_bc(int(face), kind, val)
+    keep = [D.DeviceArray(np.asarray(a)) for a in case["face_vel"]] + [D.DeviceArray(np.asarray(a)) for a in
+                                                                      case["face_D"]]
+    asm = D.Assembly(dt=case["dt"], face_D=tuple(keep[3:]), face_vel=tuple(keep[:3]), limiter="VANLEER")
+    s.build(f, asm)
+    diag, rhs = s.coefficients()
+    og = oracle_grid(case)
+    desc = oracle_assembly(og, case, face_D=case["face_D"])
+    per = [O.assemble(desc, np.ascontiguousarray(c.reshape(-1)), np.ascontiguousarray(o.reshape(-1)))
+           for c, o in zip(comps, old)]
+    ncell = int(np.prod(n))
+    np.testing.assert_array_equal(diag, np.stack([p[0] for p in per], axis=-1).reshape(7, ncell * N))
+    np.testing.assert_array_equal(rhs, np.stack([p[1] for p in per], axis=-1).reshape(-1))
+    # two implicit steps against the oracle's solve of the interleaved system
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    ocomps = [c.reshape(-1).copy() for c in comps]
+    oold = [o.reshape(-1).copy() for o in old]
+    for _ in range(2):
+        rep = D.timestep(s, f, asm, solver)
+        assert rep["converged"], rep
+        per = [O.assemble(desc, c, o) for c, o in zip(ocomps, oold)]
+        rp, cols, vals = _interleave_csr([O.export_csr(og, p[0], p[2]) for p in per])
+        b = np.stack([p[1] for p in per], axis=-1).reshape(-1)
+        x0 = np.stack([O.field_to_vector(og, c) for c in ocomps], axis=-1).reshape(-1)
+        x, info = O.bicgstab2(rp, cols, vals, b, x0, 1e-10 * np.linalg.norm(b), 5000)
+        xs = x.reshape(ncell, N)
+        for c in range(N):
+            O.copy_to_field(og, np.ascontiguousarray(xs[:, c]), ocomps[c])
+            O.exchange_halo(og, ocomps[c])
+            oold[c] = ocomps[c].copy()
+        got = f.download(0).reshape(-1, N)
+        for c in range(N):
+            assert rel_l2(interior(got[:, c], g.ghosted_shape), interior(ocomps[c], g.ghosted_shape)) < SOL_TOL
+        assert abs(rep["iters"] - info["iters"]) <= 2
