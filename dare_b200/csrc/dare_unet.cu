@@ -729,18 +729,25 @@ struct OutArgs {
 // 4 epilogue warps, producer, one MMA warp per M tile
 __host__ __device__ constexpr int out_threads(int mt) { return (5 + mt) * 32; }
 
-// dec0 forward: 16 -> 1 channel, z = res + conv.  The 9 (di, dj) shifts are
-// start addresses of the A operand (rows of a staged plane, as in
-// k_conv_fwd), the 3 dk taps are the N columns of the MMA (N = 16, 13 zero):
-//     D[q][dk] = sum_{di,dj} sum_ci X[q + (di-1, dj-1, 0)][ci] W[(di,dj,dk)][ci]
-// accumulates 9 MMAs in TMEM, and out[p] = D[p-1][0] + D[p][1] + D[p+1][2]:
-// 9 MMAs per 126 outputs instead of 27 per 128.
+// dec0 forward: 16 -> 1 channel, z = res + conv.  Each staged INPUT plane p
+// gets its own accumulator with the (di, dk) taps in N (N = 16, 9 used):
+//     D_p[q][3 di + dk] = sum_dj sum_ci X_p[q + (dj-1) W][ci] W[(di,dj,dk)][ci]
+// i.e. 3 MMAs per input plane (one per dj, whose shift is the A operand's
+// start row), and output plane I takes, for di = 0, 1, 2, the di columns of
+// the accumulator of input plane I - 1 + di:
+//     out[m] = sum_di  D_{I-1+di}[m-1][3 di] + D_{I-1+di}[m][3 di + 1] + D_{I-1+di}[m+1][3 di + 2]
+// (m = 1 .. 126 of a 128-row tile): 3 MMAs per 126 outputs per plane
+// instead of 9.  An accumulator is complete after its plane's MMAs and last
+// read by output plane p + 1, so four of them rotate (p mod 4): three read by
+// the epilogue while the MMAs fill the fourth.
+constexpr int kOutAcc = 4;
+
 template <int MT>
 __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr uint32_t WB = 9 * 2 * 16 * 16;
-    constexpr uint32_t ACOLS = MT * 16;
-    constexpr uint32_t COLS = 2 * ACOLS <= 32 ? 32 : 64;
+    constexpr uint32_t WB = 3 * 2 * 16 * 16;       // [3 dj][2 kc][16 n][8] bf16
+    constexpr uint32_t ACOLS = MT * 16;            // one accumulator (all tiles)
+    constexpr uint32_t COLS = kOutAcc * ACOLS <= 64 ? 64 : 128;
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int S = a.slots;
@@ -752,9 +759,9 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     uint64_t* bars = reinterpret_cast<uint64_t*>(dsm + 2 * MT * kTileM * 3);
     uint64_t* full = bars;
     uint64_t* empty = bars + kMaxSlots;
-    uint64_t* accf = bars + 2 * kMaxSlots;
-    uint64_t* acce = accf + 2;
-    uint64_t* drain = acce + 2;
+    uint64_t* accf = bars + 2 * kMaxSlots;       // [kOutAcc]
+    uint64_t* acce = accf + kOutAcc;             // [kOutAcc]
+    uint64_t* drain = acce + kOutAcc;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
@@ -768,7 +775,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], MT);
         }
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < kOutAcc; b++) {
             mbar_init(&accf[b], MT);
             mbar_init(&acce[b], kEpiThreads);
         }
@@ -789,6 +796,8 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     // segment row 0 is position P0 - 1 - W: D row m of tile mt (position
     // P0 - 1 + 126 mt + m) reads segment rows 126 mt + m + dj W
     const int pbase = P0 - 1 - g.W;
+    // accumulator of input plane p: (p - (I0 - 1)) mod 4
+    auto accb = [&](int p) { return (p - I0 + 1) & (kOutAcc - 1); };
 
     if (warp == 4) {
         // ---- producer: one bulk copy per chunk plane segment ----
@@ -808,44 +817,37 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
         }
         __syncwarp();
     } else if (warp >= 5) {
-        // ---- MMA: 9 (di, dj) shifts per output plane, M tile mt = warp - 5 ----
+        // ---- MMA: 3 dj shifts per input plane, M tile mt = warp - 5 ----
         const int mt = warp - 5;
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16(kTileM, 16, 0, 0);
             const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
             const uint64_t adesc = smem_desc(0, RP * 16, 128), bdesc = smem_desc(0, 16 * 16, 128);
             const uint32_t w16 = (uint32_t)g.W * 16;
-            uint32_t fph = 0, aph = 3u;
+            uint32_t fph = 0, aph = 0xFu;  // fresh accumulators pass their first wait
             bool ok = true;
-            for (int I = I0; I <= I1 && ok; I++) {
-                const int buf = (I - I0) & 1;
-                for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1 && ok; p++) {
-                    const int sp = p % S;
-                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 22);
-                    fph ^= 1u << sp;
-                }
-                if (ok) ok = role_wait(&acce[buf], (aph >> buf) & 1u, abort_flag, a.err, 23);
-                aph ^= 1u << buf;
+            for (int p = I0 - 1; p <= I1 + 1 && ok; p++) {
+                const int sp = p % S, b = accb(p);
+                ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 22);
+                fph ^= 1u << sp;
+                if (ok) ok = role_wait(&acce[b], (aph >> b) & 1u, abort_flag, a.err, 23);
+                aph ^= 1u << b;
                 if (!ok) break;
                 fence_after_sync();
-                const uint32_t sb[3] = {sl0 + (uint32_t)((I - 1) % S) * SB, sl0 + (uint32_t)(I % S) * SB,
-                                        sl0 + (uint32_t)((I + 1) % S) * SB};
+                const uint32_t ab = sl0 + (uint32_t)sp * SB + (uint32_t)(mt * kOutStride) * 16;
 #pragma unroll
-                for (int g9 = 0; g9 < 9; g9++) {
-                    const int di = g9 / 3, dj = g9 % 3;
-                    mma_bf16(tmem + buf * ACOLS + mt * 16,
-                             adesc | (((sb[di] + dj * w16 + (uint32_t)(mt * kOutStride) * 16) >> 4) & 0x3FFFu),
-                             bdesc | (((wa + (uint32_t)(g9 * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc, g9 ? 1u : 0u);
-                }
-                mma_commit(smem_u32(&accf[buf]));
-                mma_commit(smem_u32(&empty[(I - 1) % S]));
+                for (int dj = 0; dj < 3; dj++)
+                    mma_bf16(tmem + b * ACOLS + mt * 16, adesc | (((ab + dj * w16) >> 4) & 0x3FFFu),
+                             bdesc | (((wa + (uint32_t)(dj * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc, dj ? 1u : 0u);
+                mma_commit(smem_u32(&accf[b]));
+                mma_commit(smem_u32(&empty[sp]));  // plane p is read by no other MMA
             }
             mma_commit(smem_u32(drain));
             mbar_wait(drain, 0, a.err, 24);
         }
         __syncwarp();
     } else {
-        // ---- epilogue: D columns 0..2 to shared memory, out[p] = D[p-1][0] + D[p][1] + D[p+1][2] ----
+        // ---- epilogue: warps 0-3 ----
         int cof[MT];  // cell of this thread's output within a plane of internal cells, -1 if none
 #pragma unroll
         for (int mt = 0; mt < MT; mt++) {
@@ -865,34 +867,50 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
         };
         fetch(I0);
         uint32_t fph = 0;
-        for (int I = I0; I <= I1; I++) {
-            const int buf = (I - I0) & 1;
-            const bool ok = role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 25);
-            if (epi_any(!ok)) break;  // the four warps leave together
-            fph ^= 1u << buf;
-            fence_after_sync();
-            float* d = dsm + buf * MT * kTileM * 3;
+        bool ok = true;
+        // accumulators of planes I0 - 1 and I0 before the first output plane
+        for (int p = I0 - 1; p <= I0 && ok; p++) {
+            const int b = accb(p);
+            ok = role_wait(&accf[b], (fph >> b) & 1u, abort_flag, a.err, 25);
+            fph ^= 1u << b;
+        }
+        if (!epi_any(!ok)) {
+            for (int I = I0; I <= I1; I++) {
+                const int bn = accb(I + 1);
+                const bool okn = role_wait(&accf[bn], (fph >> bn) & 1u, abort_flag, a.err, 25);
+                if (epi_any(!okn)) break;  // the four warps leave together
+                fph ^= 1u << bn;
+                fence_after_sync();
+                float* d = dsm + ((I - I0) & 1) * MT * kTileM * 3;
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++) {
-                uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * 16, r);
-                tmem_wait_ld();
+                for (int mt = 0; mt < MT; mt++) {
+                    // s_k = sum_di D_{I-1+di}[row][3 di + k], k = dk
+                    float sk[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    reg_fence(r[c]);
-                    d[(mt * kTileM + tid) * 3 + c] = __uint_as_float(r[c]);
+                    for (int di = 0; di < 3; di++) {
+                        uint32_t r[16];
+                        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + accb(I - 1 + di) * ACOLS + mt * 16, r);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            reg_fence(r[3 * di + k]);
+                            sk[k] += __uint_as_float(r[3 * di + k]);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < 3; k++) d[(mt * kTileM + tid) * 3 + k] = sk[k];
                 }
-            }
-            fence_before_sync();
-            mbar_arrive(&acce[buf]);
-            epi_sync();  // d[] complete (double-buffered: the next plane writes the other half)
+                fence_before_sync();
+                mbar_arrive(&acce[accb(I - 1)]);  // plane I-1's accumulator is read for the last time
+                epi_sync();  // d[] complete (double-buffered: the next plane writes the other half)
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++) {
-                if (cof[mt] < 0) continue;
-                const float* dm = d + (mt * kTileM + tid) * 3;
-                a.out32[(int64_t)(I - 1) * cplane + cof[mt]] = res[mt] + (dm[0] + dm[3 + 1] + dm[6 + 2]);
+                for (int mt = 0; mt < MT; mt++) {
+                    if (cof[mt] < 0) continue;
+                    const float* dm = d + (mt * kTileM + tid) * 3;
+                    a.out32[(int64_t)(I - 1) * cplane + cof[mt]] = res[mt] + (dm[0] + dm[3 + 1] + dm[6 + 2]);
+                }
+                if (I < I1) fetch(I + 1);
             }
-            if (I < I1) fetch(I + 1);
         }
     }
     fence_before_sync();
@@ -1252,12 +1270,13 @@ __global__ void k_pack_tapk(const float* __restrict__ W, int flip, bf16* __restr
     }
 }
 
-// dec0 forward weights, dk along N: out[g][kc][n][e] = W[t][0][8 kc + e] with
-// t = 3 g + n for the (di, dj) group g and n = dk < 3, else 0.
+// dec0 forward weights, (di, dk) along N: out[dj][kc][n][e] = W[t][0][8 kc + e]
+// with t = 9 di + 3 dj + dk for n = 3 di + dk < 9, else 0.
 __global__ void k_pack_tapn(const float* __restrict__ W, bf16* __restrict__ out) {
-    for (int idx = threadIdx.x; idx < 9 * 2 * 16 * 8; idx += blockDim.x) {
-        const int e = idx & 7, n = (idx >> 3) & 15, kc = (idx >> 7) & 1, g9 = idx >> 8;
-        out[idx] = __float2bfloat16_rn(n < 3 ? W[(g9 * 3 + n) * 16 + kc * 8 + e] : 0.f);
+    for (int idx = threadIdx.x; idx < 3 * 2 * 16 * 8; idx += blockDim.x) {
+        const int e = idx & 7, n = (idx >> 3) & 15, kc = (idx >> 7) & 1, dj = idx >> 8;
+        const int di = n / 3, dk = n - 3 * (n / 3);
+        out[idx] = __float2bfloat16_rn(n < 9 ? W[(9 * di + 3 * dj + dk) * 16 + kc * 8 + e] : 0.f);
     }
 }
 
@@ -1564,8 +1583,8 @@ static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a, const float*
 
 static size_t out_smem(const Geom& g, int mt, int slots) {
     const int RP = round8(strip_rows(g, mt));
-    return 9 * 2 * 16 * 16 + slots * (size_t)2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 + (2 * kMaxSlots + 5) * 8 +
-           16;
+    return 3 * 2 * 16 * 16 + slots * (size_t)2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 +
+           (2 * kMaxSlots + 2 * kOutAcc + 1) * 8 + 16;
 }
 
 static int out_tiles_mt(const Geom& g) {
@@ -1576,7 +1595,7 @@ template <int MT>
 static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     auto kern = k_conv_out<MT>;
     if (!lc.ready) {
-        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
+        const uint32_t cols = kOutAcc * MT * 16 <= 64 ? 64 : 128;
         const int slots = pick_slots([&](int sl) { return out_smem(a0.g, MT, sl); }, cols);
         size_t smem = out_smem(a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
