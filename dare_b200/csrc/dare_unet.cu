@@ -30,6 +30,8 @@
 #include <random>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "dare_bicgstab2.cuh"
 #include "dare_tc.cuh"
 #include "dare_unet.cuh"
@@ -182,6 +184,13 @@ __device__ __forceinline__ bool role_wait(uint64_t* bar, uint32_t parity, volati
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// One arrival per warp, by lane 0 once the whole warp got here: the barriers
+// that collect a role's warps count warps, not threads (an arrival by every
+// thread serialises on the barrier's word, ~1 us per plane for 512 of them).
+__device__ __forceinline__ void warp_arrive(uint64_t* bar) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(bar);
+}
 
 template <int N>
 __device__ __forceinline__ void cp_wait_group() {
@@ -278,7 +287,7 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&accf[b], MT);
-            mbar_init(&acce[b], kEpiThreads);
+            mbar_init(&acce[b], kEpiThreads / 32);
         }
         mbar_init(drain, MT);
         *abort_flag = 0;
@@ -436,7 +445,7 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
                     }
                 }
             fence_before_sync();
-            mbar_arrive(&acce[buf]);
+            warp_arrive(&acce[buf]);
             epi_sync();  // the edge rows are in `ex` (double-buffered: the next plane writes the other half)
             if ((lane == 0 && warp > 0) || (lane == 31 && warp < 3)) {
                 const int src = lane == 0 ? ((warp - 1) * 2 + 0) : ((warp + 1) * 2 + 1);
@@ -491,90 +500,122 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// One-channel layers.  A tcgen05 MMA costs about the same whatever its N
-// (measured: ~150 cycles for M = 128, K = 16 and any N from 16 to 256), so
-// the 3^3 convolutions with a single input or output channel are re-cast so
-// that each MMA carries several taps:
-//   k_conv_in  (1 -> 16, FP32 input): "window" rows, row q of a staged plane
-//              holding x(q), x(q+1), ..., x(q+7) in BF16.  A K-chunk of 8 then
-//              covers the three dk taps of one (di, dj) (the other five
-//              weights are zero), and the A operand of taps (di, dj) is the
-//              window plane shifted by dj rows of the (j,k) plane: 6 MMAs per
-//              128 outputs instead of 27.
-//   k_conv_out (16 -> 1, FP32 output): the taps in N,
-//              Z[q][t] = sum_ci X[q][ci] W[t][ci] (one MMA per 128 input
-//              rows of a plane), Z staged from TMEM to shared memory, and
-//              every output row gathers its 27 terms, the accumulators of
-//              the three output planes an input plane feeds held in
-//              registers of the row's thread.
+// One-channel layers.  A tcgen05 MMA of M = 128, K = 16 costs about the same
+// for any N up to ~64 (measured: ~42 cycles per MMA when the SM's pipe is
+// saturated, ~55 from a single issuing thread), so the 3^3 convolutions with
+// a single input or output channel are re-cast so that each MMA carries
+// several taps:
+//   k_conv_in  (1 -> 16, FP32 input): 2-D tiles of 16 rows j x 8 cells k and
+//              "window" rows holding the six taps (dj, dj + 1) x (dk 0..2) of
+//              one output cell in a K-chunk of 8; the chunk two rows j further
+//              holds dj = 2, and N = 3 di x 16 output channels: one MMA per
+//              tile and input plane, whose accumulator holds the partial sums
+//              of the three output planes that input plane feeds.
+//   k_conv_out (16 -> 1, FP32 output): N = (di, dk) (9 of 16 columns),
+//              3 MMAs (one per dj) per input plane and 126 outputs; the dk
+//              terms meet across neighbouring rows in the epilogue.
+
+// Accumulators of the one-channel layers: one per staged input plane, complete
+// after that plane's MMAs and last read by output plane p + 1, so four rotate
+// (p mod 4): three read by the epilogue while the MMAs fill the fourth.
+constexpr int kOutAcc = 4;
+
+// k_conv_in: an M tile is 16 rows j x 8 cells k of a plane (row m = 8 g + t:
+// j = j0 + g, k = 8 kb + t), a CTA covers MT tiles stacked in j and marches a
+// run of planes, kInB planes at a time: every role pays its mbarrier
+// round trips (measured at 250-500 cycles for the test of an already
+// completed phase, so each role's loop is bound by their latency) once per
+// group.  Per group a TMA box of the FP32 input (cells k = 8 kb - 4 ..
+// 8 kb + 11, rows j0 - 1 .. j0 + 16 MT + 1, kInB planes; cells outside the
+// grid read zero, which are the ghost values) lands in a ring of kInRaw
+// slots; builder warps turn it into 16 MT + 2 window rows per k and plane
+// (BF16, a ring of kInWin slots), and one MMA per tile and plane multiplies a
+// window plane with the packed weights.  The epilogue reads each plane's
+// accumulator once, into running sums of the two output planes it still
+// feeds; 8 epilogue warps (two per TMEM lane quarter) take 8 output channels
+// each.
+constexpr int kInB = 2;            // planes per group
+constexpr int kInRaw = 8;          // staged FP32 boxes (groups)
+constexpr int kInWin = 3;          // window groups
+constexpr int kInAcc = 2;          // accumulator groups
+constexpr int kInEpi = 256;        // epilogue threads (8 warps)
+constexpr int kInBuilders = 128;   // window builder threads (4 warps)
+constexpr int kInBoxK = 16;        // FP32 cells per box row
+constexpr uint32_t kInWB = 2 * 48 * 16;  // packed weights [2 chunks][3 di x 16 co][8] bf16, bytes
 
 struct InArgs {
     Geom g;
-    const bf16* xpad;   // the input as BF16 over the padded cells (ghosts zero), g.total (+ slack) elements
-    const bf16* w;      // [3 di][2 pairs][2 chunks][16 co][8]
-    bf16* out;          // [g.total][16]
-    int ppc, slots;
+    const bf16* w;      // [2 chunks][3 di x 16 co][8]: chunk c, element e < 6: dj = 2 c + e / 3, dk = e % 3
+    bf16* out;          // chunk-planar [2][g.total][8]
+    int ppc;
     int* err;
+    CUtensorMap x;      // FP32 input [n0][n1][pitch >= n2], boxes kInBoxK x (16 MT + 3) x kInB
 };
 
-// 4 epilogue warps, one MMA warp per M tile, 2 window-builder warps, 1 producer warp
-__host__ __device__ constexpr int in_threads(int mt) { return (4 + mt + 2 + 1) * 32; }
-constexpr int kInBuilders = 64;
-constexpr int kPadSlack = 1024;  // elements past the padded input that a segment copy may read
-
-__host__ __device__ inline int in_rows(const Geom& g, int mt) { return fwd_rows(g, mt); }
-// BF16 elements staged per plane: the windows reach 7 rows further, the copy
-// starts up to 7 elements early (16-byte alignment) and is a multiple of 8
-__host__ __device__ inline int in_raw_elems(const Geom& g, int mt) { return (fwd_rows(g, mt) + 8 + 7 + 7) / 8 * 8; }
+// 8 epilogue warps, 1 MMA warp, 4 window-builder warps, 1 producer warp
+__host__ __device__ constexpr int in_threads() { return (8 + 1 + 4 + 1) * 32; }
+__host__ __device__ constexpr int in_win_rows(int mt) { return 16 * mt + 2; }
+__host__ __device__ constexpr uint32_t in_win_bytes(int mt) { return (uint32_t)in_win_rows(mt) * 8 * 16; }
+// one plane of a box, and one box (kInB planes, 128-byte multiple)
+__host__ __device__ constexpr uint32_t in_box_plane(int mt) { return (uint32_t)kInBoxK * (16 * mt + 3) * 4; }
+__host__ __device__ constexpr uint32_t in_raw_stride(int mt) { return (kInB * in_box_plane(mt) + 127) / 128 * 128; }
+__host__ __device__ constexpr size_t in_smem(int mt) {
+    return kInRaw * (size_t)in_raw_stride(mt) + kInWin * (size_t)kInB * in_win_bytes(mt) + kInWB +
+           (2 * kInRaw + 2 * kInWin + 2 * kInAcc + 1) * 8 + 16;
+}
 
 // enc0 forward and dec0 data gradient: 1 -> 16 channels.
 template <int MT>
-__global__ void __launch_bounds__(in_threads(MT)) k_conv_in(InArgs a) {
+__global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant__ InArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr uint32_t WB = 3 * 2 * 2 * 16 * 16;
-    constexpr uint32_t ACOLS = MT * 16;
-    constexpr uint32_t COLS = 2 * ACOLS <= 32 ? 32 : 64;
+    constexpr uint32_t AST = 64;                    // TMEM columns of one tile's accumulator (48 used)
+    constexpr uint32_t ACOLS = MT * AST;            // one plane's accumulator (all tiles)
+    constexpr uint32_t COLS = kInAcc * kInB * ACOLS;
+    constexpr int WR = in_win_rows(MT);
+    constexpr uint32_t WINB = in_win_bytes(MT), RAWS = in_raw_stride(MT), BOXP = in_box_plane(MT);
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int S = a.slots;
-    const int rows = in_rows(g, MT);
-    const int relems = in_raw_elems(g, MT);
-    const uint32_t SB = (uint32_t)((rows + 7) / 8) * 8 * 16;   // window rows x 16 bytes
-    const uint32_t RB = (uint32_t)relems * 2;
-    uint8_t* wsm = smem;
-    uint8_t* win = smem + WB;                                   // [S][SB]
-    bf16* raw = reinterpret_cast<bf16*>(win + S * SB);          // [S][relems]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(raw) + S * RB);
-    uint64_t* rawf = bars;
-    uint64_t* full = bars + kMaxSlots;
-    uint64_t* empty = bars + 2 * kMaxSlots;
-    uint64_t* accf = bars + 3 * kMaxSlots;
-    uint64_t* acce = accf + 2;
-    uint64_t* drain = acce + 2;
+    uint8_t* raw = smem;                            // [kInRaw][RAWS]: FP32 [kInB][16 MT + 3][kInBoxK]
+    uint8_t* win = raw + kInRaw * RAWS;             // [kInWin][kInB][WR][8 k][16 B]
+    uint8_t* wsm = win + kInWin * kInB * WINB;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wsm + kInWB);
+    uint64_t* rawf = bars;                          // [kInRaw] box landed
+    uint64_t* rawe = rawf + kInRaw;                 // [kInRaw] box read by the builders
+    uint64_t* full = rawe + kInRaw;                 // [kInWin] window planes built
+    uint64_t* empty = full + kInWin;                // [kInWin] window planes read by the MMAs
+    uint64_t* accf = empty + kInWin;                // [kInAcc]
+    uint64_t* acce = accf + kInAcc;                 // [kInAcc]
+    uint64_t* drain = acce + kInAcc;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
-    const int P0 = blockIdx.x * (MT * kTileM);
+    const int kbs = (g.n2 + 7) / 8;
+    const int kb = blockIdx.x % kbs, jb = blockIdx.x / kbs;
     const int I0 = 1 + blockIdx.y * a.ppc;
     if (I0 > g.n0) return;
     const int I1 = min(g.n0, I0 + a.ppc - 1);
+    const int np = I1 - I0 + 3;               // input planes I0 - 1 .. I1 + 1
+    const int ng = (np + kInB - 1) / kInB;    // groups (the last one may run past I1 + 1)
 
     if (tid == 0) {
-        for (int s = 0; s < S; s++) {
+        for (int s = 0; s < kInRaw; s++) {
             mbar_init(&rawf[s], 1);
-            mbar_init(&full[s], kInBuilders);
-            mbar_init(&empty[s], MT);
+            mbar_init(&rawe[s], kInBuilders / 32);
         }
-        for (int b = 0; b < 2; b++) {
-            mbar_init(&accf[b], MT);
-            mbar_init(&acce[b], kEpiThreads);
+        for (int s = 0; s < kInWin; s++) {
+            mbar_init(&full[s], kInBuilders / 32);
+            mbar_init(&empty[s], 1);
         }
-        mbar_init(drain, MT);
+        for (int b = 0; b < kInAcc; b++) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], kInEpi / 32);
+        }
+        mbar_init(drain, 1);
         *abort_flag = 0;
         mbar_fence_init();
     }
     if (warp == 0) tmem_alloc(tslot, COLS);
-    for (uint32_t o = tid * 16; o < WB; o += in_threads(MT) * 16)
+    for (uint32_t o = tid * 16; o < kInWB; o += in_threads() * 16)
         cp16(wsm + o, reinterpret_cast<const uint8_t*>(a.w) + o, true);
     cp_commit();
     cp_wait_all();
@@ -583,128 +624,128 @@ __global__ void __launch_bounds__(in_threads(MT)) k_conv_in(InArgs a) {
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = *tslot;
-    const int64_t pbase = (int64_t)P0 - g.W - 1;
 
-    if (warp == 4 + MT + 2) {
-        // ---- producer: one bulk copy of each plane segment of the padded BF16
-        // input (all-ghost planes 0 and n0+1 are zero-filled instead) ----
-        uint32_t eph = 0xFFu;
-        for (int p = I0 - 1; p <= I1 + 1; p++) {
-            const int sl = p % S;
-            if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 11)) break;
-            eph ^= 1u << sl;
-            bf16* dst = raw + (size_t)sl * relems;
-            if (p == 0 || p == g.n0 + 1) {
-                for (int i = lane; i < relems / 8; i += 32)
-                    reinterpret_cast<uint4*>(dst)[i] = make_uint4(0u, 0u, 0u, 0u);
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&rawf[sl]);
-            } else if (lane == 0) {
-                const int64_t Q0 = (int64_t)p * g.plane + pbase;  // > 0 for 1 <= p <= n0
-                const int64_t Qa = Q0 & ~(int64_t)7;
-                mbar_arrive_expect_tx(&rawf[sl], RB);
-                bulk_load(dst, a.xpad + Qa, RB, &rawf[sl]);
-            }
-            __syncwarp();
-        }
-    } else if (warp >= 4 + MT) {
-        // ---- window builders (2 warps): row q = x(q), ..., x(q + 7) ----
-        const int bt = tid - (4 + MT) * 32;
-        uint32_t rph = 0;
-        for (int p = I0 - 1; p <= I1 + 1; p++) {
-            const int sl = p % S;
-            if (!role_wait(&rawf[sl], (rph >> sl) & 1u, abort_flag, a.err, 12)) break;
-            rph ^= 1u << sl;
-            const int shift = (p == 0 || p == g.n0 + 1) ? 0 : (int)((((int64_t)p * g.plane + pbase)) & 7);
-            const uint16_t* x = reinterpret_cast<const uint16_t*>(raw + (size_t)sl * relems) + shift;
-            uint8_t* wrow = win + sl * SB;
-            for (int q = bt; q < rows; q += kInBuilders)
-                *reinterpret_cast<uint4*>(wrow + (size_t)q * 16) =
-                    make_uint4(x[q] | ((uint32_t)x[q + 1] << 16), x[q + 2] | ((uint32_t)x[q + 3] << 16),
-                               x[q + 4] | ((uint32_t)x[q + 5] << 16), x[q + 6] | ((uint32_t)x[q + 7] << 16));
-            fence_proxy_async();
-            mbar_arrive(&full[sl]);
-        }
-    } else if (warp >= 4) {
-        // ---- MMA: per di, taps (dj 0, dj 1) in one K = 16 MMA, dj 2 in a second;
-        // M tile mt = warp - 4 ----
-        const int mt = warp - 4;
+    if (warp == 13) {
+        // ---- producer: one TMA box per group of planes ----
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_bf16(kTileM, 16, 0, 0);
+            int q = 0;
+            for (; q < ng; q++) {
+                const int sl = q % kInRaw;
+                if (!role_wait(&rawe[sl], ((q / kInRaw) & 1) ^ 1, abort_flag, a.err, 11)) break;
+                mbar_arrive_expect_tx(&rawf[sl], kInB * BOXP);
+                tma_load_3d(raw + sl * RAWS, &a.x, 8 * kb - 4, 16 * MT * jb - 1, I0 - 2 + kInB * q, &rawf[sl]);
+            }
+            // boxes still in flight land before the CTA leaves
+            for (int r = max(0, q - kInRaw); r < q; r++) mbar_wait(&rawf[r % kInRaw], (r / kInRaw) & 1, nullptr, 0);
+        }
+        __syncwarp();
+    } else if (warp >= 9) {
+        // ---- window builders: row (jr, t) = x(jr, t-1..t+1), x(jr+1, t-1..t+1), 0, 0 ----
+        const int bt = tid - 9 * 32;
+        for (int q = 0; q < ng; q++) {
+            const int sr = q % kInRaw, sw = q % kInWin;
+            if (!role_wait(&rawf[sr], (q / kInRaw) & 1, abort_flag, a.err, 12)) break;
+            if (!role_wait(&empty[sw], ((q / kInWin) & 1) ^ 1, abort_flag, a.err, 12)) break;
+            const float* x = reinterpret_cast<const float*>(raw + sr * RAWS);
+            uint8_t* wp = win + sw * kInB * WINB;
+            for (int it = bt; it < kInB * WR * 8; it += kInBuilders) {
+                // box cell e is k = 8 kb - 4 + e: output cell 8 kb + t reads e = t + 3 .. t + 5;
+                // window rows of the group's planes follow each other as the box's planes do
+                const float* r0 = x + (it >> 3) * kInBoxK + (it & 7) + 3 + (it / (WR * 8)) * kInBoxK;
+                const float* r1 = r0 + kInBoxK;
+                *reinterpret_cast<uint4*>(wp + it * 16) =
+                    make_uint4(pack_bf16(r0[0], r0[1]), pack_bf16(r0[2], r1[0]), pack_bf16(r1[1], r1[2]), 0u);
+            }
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&full[sw]);
+                mbar_arrive(&rawe[sr]);
+            }
+        }
+    } else if (warp == 8) {
+        // ---- MMA: one per tile and input plane, D_p[m][16 di + co] ----
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(kTileM, 48, 0, 0);
             const uint32_t w0 = smem_u32(win), wa = smem_u32(wsm);
-            const uint64_t adesc01 = smem_desc(0, (uint32_t)g.W * 16, 128);  // second chunk: dj + 1
-            const uint64_t adesc2 = smem_desc(0, 0, 128);                     // second chunk: the same rows
-            const uint64_t bdesc = smem_desc(0, 16 * 16, 128);
-            uint32_t fph = 0, eph = 3u;
+            const uint64_t adesc = smem_desc(0, 2 * 128, 128);   // K chunk 1: two rows j further
+            const uint64_t bdesc = smem_desc(0, 48 * 16, 128);
             bool ok = true;
-            for (int I = I0; I <= I1 && ok; I++) {
-                const int buf = (I - I0) & 1;
-                for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1 && ok; p++) {
-                    const int sp = p % S;
-                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 13);
-                    fph ^= 1u << sp;
-                }
-                if (ok) ok = role_wait(&acce[buf], (eph >> buf) & 1u, abort_flag, a.err, 14);
-                eph ^= 1u << buf;
+            for (int q = 0; q < ng && ok; q++) {
+                const int sw = q % kInWin, ab = q & (kInAcc - 1);
+                ok = role_wait(&full[sw], (q / kInWin) & 1, abort_flag, a.err, 13);
+                if (ok) ok = role_wait(&acce[ab], ((q / kInAcc) & 1) ^ 1, abort_flag, a.err, 14);
                 if (!ok) break;
                 fence_after_sync();
 #pragma unroll
-                for (int di = 0; di < 3; di++) {
-                    const uint32_t pl = w0 + (uint32_t)((I - 1 + di) % S) * SB;
-                    {
-                        const uint32_t row0 = pl + (uint32_t)(mt * kTileM) * 16;
-                        mma_bf16(tmem + buf * ACOLS + mt * 16, adesc01 | ((row0 >> 4) & 0x3FFFu),
-                                 bdesc | (((wa + (uint32_t)((di * 2 + 0) * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc,
-                                 di ? 1u : 0u);
-                        mma_bf16(tmem + buf * ACOLS + mt * 16,
-                                 adesc2 | (((row0 + (uint32_t)g.W * 32) >> 4) & 0x3FFFu),
-                                 bdesc | (((wa + (uint32_t)((di * 2 + 1) * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc, 1u);
+                for (int b = 0; b < kInB; b++)
+#pragma unroll
+                    for (int mt = 0; mt < MT; mt++) {
+                        const uint32_t a0 = w0 + (uint32_t)(sw * kInB + b) * WINB + (uint32_t)mt * 16 * 128;
+                        mma_bf16(tmem + (ab * kInB + b) * ACOLS + mt * AST, adesc | ((a0 >> 4) & 0x3FFFu),
+                                 bdesc | ((wa >> 4) & 0x3FFFu), idesc, 0u);
                     }
-                }
-                mma_commit(smem_u32(&accf[buf]));
-                mma_commit(smem_u32(&empty[(I - 1) % S]));
+                mma_commit(smem_u32(&accf[ab]));
+                mma_commit(smem_u32(&empty[sw]));
             }
             mma_commit(smem_u32(drain));
             mbar_wait(drain, 0, a.err, 16);
         }
         __syncwarp();
     } else {
-        // ---- epilogue: BF16 16-channel rows ----
-        int pos[MT];  // in-plane output position of this thread's row, -1 if none
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 and output
+        // channels 8 (w / 4) .. + 7 of those rows ----
+        const int qd = warp & 3, h = warp >> 2, m = 32 * qd + lane;
+        int64_t pos[MT];  // in-plane output position of this thread's row, -1 if none
 #pragma unroll
         for (int mt = 0; mt < MT; mt++) {
-            const int pp = P0 + mt * kTileM + tid;
-            const int J = pp / g.W, K = pp - J * g.W;
-            pos[mt] = pp < g.plane && J >= 1 && J <= g.n1 && K >= 1 && K <= g.n2 ? pp : -1;
+            const int jo = 16 * MT * jb + 16 * mt + (m >> 3), ko = 8 * kb + (m & 7);
+            pos[mt] = jo < g.n1 && ko < g.n2 ? (int64_t)(jo + 1) * g.W + ko + 1 : -1;
         }
-        uint32_t fph = 0;
-        for (int I = I0; I <= I1; I++) {
-            const int buf = (I - I0) & 1;
-            if (!role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 17)) break;
-            fph ^= 1u << buf;
+        // input plane p = I0 - 1 + k feeds outputs p + 1 (di 0), p (di 1) and
+        // p - 1 (di 2); before it, cur holds the partial sum of output p - 1
+        // (planes p - 2 and p - 1) and nxt that of output p (plane p - 1)
+        float cur[MT][8] = {}, nxt[MT][8] = {};
+        for (int q = 0; q < ng; q++) {
+            const int ab = q & (kInAcc - 1);
+            if (!role_wait(&accf[ab], (q / kInAcc) & 1, abort_flag, a.err, 17)) break;
             fence_after_sync();
-            uint32_t r[MT][16];
+            uint32_t r[kInB][MT][3][8];
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++)
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + buf * ACOLS + mt * 16, r[mt]);
+            for (int b = 0; b < kInB; b++)
+#pragma unroll
+                for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+                    for (int di = 0; di < 3; di++)
+                        tmem_ld8(tmem + ((uint32_t)(32 * qd) << 16) + (ab * kInB + b) * ACOLS + mt * AST + 16 * di +
+                                     8 * h,
+                                 r[b][mt][di]);
             tmem_wait_ld();
-#pragma unroll
-            for (int mt = 0; mt < MT; mt++)
-#pragma unroll
-                for (int c = 0; c < 16; c++) reg_fence(r[mt][c]);
             fence_before_sync();
-            mbar_arrive(&acce[buf]);
+            warp_arrive(&acce[ab]);
 #pragma unroll
-            for (int mt = 0; mt < MT; mt++) {
-                if (pos[mt] < 0) continue;
-                const int64_t Q = (int64_t)I * g.plane + pos[mt];
-                const float* v = reinterpret_cast<const float*>(r[mt]);
-                *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, 0)) =
-                    make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
-                               pack_bf16(v[6], v[7]));
-                *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, 1)) =
-                    make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]),
-                               pack_bf16(v[14], v[15]));
+            for (int b = 0; b < kInB; b++) {
+                const int k = kInB * q + b;
+                const int I = I0 - 2 + k;  // output completed by this plane
+#pragma unroll
+                for (int mt = 0; mt < MT; mt++) {
+                    float o[8];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        reg_fence(r[b][mt][0][c]);
+                        reg_fence(r[b][mt][1][c]);
+                        reg_fence(r[b][mt][2][c]);
+                        o[c] = cur[mt][c] + __uint_as_float(r[b][mt][2][c]);
+                        cur[mt][c] = nxt[mt][c] + __uint_as_float(r[b][mt][1][c]);
+                        nxt[mt][c] = __uint_as_float(r[b][mt][0][c]);
+                    }
+                    if (k >= 2 && k < np && pos[mt] >= 0) {
+                        const int64_t Q = (int64_t)I * g.plane + pos[mt];
+                        *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, h)) =
+                            make_uint4(pack_bf16(o[0], o[1]), pack_bf16(o[2], o[3]), pack_bf16(o[4], o[5]),
+                                       pack_bf16(o[6], o[7]));
+                    }
+                }
             }
         }
     }
@@ -740,7 +781,6 @@ __host__ __device__ constexpr int out_threads(int mt) { return (5 + mt) * 32; }
 // instead of 9.  An accumulator is complete after its plane's MMAs and last
 // read by output plane p + 1, so four of them rotate (p mod 4): three read by
 // the epilogue while the MMAs fill the fourth.
-constexpr int kOutAcc = 4;
 
 template <int MT>
 __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
@@ -777,7 +817,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
         }
         for (int b = 0; b < kOutAcc; b++) {
             mbar_init(&accf[b], MT);
-            mbar_init(&acce[b], kEpiThreads);
+            mbar_init(&acce[b], kEpiThreads / 32);
         }
         mbar_init(drain, MT);
         *abort_flag = 0;
@@ -901,7 +941,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
                     for (int k = 0; k < 3; k++) d[(mt * kTileM + tid) * 3 + k] = sk[k];
                 }
                 fence_before_sync();
-                mbar_arrive(&acce[accb(I - 1)]);  // plane I-1's accumulator is read for the last time
+                warp_arrive(&acce[accb(I - 1)]);  // plane I-1's accumulator is read for the last time
                 epi_sync();  // d[] complete (double-buffered: the next plane writes the other half)
 #pragma unroll
                 for (int mt = 0; mt < MT; mt++) {
@@ -1155,19 +1195,6 @@ __global__ void k_prolong_add(Geom f, Geom c, const bf16* __restrict__ coarse, b
     }
 }
 
-// FP32 vector over the internal cells -> BF16 one-channel array over the
-// padded cells (the ghost entries are never written and stay zero).  One
-// block row per (i, j) line of cells.
-__global__ void k_embed(Geom g, const float* __restrict__ in32, bf16* __restrict__ xpad) {
-    const int lines = g.n0 * g.n1;
-    for (int line = blockIdx.x; line < lines; line += gridDim.x) {
-        const int i = line / g.n1, j = line - (line / g.n1) * g.n1;
-        const float* src = in32 + (int64_t)line * g.n2;
-        bf16* dst = xpad + ((int64_t)(i + 1) * (g.n1 + 2) + (j + 1)) * g.W + 1;
-        for (int k = threadIdx.x; k < g.n2; k += blockDim.x) dst[k] = __float2bfloat16_rn(src[k]);
-    }
-}
-
 // padded bf16 activations -> FP32 [cell][C] over the internal cells
 __global__ void k_read_act(Geom g, int C, const bf16* __restrict__ a, float* __restrict__ out) {
     const int64_t total = (int64_t)g.n0 * g.n1 * g.n2 * C;
@@ -1252,17 +1279,18 @@ __global__ void k_pack(const float* __restrict__ W, int cin, int cout, int CINK,
     }
 }
 
-// One-channel-input weights for the window layout of k_conv_in:
-// out[di][pair][chunk][n][e] = W(t, n) with dj = 2 pair + chunk, dk = e,
-// t = 9 di + 3 dj + dk when dj < 3 and dk < 3, else 0; W(t, n) = W[t][n][0]
-// (enc0, cout 16, cin 1) or, flipped for the dec0 data gradient,
-// W[26 - t][0][n] (cout 1, cin 16).
+// One-channel-input weights for the window rows of k_conv_in, the di taps
+// along N: out[c][16 di + n][e] = W(t, n) with, for e < 6, dj = 2 c + e / 3,
+// dk = e % 3, t = 9 di + 3 dj + dk when dj < 3; 0 otherwise.
+// W(t, n) = W[t][n][0] (enc0, cout 16, cin 1) or, flipped for the dec0 data
+// gradient, W[26 - t][0][n] (cout 1, cin 16).
 __global__ void k_pack_tapk(const float* __restrict__ W, int flip, bf16* __restrict__ out) {
-    for (int idx = threadIdx.x; idx < 3 * 2 * 2 * 16 * 8; idx += blockDim.x) {
-        const int e = idx & 7, n = (idx >> 3) & 15, chunk = (idx >> 7) & 1, pair = (idx >> 8) & 1, di = idx >> 9;
-        const int dj = 2 * pair + chunk, dk = e;
+    for (int idx = threadIdx.x; idx < 2 * 48 * 8; idx += blockDim.x) {
+        const int e = idx & 7, nn = (idx >> 3) % 48, c = idx / (8 * 48);
+        const int di = nn / 16, n = nn - 16 * (nn / 16);
+        const int dj = 2 * c + e / 3, dk = e - 3 * (e / 3);
         float v = 0.f;
-        if (dj < 3 && dk < 3) {
+        if (e < 6 && dj < 3) {
             const int t = di * 9 + dj * 3 + dk;
             v = flip ? W[(kTaps - 1 - t) * 16 + n] : W[t * 16 + n];
         }
@@ -1533,52 +1561,76 @@ static int pick_slots(SmemFn smem_of, uint32_t cols) {
     return best > 0 ? best : 4;
 }
 
-static size_t in_smem(const Geom& g, int mt, int slots) {
-    const size_t sb = (size_t)((in_rows(g, mt) + 7) / 8) * 8 * 16;
-    return 3 * 2 * 2 * 16 * 16 + slots * sb + slots * (size_t)in_raw_elems(g, mt) * 2 + (3 * kMaxSlots + 5) * 8 + 16;
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on the driver library); no interleave, no swizzle,
+// cells outside the tensor read zero.
+static int encode_tiled(dare_ctx* ctx, CUtensorMap* m, CUtensorMapDataType type, int rank, const void* base,
+                        const cuuint64_t* dims, const cuuint64_t* strides, const cuuint32_t* box, const cuuint32_t* es) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return set_error(ctx, DARE_ERR_CUDA, "unet: cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const CUresult r = encode(m, type, (cuuint32_t)rank, const_cast<void*>(base), dims, strides, box, es,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ctx, DARE_ERR_CUDA, "unet: cuTensorMapEncodeTiled failed");
+    return DARE_OK;
 }
 
-static int in_tiles_mt(const Geom& g) { return g.plane > 2 * kTileM ? 2 : 1; }
+// tcgen05 tile count of k_conv_in per CTA (16 rows j each)
+constexpr int kInMT = 1;
 
 template <int MT>
-static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a0) {
+static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, InArgs& a) {
     auto kern = k_conv_in<MT>;
     if (!lc.ready) {
-        const uint32_t cols = 2 * MT * 16 <= 32 ? 32 : 64;
-        const int slots = pick_slots([&](int sl) { return in_smem(a0.g, MT, sl); }, cols);
-        size_t smem = in_smem(a0.g, MT, slots);
-        if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
+        const uint32_t cols = kInAcc * kInB * MT * 64;
+        size_t smem = in_smem(MT);
         int occ = 0, rc;
-        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, in_threads(MT)))) return rc;
-        // (the launch checks above keep the ring at >= 4 planes: 3 in use + 1 loading)
-        const int n0 = a0.g.n0;
-        const int tiles = (a0.g.plane + MT * kTileM - 1) / (MT * kTileM);
-        const int ppc = pick_ppc(n0, tiles, (int64_t)ctx->num_sms * occ);
+        if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, in_threads()))) return rc;
+        const Geom& g = a.g;
+        const int tiles = ((g.n2 + 7) / 8) * ((g.n1 + 16 * MT - 1) / (16 * MT));
+        const int ppc = pick_ppc(g.n0, tiles, (int64_t)ctx->num_sms * occ);
         lc.ppc = ppc;
         lc.occ = occ;
         lc.mt = MT;
-        lc.slots = slots;
-        lc.grid = dim3(tiles, (n0 + ppc - 1) / ppc, 1);
+        lc.slots = kInRaw;
+        lc.grid = dim3(tiles, (g.n0 + ppc - 1) / ppc, 1);
         lc.smem = smem;
         lc.cols = cols;
         lc.ready = true;
     }
-    InArgs a = a0;
     a.ppc = lc.ppc;
-    a.slots = lc.slots;
-    kern<<<lc.grid, in_threads(MT), lc.smem, ctx->stream>>>(a);
+    kern<<<lc.grid, in_threads(), lc.smem, ctx->stream>>>(a);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
 
-// in32 (FP32 over the internal cells) is first written into the padded BF16
-// array x0, which the kernel then stages plane by plane with bulk copies.
-static int launch_in(dare_ctx* ctx, LaunchCfg& lc, const InArgs& a, const float* in32) {
+// The kernel reads in32 (FP32 over the internal cells) through a TMA map;
+// a row pitch that is not a multiple of 16 bytes (n2 % 4 != 0) or a base
+// that is not 16-byte aligned goes through a pitched copy in `stage` first.
+static int launch_in(dare_ctx* ctx, LaunchCfg& lc, InArgs& a, const float* in32, float* stage) {
     const Geom& g = a.g;
-    k_embed<<<(int)std::min<int64_t>((int64_t)g.n0 * g.n1, (int64_t)ctx->num_sms * 16), 128, 0, ctx->stream>>>(
-        g, in32, const_cast<bf16*>(a.xpad));
-    DARE_LAUNCHED(ctx);
-    return in_tiles_mt(a.g) == 2 ? launch_in_t<2>(ctx, lc, a) : launch_in_t<1>(ctx, lc, a);
+    const float* base = in32;
+    int64_t pitch = g.n2;
+    if ((g.n2 & 3) || (reinterpret_cast<uintptr_t>(in32) & 15)) {
+        pitch = (g.n2 + 3) & ~3;
+        DARE_CUDA(ctx, cudaMemcpy2DAsync(stage, (size_t)pitch * 4, in32, (size_t)g.n2 * 4, (size_t)g.n2 * 4,
+                                         (size_t)g.n0 * g.n1, cudaMemcpyDeviceToDevice, ctx->stream));
+        base = stage;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)g.n2, (cuuint64_t)g.n1, (cuuint64_t)g.n0};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)pitch * g.n1 * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)kInBoxK, (cuuint32_t)(16 * kInMT + 3), (cuuint32_t)kInB};
+    const cuuint32_t es[3] = {1, 1, 1};
+    int rc;
+    if ((rc = encode_tiled(ctx, &a.x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es))) return rc;
+    return launch_in_t<kInMT>(ctx, lc, a);
 }
 
 static size_t out_smem(const Geom& g, int mt, int slots) {
@@ -1639,11 +1691,10 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
     if (l == ENC0) {
         InArgs a{};
         a.g = net->geo[0];
-        a.xpad = net->X0;
         a.w = L.wf;
         a.out = out;
         a.err = net->err;
-        return launch_in(net->ctx, L.fwd, a, in32);
+        return launch_in(net->ctx, L.fwd, a, in32, net->X0);
     }
     if (l == DEC0) {
         OutArgs a{};
@@ -1673,11 +1724,10 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
     if (l == DEC0) {
         InArgs a{};
         a.g = net->geo[0];
-        a.xpad = net->X0;
         a.w = L.wb;
         a.out = dx;
         a.err = net->err;
-        return launch_in(net->ctx, L.bwd, a, dy32);
+        return launch_in(net->ctx, L.bwd, a, dy32, net->X0);
     }
     FwdArgs a{};
     a.g = net->geo[L.level];
@@ -1896,6 +1946,7 @@ static void unet_free(dare_unet* net) {
     cudaFree(net->adam_m);
     cudaFree(net->adam_v);
     cudaFree(net->act_block);
+    cudaFree(net->X0);
     cudaFree(net->z);
     cudaFree(net->g);
     cudaFree(net->part);
@@ -1913,6 +1964,8 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     for (int d = 0; d < 3; d++)
         if (n[d] < 8 || n[d] % 8 != 0)
             return set_error(ctx, DARE_ERR_BAD_ARG, "dare_unet_create: every grid size must be a positive multiple of 8");
+    if (n[2] + 2 + 8 >= kActSlackRows)
+        return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_create: grid too wide for the staged convolutions");
     cudaSetDevice(ctx->device);
     dare_unet* net = new dare_unet();
     net->ctx = ctx;
@@ -1930,11 +1983,11 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         const Geom& g = net->geo[L.level];
         L.nt = pick_nt(L.cink, L.coutk, g);
         L.ntb = pick_nt(L.coutk, L.cink, g);
-        const bool fits_fwd = l == ENC0   ? in_smem(g, 1, 4) <= kMaxSmem
+        const bool fits_fwd = l == ENC0   ? in_smem(kInMT) <= kMaxSmem
                               : l == DEC0 ? out_smem(g, 1, 4) <= kMaxSmem
                                           : fwd_smem(L.cink, L.nt, g, 1, 4) <= kMaxSmem;
         const bool fits_bwd = l == ENC0   ? true
-                              : l == DEC0 ? in_smem(g, 1, 4) <= kMaxSmem
+                              : l == DEC0 ? in_smem(kInMT) <= kMaxSmem
                                           : fwd_smem(L.coutk, L.ntb, g, 1, 4) <= kMaxSmem;
         if (!fits_fwd || !fits_bwd || wgr_smem(L.cink, L.coutk, g, l == ENC0, l == DEC0) > kMaxSmem) {
             delete net;
@@ -1951,11 +2004,13 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     struct Slot {
         bf16** p;
         int level, c, extra;
-    } slots[] = {{&net->X0, 0, 1, kPadSlack}, {&net->S0, 0, 16}, {&net->P1, 1, 16}, {&net->S1, 1, 32}, {&net->P2, 2, 32}, {&net->S2, 2, 64},
+    } slots[] = {{&net->S0, 0, 16}, {&net->P1, 1, 16}, {&net->S1, 1, 32}, {&net->P2, 2, 32}, {&net->S2, 2, 64},
                  {&net->P3, 3, 64}, {&net->E3, 3, 64}, {&net->dS0, 0, 16}, {&net->dD1, 1, 16}, {&net->dS1, 1, 32},
                  {&net->dD2, 2, 32}, {&net->dS2, 2, 64}, {&net->dD3, 3, 64}, {&net->dE3, 3, 64}, {&net->dP3, 3, 64},
                  {&net->dP2, 2, 32}, {&net->dP1, 1, 16}};
-    size_t bytes = 0;
+    // a staged plane segment reaches up to W + 8 rows before the start of an
+    // array (the unused halo of the ghost plane 0) and kActSlackRows bounds W
+    size_t bytes = (size_t)kActSlackRows * 16;
     std::vector<size_t> offs;
     for (auto& s : slots) {
         offs.push_back(bytes);
@@ -1967,6 +2022,9 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     for (size_t i = 0; i < sizeof(slots) / sizeof(slots[0]) && e == cudaSuccess; i++)
         *slots[i].p = reinterpret_cast<bf16*>(static_cast<uint8_t*>(net->act_block) + offs[i]);
     const size_t pb = net->nparam * sizeof(float);
+    // (grid sizes are multiples of 8, so the pitched copy is only for a
+    // caller's vector that does not start on a 16-byte boundary)
+    if (e == cudaSuccess) e = cudaMalloc(&net->X0, (size_t)net->ncell * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&net->w, pb);
     if (e == cudaSuccess) e = cudaMalloc(&net->grad, pb);
     if (e == cudaSuccess) e = cudaMalloc(&net->adam_m, pb);

@@ -33,7 +33,8 @@ __host__ __device__ inline int round8(int rows) { return (rows + 7) / 8 * 8; }
 __host__ __device__ inline int64_t act_off(int64_t total, int64_t Q, int kc) { return ((int64_t)kc * total + Q) * 8; }
 // Rows past either end of a chunk plane that a staged segment may read (they
 // feed only outputs that are not stored); the activation block keeps this
-// many spare rows after its last array.
+// many spare rows before its first array and after its last, and grids are
+// limited to rows of W + 8 < kActSlackRows positions.
 constexpr int64_t kActSlackRows = 8192;
 
 struct Geom {
@@ -143,8 +144,8 @@ struct dare_unet {
     dare_gpu::unet::bf16* dP3 = nullptr;
     dare_gpu::unet::bf16* dP2 = nullptr;
     dare_gpu::unet::bf16* dP1 = nullptr;
-    dare_gpu::unet::bf16* X0 = nullptr;   // k_conv_in input: a FP32 vector as BF16 over the padded level-0 cells
     void* act_block = nullptr;            // one allocation for all of the above
+    float* X0 = nullptr;                  // k_conv_in input with a 16-byte row pitch, when the caller's has none
     float* z = nullptr;                   // forward output during training
     float* g = nullptr;                   // dL/dz
     float* part = nullptr;                // weight-gradient partial sums
