@@ -515,10 +515,18 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
 //              3 MMAs (one per dj) per input plane and 126 outputs; the dk
 //              terms meet across neighbouring rows in the epilogue.
 
-// Accumulators of the one-channel layers: one per staged input plane, complete
-// after that plane's MMAs and last read by output plane p + 1, so four rotate
-// (p mod 4): three read by the epilogue while the MMAs fill the fourth.
-constexpr int kOutAcc = 4;
+// Both kernels read each input plane's accumulator once, into running sums
+// of the output planes it still feeds.  A test of an already completed
+// mbarrier phase was measured at 250-500 cycles, and every role pays two or
+// three per round of its loop, so the loops are latency-bound: k_conv_in
+// takes its planes two per round, while k_conv_out (whose staged planes are
+// ~25 KB at 256^2) gains more from CTAs per SM than from groups (measured at
+// 256^3: groups of two with a 2-group ring 242 us, single planes with 3 CTAs
+// per SM 183 us).
+
+// k_conv_out: planes per group, and accumulator groups
+constexpr int kOutB = 1;
+constexpr int kOutG = 4;
 
 // k_conv_in: an M tile is 16 rows j x 8 cells k of a plane (row m = 8 g + t:
 // j = j0 + g, k = 8 kb + t), a CTA covers MT tiles stacked in j and marches a
@@ -774,34 +782,34 @@ __host__ __device__ constexpr int out_threads(int mt) { return (5 + mt) * 32; }
 // gets its own accumulator with the (di, dk) taps in N (N = 16, 9 used):
 //     D_p[q][3 di + dk] = sum_dj sum_ci X_p[q + (dj-1) W][ci] W[(di,dj,dk)][ci]
 // i.e. 3 MMAs per input plane (one per dj, whose shift is the A operand's
-// start row), and output plane I takes, for di = 0, 1, 2, the di columns of
-// the accumulator of input plane I - 1 + di:
-//     out[m] = sum_di  D_{I-1+di}[m-1][3 di] + D_{I-1+di}[m][3 di + 1] + D_{I-1+di}[m+1][3 di + 2]
-// (m = 1 .. 126 of a 128-row tile): 3 MMAs per 126 outputs per plane
-// instead of 9.  An accumulator is complete after its plane's MMAs and last
-// read by output plane p + 1, so four of them rotate (p mod 4): three read by
-// the epilogue while the MMAs fill the fourth.
-
+// start row).  Output plane I takes, for di = 0, 1, 2, the di columns of the
+// accumulator of input plane I - 1 + di:
+//     s_k(I)[m] = sum_di D_{I-1+di}[m][3 di + k]
+//     out[m]    = s_0(I)[m-1] + s_1(I)[m] + s_2(I)[m+1]
+// (m = 1 .. 126 of a 128-row tile).  The epilogue reads each accumulator once
+// into running sums of s(p - 1), s(p) and s(p + 1); the three s_k of every row
+// then meet their neighbours through shared memory.  Planes go kOutB to a
+// group (one staged slot, one set of accumulators, one round of barriers).
 template <int MT>
 __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr uint32_t WB = 3 * 2 * 16 * 16;       // [3 dj][2 kc][16 n][8] bf16
-    constexpr uint32_t ACOLS = MT * 16;            // one accumulator (all tiles)
-    constexpr uint32_t COLS = kOutAcc * ACOLS <= 64 ? 64 : 128;
+    constexpr uint32_t ACOLS = MT * 16;            // one plane's accumulator (all tiles)
+    constexpr uint32_t COLS = kOutG * kOutB * ACOLS <= 64 ? 64 : 128;
     const Geom g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int S = a.slots;
+    const int S = a.slots;                     // staged groups
     const int RP = round8(strip_rows(g, MT));  // staged rows per chunk plane
-    const uint32_t SB = 2u * RP * 16;
+    const uint32_t SB = 2u * RP * 16;          // one staged plane
     uint8_t* wsm = smem;
-    uint8_t* slots = smem + WB;
-    float* dsm = reinterpret_cast<float*>(slots + S * SB);  // [2][MT][128][3]
+    uint8_t* slots = smem + WB;                // [S][kOutB][2 kc][RP][16 B]
+    float* dsm = reinterpret_cast<float*>(slots + S * kOutB * SB);  // [2][MT][128][3]
     uint64_t* bars = reinterpret_cast<uint64_t*>(dsm + 2 * MT * kTileM * 3);
     uint64_t* full = bars;
     uint64_t* empty = bars + kMaxSlots;
-    uint64_t* accf = bars + 2 * kMaxSlots;       // [kOutAcc]
-    uint64_t* acce = accf + kOutAcc;             // [kOutAcc]
-    uint64_t* drain = acce + kOutAcc;
+    uint64_t* accf = bars + 2 * kMaxSlots;       // [kOutG]
+    uint64_t* acce = accf + kOutG;               // [kOutG]
+    uint64_t* drain = acce + kOutG;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
@@ -809,13 +817,15 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     const int I0 = 1 + blockIdx.y * a.ppc;
     if (I0 > g.n0) return;
     const int I1 = min(g.n0, I0 + a.ppc - 1);
+    const int np = I1 - I0 + 3;               // input planes I0 - 1 .. I1 + 1
+    const int ng = (np + kOutB - 1) / kOutB;  // groups (the last one may run past I1 + 1)
 
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], MT);
         }
-        for (int b = 0; b < kOutAcc; b++) {
+        for (int b = 0; b < kOutG; b++) {
             mbar_init(&accf[b], MT);
             mbar_init(&acce[b], kEpiThreads / 32);
         }
@@ -836,23 +846,23 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
     // segment row 0 is position P0 - 1 - W: D row m of tile mt (position
     // P0 - 1 + 126 mt + m) reads segment rows 126 mt + m + dj W
     const int pbase = P0 - 1 - g.W;
-    // accumulator of input plane p: (p - (I0 - 1)) mod 4
-    auto accb = [&](int p) { return (p - I0 + 1) & (kOutAcc - 1); };
 
     if (warp == 4) {
-        // ---- producer: one bulk copy per chunk plane segment ----
+        // ---- producer: one bulk copy per chunk plane segment; planes past
+        // I1 + 1 in the last group are not copied (their slot keeps stale
+        // rows whose accumulators are never read) ----
         if (lane == 0) {
-            const uint32_t bytes = 2u * RP * 16;
-            uint32_t eph = 0xFFu;
-            for (int p = I0 - 1; p <= I1 + 1; p++) {
-                const int sl = p % S;
-                if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 21)) break;
-                eph ^= 1u << sl;
-                mbar_arrive_expect_tx(&full[sl], bytes);
-                const int64_t y0 = (int64_t)p * g.plane + pbase;
-                for (int kc = 0; kc < 2; kc++)
-                    bulk_load(slots + sl * SB + (size_t)kc * RP * 16, a.in + act_off(g.total, y0, kc),
-                              (uint32_t)RP * 16, &full[sl]);
+            for (int q = 0; q < ng; q++) {
+                const int sl = q % S;
+                if (!role_wait(&empty[sl], ((q / S) & 1) ^ 1, abort_flag, a.err, 21)) break;
+                const int nb = min(kOutB, np - kOutB * q);
+                mbar_arrive_expect_tx(&full[sl], (uint32_t)nb * 2u * RP * 16);
+                for (int b = 0; b < nb; b++) {
+                    const int64_t y0 = (int64_t)(I0 - 1 + kOutB * q + b) * g.plane + pbase;
+                    for (int kc = 0; kc < 2; kc++)
+                        bulk_load(slots + (size_t)(sl * kOutB + b) * SB + (size_t)kc * RP * 16,
+                                  a.in + act_off(g.total, y0, kc), (uint32_t)RP * 16, &full[sl]);
+                }
             }
         }
         __syncwarp();
@@ -864,23 +874,24 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
             const uint32_t sl0 = smem_u32(slots), wa = smem_u32(wsm);
             const uint64_t adesc = smem_desc(0, RP * 16, 128), bdesc = smem_desc(0, 16 * 16, 128);
             const uint32_t w16 = (uint32_t)g.W * 16;
-            uint32_t fph = 0, aph = 0xFu;  // fresh accumulators pass their first wait
             bool ok = true;
-            for (int p = I0 - 1; p <= I1 + 1 && ok; p++) {
-                const int sp = p % S, b = accb(p);
-                ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 22);
-                fph ^= 1u << sp;
-                if (ok) ok = role_wait(&acce[b], (aph >> b) & 1u, abort_flag, a.err, 23);
-                aph ^= 1u << b;
+            for (int q = 0; q < ng && ok; q++) {
+                const int sl = q % S, ag = q & (kOutG - 1);
+                ok = role_wait(&full[sl], (q / S) & 1, abort_flag, a.err, 22);
+                if (ok) ok = role_wait(&acce[ag], ((q / kOutG) & 1) ^ 1, abort_flag, a.err, 23);
                 if (!ok) break;
                 fence_after_sync();
-                const uint32_t ab = sl0 + (uint32_t)sp * SB + (uint32_t)(mt * kOutStride) * 16;
 #pragma unroll
-                for (int dj = 0; dj < 3; dj++)
-                    mma_bf16(tmem + b * ACOLS + mt * 16, adesc | (((ab + dj * w16) >> 4) & 0x3FFFu),
-                             bdesc | (((wa + (uint32_t)(dj * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc, dj ? 1u : 0u);
-                mma_commit(smem_u32(&accf[b]));
-                mma_commit(smem_u32(&empty[sp]));  // plane p is read by no other MMA
+                for (int b = 0; b < kOutB; b++) {
+                    const uint32_t ab = sl0 + (uint32_t)(sl * kOutB + b) * SB + (uint32_t)(mt * kOutStride) * 16;
+#pragma unroll
+                    for (int dj = 0; dj < 3; dj++)
+                        mma_bf16(tmem + (ag * kOutB + b) * ACOLS + mt * 16, adesc | (((ab + dj * w16) >> 4) & 0x3FFFu),
+                                 bdesc | (((wa + (uint32_t)(dj * 2 * 16 * 16)) >> 4) & 0x3FFFu), idesc,
+                                 dj ? 1u : 0u);
+                }
+                mma_commit(smem_u32(&accf[ag]));
+                mma_commit(smem_u32(&empty[sl]));
             }
             mma_commit(smem_u32(drain));
             mbar_wait(drain, 0, a.err, 24);
@@ -898,7 +909,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
                           : -1;
         }
         const int64_t cplane = (int64_t)g.n1 * g.n2;
-        // the residual term of plane I is loaded while plane I's MMAs run
+        // the residual term of output plane I is loaded one plane ahead
         float res[MT];
         auto fetch = [&](int I) {
 #pragma unroll
@@ -906,50 +917,49 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
                 res[mt] = a.res32 && cof[mt] >= 0 ? a.res32[(int64_t)(I - 1) * cplane + cof[mt]] : 0.f;
         };
         fetch(I0);
-        uint32_t fph = 0;
-        bool ok = true;
-        // accumulators of planes I0 - 1 and I0 before the first output plane
-        for (int p = I0 - 1; p <= I0 && ok; p++) {
-            const int b = accb(p);
-            ok = role_wait(&accf[b], (fph >> b) & 1u, abort_flag, a.err, 25);
-            fph ^= 1u << b;
-        }
-        if (!epi_any(!ok)) {
-            for (int I = I0; I <= I1; I++) {
-                const int bn = accb(I + 1);
-                const bool okn = role_wait(&accf[bn], (fph >> bn) & 1u, abort_flag, a.err, 25);
-                if (epi_any(!okn)) break;  // the four warps leave together
-                fph ^= 1u << bn;
-                fence_after_sync();
-                float* d = dsm + ((I - I0) & 1) * MT * kTileM * 3;
+        // input plane p = I0 - 1 + k: before it, cur holds the partial s of
+        // output p - 1 (planes p - 2, p - 1) and nxt that of output p (plane p - 1)
+        float cur[MT][3] = {}, nxt[MT][3] = {};
+        for (int q = 0; q < ng; q++) {
+            const int ag = q & (kOutG - 1);
+            const bool okw = role_wait(&accf[ag], (q / kOutG) & 1, abort_flag, a.err, 25);
+            if (epi_any(!okw)) break;  // the four warps leave together
+            fence_after_sync();
+            uint32_t r[kOutB][MT][16];
+#pragma unroll
+            for (int b = 0; b < kOutB; b++)
+#pragma unroll
+                for (int mt = 0; mt < MT; mt++)
+                    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (ag * kOutB + b) * ACOLS + mt * 16, r[b][mt]);
+            tmem_wait_ld();
+            fence_before_sync();
+            warp_arrive(&acce[ag]);
+#pragma unroll
+            for (int b = 0; b < kOutB; b++) {
+                const int k = kOutB * q + b;
+                const int I = I0 - 2 + k;  // output completed by this plane
+                float* d = dsm + (k & 1) * MT * kTileM * 3;
 #pragma unroll
                 for (int mt = 0; mt < MT; mt++) {
-                    // s_k = sum_di D_{I-1+di}[row][3 di + k], k = dk
-                    float sk[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                    for (int di = 0; di < 3; di++) {
-                        uint32_t r[16];
-                        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + accb(I - 1 + di) * ACOLS + mt * 16, r);
-                        tmem_wait_ld();
+                    for (int c = 0; c < 9; c++) reg_fence(r[b][mt][c]);
 #pragma unroll
-                        for (int k = 0; k < 3; k++) {
-                            reg_fence(r[3 * di + k]);
-                            sk[k] += __uint_as_float(r[3 * di + k]);
-                        }
+                    for (int kk = 0; kk < 3; kk++) {
+                        d[(mt * kTileM + tid) * 3 + kk] = cur[mt][kk] + __uint_as_float(r[b][mt][6 + kk]);
+                        cur[mt][kk] = nxt[mt][kk] + __uint_as_float(r[b][mt][3 + kk]);
+                        nxt[mt][kk] = __uint_as_float(r[b][mt][kk]);
                     }
-#pragma unroll
-                    for (int k = 0; k < 3; k++) d[(mt * kTileM + tid) * 3 + k] = sk[k];
                 }
-                fence_before_sync();
-                warp_arrive(&acce[accb(I - 1)]);  // plane I-1's accumulator is read for the last time
                 epi_sync();  // d[] complete (double-buffered: the next plane writes the other half)
+                if (k >= 2 && k < np) {
 #pragma unroll
-                for (int mt = 0; mt < MT; mt++) {
-                    if (cof[mt] < 0) continue;
-                    const float* dm = d + (mt * kTileM + tid) * 3;
-                    a.out32[(int64_t)(I - 1) * cplane + cof[mt]] = res[mt] + (dm[0] + dm[3 + 1] + dm[6 + 2]);
+                    for (int mt = 0; mt < MT; mt++) {
+                        if (cof[mt] < 0) continue;
+                        const float* dm = d + (mt * kTileM + tid) * 3;
+                        a.out32[(int64_t)(I - 1) * cplane + cof[mt]] = res[mt] + (dm[0] + dm[3 + 1] + dm[6 + 2]);
+                    }
+                    if (I < I1) fetch(I + 1);
                 }
-                if (I < I1) fetch(I + 1);
             }
         }
     }
@@ -1633,22 +1643,39 @@ static int launch_in(dare_ctx* ctx, LaunchCfg& lc, InArgs& a, const float* in32,
     return launch_in_t<kInMT>(ctx, lc, a);
 }
 
+// shared memory of k_conv_out with `slots` staged groups of kOutB planes
 static size_t out_smem(const Geom& g, int mt, int slots) {
     const int RP = round8(strip_rows(g, mt));
-    return 3 * 2 * 16 * 16 + slots * (size_t)2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 +
-           (2 * kMaxSlots + 2 * kOutAcc + 1) * 8 + 16;
+    return 3 * 2 * 16 * 16 + slots * (size_t)kOutB * 2 * RP * 16 + 2 * (size_t)mt * kTileM * 3 * 4 +
+           (2 * kMaxSlots + 2 * kOutG + 1) * 8 + 16;
+}
+
+// staged groups: the most CTAs per SM, then the deepest ring (2 .. 8 groups)
+static int out_slots(const Geom& g, int mt, uint32_t cols) {
+    constexpr size_t kSmemPerSM = 233472;
+    int best = 2, best_occ = 0;
+    for (int sl = 2; sl <= kMaxSlots; sl++) {
+        const size_t smem = out_smem(g, mt, sl);
+        if (smem > kMaxSmem) break;
+        const int occ = (int)std::min<size_t>(kSmemPerSM / (smem + 1024), 512 / cols);
+        if (occ >= best_occ) {
+            best_occ = occ;
+            best = sl;
+        }
+    }
+    return best;
 }
 
 static int out_tiles_mt(const Geom& g) {
-    return g.plane > 2 * kOutStride && out_smem(g, 2, 4) <= kMaxSmem ? 2 : 1;
+    return g.plane > 2 * kOutStride && out_smem(g, 2, 2) <= kMaxSmem ? 2 : 1;
 }
 
 template <int MT>
 static int launch_out_t(dare_ctx* ctx, LaunchCfg& lc, const OutArgs& a0) {
     auto kern = k_conv_out<MT>;
     if (!lc.ready) {
-        const uint32_t cols = kOutAcc * MT * 16 <= 64 ? 64 : 128;
-        const int slots = pick_slots([&](int sl) { return out_smem(a0.g, MT, sl); }, cols);
+        const uint32_t cols = kOutG * kOutB * MT * 16 <= 64 ? 64 : 128;
+        const int slots = out_slots(a0.g, MT, cols);
         size_t smem = out_smem(a0.g, MT, slots);
         if (smem > kMaxSmem) return set_error(ctx, DARE_ERR_UNSUPPORTED, "unet: level too wide for the staged conv");
         int occ = 0, rc;
@@ -1984,7 +2011,7 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
         L.nt = pick_nt(L.cink, L.coutk, g);
         L.ntb = pick_nt(L.coutk, L.cink, g);
         const bool fits_fwd = l == ENC0   ? in_smem(kInMT) <= kMaxSmem
-                              : l == DEC0 ? out_smem(g, 1, 4) <= kMaxSmem
+                              : l == DEC0 ? out_smem(g, 1, 2) <= kMaxSmem
                                           : fwd_smem(L.cink, L.nt, g, 1, 4) <= kMaxSmem;
         const bool fits_bwd = l == ENC0   ? true
                               : l == DEC0 ? in_smem(kInMT) <= kMaxSmem
