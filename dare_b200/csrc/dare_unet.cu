@@ -1385,8 +1385,22 @@ static size_t fwd_smem(int cin, int nt, const Geom& g, int mt, int slots) {
 
 // two M tiles per step on planes wider than two tiles, when a 4-slot ring of
 // the wider plane segments still fits
+// M tiles per CTA of k_conv_fwd: one tile when that at least doubles the CTAs
+// an SM holds (shared memory with the shallowest ring, TMEM columns), two
+// otherwise (fewer halo rows per output).  A CTA's loop over its planes is
+// latency-bound, so CTAs per SM count more than rows per CTA (enc1 at 256^3:
+// 116 us with two tiles at one CTA per SM, 96 us with one tile at two).
 static int pick_mt(const Geom& g, int cin, int nt) {
-    return g.plane > 2 * kOutStride && fwd_smem(cin, nt, g, 2, 4) <= kMaxSmem ? 2 : 1;
+    auto occ = [&](int mt) -> int {
+        const size_t smem = fwd_smem(cin, nt, g, mt, 4);
+        if (smem > kMaxSmem) return 0;
+        const uint32_t acols = 2 * mt * (3 * nt <= 64 ? 64 : 128);
+        const uint32_t cols = acols <= 128 ? 128 : (acols <= 256 ? 256 : 512);
+        return (int)std::min<size_t>(233472 / (smem + 1024), 512 / cols);
+    };
+    if (g.plane <= 2 * kOutStride) return 1;
+    const int o1 = occ(1), o2 = occ(2);
+    return o2 > 0 && o1 < 2 * o2 ? 2 : 1;
 }
 
 // Planes per CTA of a plane-marching grid with `units` CTAs per chunk of
