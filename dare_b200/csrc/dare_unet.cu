@@ -555,7 +555,10 @@ struct InArgs {
     Geom g;
     const bf16* w;      // [2 chunks][3 di x 16 co][8]: chunk c, element e < 6: dj = 2 c + e / 3, dk = e % 3
     bf16* out;          // chunk-planar [2][g.total][8]
-    int ppc;
+    bf16* pool;         // if set: pool_scale x (sum of the 2x2x2 children of `out`), chunk-planar on level cg
+    Geom cg;
+    float pool_scale;
+    int ppc;            // even: a CTA's output planes start on an odd plane I and pair up
     int* err;
     CUtensorMap x;      // FP32 input [n0][n1][pitch >= n2], boxes kInBoxK x (16 MT + 3) x kInB
 };
@@ -714,6 +717,7 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
         // p - 1 (di 2); before it, cur holds the partial sum of output p - 1
         // (planes p - 2 and p - 1) and nxt that of output p (plane p - 1)
         float cur[MT][8] = {}, nxt[MT][8] = {};
+        float pooled[MT][8];  // 2x2 sum of the first (odd) plane of a pair, on the lanes with j, k even
         for (int q = 0; q < ng; q++) {
             const int ab = q & (kInAcc - 1);
             if (!role_wait(&accf[ab], (q / kInAcc) & 1, abort_flag, a.err, 17)) break;
@@ -747,11 +751,45 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
                         cur[mt][c] = nxt[mt][c] + __uint_as_float(r[b][mt][1][c]);
                         nxt[mt][c] = __uint_as_float(r[b][mt][0][c]);
                     }
-                    if (k >= 2 && k < np && pos[mt] >= 0) {
-                        const int64_t Q = (int64_t)I * g.plane + pos[mt];
-                        *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, h)) =
-                            make_uint4(pack_bf16(o[0], o[1]), pack_bf16(o[2], o[3]), pack_bf16(o[4], o[5]),
-                                       pack_bf16(o[6], o[7]));
+                    if (k >= 2 && k < np) {
+                        const uint4 ov = make_uint4(pack_bf16(o[0], o[1]), pack_bf16(o[2], o[3]),
+                                                    pack_bf16(o[4], o[5]), pack_bf16(o[6], o[7]));
+                        if (pos[mt] >= 0) {
+                            const int64_t Q = (int64_t)I * g.plane + pos[mt];
+                            *reinterpret_cast<uint4*>(a.out + act_off(g.total, Q, h)) = ov;
+                        }
+                        if (a.pool) {
+                            // the children in the order of k_restrict: planes I, I + 1; in
+                            // each, (j, k), (j, k+1), (j+1, k), (j+1, k+1) -- lanes +0, +1, +8, +9.
+                            // I0 is odd and a group holds an even number of planes, so
+                            // output plane I is the second of its pair when b is odd.
+                            static_assert(kInB % 2 == 0, "plane pairs must not straddle groups");
+                            const bool second = (b & 1) != 0;
+                            const float v[8] = {bf16_lo(ov.x), bf16_hi(ov.x), bf16_lo(ov.y), bf16_hi(ov.y),
+                                                bf16_lo(ov.z), bf16_hi(ov.z), bf16_lo(ov.w), bf16_hi(ov.w)};
+#pragma unroll
+                            for (int c = 0; c < 8; c++) {
+                                const float v1 = __shfl_down_sync(0xffffffffu, v[c], 1);
+                                const float v8 = __shfl_down_sync(0xffffffffu, v[c], 8);
+                                const float v9 = __shfl_down_sync(0xffffffffu, v[c], 9);
+                                float acc = second ? pooled[mt][c] + v[c] : v[c];
+                                acc += v1;
+                                acc += v8;
+                                acc += v9;
+                                pooled[mt][c] = acc;
+                            }
+                            if (second && (lane & 9) == 0 && pos[mt] >= 0) {
+                                const int jo = 16 * MT * jb + 16 * mt + (m >> 3), ko = 8 * kb + (m & 7);
+                                const int64_t Qc =
+                                    ((int64_t)((I - 2) / 2 + 1) * (a.cg.n1 + 2) + (jo / 2 + 1)) * a.cg.W + ko / 2 + 1;
+                                const float sc = a.pool_scale;
+                                *reinterpret_cast<uint4*>(a.pool + act_off(a.cg.total, Qc, h)) = make_uint4(
+                                    pack_bf16(pooled[mt][0] * sc, pooled[mt][1] * sc),
+                                    pack_bf16(pooled[mt][2] * sc, pooled[mt][3] * sc),
+                                    pack_bf16(pooled[mt][4] * sc, pooled[mt][5] * sc),
+                                    pack_bf16(pooled[mt][6] * sc, pooled[mt][7] * sc));
+                            }
+                        }
                     }
                 }
             }
@@ -1619,7 +1657,8 @@ static int launch_in_t(dare_ctx* ctx, LaunchCfg& lc, InArgs& a) {
         if ((rc = occupancy_fit(ctx, kern, smem, cols, &occ, in_threads()))) return rc;
         const Geom& g = a.g;
         const int tiles = ((g.n2 + 7) / 8) * ((g.n1 + 16 * MT - 1) / (16 * MT));
-        const int ppc = pick_ppc(g.n0, tiles, (int64_t)ctx->num_sms * occ);
+        const int ppc0 = pick_ppc(g.n0, tiles, (int64_t)ctx->num_sms * occ);
+        const int ppc = ppc0 + (ppc0 & 1);  // pairs of output planes stay in one CTA (n0 is even)
         lc.ppc = ppc;
         lc.occ = occ;
         lc.mt = MT;
@@ -1734,6 +1773,9 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
         a.g = net->geo[0];
         a.w = L.wf;
         a.out = out;
+        a.pool = net->P1;  // the average pool to level 1 rides on the epilogue
+        a.cg = net->geo[1];
+        a.pool_scale = 0.125f;
         a.err = net->err;
         return launch_in(net->ctx, L.fwd, a, in32, net->X0);
     }
@@ -1767,6 +1809,9 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
         a.g = net->geo[0];
         a.w = L.wb;
         a.out = dx;
+        a.pool = net->dD1;  // the restriction (sum) to level 1, transposing the prolongation
+        a.cg = net->geo[1];
+        a.pool_scale = 1.f;
         a.err = net->err;
         return launch_in(net->ctx, L.bwd, a, dy32, net->X0);
     }
@@ -1834,8 +1879,8 @@ static int prolong_add(dare_unet* net, int fl, const bf16* coarse, bf16* fine, f
 
 int apply(dare_unet* net, const float* u, float* z) {
     int rc;
+    // enc0 also writes P1, the average pool of S0
     if ((rc = conv_forward(net, ENC0, nullptr, u, OUT_STORE, net->S0, nullptr, nullptr, nullptr))) return rc;
-    if ((rc = restrict_to<16>(net, 0, net->S0, net->P1, 0.125f))) return rc;
     if ((rc = conv_forward(net, ENC1, net->P1, nullptr, OUT_STORE, net->S1, nullptr, nullptr, nullptr))) return rc;
     if ((rc = restrict_to<32>(net, 1, net->S1, net->P2, 0.125f))) return rc;
     if ((rc = conv_forward(net, ENC2, net->P2, nullptr, OUT_STORE, net->S2, nullptr, nullptr, nullptr))) return rc;
@@ -1856,8 +1901,8 @@ int apply(dare_unet* net, const float* u, float* z) {
 static int backward(dare_unet* net, const float* u, const float* g, float scale) {
     int rc;
     if ((rc = conv_wgrad(net, DEC0, net->S0, nullptr, nullptr, g, scale))) return rc;
+    // (also writes dD1, the restriction of dS0)
     if ((rc = conv_dgrad(net, DEC0, nullptr, g, net->dS0))) return rc;
-    if ((rc = restrict_to<16>(net, 0, net->dS0, net->dD1, 1.f))) return rc;
     if ((rc = conv_wgrad(net, DEC1, net->S1, nullptr, net->dD1, nullptr, scale))) return rc;
     if ((rc = conv_dgrad(net, DEC1, net->dD1, nullptr, net->dS1))) return rc;
     if ((rc = restrict_to<32>(net, 1, net->dS1, net->dD2, 1.f))) return rc;
