@@ -58,6 +58,29 @@ def test_forward_matches_oracle(ctx, n):
     assert all(e < FWD_TOL for e in errs.values()), errs
 
 
+def test_input_off_the_16_byte_grid(ctx):
+    """enc0 reads its FP32 input through a TMA map, which needs a 16-byte
+    base: a vector that starts 4 bytes off goes through a pitched staging
+    copy first and must give the same output, bit for bit."""
+    import dare_b200 as D
+    torch = _torch()
+    n = (16, 24, 32)
+    net = D.LearnedPreconditioner(ctx, n, seed=3)
+    net.set_weights(_weights(12, net.num_params))
+    N = int(np.prod(n))
+    g = torch.Generator().manual_seed(6)
+    buf = torch.randn(N + 4, generator=g, dtype=torch.float32).cuda()
+    shifted = buf[1:N + 1]
+    assert shifted.data_ptr() % 16 == 4
+    aligned = shifted.clone()
+    assert aligned.data_ptr() % 16 == 0
+    z0, z1 = torch.empty(N, device="cuda"), torch.empty(N, device="cuda")
+    net.apply(aligned.data_ptr(), z0.data_ptr())
+    net.apply(shifted.data_ptr(), z1.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(z0, z1)
+
+
 def test_identity_at_initialisation(ctx):
     # dec0 starts at zero: N = I exactly before any training
     import dare_b200 as D
