@@ -655,8 +655,9 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
         const int bt = tid - 9 * 32;
         for (int q = 0; q < ng; q++) {
             const int sr = q % kInRaw, sw = q % kInWin;
-            if (!role_wait(&rawf[sr], (q / kInRaw) & 1, abort_flag, a.err, 12)) break;
-            if (!role_wait(&empty[sw], ((q / kInWin) & 1) ^ 1, abort_flag, a.err, 12)) break;
+            bool ok = role_wait(&rawf[sr], (q / kInRaw) & 1, abort_flag, a.err, 12);
+            if (ok) ok = role_wait(&empty[sw], ((q / kInWin) & 1) ^ 1, abort_flag, a.err, 12);
+            if (!__all_sync(0xffffffffu, ok)) break;  // the warp leaves together (__syncwarp below)
             const float* x = reinterpret_cast<const float*>(raw + sr * RAWS);
             uint8_t* wp = win + sw * kInB * WINB;
             for (int it = bt; it < kInB * WR * 8; it += kInBuilders) {
@@ -720,7 +721,8 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
         float pooled[MT][8];  // 2x2 sum of the first (odd) plane of a pair, on the lanes with j, k even
         for (int q = 0; q < ng; q++) {
             const int ab = q & (kInAcc - 1);
-            if (!role_wait(&accf[ab], (q / kInAcc) & 1, abort_flag, a.err, 17)) break;
+            const bool okw = role_wait(&accf[ab], (q / kInAcc) & 1, abort_flag, a.err, 17);
+            if (!__all_sync(0xffffffffu, okw)) break;  // tcgen05.ld below is warp-collective
             fence_after_sync();
             uint32_t r[kInB][MT][3][8];
 #pragma unroll
