@@ -343,12 +343,15 @@ __device__ __forceinline__ double face_rr(double a, double b, double c, double d
 // A warp covers 31 cells of a k row: lane 0 is the cell below them and only
 // supplies its T face.  Every coefficient comes from the same operations on the same operands as
 // the per-cell evaluation of k_assemble, so the results are bit-identical.
-// (Loading the next plane's operands one plane ahead needs ~40 more
-// registers, i.e. 2 instead of 3 blocks per SM, and measured slower.)
+// The kernel is latency-bound (FP64 divisions, loads): it is held to 64
+// registers so four blocks share an SM (a few spilled words; 0.79 ms at 256^3
+// against 0.86 ms with 80 registers at three blocks, no gain at five).
+// Loading the next plane's operands one plane ahead needs ~40 more
+// registers and measured slower.
 constexpr int kAsmK = 31, kAsmJ = 8;
 
 template <int LIM>
-__global__ void __launch_bounds__(256, 3) k_assemble3(GridDev g, AsmParams a, const double* __restrict__ phi,
+__global__ void __launch_bounds__(256, 4) k_assemble3(GridDev g, AsmParams a, const double* __restrict__ phi,
                                                       const double* __restrict__ phi_old, double* __restrict__ diag,
                                                       double* __restrict__ rhs_out, double* __restrict__ x0,
                                                       int planes) {
