@@ -75,16 +75,34 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, interval_ms: int = 50):
         self.path = tempfile.mktemp(prefix="dare_clocks_", suffix=".csv")
         self.proc = None
+        self.skip = 0
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-i",
-                 str(gpu_index), "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 str(gpu_index), "-lms", str(interval_ms)], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a while to start: wait (at most 5 s) for its first
+        # sample, so that sampling runs before the timed region begins
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
+
+    def _complete_lines(self) -> list:
+        with open(self.path) as fh:
+            return [line for line in fh if line.endswith("\n")]
+
+    def mark(self):
+        """Call right before the timed region: earlier samples are not counted."""
+        if self.proc is not None:
+            self.skip = len(self._complete_lines())
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -97,7 +115,7 @@ class ClockSampler:
         self.fh.close()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in self._complete_lines()[self.skip:]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -252,6 +270,7 @@ def run_dare(args):
     iters = []
     barrier()
     ctx.synchronize()
+    clocks.mark()
     ctx.timer_start()
     for _ in range(args.steps):
         rep = D.timestep(system, field, asm, solver)
