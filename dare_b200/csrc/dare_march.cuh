@@ -404,8 +404,13 @@ __device__ __forceinline__ Pair<T> ld_pair(const T* p) {
 // (8 bytes for FP32), halving the per-cell copies, index arithmetic and
 // barrier waits; the operand rows are padded so those copies stay aligned.
 // ---------------------------------------------------------------------------
+// Register budgets, measured at 256^3: one cell per thread runs best at two
+// blocks per SM (held to 3 blocks, i.e. 80 registers, steps 2 and 4 went
+// from 0.343 / 0.353 ms to 0.408 / 0.433 ms); two cells per thread gain from
+// a third and fourth block (steps 1 and 3: 0.264 -> 0.257 ms).
 template <class K, int CPT = 1>
-__global__ void __launch_bounds__(256) k_march(GridDev g, K kern, SolverState* st, double* partials, MarchCfg m) {
+__global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K kern, SolverState* st, double* partials,
+                                                                   MarchCfg m) {
     using T = typename K::type;
     constexpr int NZ = K::NZ, NP = K::NP;
     constexpr int QA = K::Q > 0 ? K::Q : 1;
