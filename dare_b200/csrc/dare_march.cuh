@@ -404,10 +404,12 @@ __device__ __forceinline__ Pair<T> ld_pair(const T* p) {
 // (8 bytes for FP32), halving the per-cell copies, index arithmetic and
 // barrier waits; the operand rows are padded so those copies stay aligned.
 // ---------------------------------------------------------------------------
-// Register budgets, measured at 256^3: one cell per thread runs best at two
-// blocks per SM (held to 3 blocks, i.e. 80 registers, steps 2 and 4 went
-// from 0.343 / 0.353 ms to 0.408 / 0.433 ms); two cells per thread gain from
-// a third and fourth block (steps 1 and 3: 0.264 -> 0.257 ms).
+// Register budgets, measured at 256^3: two cells per thread held to 80
+// registers (steps 1 and 3: 0.264 -> 0.257 ms); one cell per thread up to 128,
+// two blocks per SM (held to 80 registers, steps 2 and 4 went from
+// 0.343 / 0.353 ms to 0.408 / 0.433 ms, also when the maximum shared-memory
+// carveout then let three blocks in; that carveout also slowed steps 1 and 3
+// to 0.354 ms, so the default carveout stays).
 template <class K, int CPT = 1>
 __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K kern, SolverState* st, double* partials,
                                                                    MarchCfg m) {
