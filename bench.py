@@ -221,17 +221,10 @@ def run_dare(args):
 
     import dare_b200 as D
     from dare_b200 import workloads as W
+    from dare_b200.replicas import Replicas
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ranks = Replicas("nccl")
+    rank, world, local = ranks.rank, ranks.world, ranks.local
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
 
@@ -254,16 +247,7 @@ def run_dare(args):
     ctx.reset_kernel_stats()
     ctx.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     clocks = ClockSampler(local)
     launches0 = ctx.launch_count
@@ -352,9 +336,7 @@ def run_dare(args):
             "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
