@@ -35,7 +35,7 @@ if ROOT not in sys.path:
 METRIC = "implicit steps/s & time-to-1e-10 residual: learned vs plain BiCGStab2, 1 B200"
 UNIT = "steps/s"
 # Algorithmic bytes per cell and launch (FP64, each operand streamed once; the
-# SpMV inputs at the 6 neighbours come from cache).  See DESIGN.md.
+# SpMV inputs at the 6 neighbours come from cache).
 BYTES_PER_CELL = {
     "assemble": 8 + 8 + 24 + 56 + 8 + 8,   # phi, phi_old, 3 face velocities; 7 diagonals, rhs, x0
     "step1": 88,    # r, u, 6 off-diagonals, r_hat; u', v
@@ -404,7 +404,7 @@ def learned_comparison(D, ctx, system, field, asm, n, args):
 
 
 # ----------------------------------------------------------------------------
-# the other configurations (reported in DESIGN.md / profiles/, not the headline)
+# the other configurations (reported beside the headline, not as it)
 # ----------------------------------------------------------------------------
 def _gpu_setup_field(D, ctx, case):
     grid = D.Grid(ctx, case["n"], case["size"], 2, case["periodic"])

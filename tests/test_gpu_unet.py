@@ -140,7 +140,7 @@ def _operator(ctx, n, seed):
     return training.Operator(ctx, training.sample_case(n, seed, "cuda:0"))
 
 
-def test_learned_solver_fallback_and_residual_judge(ctx):
+def test_learned_solver_fallback_and_fp64_residual(ctx):
     import dare_b200 as D
     n = 32
     net = D.LearnedPreconditioner(ctx, (n, n, n), seed=5)
@@ -154,7 +154,7 @@ def test_learned_solver_fallback_and_residual_judge(ctx):
     rep = net.solve(op.system, solver, net.learned_params(iteration_budget=1))
     assert rep["fallback_used"] == 1 and rep["converged"] == 1
     assert rep["true_res_abs"] <= rep["tol_abs"] * 1.0000001
-    # a normal budget: converged by the learned phase, judged by the FP64 residual
+    # a normal budget: converged by the learned phase, checked by the FP64 residual
     op.assemble()
     rep = net.solve(op.system, solver)
     print(plain, rep)
