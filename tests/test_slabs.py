@@ -1,0 +1,99 @@
+"""Slab decomposition of the implicit step's solve (the reference's MPI
+distribution, restated in oracle/slabs.py for the multi-GPU slab path): a
+rank owns runs of i-planes, exchanges one boundary plane with each
+i-neighbour before every SpMV and sums every dot product over ranks.  Run as
+gloo ranks on CPU and checked against the serial oracle solve."""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from oracle import oracle as O
+from oracle import slabs as S
+from tests.helpers import oracle_assembly, oracle_grid
+
+N = (9, 6, 5)
+
+
+def _system(periodic):
+    """A TVD convection-diffusion implicit step (van Leer, diffusion, DDT) as
+    the oracle assembles and exports it."""
+    rng = np.random.default_rng(21)
+    case = {"n": N, "size": (1.0, 0.8, 1.3), "periodic": periodic, "dt": 0.02, "D": 3e-3,
+            "phi0": rng.random(tuple(x + 4 for x in N)), "limiter": "VANLEER",
+            "face_vel": [rng.normal(size=tuple(x + (1 if e == d else 0) for e, x in enumerate(N)))
+                         for d in range(3)]}
+    # a non-periodic axis gets a Dirichlet face below and a Neumann face above
+    case["bc"] = {2 * d + 1: (1, 1.0 + d) for d in range(3) if not periodic[d]}
+    case["bc"].update({2 * d + 2: (2, 0.0) for d in range(3) if not periodic[d]})
+    og = oracle_grid(case)
+    phi = np.ascontiguousarray(case["phi0"].reshape(-1))
+    diag, rhs, mask = O.assemble(oracle_assembly(og, case), phi, phi)
+    rp, cols, vals = O.export_csr(og, diag, mask)
+    x0 = O.field_to_vector(og, phi)
+    tol = 1e-12 * float(np.linalg.norm(rhs))
+    return rp, cols, vals, rhs, x0, tol
+
+
+def _serial(periodic, jacobi):
+    rp, cols, vals, rhs, x0, tol = _system(periodic)
+    slab = S.Slab(N, rp, cols, vals, 0, N[0], bool(periodic[0]))
+    return S.bicgstab2(slab, S.Comm(None, 0, 1, bool(periodic[0])), rhs, x0, tol, 500, jacobi)
+
+
+@pytest.mark.parametrize("jacobi", [False, True])
+def test_serial_restatement_matches_oracle(jacobi):
+    periodic = (1, 1, 1)
+    rp, cols, vals, rhs, x0, tol = _system(periodic)
+    x, info = _serial(periodic, jacobi)
+    ox, oinfo = O.bicgstab2(rp, cols, vals, rhs, x0, tol, 500, O.PREC_JACOBI if jacobi else O.PREC_NONE)
+    assert info["converged"] and oinfo["converged"]
+    assert abs(info["iters"] - oinfo["iters"]) <= 1
+    assert np.linalg.norm(x - ox) <= 1e-10 * np.linalg.norm(ox)
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, periodic, jacobi, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    rp, cols, vals, rhs, x0, tol = _system(periodic)
+    i0, i1 = S.slab_range(N[0], world, rank)
+    P = N[1] * N[2]
+    slab = S.Slab(N, rp, cols, vals, i0, i1, bool(periodic[0]))
+    x, info = S.bicgstab2(slab, S.Comm(dist, rank, world, bool(periodic[0])), rhs[i0 * P:i1 * P],
+                          x0[i0 * P:i1 * P], tol, 500, jacobi)
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(os.path.join(out, f"x{rank}.npy"), x)
+    with open(os.path.join(out, f"i{rank}.json"), "w") as fh:
+        json.dump({"i0": i0, "i1": i1, **{k: float(v) for k, v in info.items()}}, fh)
+
+
+@pytest.mark.parametrize("world,periodic,jacobi", [(2, (1, 1, 1), False), (3, (1, 0, 1), True),
+                                                   (2, (0, 1, 1), True)])
+def test_slab_ranks_match_serial_solve(tmp_path, world, periodic, jacobi):
+    mp.spawn(_rank, args=(world, _free_port(), periodic, jacobi, str(tmp_path)), nprocs=world, join=True)
+    infos = [json.load(open(tmp_path / f"i{r}.json")) for r in range(world)]
+    # the slabs tile the planes in order
+    assert infos[0]["i0"] == 0 and infos[-1]["i1"] == N[0]
+    assert all(infos[r]["i1"] == infos[r + 1]["i0"] for r in range(world - 1))
+    # every rank takes the same decisions (the scalars come from the same sums)
+    assert len({(i["iters"], i["status"], i["converged"]) for i in infos}) == 1
+    x = np.concatenate([np.load(tmp_path / f"x{r}.npy") for r in range(world)])
+    sx, sinfo = _serial(periodic, jacobi)
+    rp, cols, vals, rhs, x0, tol = _system(periodic)
+    ox, oinfo = O.bicgstab2(rp, cols, vals, rhs, x0, tol, 500, O.PREC_JACOBI if jacobi else O.PREC_NONE)
+    assert infos[0]["converged"] == 1
+    assert abs(infos[0]["iters"] - sinfo["iters"]) <= 1 and abs(infos[0]["iters"] - oinfo["iters"]) <= 1
+    # partial sums are added in another order across ranks: rounding-level differences only
+    assert np.linalg.norm(x - sx) <= 1e-10 * np.linalg.norm(sx)
+    assert np.linalg.norm(x - ox) <= 1e-9 * np.linalg.norm(ox)
