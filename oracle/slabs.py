@@ -40,11 +40,13 @@ class Slab:
     """The rows of one rank: CSR rows of the cells of planes [i0, i1) with
     their columns renumbered into the extended local vector
     [plane i0 - 1 | own planes | plane i1] (the halo planes, wrapped when
-    the grid is periodic along i)."""
+    the grid is periodic along i).  With `ncomp` components the rows and
+    columns are cell * ncomp + c (MatrixBlock_Cartesian.inl:127-240), so a
+    plane holds n1 n2 ncomp entries."""
 
-    def __init__(self, n, rowptr, cols, vals, i0: int, i1: int, periodic_i: bool):
+    def __init__(self, n, rowptr, cols, vals, i0: int, i1: int, periodic_i: bool, ncomp: int = 1):
         n0, n1, n2 = n
-        self.P = n1 * n2
+        self.P = n1 * n2 * ncomp
         self.n0, self.i0, self.i1 = n0, i0, i1
         self.periodic_i = periodic_i
         r0, r1 = i0 * self.P, i1 * self.P

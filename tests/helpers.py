@@ -119,3 +119,20 @@ def diag_to_csr(dim, n, diag, periodic=None):
         hi = np.ones(idx.shape[1], dtype=bool) if pp[d] else idx[d] < nn[d] - 1
         mask |= (lo.astype(np.uint8) << (2 * d + 1)) | (hi.astype(np.uint8) << (2 * d + 2))
     return O.export_csr(og, np.ascontiguousarray(diag), mask)
+
+
+def interleave_csr(csrs):
+    """Rows cell * N + c and columns neighbour * N + c from one CSR per component
+    (MatrixBlock_Cartesian.inl:127-240: no coupling between components)."""
+    N = len(csrs)
+    rp0 = csrs[0][0]
+    ncell = rp0.size - 1
+    rows, cols, vals = [], [], []
+    for cell in range(ncell):
+        for c, (rp, co, va) in enumerate(csrs):
+            a, b = rp[cell], rp[cell + 1]
+            rows.append(b - a)
+            cols.append(co[a:b] * N + c)
+            vals.append(va[a:b])
+    rowptr = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
+    return rowptr, np.concatenate(cols).astype(np.int64), np.concatenate(vals)

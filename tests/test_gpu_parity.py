@@ -12,7 +12,7 @@ import dare_b200 as D
 from dare_b200 import workloads as W
 from oracle import oracle as O
 from tests.helpers import (coupled_components_diag, diag_to_csr, interior, oracle_assembly, oracle_grid,
-                           oracle_timeloop, profile_functor_diag, rel_l2)
+                           oracle_timeloop, profile_functor_diag, rel_l2, interleave_csr)
 
 pytestmark = pytest.mark.gpu
 
@@ -428,23 +428,6 @@ def test_vtk_writer_device_matches_host(ctx, tmp_path):
 
 
 # ---- several field components (Field<Grid,SC,N>, MatrixBlock<...,N>) ----------
-def _interleave_csr(csrs):
-    """Rows cell * N + c and columns neighbour * N + c from one CSR per component
-    (MatrixBlock_Cartesian.inl:127-240: no coupling between components)."""
-    N = len(csrs)
-    rp0 = csrs[0][0]
-    ncell = rp0.size - 1
-    rows, cols, vals = [], [], []
-    for cell in range(ncell):
-        for c, (rp, co, va) in enumerate(csrs):
-            a, b = rp[cell], rp[cell + 1]
-            rows.append(b - a)
-            cols.append(co[a:b] * N + c)
-            vals.append(va[a:b])
-    rowptr = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
-    return rowptr, np.concatenate(cols).astype(np.int64), np.concatenate(vals)
-
-
 @pytest.mark.parametrize("dim", [1, 2, 3])
 def test_multicomponent_linear_profiles(ctx, dim):
     """test_integration_Cartesian_Trilinos.cpp (N = 3 components, SolveScalar
@@ -472,7 +455,7 @@ def test_multicomponent_linear_profiles(ctx, dim):
         assert np.max(np.abs(x[:, c] - (w + (e - w) * (i + 0.5) / nn[0]))) < 1e-8
     # the exported pattern interleaves the components, and the oracle's
     # BiCGStab2 on that matrix gives the same solution
-    rp, cols, vals = _interleave_csr([diag_to_csr(dim, n, p[0]) for p in parts])
+    rp, cols, vals = interleave_csr([diag_to_csr(dim, n, p[0]) for p in parts])
     grp, gcols, gvals = s.export_csr()
     np.testing.assert_array_equal(grp, rp)
     np.testing.assert_array_equal(gcols, cols)
@@ -525,7 +508,7 @@ def test_multicomponent_assembly_and_timeloop(ctx, periodic):
         rep = D.timestep(s, f, asm, solver)
         assert rep["converged"], rep
         per = [O.assemble(desc, c, o) for c, o in zip(ocomps, oold)]
-        rp, cols, vals = _interleave_csr([O.export_csr(og, p[0], p[2]) for p in per])
+        rp, cols, vals = interleave_csr([O.export_csr(og, p[0], p[2]) for p in per])
         b = np.stack([p[1] for p in per], axis=-1).reshape(-1)
         x0 = np.stack([O.field_to_vector(og, c) for c in ocomps], axis=-1).reshape(-1)
         x, info = O.bicgstab2(rp, cols, vals, b, x0, 1e-10 * np.linalg.norm(b), 5000)

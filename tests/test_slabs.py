@@ -13,15 +13,15 @@ import torch.multiprocessing as mp
 
 from oracle import oracle as O
 from oracle import slabs as S
-from tests.helpers import oracle_assembly, oracle_grid
+from tests.helpers import interleave_csr, oracle_assembly, oracle_grid
 
 N = (9, 6, 5)
 
 
-def _system(periodic):
+def _system(periodic, seed=21):
     """A TVD convection-diffusion implicit step (van Leer, diffusion, DDT) as
     the oracle assembles and exports it."""
-    rng = np.random.default_rng(21)
+    rng = np.random.default_rng(seed)
     case = {"n": N, "size": (1.0, 0.8, 1.3), "periodic": periodic, "dt": 0.02, "D": 3e-3,
             "phi0": rng.random(tuple(x + 4 for x in N)), "limiter": "VANLEER",
             "face_vel": [rng.normal(size=tuple(x + (1 if e == d else 0) for e, x in enumerate(N)))
@@ -96,4 +96,43 @@ def test_slab_ranks_match_serial_solve(tmp_path, world, periodic, jacobi):
     assert abs(infos[0]["iters"] - sinfo["iters"]) <= 1 and abs(infos[0]["iters"] - oinfo["iters"]) <= 1
     # partial sums are added in another order across ranks: rounding-level differences only
     assert np.linalg.norm(x - sx) <= 1e-10 * np.linalg.norm(sx)
+    assert np.linalg.norm(x - ox) <= 1e-9 * np.linalg.norm(ox)
+
+
+def _system2(periodic):
+    """Two components, each its own velocity and field (no coupling), rows
+    and columns cell * 2 + c."""
+    a, b = _system(periodic, 21), _system(periodic, 22)
+    rp, cols, vals = interleave_csr([a[:3], b[:3]])
+    rhs = np.stack([a[3], b[3]], axis=1).reshape(-1)
+    x0 = np.stack([a[4], b[4]], axis=1).reshape(-1)
+    return rp, cols, vals, rhs, x0, 1e-12 * float(np.linalg.norm(rhs))
+
+
+def _rank2(rank, world, port, periodic, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    rp, cols, vals, rhs, x0, tol = _system2(periodic)
+    i0, i1 = S.slab_range(N[0], world, rank)
+    P = N[1] * N[2] * 2
+    slab = S.Slab(N, rp, cols, vals, i0, i1, bool(periodic[0]), ncomp=2)
+    x, info = S.bicgstab2(slab, S.Comm(dist, rank, world, bool(periodic[0])), rhs[i0 * P:i1 * P],
+                          x0[i0 * P:i1 * P], tol, 500, True)
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(os.path.join(out, f"x{rank}.npy"), x)
+    with open(os.path.join(out, f"i{rank}.json"), "w") as fh:
+        json.dump({k: float(v) for k, v in info.items()}, fh)
+
+
+def test_slab_ranks_two_components(tmp_path):
+    periodic = (1, 1, 1)
+    mp.spawn(_rank2, args=(2, _free_port(), periodic, str(tmp_path)), nprocs=2, join=True)
+    infos = [json.load(open(tmp_path / f"i{r}.json")) for r in range(2)]
+    assert infos[0] == infos[1] and infos[0]["converged"] == 1
+    x = np.concatenate([np.load(tmp_path / f"x{r}.npy") for r in range(2)])
+    rp, cols, vals, rhs, x0, tol = _system2(periodic)
+    ox, oinfo = O.bicgstab2(rp, cols, vals, rhs, x0, tol, 500, O.PREC_JACOBI)
+    assert abs(infos[0]["iters"] - oinfo["iters"]) <= 1
     assert np.linalg.norm(x - ox) <= 1e-9 * np.linalg.norm(ox)
