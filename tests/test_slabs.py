@@ -136,3 +136,50 @@ def test_slab_ranks_two_components(tmp_path):
     ox, oinfo = O.bicgstab2(rp, cols, vals, rhs, x0, tol, 500, O.PREC_JACOBI)
     assert abs(infos[0]["iters"] - oinfo["iters"]) <= 1
     assert np.linalg.norm(x - ox) <= 1e-9 * np.linalg.norm(ox)
+
+
+def test_slab_assembly_from_two_halo_planes():
+    """A rank assembles its own rows from its planes of phi and phi_old plus
+    two planes from each i-neighbour (the van Leer face of cell i reads
+    i - 2: HaloBuffer's ghost width is 2) and its slice of the face
+    velocities; the result is the global assembly's rows, bit for bit.
+    (A slab is emulated as a grid periodic along i whose ghost planes hold
+    the neighbours' planes.  On a periodic axis the staggered field's last
+    face is its first (CartesianRepresentation.inl:64-76), so the i-faces
+    here do not vary along i: the slab's upper face then equals the
+    neighbour's first face either way.)"""
+    n0, n1, n2 = 10, 6, 5
+    h = 0.125   # dx exactly representable, hence the same on every slab
+    rng = np.random.default_rng(5)
+    phi = rng.random((n0 + 4, n1 + 4, n2 + 4))
+    old = rng.random((n0 + 4, n1 + 4, n2 + 4))
+    fv = [rng.normal(size=tuple(x + (1 if e == d else 0) for e, x in enumerate((n0, n1, n2)))) for d in range(3)]
+    fv[0] = np.ascontiguousarray(np.broadcast_to(fv[0][:1], fv[0].shape))
+    case = {"n": (n0, n1, n2), "size": (n0 * h, 0.75, 1.25), "periodic": (1, 1, 1), "dt": 0.02, "D": 3e-3,
+            "limiter": "VANLEER", "face_vel": fv}
+    og = oracle_grid(case)
+    pf, of = phi.reshape(-1).copy(), old.reshape(-1).copy()
+    O.exchange_halo(og, pf)
+    O.exchange_halo(og, of)
+    diag, rhs, _ = O.assemble(oracle_assembly(og, case), pf, of)
+    phi3, old3 = pf.reshape(phi.shape), of.reshape(old.shape)
+    P = n1 * n2
+    for world in (2, 3):
+        for rank in range(world):
+            i0, i1 = S.slab_range(n0, world, rank)
+            nl = i1 - i0
+            # ghosted planes of the slab = global ghosted planes i0 .. i1 + 3
+            lp = np.ascontiguousarray(phi3[i0:i1 + 4]).reshape(-1)
+            lo = np.ascontiguousarray(old3[i0:i1 + 4]).reshape(-1)
+            lcase = dict(case, n=(nl, n1, n2), size=(nl * h, 0.75, 1.25),
+                         face_vel=[np.ascontiguousarray(fv[0][i0:i1 + 1]), np.ascontiguousarray(fv[1][i0:i1]),
+                                   np.ascontiguousarray(fv[2][i0:i1])])
+            desc = oracle_assembly(oracle_grid(lcase), lcase)
+            ld, lr, _ = O.assemble(desc, lp, lo)
+            assert np.array_equal(ld, diag[:, i0 * P:i1 * P]) and np.array_equal(lr, rhs[i0 * P:i1 * P])
+            # with only one halo plane per side the TVD corrections differ
+            bad = lp.reshape(nl + 4, n1 + 4, n2 + 4).copy()
+            bad[0] += 10.0
+            bad[-1] += 10.0
+            bd, br, _ = O.assemble(desc, np.ascontiguousarray(bad.reshape(-1)), lo)
+            assert not np.array_equal(br, rhs[i0 * P:i1 * P])
