@@ -66,6 +66,31 @@ class Slab:
             raise ValueError("a row reaches past the neighbouring planes: not a 7-point slab")
         self.lcols = (rel + 1) * self.P + inplane   # index into [halo_lo | own | halo_hi]
 
+    @classmethod
+    def from_local(cls, n_local, rowptr, cols, vals, ncomp: int = 1):
+        """A slab from the CSR a rank exports for its own grid of n_local[0]
+        planes numbered as if periodic along i: a column one plane below the
+        first plane (or above the last) wrapped onto the far plane, and is
+        renumbered into the halo by its plane offset from the row
+        (needs at least three planes)."""
+        nl = n_local[0]
+        if nl < 3:
+            raise ValueError("a slab of fewer than three planes cannot tell a wrapped column from an own one")
+        self = cls.__new__(cls)
+        self.P = n_local[1] * n_local[2] * ncomp
+        self.n0, self.i0, self.i1, self.periodic_i = nl, 0, nl, True
+        self.nrows = nl * self.P
+        self.rowptr = np.asarray(rowptr, dtype=np.int64)
+        self.vals = np.asarray(vals, dtype=np.float64)
+        gcols = np.asarray(cols, dtype=np.int64)
+        rplane = np.repeat(np.arange(self.nrows) // self.P, np.diff(self.rowptr))
+        cplane = gcols // self.P
+        delta = (cplane - rplane + 1) % nl - 1
+        if np.any(delta > 1):
+            raise ValueError("a row reaches past the neighbouring planes: not a 7-point slab")
+        self.lcols = (rplane + delta + 1) * self.P + (gcols - cplane * self.P)
+        return self
+
     def spmv(self, xext: np.ndarray) -> np.ndarray:
         """y = A x for the own rows; `xext` is the extended local vector."""
         prod = self.vals * xext[self.lcols]
@@ -90,30 +115,35 @@ class Comm:
         hi = self.rank + 1 if self.rank < self.world - 1 else (0 if self.periodic_i else None)
         return lo, hi
 
+    def swap(self, first: np.ndarray, last: np.ndarray):
+        """Sends `first` (this rank's lowest planes) to the lower neighbour and
+        `last` (its highest) to the upper one; returns what they sent in
+        return: (the lower neighbour's highest planes, the upper neighbour's
+        lowest).  Zeros where there is no neighbour."""
+        below, above = np.zeros_like(first), np.zeros_like(last)
+        lo, hi = self._neighbours()
+        if self.world == 1:
+            if self.periodic_i:
+                below, above = last.copy(), first.copy()
+            return below, above
+        import torch
+        t_below, t_above = torch.from_numpy(below), torch.from_numpy(above)
+        reqs = []
+        # tag 0: planes travelling up (my highest are the upper rank's lower halo), tag 1: down
+        if lo is not None:
+            reqs.append(self.dist.irecv(t_below, src=lo, tag=0))
+            reqs.append(self.dist.isend(torch.from_numpy(np.ascontiguousarray(first)), dst=lo, tag=1))
+        if hi is not None:
+            reqs.append(self.dist.irecv(t_above, src=hi, tag=1))
+            reqs.append(self.dist.isend(torch.from_numpy(np.ascontiguousarray(last)), dst=hi, tag=0))
+        for r in reqs:
+            r.wait()
+        return below, above
+
     def extend(self, x: np.ndarray, P: int) -> np.ndarray:
         """[plane below | x | plane above], the planes from the neighbouring
         ranks (zeros where there is none: those columns do not occur)."""
-        import torch
-        lo, hi = self._neighbours()
-        below, above = np.zeros(P), np.zeros(P)
-        if self.world == 1:
-            if self.periodic_i:
-                below, above = x[-P:].copy(), x[:P].copy()
-        else:
-            t_below, t_above = torch.zeros(P, dtype=torch.float64), torch.zeros(P, dtype=torch.float64)
-            first = torch.from_numpy(np.ascontiguousarray(x[:P]))
-            last = torch.from_numpy(np.ascontiguousarray(x[-P:]))
-            reqs = []
-            # tag 0: a plane travelling up (my last plane is the upper rank's lower halo), tag 1: down
-            if lo is not None:
-                reqs.append(self.dist.irecv(t_below, src=lo, tag=0))
-                reqs.append(self.dist.isend(first, dst=lo, tag=1))
-            if hi is not None:
-                reqs.append(self.dist.irecv(t_above, src=hi, tag=1))
-                reqs.append(self.dist.isend(last, dst=hi, tag=0))
-            for r in reqs:
-                r.wait()
-            below, above = t_below.numpy(), t_above.numpy()
+        below, above = self.swap(x[:P], x[-P:])
         return np.concatenate([below, x, above])
 
     def allsum(self, values) -> np.ndarray:

@@ -13,7 +13,7 @@ import torch.multiprocessing as mp
 
 from oracle import oracle as O
 from oracle import slabs as S
-from tests.helpers import interleave_csr, oracle_assembly, oracle_grid
+from tests.helpers import interleave_csr, oracle_assembly, oracle_grid, oracle_timeloop
 
 N = (9, 6, 5)
 
@@ -183,3 +183,78 @@ def test_slab_assembly_from_two_halo_planes():
             bad[-1] += 10.0
             bd, br, _ = O.assemble(desc, np.ascontiguousarray(bad.reshape(-1)), lo)
             assert not np.array_equal(br, rhs[i0 * P:i1 * P])
+
+
+STEPS = 2
+
+
+def _steps_case():
+    """A periodic van Leer convection-diffusion case whose i-faces do not vary
+    along i (see the assembly test) and whose ghosts are already exchanged."""
+    n0, n1, n2, h = 10, 6, 5, 0.125
+    rng = np.random.default_rng(9)
+    fv = [rng.normal(size=tuple(x + (1 if e == d else 0) for e, x in enumerate((n0, n1, n2)))) for d in range(3)]
+    fv[0] = np.ascontiguousarray(np.broadcast_to(fv[0][:1], fv[0].shape))
+    case = {"n": (n0, n1, n2), "size": (n0 * h, 0.75, 1.25), "periodic": (1, 1, 1), "dt": 0.02, "D": 3e-3,
+            "limiter": "VANLEER", "face_vel": fv, "rel_tol": 1e-12}
+    phi = rng.random((n0 + 4) * (n1 + 4) * (n2 + 4))
+    O.exchange_halo(oracle_grid(case), phi)
+    case["phi0"] = phi.reshape(n0 + 4, n1 + 4, n2 + 4)
+    return case, h
+
+
+def _rank_steps(rank, world, port, out):
+    """One rank of the distributed driver loop: assemble the slab, solve it,
+    copy back, exchange two halo planes of the field, keep it as the old level."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    case, h = _steps_case()
+    n0, n1, n2 = case["n"]
+    i0, i1 = S.slab_range(n0, world, rank)
+    nl = i1 - i0
+    fv = case["face_vel"]
+    lcase = dict(case, n=(nl, n1, n2), size=(nl * h, 0.75, 1.25),
+                 face_vel=[np.ascontiguousarray(fv[0][i0:i1 + 1]), np.ascontiguousarray(fv[1][i0:i1]),
+                           np.ascontiguousarray(fv[2][i0:i1])])
+    lg = oracle_grid(lcase)
+    desc = oracle_assembly(lg, lcase)
+    comm = S.Comm(dist, rank, world, True)
+    phi = np.ascontiguousarray(case["phi0"][i0:i1 + 4]).reshape(-1).copy()
+    old = phi.copy()
+    iters = []
+    for _ in range(STEPS):
+        diag, rhs, mask = O.assemble(desc, phi, old)
+        slab = S.Slab.from_local((nl, n1, n2), *O.export_csr(lg, diag, mask))
+        x0 = O.field_to_vector(lg, phi)
+        tol = case["rel_tol"] * float(np.sqrt(comm.allsum([float(np.dot(rhs, rhs))])[0]))
+        x, info = S.bicgstab2(slab, comm, rhs, x0, tol, 5000, True)
+        O.copy_to_field(lg, x, phi)
+        O.exchange_halo(lg, phi)            # the j and k ghosts (its i ghosts are replaced next)
+        f3 = phi.reshape(nl + 4, n1 + 4, n2 + 4)
+        below, above = comm.swap(f3[2:4].copy(), f3[nl:nl + 2].copy())
+        f3[0:2], f3[nl + 2:nl + 4] = below, above
+        old[:] = phi
+        iters.append(info["iters"])
+    dist.barrier()
+    dist.destroy_process_group()
+    np.save(os.path.join(out, f"f{rank}.npy"), phi.reshape(nl + 4, n1 + 4, n2 + 4)[2:nl + 2])
+    with open(os.path.join(out, f"s{rank}.json"), "w") as fh:
+        json.dump({"iters": iters}, fh)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_time_steps_match_serial_loop(tmp_path, world):
+    """The reference's driver loop (Build, Solve, CopyTo, ExchangeHaloCells,
+    CopyDataVectorsToOldTimeStep) distributed over slabs gives the serial
+    loop's field."""
+    mp.spawn(_rank_steps, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    case, _ = _steps_case()
+    hist, siters = oracle_timeloop(case, STEPS)
+    n0, n1, n2 = case["n"]
+    want = hist[-1].reshape(n0 + 4, n1 + 4, n2 + 4)[2:n0 + 2]
+    got = np.concatenate([np.load(tmp_path / f"f{r}.npy") for r in range(world)])
+    iters = [json.load(open(tmp_path / f"s{r}.json"))["iters"] for r in range(world)]
+    assert all(it == iters[0] for it in iters)
+    assert all(abs(a - b) <= 1 for a, b in zip(iters[0], siters))
+    assert np.linalg.norm(got - want) <= 1e-10 * np.linalg.norm(want)
