@@ -79,3 +79,20 @@ def test_clock_sampler_without_nvidia_smi(tmp_path, monkeypatch):
     c.mark()
     rec = c.stop()
     assert rec["sm_mhz"] is None and rec["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_reference_arm_under_torchrun():
+    """Launched as the multi-GPU runs are (torchrun, two ranks, the same
+    flags), the reference arm prints one line from rank 0 and every rank
+    exits 0."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                          "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                          "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
