@@ -52,9 +52,13 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["dare", "reference"], default="dare")
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--n", "--cells-per-side", dest="n", type=int, default=256,
+                    help="cells per side (--cells-per-side under torchrun, whose parser claims --n)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=2,
+                    help="implicit steps of the CPU oracle: the cpu_baseline sample and the parity check")
+    ap.add_argument("--profile-steps", type=int, default=3,
+                    help="untimed steps with per-kernel CUDA events (roofline.kernels)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=["tvd", "gauss64", "hetero", "batched", "unet"], default="tvd",
@@ -140,20 +144,33 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-NCU_NAMES = {"assemble": "k_assemble", "step1": "k_march<FStep1>", "step2": "k_march<FStep2>",
+NCU_NAMES = {"assemble": "k_assemble3", "step1": "k_march<FStep1>", "step2": "k_march<FStep2>",
              "step3": "k_march<FStep3>", "step4": "k_march<FStep4>", "step5": "k_step5"}
 
 
 def ncu_traffic(kernel: str, n: int):
-    """DRAM bytes per launch (read + write) from the committed ncu summary
-    (profiles/traffic.json: per-cell figures of a 128^3 capture, scaled by
-    the cell count)."""
+    """DRAM bytes of one launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    from the committed ncu summary profiles/traffic.json, with where the
+    figure comes from: a capture of one launch at this grid size when the
+    summary holds one, else per-cell figures of a smaller capture scaled by
+    the cell count (on small grids part of the writes stay in L2, so a
+    scaled figure understates DRAM traffic)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
             t = json.load(fh)
-        return t[NCU_NAMES[kernel]]["bytes_per_cell"] * n ** 3
     except Exception:
-        return None
+        return None, None
+    name = NCU_NAMES[kernel]
+    for cap in t.get("captures", []):
+        if cap.get("cells") == n ** 3 and name in cap.get("kernels", {}):
+            k = cap["kernels"][name]
+            return k["read_bytes"] + k["write_bytes"], f"ncu, one launch at {cap['grid']}"
+    for cap in t.get("captures", []):
+        if name in cap.get("kernels", {}):
+            k = cap["kernels"][name]
+            return ((k["read_bytes"] + k["write_bytes"]) * n ** 3 / cap["cells"],
+                    f"ncu at {cap['grid']}, scaled by cells")
+    return None, None
 
 
 # ----------------------------------------------------------------------------
@@ -179,7 +196,7 @@ def cpu_steps(case, steps: int, n: int):
         times.append(time.perf_counter() - t0)
         iters.append(info["iters"])
         del diag, rp, cols, vals
-    return times, iters, O.num_threads()
+    return times, iters, O.num_threads(), phi
 
 
 def host_case(n, seed):
@@ -192,7 +209,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     case = host_case(args.n, args.seed)
-    times, iters, cores = cpu_steps(case, args.warmup + args.steps, args.n)
+    times, iters, cores, _ = cpu_steps(case, args.warmup + args.steps, args.n)
     timed = times[args.warmup:]
     total = sum(timed)
     value = len(timed) / total
@@ -208,6 +225,8 @@ def run_reference(args):
                                    "assembly, CSR build, BiCGStab2, copy back), OpenMP on all host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "iterations_per_step": statistics.mean(iters),
+        "parallelism": "one CPU run on rank 0's host (all its cores)",
+        "value_scope": "one CPU run: the host's steps/s, not multiplied by n_gpus",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -243,12 +262,12 @@ def run_dare(args):
 
     for _ in range(args.warmup):
         D.timestep(system, field, asm, solver)
-    ctx.set_profiling(True)
-    ctx.reset_kernel_stats()
     ctx.synchronize()
 
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
+    # the headline: the product path (iterations replayed from CUDA graphs,
+    # no per-kernel events), exactly K steps between two barriers
     clocks = ClockSampler(local)
     launches0 = ctx.launch_count
     iters = []
@@ -268,7 +287,15 @@ def run_dare(args):
     ms = max_over_ranks(ms)
     value = world * args.steps / (ms * 1e-3)
 
-    # per-kernel durations (CUDA events on the launching stream, timed region)
+    # per-kernel durations: a separate, untimed pass of the same steps with a
+    # CUDA event around every kernel (launched directly on the context's
+    # stream); every iteration that ran is counted, the last one included
+    ctx.set_profiling(True)
+    ctx.reset_kernel_stats()
+    prof_iters = []
+    for _ in range(args.profile_steps):
+        prof_iters.append(D.timestep(system, field, asm, solver)["iters"])
+    ctx.synchronize()
     kstats = {}
     for name in BYTES_PER_CELL:
         tot, cnt = ctx.kernel_stats(name)
@@ -281,9 +308,12 @@ def run_dare(args):
     if dom:
         algo = BYTES_PER_CELL[dom] * n ** 3
         achieved = algo / (kstats[dom]["ms_avg"] * 1e-3) / 1e9
+        traffic, traffic_src = ncu_traffic(dom, n)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(dom, n),
-                    "algorithmic_bytes": algo}
+                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                    "traffic_source": traffic_src, "algorithmic_bytes": algo,
+                    "timing": f"CUDA events around each kernel over {args.profile_steps} untimed steps "
+                              f"({sum(prof_iters)} iterations, every one counted)"}
         roofline["kernels"] = {k: {**v, "GBps": BYTES_PER_CELL[k] * n ** 3 / (v["ms_avg"] * 1e-3) / 1e9}
                                for k, v in kstats.items()}
 
@@ -306,14 +336,24 @@ def run_dare(args):
         e2e = {"value": world * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes}
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hcase = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in case.items() if k != "face_vel"}
         hcase["face_vel"] = [a.cpu().numpy() for a in case["face_vel"]]
-        times, citers, cores = cpu_steps(hcase, args.cpu_steps, n)
+        times, citers, cores, cpu_phi = cpu_steps(hcase, args.cpu_steps, n)
         cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{len(times)} full implicit steps of the same {n}^3 workload from the same initial "
                          f"field (CPU oracle, OpenMP), iterations {citers}"}
+        # parity at the full size: the same steps on the GPU from the same
+        # initial field, final fields compared (internal and ghost cells)
+        field.upload(phi0, 0)
+        field.upload(phi0, 1)
+        giters = [D.timestep(system, field, asm, solver)["iters"] for _ in range(args.cpu_steps)]
+        gpu_phi = field.download(0)
+        diff = gpu_phi - cpu_phi
+        parity = {"steps": args.cpu_steps, "rel_l2": float(np.linalg.norm(diff) / np.linalg.norm(cpu_phi)),
+                  "max_abs": float(np.abs(diff).max()), "iters_gpu": giters, "iters_cpu": citers,
+                  "bar": "rel_l2 < 1e-9 (solutions at the same 1e-10 relative residual)"}
 
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
@@ -327,11 +367,14 @@ def run_dare(args):
             "data": "synthetic (seeded divergence-free velocity, smooth scalar in [0,1])",
             "config": {"workload": f"TVD convection-diffusion {n}^3 periodic, van Leer, D=1e-4, Pe 5, CFL 0.5, "
                                    "Jacobi-BiCGStab2 to 1e-10 relative",
-                       "cells": n ** 3, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (system ~3.6 GB per GPU)"},
+                       "cells": n ** 3},
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (system ~3.6 GB per GPU)",
+            "parity": parity,
             "time_to_residual_ms": ms / args.steps, "iterations_per_step": statistics.mean(iters),
             "cell_updates_per_s": value * n ** 3,
-            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e); learned-preconditioned solve in 'learned'",
+            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e; iterations replayed from CUDA graphs); "
+                      "learned-preconditioned solve in 'learned'",
             "learned": learned,
             "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
         }

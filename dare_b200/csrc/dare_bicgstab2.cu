@@ -297,6 +297,9 @@ int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbloc
         if (check_every < 1) check_every = 1;
         if (check_every > 8) check_every = 8;
     }
+    // profiling checks after every pair, so each recorded duration belongs
+    // to a known iteration
+    if (prof) check_every = 1;
     const int max_pairs = max_it / 2 + 2;
     for (int gi = 0; gi < max_pairs; gi++) {
         if (prof) {
@@ -311,10 +314,18 @@ int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbloc
         if ((gi + 1) % check_every == 0 || gi + 1 == max_pairs) {
             DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
             DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            if (st_host->done) break;
-            if (prof && check_every == 1) {
-                // all ten kernels of this pair did real work: record their durations
-                for (int it = 0; it < 2; it++)
+            if (prof) {
+                // Iterations of this pair that ran in full: both while the
+                // solve goes on; on convergence the flag is raised by the
+                // last kernel of iteration k (k = 2 gi + 1 or 2 gi + 2), and
+                // the kernels after it returned at once.  A pair that ended
+                // in another status is not recorded.
+                int real = 2;
+                if (st_host->done) {
+                    real = st_host->status == ST_CONVERGED ? st_host->k - 2 * gi : 0;
+                    real = real < 0 ? 0 : real > 2 ? 2 : real;
+                }
+                for (int it = 0; it < real; it++)
                     for (int q = 0; q < 5; q++) {
                         float ms = 0.f;
                         if (cudaEventElapsedTime(&ms, ctx->ev[it * 5 + q], ctx->ev[it * 5 + q + 1]) == cudaSuccess) {
@@ -325,6 +336,7 @@ int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbloc
                         }
                     }
             }
+            if (st_host->done) break;
         }
     }
     DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));

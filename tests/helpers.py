@@ -58,6 +58,26 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+COEF_RTOL = 1e-13   # assembled FP64 coefficients, relative
+
+
+def assert_coef_close(got, ref, rtol=COEF_RTOL):
+    """Assembled coefficients within `rtol` relative: per entry
+    |got - ref| <= rtol |ref| + rtol max|ref of that slot| (the second term
+    covers entries that are sums with cancellation, e.g. a deferred-correction
+    rhs where phi_old = 0).  NaN where the reference has NaN (VANALBADA at
+    r = +-inf)."""
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    assert got.shape == ref.shape
+    rows = ref.reshape(-1, ref.shape[-1]) if ref.ndim > 1 else ref[None, :]
+    grows = got.reshape(rows.shape)
+    for g, r in zip(grows, rows):
+        fin = np.isfinite(r)
+        scale = np.abs(r[fin]).max() if fin.any() else 0.0
+        np.testing.assert_allclose(g, r, rtol=rtol, atol=rtol * scale, equal_nan=True)
+
+
 def profile_functor_diag(dim, n, west=0.0, east=1.0):
     """SoA coefficients of test_integration_Cartesian_Trilinos.cpp SolveScalar(X)
     (1D :99-130, 2D :245-294, 3D :602-672): centre 2*dim, neighbours -1,

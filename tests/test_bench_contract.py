@@ -32,6 +32,8 @@ def test_reference_arm_line():
     assert line["e2e"] == {"value": line["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["iterations_per_step"] > 0
+    # the workload description is the one the GPU arm prints
+    assert set(line["config"]) == {"workload", "cells"} and line["config"]["cells"] == 24 ** 3
 
 
 def _fake_smi(tmp_path, reasons):
@@ -91,8 +93,9 @@ def test_reference_arm_under_torchrun():
         port = s.getsockname()[1]
     out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
                           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-                          "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"],
+                          "--impl", "reference", "--gpus", "2", "--cells-per-side", "16", "--steps", "1", "--warmup", "0"],
                          capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
+    assert lines[0]["config"]["cells"] == 16 ** 3
