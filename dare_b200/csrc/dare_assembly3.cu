@@ -20,8 +20,9 @@
 // Flux limiters as psi(r) * den, with r = num / den, num = phi_U - phi_UU,
 // den = phi_D - phi_U (FluxLimiter.h:41-173):
 //   van Leer  (r + |r|) / (1 + |r|) * den = 2 num den / (num + den) when num
-//             and den have the same sign, else 0 (one division instead of two;
-//             r = 0/0 -> 0 and r = +-inf -> 2 * 0 = 0 as in the r form)
+//             and den have the same sign, else 0 (one division instead of two,
+//             by Newton-Raphson, div_nr; r = 0/0 -> 0 and r = +-inf -> 2 * 0 = 0
+//             as in the r form)
 //   MINMOD    max(0, min(r, 1)) * den = |num| < |den| ? num : den when num and
 //             den have the same sign, else 0 (no division)
 //   CDS, UPWIND  den, 0
@@ -85,12 +86,36 @@ struct A3Params {
     const double* face_D[3];
 };
 
+// a / b for normal, finite b by Newton-Raphson refinement of the hardware
+// reciprocal estimate (PTX rcp.approx.ftz.f64): each step y <- y + y (1 - b y)
+// squares the relative error e of y, and the residual correction of the
+// quotient, q + y (a - b q) (Markstein's correction), squares it once more,
+// so an estimate with e <= 2^-7 already ends below 2^-56.  The result is
+// within an ulp or two of the IEEE quotient, without the IEEE division's
+// special-case branches (the assembly parity tests hold it to 1e-13 of the
+// CPU path's IEEE divisions, also on fields spanning twelve decades).  Used
+// by the van Leer limiter, where b = num + den is a sum of two same-signed
+// differences of field values.
+__device__ __forceinline__ double div_nr(double a, double b) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    double e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    const double q = a * y;
+    const double r = fma(-b, q, a);
+    return fma(r, y, q);
+}
+
 template <int LIM>
 __device__ __forceinline__ double face_flux(double a, double b, double c, double d, double v) {
     const bool vp = v >= 0.;
     const double pUU = vp ? a : d, pU = vp ? b : c, pD = vp ? c : b;
     const double num = pU - pUU, den = pD - pU;
-    const bool same = (num > 0. && den > 0.) || (num < 0. && den < 0.);
+    // num and den of the same sign (r > 0); a product below the smallest
+    // normal reads as r <= 0, which changes rr by less than that product
+    const bool same = num * den > 0.;
     if constexpr (LIM == DARE_LIMITER_CDS) {
         return (-0.5 * den) * v;
     } else if constexpr (LIM == DARE_LIMITER_UPWIND) {
@@ -100,7 +125,7 @@ __device__ __forceinline__ double face_flux(double a, double b, double c, double
         return (-0.5 * pd) * v;
     } else if constexpr (LIM == DARE_LIMITER_VANLEER) {
         // -0.5 * (2 num den / (num + den)) * v; den / (num + den) lies in (0, 1)
-        return same ? -(num * (den / (num + den))) * v : 0.;
+        return same ? -(num * div_nr(den, num + den)) * v : 0.;
     } else {
         const double psi = limiter_value(LIM, num / den);
         return ((-0.5 * psi) * den) * v;

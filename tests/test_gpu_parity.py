@@ -99,6 +99,14 @@ def _random_case(kind, seed=0):
         if kind == "tiles3d":
             c["bc"] = {3: (1, 0.5), 4: (2, 0.0), 5: (2, 0.0), 6: (1, -1.0)}
         return c
+    if kind == "range3d":
+        # phi spanning twelve decades with random signs: the limiter's
+        # divisions see operands of every magnitude
+        c = _random_case("tiles3d-periodic", seed)
+        shape = c["phi0"].shape
+        c["phi0"] = rng.choice([-1.0, 1.0], size=shape) * 10.0 ** rng.uniform(-6, 6, size=shape)
+        c["limiter"] = "VANLEER"
+        return c
     if kind.startswith("scheme3d"):
         # the Divergence time schemes on the 3-D kernel (several tiles)
         c = _random_case("tiles3d", seed)
@@ -127,7 +135,7 @@ def _random_case(kind, seed=0):
 
 
 ASM_CASES = ["diffusion3d", "tvd3d-VANLEER", "tvd3d-CDS", "tvd3d-UPWIND", "tvd3d-MINMOD", "tvd3d-VANALBADA",
-             "facediff3d", "mixed3d", "tiles3d", "tiles3d-periodic", "tvd2d", "tvd1d",
+             "facediff3d", "mixed3d", "tiles3d", "tiles3d-periodic", "range3d", "tvd2d", "tvd1d",
              "scheme3d-EULER_FORWARD", "scheme3d-CRANK_NICHOLSON", "scheme3d-ADAMS_BASHFORTH",
              "scheme3d-ADAMS_MOULTON", "scheme2d-CRANK_NICHOLSON", "scheme2d-ADAMS_MOULTON"]
 
