@@ -66,8 +66,10 @@ def parse_args(argv=None):
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
-    ap.add_argument("--learn-operators", type=int, default=8,
-                    help="128^3 operators the preconditioner is trained on (4 implicit steps each)")
+    ap.add_argument("--learn-operators", type=int, default=48,
+                    help="128^3 operators of the training distribution the preconditioner is trained on")
+    ap.add_argument("--learn-steps", type=int, default=54,
+                    help="implicit steps per training operator (each gives the plain solver's iterates as pairs)")
     return ap.parse_args(argv)
 
 
@@ -400,29 +402,33 @@ def _timed_solve(ctx, system, field, asm, fn, reps=2):
 
 
 def learned_comparison(D, ctx, system, field, asm, n, args):
-    """Time-to-1e-10 of one implicit step: plain FP64 Jacobi-BiCGStab2 against
-    the learned-preconditioned mixed-precision BiCGStab2.  The network is
-    trained here, on the GPU, on 128^3 operators of the training distribution
-    (constant or log-normal D, Pe in [1, 10], CFL 0.5), then evaluated on
-    held-out 128^3 operators and, with the same weights, on this workload."""
+    """Time-to-1e-10 of one implicit step: plain FP64 Jacobi-BiCGStab2, the
+    FP32-inner / FP64-refinement Jacobi solve, and the learned-preconditioned
+    mixed-precision BiCGStab2 with the coarse-correction network
+    N(u) = u + P U(R u).  The network is trained here, on the GPU, on the
+    plain solver's (residual, error) pairs of 128^3 operators of the training
+    distribution (constant or log-normal D, Pe in [1, 10], CFL 0.5), then
+    evaluated on held-out 128^3 operators and, with the same weights, on this
+    workload."""
     from dare_b200 import training
     out = {}
     t0 = time.perf_counter()
     m = 128
-    net128 = D.LearnedPreconditioner(ctx, (m, m, m), seed=args.seed + 1)
-    reps = training.train(net128, ctx, m, operators=args.learn_operators, steps_per_operator=4,
-                          params=net128.train_params(steps=8, batch=4), seed=args.seed + 1000)
-    out["training"] = {"grid": f"{m}^3", "operators": args.learn_operators, "implicit_steps": len(reps),
+    net128 = D.LearnedPreconditioner(ctx, (m, m, m), seed=args.seed + 1, coarse=True)
+    reps = training.train(net128, ctx, m, operators=args.learn_operators, steps_per_operator=args.learn_steps,
+                          params=net128.train_params(steps=2, batch=4, lr=3e-4), seed=args.seed + 1000)
+    out["training"] = {"grid": f"{m}^3 operators, network on {m // 2}^3 (coarse-correction form)",
+                       "operators": args.learn_operators, "implicit_steps": len(reps),
                        "pairs": sum(r["pairs_added"] for r in reps), "adam_steps": sum(r["steps"] for r in reps),
-                       "loss_first": reps[0]["loss_first"], "loss_last_mean4": float(np.mean([r["loss_last"]
-                                                                                             for r in reps[-4:]])),
+                       "loss_first": reps[0]["loss_first"],
+                       "loss_last_mean16": float(np.mean([r["loss_last"] for r in reps[-16:]])),
                        "wall_s": time.perf_counter() - t0}
     plain = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
     refine = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1},
                          precision="FP32_REFINE")
-    ident128 = D.LearnedPreconditioner(ctx, (m, m, m), seed=args.seed + 1)
+    ident128 = D.LearnedPreconditioner(ctx, (m, m, m), seed=args.seed + 1, coarse=True)
     held = []
-    for seed in (args.seed + 9001, args.seed + 9002):
+    for seed in (args.seed + 9001, args.seed + 9002, args.seed + 9003, args.seed + 9004):
         op = training.Operator(ctx, training.sample_case(m, seed, "cuda:0"))
         row = {"peclet": op.case["peclet"], "heterogeneous_D": "cell_D" in op.case}
         for name, fn in (("plain_fp64", lambda: plain.solve(op.system)),
@@ -430,17 +436,30 @@ def learned_comparison(D, ctx, system, field, asm, n, args):
                          ("learned_untrained", lambda: ident128.solve(op.system, plain)),
                          ("learned", lambda: net128.solve(op.system, plain))):
             row[name] = _timed_solve(ctx, op.system, op.field, op.asm, fn)
+        row["trained_beats_identity"] = row["learned"]["inner_iters"] < row["learned_untrained"]["inner_iters"]
         held.append(row)
         del op
     out["held_out_128"] = held
-    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=args.seed + 1)
+    out["trained_beats_identity_on_every_held_out"] = all(r["trained_beats_identity"] for r in held)
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=args.seed + 1, coarse=True)
     net.set_weights(net128.get_weights())
-    res = {"grid": f"{n}^3 (this workload, weights trained at {m}^3)"}
+    res = {"grid": f"{n}^3 (this workload; network on {n // 2}^3, weights trained with {m}^3 operators)"}
     for name, fn in (("plain_fp64", lambda: plain.solve(system)),
                      ("fp32_refine_jacobi", lambda: refine.solve(system)),
                      ("learned", lambda: net.solve(system, plain))):
         res[name] = _timed_solve(ctx, system, field, asm, fn)
     res["learned_speedup_vs_plain"] = res["plain_fp64"]["ms"] / res["learned"]["ms"]
+    res["learned_speedup_vs_fp32_refine"] = res["fp32_refine_jacobi"]["ms"] / res["learned"]["ms"]
+    # one network application at this size (CUDA events, 20 applies)
+    import torch
+    u = torch.randn(n ** 3, device="cuda", dtype=torch.float32)
+    z = torch.empty_like(u)
+    net.apply(u.data_ptr(), z.data_ptr())
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(20):
+        net.apply(u.data_ptr(), z.data_ptr())
+    res["network_apply_ms"] = ctx.timer_stop() / 20
     out["bench_workload"] = res
     out["target_3x_met"] = res["learned_speedup_vs_plain"] >= 3.0
     return out

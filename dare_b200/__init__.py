@@ -155,6 +155,8 @@ _SIGS += [
     ("dare_unet_train_params_default", None, [C.POINTER(UNetTrainParams)]),
     ("dare_learned_params_default", None, [C.POINTER(LearnedParams)]),
     ("dare_unet_create", C.c_int, [_P, C.POINTER(C.c_int), C.c_uint64, C.POINTER(_P)]),
+    ("dare_unet_create_coarse", C.c_int, [_P, C.POINTER(C.c_int), C.c_uint64, C.POINTER(_P)]),
+    ("dare_unet_system_shape", C.c_int, [_P, C.POINTER(C.c_int)]),
     ("dare_unet_destroy", C.c_int, [_P]),
     ("dare_unet_num_params", C.c_int64, [_P]),
     ("dare_unet_get_weights", C.c_int, [_P, _P, C.c_int64]),
@@ -620,24 +622,32 @@ class Batch:
 
 
 class LearnedPreconditioner:
-    """The linear conv U-Net preconditioner N(u) = u + U(u) of the Jacobi-folded
-    system (dare_unet): 8 bias-free 3x3x3 convolutions over 4 levels, BF16
-    weights, FP32 tensor-core accumulation, trained on the GPU."""
+    """The linear conv U-Net preconditioner of the Jacobi-folded system
+    (dare_unet): 8 bias-free 3x3x3 convolutions over 4 levels, BF16 weights,
+    FP32 tensor-core accumulation, trained on the GPU.  ``coarse=False``:
+    N(u) = u + U(u) on the system's grid ``n``; ``coarse=True``: the
+    coarse-correction form N(u) = u + P U(R u), the network on the 2x
+    restricted grid n / 2 (``net_shape``)."""
 
     LAYERS = (("enc0", 0, 1, 16), ("enc1", 1, 16, 32), ("enc2", 2, 32, 64), ("enc3", 3, 64, 64),
               ("dec3", 3, 64, 64), ("dec2", 2, 64, 32), ("dec1", 1, 32, 16), ("dec0", 0, 16, 1))
     ACTIVATIONS = (("S0", 0, 16), ("P1", 1, 16), ("S1", 1, 32), ("P2", 2, 32), ("S2", 2, 64), ("P3", 3, 64),
                    ("E3", 3, 64))
 
-    def __init__(self, ctx: Context, n, seed: int = 0):
+    def __init__(self, ctx: Context, n, seed: int = 0, coarse: bool = False):
         self.ctx = ctx
         self.n = tuple(int(x) for x in n)
+        self.coarse = bool(coarse)
         nn = (C.c_int * 3)(*self.n)
         h = C.c_void_p()
-        _check(lib().dare_unet_create(ctx.h, nn, C.c_uint64(seed), C.byref(h)), ctx.h, "unet_create")
+        create = lib().dare_unet_create_coarse if coarse else lib().dare_unet_create
+        _check(create(ctx.h, nn, C.c_uint64(seed), C.byref(h)), ctx.h, "unet_create")
         self.h = h
         self.num_params = int(lib().dare_unet_num_params(h))
         self.num_cells = self.n[0] * self.n[1] * self.n[2]
+        # the grid the convolutions (and the training pairs) live on
+        self.net_shape = tuple(x // 2 for x in self.n) if coarse else self.n
+        self.net_cells = int(np.prod(self.net_shape))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -667,7 +677,7 @@ class LearnedPreconditioner:
 
     def activation(self, which: int) -> np.ndarray:
         _, lev, ch = self.ACTIVATIONS[which]
-        cells = int(np.prod([x >> lev for x in self.n]))
+        cells = int(np.prod([x >> lev for x in self.net_shape]))
         a = np.empty(cells * ch, dtype=np.float32)
         _check(lib().dare_unet_read_activation(self.h, which, _ptr(a), a.size), self.ctx.h, "unet_read_activation")
         return a.reshape(cells, ch)

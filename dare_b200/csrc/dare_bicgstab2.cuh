@@ -14,6 +14,7 @@ enum : int { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXIT = 2, ST_BREAKDOWN = 3, S
 struct SolverState {
     double alpha, beta, rho0, rho1, gamma, omega1, omega2, mu, nu, tau;
     double rnorm, rnorm0, bnorm2, tol;
+    double alpha1, beta1;  // learned solve: alpha of step 7 and beta of step 11 (its flexible update)
     int k, max_it, done, status, step, tol_relative;
     unsigned int count;   // reduction arrivals (reset by the last arrival)
     unsigned int queue;   // next work item of a marching kernel

@@ -27,9 +27,10 @@
 // continues from the current iterate.  The reported residual is always the
 // FP64 ||b - A x||_2.
 //
-// One inner iteration is one CUDA graph: 4 network applications (11
+// One inner iteration is one CUDA graph: 4 network applications (13
 // tensor-core/level-transfer kernels each), 4 SpMV kernels with fused dot
-// products, 5 vector kernels.  The inner solve may stop after its first
+// products (plane-marching, dare_march.cuh), 6 vector kernels.  The FP64
+// residual of the refinement also runs in the marching engine.  The inner solve may stop after its first
 // iteration (the reference's `k > 1` rule applies to its own solve, not to
 // this inner correction).  Scalars live on the device; kernels after a
 // breakdown see `done` and skip their work.
@@ -38,7 +39,7 @@
 #include <cstring>
 #include <new>
 
-#include "dare_bicgstab2.cuh"
+#include "dare_march.cuh"
 #include "dare_unet.cuh"
 
 using namespace dare_gpu;
@@ -46,15 +47,8 @@ using namespace dare_gpu;
 namespace dare_gpu {
 namespace learned {
 
-enum : int { L_RUNNING = 0, L_CONVERGED = 1, L_MAXIT = 2, L_BREAKDOWN = 3, L_NAN = 4 };
-
-struct LState {
-    double rho0, alpha, beta, omega1, omega2, rnorm, rnorm0, tol;
-    double alpha1, beta1;  // alpha of step 7 and beta of step 11 (the flexible update)
-    int k, max_it, done, status, step;
-    unsigned int count;
-};
-
+// The solve's scalars live in a SolverState (the marching kernels' queue
+// and reduction counters are part of it); status codes ST_*.
 struct Vecs {
     float *rh, *r, *u, *v, *s, *w, *t, *d, *zu, *zr, *zv, *zs, *rin;
 };
@@ -69,8 +63,9 @@ struct dare_learned_ws {
     float* vec = nullptr;      // kNumVecs n
     double* partials = nullptr;
     double* scal = nullptr;    // [0] outer norms
-    dare_gpu::learned::LState* st = nullptr;
-    dare_gpu::learned::LState* st_host = nullptr;
+    dare_gpu::SolverState* st = nullptr;
+    dare_gpu::SolverState* st_host = nullptr;
+    dare_gpu::MarchCfg march32;   // tiles of the FP32 marching kernels
     cudaGraphExec_t graph = nullptr;
     const dare_unet* graph_net = nullptr;
     int64_t graph_kernels = 0;  // kernels in one captured iteration
@@ -94,41 +89,99 @@ namespace learned {
 #define GRID_LOOP(c, n) \
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < (n); c += (int64_t)gridDim.x * blockDim.x)
 
-__device__ __forceinline__ float ahat_apply(const GridDev& g, const float* __restrict__ ah, const float* __restrict__ z,
-                                            int64_t c) {
-    const int64_t nyz = (int64_t)g.n[1] * g.n[2];
-    const int i = (int)(c / nyz), j = (int)((c / g.n[2]) % g.n[1]), k = (int)(c % g.n[2]);
-    int64_t nb[7];
-    neighbour_ordinals(g, i, j, k, c, nb);
-    float v = z[c];
-#pragma unroll
-    for (int q = 0; q < 6; q++) v += ah[q * g.ncell + c] * z[nb[q + 1]];
-    return v;
-}
-
-// FP64 r = b - A x -> FP32 rin; ||r||_2 -> *out
-__global__ void __launch_bounds__(256) k_residual(GridDev g, const double* __restrict__ diag,
-                                                  const double* __restrict__ b, const double* __restrict__ x,
-                                                  float* __restrict__ rin, LState* st, double* partials, double* out) {
-    const int64_t n = g.ncell, nyz = (int64_t)g.n[1] * g.n[2];
-    double acc[1] = {0.};
-    GRID_LOOP(c, n) {
-        const int i = (int)(c / nyz), j = (int)((c / g.n[2]) % g.n[1]), k = (int)(c % g.n[2]);
-        int64_t nb[7];
-        neighbour_ordinals(g, i, j, k, c, nb);
-        double ax = 0.;
-#pragma unroll
-        for (int q = 0; q < 7; q++) ax += diag[q * n + c] * x[nb[q]];
-        const double r = b[c] - ax;
+// r = b - A x with the assembled FP64 operator, stored as FP32 for the inner
+// solve, and ||r||_2 -> *out
+struct FLResidual {
+    using type = double;
+    static constexpr int Q = 1, NZ = 1, NP = 8;
+    static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;
+    const double* zs[2];   // x
+    const double* ps[NP];  // 7 coefficients, b
+    float* rin;
+    double* out;
+    __device__ void load(const SolverState*) {}
+    __device__ double zc(double a, double) const { return a; }
+    __device__ void center(int64_t c, const double (&zz)[7], const double* p, double* acc) const {
+        const double r = p[7] - apply_pre<double, false>(p, zz);
         rin[c] = (float)r;
         acc[0] += r * r;
     }
-    double tot[1];
-    if (!grid_reduce<1>(acc, partials, &st->count, tot)) return;
-    if (threadIdx.x == 0) *out = sqrt(tot[0]);
+    __device__ void done(SolverState*, const double* tot) const { *out = sqrt(tot[0]); }
+};
+
+__device__ __forceinline__ void fail(SolverState* st, int step) {
+    st->done = 1;
+    st->status = ST_BREAKDOWN;
+    st->step = step;
 }
 
-__global__ void __launch_bounds__(256) k_bnorm(int64_t n, const double* __restrict__ b, LState* st, double* partials,
+// out = Ahat z for a network output z, with <out, r_hat_0>.  MODE 0 (steps
+// 6-7 and 13-14): gamma -> alpha = rho0 / gamma; MODE 1 (steps 9-11):
+// rho1 -> beta = alpha rho1 / rho0.
+template <int MODE, int STEP>
+struct FLSpmvDot {
+    using type = float;
+    static constexpr int Q = 1, NZ = 1, NC = 6, NP = 7;
+    static constexpr bool kCheckDone = true;
+    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
+    const float* zs[2];   // z
+    const float* ps[NP];  // 6 folded off-diagonals, r_hat_0
+    float* out;
+    __device__ void load(const SolverState*) {}
+    __device__ float zc(float a, float) const { return a; }
+    __device__ void center(int64_t c, const float (&zz)[7], const float* p, double* acc) const {
+        const float v = apply_pre<float, true>(p, zz);
+        out[c] = v;
+        acc[0] += (double)v * (double)p[NC];
+    }
+    __device__ void done(SolverState* st, const double* tot) const {
+        if (MODE == 0) {
+            if (tot[0] == 0.) return fail(st, STEP);
+            st->alpha = st->rho0 / tot[0];
+            if (STEP == 7) st->alpha1 = st->alpha;
+        } else {
+            st->beta = st->alpha * tot[0] / st->rho0;
+            st->beta1 = st->beta;
+            st->rho0 = tot[0];
+        }
+    }
+};
+
+// (18)-(23): t = Ahat zs; <r,s>, <s,s>, <s,t>, <t,t>, <r,t>; omega1, omega2
+struct FLSpmvOmega {
+    using type = float;
+    static constexpr int Q = 5, NZ = 1, NC = 6, NP = 8;
+    static constexpr bool kCheckDone = true;
+    static constexpr bool kPairs = false;
+    const float* zs[2];   // zs
+    const float* ps[NP];  // 6 folded off-diagonals, r, s
+    float* t;
+    __device__ void load(const SolverState*) {}
+    __device__ float zc(float a, float) const { return a; }
+    __device__ void center(int64_t c, const float (&zz)[7], const float* p, double* acc) const {
+        const float tv = apply_pre<float, true>(p, zz);
+        t[c] = tv;
+        const double r = p[NC], s = p[NC + 1], td = tv;
+        acc[0] += r * s;
+        acc[1] += s * s;
+        acc[2] += s * td;
+        acc[3] += td * td;
+        acc[4] += r * td;
+    }
+    __device__ void done(SolverState* st, const double* tot) const {
+        double om1 = tot[0], mu = tot[1], nu = tot[2], tau = tot[3], om2 = tot[4];
+        if (mu == 0.) return fail(st, 20);
+        tau -= nu * nu / mu;
+        if (tau == 0.) return fail(st, 21);
+        om2 = (om2 - nu * om1 / mu) / tau;
+        om1 = (om1 - nu * om2) / mu;
+        st->omega1 = om1;
+        st->omega2 = om2;
+    }
+};
+
+__global__ void __launch_bounds__(256) k_bnorm(int64_t n, const double* __restrict__ b, SolverState* st, double* partials,
                                                double* out) {
     double acc[1] = {0.};
     GRID_LOOP(c, n) acc[0] += b[c] * b[c];
@@ -142,7 +195,7 @@ __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, in
 }
 
 // start of an inner solve: r = rh = rin, u = v = w = d = 0
-__global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, LState* st, double* partials, double rel_tol,
+__global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, SolverState* st, double* partials, double rel_tol,
                                               int max_it) {
     double acc[1] = {0.};
     GRID_LOOP(c, n) {
@@ -166,25 +219,19 @@ __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, LState* st, do
         st->beta = 0.;
         st->k = 1;
         st->max_it = max_it;
-        st->status = L_RUNNING;
+        st->status = ST_RUNNING;
         st->step = 0;
         st->done = (st->rnorm0 == 0.) ? 1 : 0;
-        if (st->done) st->status = L_CONVERGED;
+        if (st->done) st->status = ST_CONVERGED;
         if (!(st->rnorm0 == st->rnorm0)) {
             st->done = 1;
-            st->status = L_NAN;
+            st->status = ST_NAN;
         }
     }
 }
 
-__device__ __forceinline__ void fail(LState* st, int step) {
-    st->done = 1;
-    st->status = L_BREAKDOWN;
-    st->step = step;
-}
-
 // (3), (4): rho1 = <rh, r>, beta
-__global__ void __launch_bounds__(256) k_rho(int64_t n, Vecs vs, LState* st, double* partials) {
+__global__ void __launch_bounds__(256) k_rho(int64_t n, Vecs vs, SolverState* st, double* partials) {
     if (st->done) return;
     double acc[1] = {0.};
     GRID_LOOP(c, n) acc[0] += (double)vs.rh[c] * vs.r[c];
@@ -201,55 +248,28 @@ __global__ void __launch_bounds__(256) k_rho(int64_t n, Vecs vs, LState* st, dou
 }
 
 // (5) u = r - beta u
-__global__ void k_upd_u(int64_t n, Vecs vs, const LState* st) {
+__global__ void k_upd_u(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float beta = (float)st->beta;
     GRID_LOOP(c, n) vs.u[c] = vs.r[c] - beta * vs.u[c];
 }
 
-// out = Ahat z with <out, rh> (mode 0: gamma -> alpha, steps 7 and 14;
-// mode 1: rho1 -> beta, step 11)
-__global__ void __launch_bounds__(256) k_spmv_dot(GridDev g, const float* __restrict__ ah, Vecs vs,
-                                                  const float* __restrict__ z, float* out, LState* st,
-                                                  double* partials, int mode, int step) {
-    if (st->done) return;
-    double acc[1] = {0.};
-    GRID_LOOP(c, g.ncell) {
-        const float v = ahat_apply(g, ah, z, c);
-        out[c] = v;
-        acc[0] += (double)v * vs.rh[c];
-    }
-    double tot[1];
-    if (!grid_reduce<1>(acc, partials, &st->count, tot)) return;
-    if (threadIdx.x == 0) {
-        if (mode == 0) {
-            if (tot[0] == 0.) return fail(st, step);
-            st->alpha = st->rho0 / tot[0];
-            if (step == 7) st->alpha1 = st->alpha;
-        } else {
-            st->beta = st->alpha * tot[0] / st->rho0;
-            st->beta1 = st->beta;
-            st->rho0 = tot[0];
-        }
-    }
-}
-
 // (8): r -= alpha v (the matching x update is folded into k_upd_final)
-__global__ void k_upd_r(int64_t n, Vecs vs, const LState* st) {
+__global__ void k_upd_r(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float alpha = (float)st->alpha;
     GRID_LOOP(c, n) vs.r[c] -= alpha * vs.v[c];
 }
 
 // (12) v = s - beta v
-__global__ void k_upd_v(int64_t n, Vecs vs, const LState* st) {
+__global__ void k_upd_v(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float beta = (float)st->beta;
     GRID_LOOP(c, n) vs.v[c] = vs.s[c] - beta * vs.v[c];
 }
 
 // (15)-(17)
-__global__ void k_upd3(int64_t n, Vecs vs, const LState* st) {
+__global__ void k_upd3(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float alpha = (float)st->alpha, beta = (float)st->beta;
     GRID_LOOP(c, n) {
@@ -260,38 +280,9 @@ __global__ void k_upd3(int64_t n, Vecs vs, const LState* st) {
     }
 }
 
-// (18)-(23): t = Ahat z, the five inner products and the omegas
-__global__ void __launch_bounds__(256) k_spmv_omega(GridDev g, const float* __restrict__ ah, Vecs vs, LState* st,
-                                                    double* partials) {
-    if (st->done) return;
-    double acc[5] = {0., 0., 0., 0., 0.};
-    GRID_LOOP(c, g.ncell) {
-        const float t = ahat_apply(g, ah, vs.zs, c);
-        vs.t[c] = t;
-        const double r = vs.r[c], s = vs.s[c];
-        acc[0] += r * s;
-        acc[1] += s * s;
-        acc[2] += s * t;
-        acc[3] += (double)t * t;
-        acc[4] += r * t;
-    }
-    double tot[5];
-    if (!grid_reduce<5>(acc, partials, &st->count, tot)) return;
-    if (threadIdx.x == 0) {
-        double om1 = tot[0], mu = tot[1], nu = tot[2], tau = tot[3], om2 = tot[4];
-        if (mu == 0.) return fail(st, 20);
-        tau -= nu * nu / mu;
-        if (tau == 0.) return fail(st, 21);
-        om2 = (om2 - nu * om1 / mu) / tau;
-        om1 = (om1 - nu * om2) / mu;
-        st->omega1 = om1;
-        st->omega2 = om2;
-    }
-}
-
 // (10), (24) in flexible form: d += (a1 - a2 b1) zu + (a2 + w1) zr - w1 a2 zv + w2 zs;
 // (25): r -= w1 s + w2 t; u -= w1 v + w2 w; convergence test on ||r||
-__global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, LState* st, double* partials) {
+__global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, SolverState* st, double* partials) {
     if (st->done) return;
     const double a1 = st->alpha1, a2 = st->alpha, b1 = st->beta1, om1 = st->omega1, om2 = st->omega2;
     const float cu = (float)(a1 - a2 * b1), cr = (float)(a2 + om1), cv = (float)(-om1 * a2), cs = (float)om2;
@@ -312,13 +303,13 @@ __global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, LState* s
         st->rnorm = rn;
         if (!(rn == rn)) {
             st->done = 1;
-            st->status = L_NAN;
+            st->status = ST_NAN;
         } else if (rn <= st->tol) {
             st->done = 1;
-            st->status = L_CONVERGED;
+            st->status = ST_CONVERGED;
         } else if (++st->k > st->max_it) {
             st->done = 1;
-            st->status = L_MAXIT;
+            st->status = ST_MAXIT;
         }
     }
 }
@@ -333,34 +324,43 @@ __global__ void k_to_precond_var(int64_t n, const double* __restrict__ dc, doubl
     GRID_LOOP(c, n) x[c] = dc[c] * x[c];
 }
 
-static int launch_iteration(dare_ctx* ctx, dare_unet* net, const GridDev& g, const float* ah, const Vecs& vs,
-                            LState* st, double* partials) {
+static int launch_iteration(dare_ctx* ctx, dare_unet* net, const GridDev& g, const MarchCfg& m, const float* ah,
+                            const Vecs& vs, SolverState* st, double* partials) {
     const int64_t n = g.ncell;
     const int eb = grid_blocks(ctx, n, 256, 8);
     cudaStream_t s = ctx->stream;
     int rc;
+    auto spmv_dot = [&](auto f, const float* z, float* out) {
+        f.zs[0] = z;
+        for (int q = 0; q < 6; q++) f.ps[q] = ah + (size_t)q * n;
+        f.ps[6] = vs.rh;
+        f.out = out;
+        return launch_march(ctx, g, m, f, st, partials);
+    };
     k_rho<<<eb, 256, 0, s>>>(n, vs, st, partials);
     DARE_LAUNCHED(ctx);
     k_upd_u<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
     if ((rc = unet::apply(net, vs.u, vs.zu))) return rc;
-    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.zu, vs.v, st, partials, 0, 7);
-    DARE_LAUNCHED(ctx);
+    if ((rc = spmv_dot(FLSpmvDot<0, 7>{}, vs.zu, vs.v))) return rc;
     k_upd_r<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
     if ((rc = unet::apply(net, vs.r, vs.zr))) return rc;
-    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.zr, vs.s, st, partials, 1, 11);
-    DARE_LAUNCHED(ctx);
+    if ((rc = spmv_dot(FLSpmvDot<1, 11>{}, vs.zr, vs.s))) return rc;
     k_upd_v<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
     if ((rc = unet::apply(net, vs.v, vs.zv))) return rc;
-    k_spmv_dot<<<eb, 256, 0, s>>>(g, ah, vs, vs.zv, vs.w, st, partials, 0, 14);
-    DARE_LAUNCHED(ctx);
+    if ((rc = spmv_dot(FLSpmvDot<0, 14>{}, vs.zv, vs.w))) return rc;
     k_upd3<<<eb, 256, 0, s>>>(n, vs, st);
     DARE_LAUNCHED(ctx);
     if ((rc = unet::apply(net, vs.s, vs.zs))) return rc;
-    k_spmv_omega<<<eb, 256, 0, s>>>(g, ah, vs, st, partials);
-    DARE_LAUNCHED(ctx);
+    FLSpmvOmega fo{};
+    fo.zs[0] = vs.zs;
+    for (int q = 0; q < 6; q++) fo.ps[q] = ah + (size_t)q * n;
+    fo.ps[6] = vs.r;
+    fo.ps[7] = vs.s;
+    fo.t = vs.t;
+    if ((rc = launch_march(ctx, g, m, fo, st, partials))) return rc;
     k_upd_final<<<eb, 256, 0, s>>>(n, vs, st, partials);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
@@ -392,7 +392,8 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     if (net->ctx != ctx) return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: network on another context");
     if (s->ncomp != 1)
         return set_error(ctx, DARE_ERR_UNSUPPORTED, "bicgstab2_learned: the network preconditions one field component");
-    if (g.dim != 3 || g.n[0] != net->n[0] || g.n[1] != net->n[1] || g.n[2] != net->n[2])
+    const int* sys_n = net->coarse ? net->fine : net->n;
+    if (g.dim != 3 || g.n[0] != sys_n[0] || g.n[1] != sys_n[1] || g.n[2] != sys_n[2])
         return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: grid does not match the network");
     if (lp->iteration_budget < 1 || lp->inner_max_it < 1 || !(lp->inner_rel_tol > 0.))
         return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: bad learned parameters");
@@ -409,13 +410,14 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         if (e == cudaSuccess) e = cudaMalloc(&lw->vec, (size_t)n * kNumVecs * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&lw->partials, (size_t)kMaxQ * kMaxBlocks * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&lw->scal, 4 * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&lw->st, sizeof(LState));
-        if (e == cudaSuccess) e = cudaMemset(lw->st, 0, sizeof(LState));
-        if (e == cudaSuccess) e = cudaMallocHost(&lw->st_host, sizeof(LState));
+        if (e == cudaSuccess) e = cudaMalloc(&lw->st, sizeof(SolverState));
+        if (e == cudaSuccess) e = cudaMemset(lw->st, 0, sizeof(SolverState));
+        if (e == cudaSuccess) e = cudaMallocHost(&lw->st_host, sizeof(SolverState));
         if (e != cudaSuccess) {
             dare_learned_ws_free(lw);
             return check_cuda(ctx, e, "bicgstab2_learned workspace");
         }
+        lw->march32 = march_config(ctx, g, sizeof(float));
         ws->learned = lw;
     }
     dare_learned_ws* lw = ws->learned;
@@ -430,7 +432,7 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     if ((rc = launch_fold(ctx, g, ws->march, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
     k_to_f32<<<eb, 256, 0, ctx->stream>>>(ws->ahat, lw->ahat32, 6 * n);
     DARE_LAUNCHED(ctx);
-    DARE_CUDA(ctx, cudaMemsetAsync(lw->st, 0, sizeof(LState), ctx->stream));
+    DARE_CUDA(ctx, cudaMemsetAsync(lw->st, 0, sizeof(SolverState), ctx->stream));
     k_bnorm<<<eb, 256, 0, ctx->stream>>>(n, s->rhs, lw->st, lw->partials, lw->scal);
     DARE_LAUNCHED(ctx);
     double bnorm = 0.;
@@ -446,7 +448,7 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         cudaGraph_t graph = nullptr;
         DARE_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         const int64_t before = ctx->launches;
-        rc = launch_iteration(ctx, net, g, lw->ahat32, vs, lw->st, lw->partials);
+        rc = launch_iteration(ctx, net, g, lw->march32, lw->ahat32, vs, lw->st, lw->partials);
         lw->graph_kernels = ctx->launches - before;
         ctx->launches = before;
         cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
@@ -468,8 +470,13 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     bool converged = false;
     int refinements = 0, inner_total = 0;
     for (int it = 0;; it++) {
-        k_residual<<<eb, 256, 0, ctx->stream>>>(g, s->diag, s->rhs, s->x, vs.rin, lw->st, lw->partials, lw->scal);
-        DARE_LAUNCHED(ctx);
+        FLResidual fr{};
+        fr.zs[0] = s->x;
+        set_coef_streams<double, false, 8>(OpT<double>{s->diag, s->diag + n, n}, fr.ps);   // W..T, then C
+        fr.ps[7] = s->rhs;
+        fr.rin = vs.rin;
+        fr.out = lw->scal;
+        if ((rc = launch_march(ctx, g, ws->march, fr, lw->st, lw->partials))) return rc;
         if ((rc = read_scalar(ctx, lw->scal, &rnorm))) return rc;
         if (rnorm <= tol_abs) {
             converged = true;
@@ -483,15 +490,15 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         for (int j = 0; j < cap; j++) {
             DARE_CUDA(ctx, cudaGraphLaunch(lw->graph, ctx->stream));
             ctx->launches += lw->graph_kernels;
-            DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(LState), cudaMemcpyDeviceToHost, ctx->stream));
+            DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
             DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
             if (lw->st_host->done) break;
         }
-        DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(LState), cudaMemcpyDeviceToHost, ctx->stream));
+        DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
         DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        const LState st = *lw->st_host;
+        const SolverState st = *lw->st_host;
         inner_total += std::min(st.k, cap);
-        if (st.status == L_NAN) break;
+        if (st.status == ST_NAN) break;
         // x += D^-1 d
         k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, vs.d, s->x);
         DARE_LAUNCHED(ctx);

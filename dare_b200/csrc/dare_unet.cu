@@ -1416,6 +1416,52 @@ __global__ void k_warm(int64_t n, const double* __restrict__ diag, const double*
 }
 
 // ---------------------------------------------------------------------------
+// coarse-correction form: level transfers between the system's grid (2 c0,
+// 2 c1, 2 c2) and the network's grid (c0, c1, c2), FP32, cell layout.
+// uc = R u: the mean of the 8 children.  A thread makes two neighbouring
+// coarse cells (K = 2 K2, 2 K2 + 1) from four 16-byte loads of fine rows
+// (the coarse sizes are multiples of 8, so rows split into whole pairs).
+__global__ void __launch_bounds__(256) k_pool8(int c0, int c1, int c2, const float* __restrict__ f,
+                                               float* __restrict__ c) {
+    const int h2 = c2 / 2;
+    const int64_t nq = (int64_t)c0 * c1 * h2;
+    const int64_t F2 = 2 * (int64_t)c2, F1 = 2 * (int64_t)c1;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nq; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t K2 = q % h2, JI = q / h2, J = JI % c1, I = JI / c1;
+        float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const float4 v = *reinterpret_cast<const float4*>(f + ((2 * I + a) * F1 + 2 * J + b) * F2 + 4 * K2);
+                s0 += v.x + v.y;
+                s1 += v.z + v.w;
+            }
+        *reinterpret_cast<float2*>(c + JI * c2 + 2 * K2) = make_float2(0.125f * s0, 0.125f * s1);
+    }
+}
+
+// z = u + P (zc - uc): every fine cell adds its parent's network correction;
+// a thread handles four fine cells along k (two parents) with 16-byte
+// accesses
+__global__ void __launch_bounds__(256) k_coarse_add(int c0, int c1, int c2, const float* __restrict__ u,
+                                                    const float* __restrict__ zc, const float* __restrict__ uc,
+                                                    float* __restrict__ z) {
+    const int h2 = c2 / 2;
+    const int64_t F2 = 2 * (int64_t)c2, F1 = 2 * (int64_t)c1;
+    const int64_t nq = (int64_t)2 * c0 * F1 * h2;   // fine cells / 4
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nq; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t K2 = q % h2, row = q / h2;          // row = fine (i, j)
+        const int64_t j = row % F1, i = row / F1;
+        const int64_t p = ((i >> 1) * c1 + (j >> 1)) * c2 + 2 * K2;
+        const float2 zz = *reinterpret_cast<const float2*>(zc + p), uu = *reinterpret_cast<const float2*>(uc + p);
+        const float d0 = zz.x - uu.x, d1 = zz.y - uu.y;
+        const float4 v = *reinterpret_cast<const float4*>(u + row * F2 + 4 * K2);
+        *reinterpret_cast<float4*>(z + row * F2 + 4 * K2) = make_float4(v.x + d0, v.y + d0, v.z + d1, v.w + d1);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host side: launch configuration and dispatch
 static size_t fwd_smem(int cin, int nt, const Geom& g, int mt, int slots) {
     const int RP = round8(strip_rows(g, mt));
@@ -1882,7 +1928,8 @@ static int prolong_add(dare_unet* net, int fl, const bf16* coarse, bf16* fine, f
     return DARE_OK;
 }
 
-int apply(dare_unet* net, const float* u, float* z) {
+// z = u + U(u) on the network's own grid
+static int apply_grid(dare_unet* net, const float* u, float* z) {
     int rc;
     // enc0 also writes P1, the average pool of S0
     if ((rc = conv_forward(net, ENC0, nullptr, u, OUT_STORE, net->S0, nullptr, nullptr, nullptr))) return rc;
@@ -1899,6 +1946,36 @@ int apply(dare_unet* net, const float* u, float* z) {
     if ((rc = conv_forward(net, DEC1, net->S1, nullptr, OUT_STORE, net->dD1, nullptr, nullptr, nullptr))) return rc;
     if ((rc = prolong_add<16>(net, 0, net->dD1, net->S0, 1.f))) return rc;
     return conv_forward(net, DEC0, net->S0, nullptr, OUT_F32, nullptr, nullptr, z, u);
+}
+
+int apply(dare_unet* net, const float* u, float* z) {
+    if (!net->coarse) return apply_grid(net, u, z);
+    // coarse form: z = u + P (N_c(R u) - R u), N_c(v) = v + U(v) on the coarse grid
+    dare_ctx* ctx = net->ctx;
+    float* uc = net->cbuf;
+    float* zc = net->cbuf + net->ncell;
+    // (16-byte accesses: u and z must be 16-byte aligned; an unaligned
+    // caller vector is copied first)
+    const float* uin = u;
+    float* zout = z;
+    if ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(z)) & 15) {
+        if (!net->fbuf) DARE_CUDA(ctx, cudaMalloc(&net->fbuf, (size_t)2 * net->fine_ncell * sizeof(float)));
+        DARE_CUDA(ctx, cudaMemcpyAsync(net->fbuf, u, net->fine_ncell * sizeof(float), cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+        uin = net->fbuf;
+        zout = net->fbuf + net->fine_ncell;
+    }
+    k_pool8<<<eblocks(ctx, net->ncell / 2), 256, 0, ctx->stream>>>(net->n[0], net->n[1], net->n[2], uin, uc);
+    DARE_LAUNCHED(ctx);
+    int rc = apply_grid(net, uc, zc);
+    if (rc) return rc;
+    k_coarse_add<<<eblocks(ctx, net->fine_ncell / 4), 256, 0, ctx->stream>>>(net->n[0], net->n[1], net->n[2], uin, zc,
+                                                                              uc, zout);
+    DARE_LAUNCHED(ctx);
+    if (zout != z)
+        DARE_CUDA(ctx, cudaMemcpyAsync(z, zout, net->fine_ncell * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
 }
 
 // Backward pass of the last apply() for input u and output gradient g;
@@ -1969,7 +2046,7 @@ static int loss_grad(dare_unet* net, const float* const* r, const float* const* 
     DARE_CUDA(ctx, cudaMemsetAsync(net->dscal, 0, sizeof(double), ctx->stream));
     const float scale = 1.f / (float)count;
     for (int b = 0; b < count; b++) {
-        if ((rc = apply(net, r[b], net->z))) return rc;
+        if ((rc = apply_grid(net, r[b], net->z))) return rc;   // pairs live on the network's grid
         k_loss_grad<<<eblocks(ctx, net->ncell), 256, 0, ctx->stream>>>(net->ncell, net->z, e[b], en2[b], scale,
                                                                        net->g, net->dscal);
         DARE_LAUNCHED(ctx);
@@ -2047,6 +2124,8 @@ static void unet_free(dare_unet* net) {
     cudaFree(net->ring_e);
     cudaFree(net->ring_en);
     cudaFree(net->sol);
+    cudaFree(net->cbuf);
+    cudaFree(net->fbuf);
 }
 
 int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** out) {
@@ -2157,6 +2236,37 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     }
     *out = net;
     return DARE_OK;
+}
+
+int dare_unet_create_coarse(dare_ctx* ctx, const int n_fine[3], uint64_t seed, dare_unet** out) {
+    if (!ctx || !n_fine || !out) return DARE_ERR_BAD_ARG;
+    *out = nullptr;
+    int nc[3];
+    for (int d = 0; d < 3; d++) {
+        if (n_fine[d] < 16 || n_fine[d] % 16 != 0)
+            return set_error(ctx, DARE_ERR_BAD_ARG,
+                             "dare_unet_create_coarse: every grid size must be a positive multiple of 16");
+        nc[d] = n_fine[d] / 2;
+    }
+    dare_unet* net = nullptr;
+    int rc = dare_unet_create(ctx, nc, seed, &net);
+    if (rc) return rc;
+    net->coarse = 1;
+    for (int d = 0; d < 3; d++) net->fine[d] = n_fine[d];
+    net->fine_ncell = (int64_t)n_fine[0] * n_fine[1] * n_fine[2];
+    cudaError_t e = cudaMalloc(&net->cbuf, (size_t)net->ncell * 2 * sizeof(float));
+    if (e != cudaSuccess) {
+        dare_unet_destroy(net);
+        return check_cuda(ctx, e, "dare_unet_create_coarse");
+    }
+    *out = net;
+    return DARE_OK;
+}
+
+int dare_unet_system_shape(const dare_unet* net, int n[3]) {
+    if (!net || !n) return DARE_ERR_BAD_ARG;
+    for (int d = 0; d < 3; d++) n[d] = net->coarse ? net->fine[d] : net->n[d];
+    return net->coarse;
 }
 
 int dare_unet_destroy(dare_unet* net) {
@@ -2276,28 +2386,32 @@ int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const 
     if (!net || !s || !p || !rep || p->batch < 1 || p->steps < 0) return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = net->ctx;
     const GridDev& g = s->grid->dev;
-    if (g.dim != 3 || g.n[0] != net->n[0] || g.n[1] != net->n[1] || g.n[2] != net->n[2])
+    const int* sys_n = net->coarse ? net->fine : net->n;
+    if (g.dim != 3 || g.n[0] != sys_n[0] || g.n[1] != sys_n[1] || g.n[2] != sys_n[2])
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_unet_train_on_system: grid does not match the network");
     if (s->ncomp != 1)
         return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_unet_train_on_system: one field component only");
     cudaSetDevice(ctx->device);
     std::memset(rep, 0, sizeof(*rep));
-    const int64_t n = net->ncell;
+    const int64_t n = net->ncell;                           // pairs in the ring: the network's grid
+    const int64_t nf = net->coarse ? net->fine_ncell : n;   // the system's grid
     if (!net->ring_r) {
-        // ring of pairs: up to 256, at most ~4 GB
+        // ring of pairs: up to 256 (2048 for the coarse form), at most ~4 GB
         const size_t pair_bytes = (size_t)n * 2 * sizeof(float);
-        int cap = (int)std::min<size_t>(256, std::max<size_t>(8, ((size_t)4 << 30) / pair_bytes));
+        const size_t most = net->coarse ? 2048 : 256;
+        int cap = (int)std::min<size_t>(most, std::max<size_t>(8, ((size_t)4 << 30) / pair_bytes));
         cudaError_t e = cudaMalloc(&net->ring_r, (size_t)cap * n * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&net->ring_e, (size_t)cap * n * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&net->ring_en, (size_t)cap * sizeof(float));
-        if (e == cudaSuccess) e = cudaMalloc(&net->sol, (size_t)2 * n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&net->sol, (size_t)2 * nf * sizeof(double));
+        if (e == cudaSuccess && net->coarse) e = cudaMalloc(&net->fbuf, (size_t)2 * nf * sizeof(float));
         if (e != cudaSuccess) return check_cuda(ctx, e, "dare_unet_train_on_system");
         net->ring_cap = cap;
     }
     double* x0 = net->sol;
-    double* xs = net->sol + n;
-    const int eb = eblocks(ctx, n);
-    DARE_CUDA(ctx, cudaMemcpyAsync(x0, s->x, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    double* xs = net->sol + nf;
+    const int eb = eblocks(ctx, nf);
+    DARE_CUDA(ctx, cudaMemcpyAsync(x0, s->x, nf * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
 
     // the plain solve to the tolerance, warm-started at x0
     dare_solver_params sp;
@@ -2307,14 +2421,16 @@ int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const 
     sp.max_it = 1000;
     sp.compute_true_residual = 0;
     dare_solve_report sr;
-    k_warm<<<eb, 256, 0, ctx->stream>>>(n, s->diag, x0, s->x);
+    k_warm<<<eb, 256, 0, ctx->stream>>>(nf, s->diag, x0, s->x);
     DARE_LAUNCHED(ctx);
     int rc = dare_bicgstab2_fp64(s, &sp, &sr);
     if (rc) return rc;
     rep->plain_iters = sr.iters;
-    DARE_CUDA(ctx, cudaMemcpyAsync(xs, s->x, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    DARE_CUDA(ctx, cudaMemcpyAsync(xs, s->x, nf * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
 
-    // its iterates x_k, k = 0 .. K-1, as pairs
+    // its iterates x_k, k = 0 .. K-1, as pairs; the coarse form keeps their
+    // restrictions (the fine loss ||r + P U(R r) - e||^2 is 8 ||R r + U(R r)
+    // - R e||^2 plus a term without U, for the average R and the nearest P)
     const int K = std::min(std::max(sr.iters, 1), p->max_pairs_per_rhs);
     for (int k = 0; k < K; k++) {
         const double* xk = x0;
@@ -2323,17 +2439,28 @@ int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const 
             q.tol = 0.;
             q.tol_relative = 0;
             q.max_it = k;
-            k_warm<<<eb, 256, 0, ctx->stream>>>(n, s->diag, x0, s->x);
+            k_warm<<<eb, 256, 0, ctx->stream>>>(nf, s->diag, x0, s->x);
             DARE_LAUNCHED(ctx);
             dare_solve_report qr;
             if ((rc = dare_bicgstab2_fp64(s, &q, &qr))) return rc;
             xk = s->x;
         }
         const int slot = net->ring_next;
+        float* rs = net->ring_r + (size_t)slot * n;
+        float* es = net->ring_e + (size_t)slot * n;
         DARE_CUDA(ctx, cudaMemsetAsync(net->dscal + 2, 0, sizeof(double), ctx->stream));
-        k_make_pair<<<eb, 256, 0, ctx->stream>>>(g, s->diag, s->rhs, xk, xs, net->ring_r + (size_t)slot * n,
-                                                 net->ring_e + (size_t)slot * n, net->dscal + 2);
+        k_make_pair<<<eb, 256, 0, ctx->stream>>>(g, s->diag, s->rhs, xk, xs, net->coarse ? net->fbuf : rs,
+                                                 net->coarse ? net->fbuf + nf : es, net->dscal + 2);
         DARE_LAUNCHED(ctx);
+        if (net->coarse) {
+            k_pool8<<<eblocks(ctx, n / 2), 256, 0, ctx->stream>>>(net->n[0], net->n[1], net->n[2], net->fbuf, rs);
+            DARE_LAUNCHED(ctx);
+            k_pool8<<<eblocks(ctx, n / 2), 256, 0, ctx->stream>>>(net->n[0], net->n[1], net->n[2], net->fbuf + nf, es);
+            DARE_LAUNCHED(ctx);
+            DARE_CUDA(ctx, cudaMemsetAsync(net->dscal + 2, 0, sizeof(double), ctx->stream));
+            k_sqnorm<<<eblocks(ctx, n), 256, 0, ctx->stream>>>(n, es, net->dscal + 2);
+            DARE_LAUNCHED(ctx);
+        }
         k_store_norm<<<1, 1, 0, ctx->stream>>>(net->dscal + 2, net->ring_en + slot);
         DARE_LAUNCHED(ctx);
         net->ring_next = (net->ring_next + 1) % net->ring_cap;
@@ -2341,7 +2468,7 @@ int dare_unet_train_on_system(dare_unet* net, dare_system* s, double tol, const 
         rep->pairs_added++;
         net->pairs_seen++;
     }
-    DARE_CUDA(ctx, cudaMemcpyAsync(s->x, xs, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    DARE_CUDA(ctx, cudaMemcpyAsync(s->x, xs, nf * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
 
     // optimiser steps on minibatches drawn from the ring
     std::mt19937_64 rng(p->seed ^ net->rng);

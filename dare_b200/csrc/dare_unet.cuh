@@ -114,8 +114,17 @@ struct Layer {
 
 struct dare_unet {
     dare_ctx* ctx = nullptr;
-    int n[3] = {0, 0, 0};
+    int n[3] = {0, 0, 0};      // the grid the convolutions run on
     int64_t ncell = 0;
+    // Coarse-correction form: the network acts on the 2x restricted grid of
+    // the system's grid `fine`, N(u) = u + P (U(R u)) with R the average of
+    // the 8 children and P the nearest prolongation (no full-resolution
+    // convolution); 0 for the full-resolution form N(u) = u + U(u).
+    int coarse = 0;
+    int fine[3] = {0, 0, 0};
+    int64_t fine_ncell = 0;
+    float* cbuf = nullptr;     // coarse form: R u and the network's output (2 ncell)
+    float* fbuf = nullptr;     // coarse form: a fine (residual, error) pair before restriction (2 fine_ncell)
     dare_gpu::unet::Geom geo[dare_gpu::unet::kLevels];
     dare_gpu::unet::Layer layer[dare_gpu::unet::kLayers];
     int64_t nparam = 0;
@@ -168,6 +177,7 @@ struct dare_unet {
 namespace dare_gpu {
 namespace unet {
 // z = N(u) on the context's stream (no synchronisation); used by the solver.
+// u and z live on the system's grid (the fine grid of a coarse-form network).
 int apply(dare_unet* net, const float* u, float* z);
 }  // namespace unet
 }  // namespace dare_gpu

