@@ -66,9 +66,9 @@ def parse_args(argv=None):
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
-    ap.add_argument("--learn-operators", type=int, default=48,
+    ap.add_argument("--learn-operators", type=int, default=64,
                     help="128^3 operators of the training distribution the preconditioner is trained on")
-    ap.add_argument("--learn-steps", type=int, default=54,
+    ap.add_argument("--learn-steps", type=int, default=76,
                     help="implicit steps per training operator (each gives the plain solver's iterates as pairs)")
     return ap.parse_args(argv)
 

@@ -245,6 +245,19 @@ int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double
     return launch_march(ctx, g, m, f, st, partials);
 }
 
+int launch_fold32(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, float* ahat32,
+                  SolverState* st, double* partials) {
+    const int eb = grid_blocks(ctx, g.ncell, 256, 8);
+    k_invdiag<<<eb, 256, 0, ctx->stream>>>(diag, invd, g.ncell);
+    DARE_LAUNCHED(ctx);
+    FFold32 f{};
+    f.zs[0] = invd;
+    for (int q = 0; q < 6; q++) f.ps[q] = diag + (q + 1) * g.ncell;
+    f.ahat = ahat32;
+    f.n = g.ncell;
+    return launch_march(ctx, g, m, f, st, partials);
+}
+
 int launch_scale(dare_ctx* ctx, int64_t n, const double* invd, double* x) {
     const int eb = grid_blocks(ctx, n, 256, 8);
     k_scale<<<eb, 256, 0, ctx->stream>>>(n, invd, x);

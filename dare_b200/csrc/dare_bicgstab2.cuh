@@ -145,6 +145,9 @@ int launch_true_residual(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, con
                          const double* x, const double* b, SolverState* st, double* partials, double* out);
 int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, double* ahat,
                 SolverState* st, double* partials);
+// invd = 1 / diag and the folded off-diagonals rounded to FP32 (no FP64 copy)
+int launch_fold32(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, float* ahat32,
+                  SolverState* st, double* partials);
 int launch_scale(dare_ctx* ctx, int64_t n, const double* invd, double* x);
 
 }  // namespace dare_gpu

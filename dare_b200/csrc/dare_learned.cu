@@ -190,23 +190,36 @@ __global__ void __launch_bounds__(256) k_bnorm(int64_t n, const double* __restri
     if (threadIdx.x == 0) *out = sqrt(tot[0]);
 }
 
-__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
-    GRID_LOOP(c, n) b[c] = (float)a[c];
+// The vector kernels below work on four cells at a time (16-byte accesses):
+// the learned solve's grids have sizes that are multiples of 8, so n is a
+// multiple of 4 and every vector of the workspace starts 16-byte aligned.
+__device__ __forceinline__ float4 ld4(const float* p, int64_t q) { return reinterpret_cast<const float4*>(p)[q]; }
+__device__ __forceinline__ void st4(float* p, int64_t q, float4 v) { reinterpret_cast<float4*>(p)[q] = v; }
+__device__ __forceinline__ double sq4(float4 a) {
+    return (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w;
+}
+__device__ __forceinline__ double dot4(float4 a, float4 b) {
+    return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+}
+// a - c b, component by component
+__device__ __forceinline__ float4 axmy(float4 a, float c, float4 b) {
+    return make_float4(a.x - c * b.x, a.y - c * b.y, a.z - c * b.z, a.w - c * b.w);
 }
 
 // start of an inner solve: r = rh = rin, u = v = w = d = 0
 __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, SolverState* st, double* partials, double rel_tol,
                                               int max_it) {
     double acc[1] = {0.};
-    GRID_LOOP(c, n) {
-        const float r = vs.rin[c];
-        vs.r[c] = r;
-        vs.rh[c] = r;
-        vs.u[c] = 0.f;
-        vs.v[c] = 0.f;
-        vs.w[c] = 0.f;
-        vs.d[c] = 0.f;
-        acc[0] += (double)r * r;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    GRID_LOOP(q, n / 4) {
+        const float4 r = ld4(vs.rin, q);
+        st4(vs.r, q, r);
+        st4(vs.rh, q, r);
+        st4(vs.u, q, zero);
+        st4(vs.v, q, zero);
+        st4(vs.w, q, zero);
+        st4(vs.d, q, zero);
+        acc[0] += sq4(r);
     }
     double tot[1];
     if (!grid_reduce<1>(acc, partials, &st->count, tot)) return;
@@ -234,7 +247,7 @@ __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, SolverState* s
 __global__ void __launch_bounds__(256) k_rho(int64_t n, Vecs vs, SolverState* st, double* partials) {
     if (st->done) return;
     double acc[1] = {0.};
-    GRID_LOOP(c, n) acc[0] += (double)vs.rh[c] * vs.r[c];
+    GRID_LOOP(q, n / 4) acc[0] += dot4(ld4(vs.rh, q), ld4(vs.r, q));
     double tot[1];
     if (!grid_reduce<1>(acc, partials, &st->count, tot)) return;
     if (threadIdx.x == 0) {
@@ -251,32 +264,32 @@ __global__ void __launch_bounds__(256) k_rho(int64_t n, Vecs vs, SolverState* st
 __global__ void k_upd_u(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float beta = (float)st->beta;
-    GRID_LOOP(c, n) vs.u[c] = vs.r[c] - beta * vs.u[c];
+    GRID_LOOP(q, n / 4) st4(vs.u, q, axmy(ld4(vs.r, q), beta, ld4(vs.u, q)));
 }
 
 // (8): r -= alpha v (the matching x update is folded into k_upd_final)
 __global__ void k_upd_r(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float alpha = (float)st->alpha;
-    GRID_LOOP(c, n) vs.r[c] -= alpha * vs.v[c];
+    GRID_LOOP(q, n / 4) st4(vs.r, q, axmy(ld4(vs.r, q), alpha, ld4(vs.v, q)));
 }
 
 // (12) v = s - beta v
 __global__ void k_upd_v(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float beta = (float)st->beta;
-    GRID_LOOP(c, n) vs.v[c] = vs.s[c] - beta * vs.v[c];
+    GRID_LOOP(q, n / 4) st4(vs.v, q, axmy(ld4(vs.s, q), beta, ld4(vs.v, q)));
 }
 
 // (15)-(17)
 __global__ void k_upd3(int64_t n, Vecs vs, const SolverState* st) {
     if (st->done) return;
     const float alpha = (float)st->alpha, beta = (float)st->beta;
-    GRID_LOOP(c, n) {
-        const float r = vs.r[c];
-        vs.u[c] = r - beta * vs.u[c];
-        vs.r[c] = r - alpha * vs.v[c];
-        vs.s[c] -= alpha * vs.w[c];
+    GRID_LOOP(q, n / 4) {
+        const float4 r = ld4(vs.r, q);
+        st4(vs.u, q, axmy(r, beta, ld4(vs.u, q)));
+        st4(vs.r, q, axmy(r, alpha, ld4(vs.v, q)));
+        st4(vs.s, q, axmy(ld4(vs.s, q), alpha, ld4(vs.w, q)));
     }
 }
 
@@ -288,13 +301,26 @@ __global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, SolverSta
     const float cu = (float)(a1 - a2 * b1), cr = (float)(a2 + om1), cv = (float)(-om1 * a2), cs = (float)om2;
     const float w1 = (float)om1, w2 = (float)om2;
     double acc[1] = {0.};
-    GRID_LOOP(c, n) {
-        const float r = vs.r[c], s = vs.s[c];
-        vs.d[c] += cu * vs.zu[c] + cr * vs.zr[c] + cv * vs.zv[c] + cs * vs.zs[c];
-        const float rn = r - w1 * s - w2 * vs.t[c];
-        vs.r[c] = rn;
-        vs.u[c] -= w1 * vs.v[c] + w2 * vs.w[c];
-        acc[0] += (double)rn * rn;
+    GRID_LOOP(q, n / 4) {
+        const float4 zu = ld4(vs.zu, q), zr = ld4(vs.zr, q), zv = ld4(vs.zv, q), zs = ld4(vs.zs, q);
+        float4 d = ld4(vs.d, q);
+        d.x += cu * zu.x + cr * zr.x + cv * zv.x + cs * zs.x;
+        d.y += cu * zu.y + cr * zr.y + cv * zv.y + cs * zs.y;
+        d.z += cu * zu.z + cr * zr.z + cv * zv.z + cs * zs.z;
+        d.w += cu * zu.w + cr * zr.w + cv * zv.w + cs * zs.w;
+        st4(vs.d, q, d);
+        const float4 r = ld4(vs.r, q), s = ld4(vs.s, q), t = ld4(vs.t, q);
+        const float4 rn = make_float4(r.x - w1 * s.x - w2 * t.x, r.y - w1 * s.y - w2 * t.y,
+                                      r.z - w1 * s.z - w2 * t.z, r.w - w1 * s.w - w2 * t.w);
+        st4(vs.r, q, rn);
+        const float4 v = ld4(vs.v, q), w = ld4(vs.w, q);
+        float4 u = ld4(vs.u, q);
+        u.x -= w1 * v.x + w2 * w.x;
+        u.y -= w1 * v.y + w2 * w.y;
+        u.z -= w1 * v.z + w2 * w.z;
+        u.w -= w1 * v.w + w2 * w.w;
+        st4(vs.u, q, u);
+        acc[0] += sq4(rn);
     }
     double tot[1];
     if (!grid_reduce<1>(acc, partials, &st->count, tot)) return;
@@ -395,6 +421,8 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     const int* sys_n = net->coarse ? net->fine : net->n;
     if (g.dim != 3 || g.n[0] != sys_n[0] || g.n[1] != sys_n[1] || g.n[2] != sys_n[2])
         return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: grid does not match the network");
+    if (g.ncell % 4)   // the vector kernels take four cells at a time (sizes are multiples of 8)
+        return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: cell count must be a multiple of 4");
     if (lp->iteration_budget < 1 || lp->inner_max_it < 1 || !(lp->inner_rel_tol > 0.))
         return set_error(ctx, DARE_ERR_BAD_ARG, "bicgstab2_learned: bad learned parameters");
     cudaSetDevice(ctx->device);
@@ -428,10 +456,8 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
                                &vs.d, &vs.zu, &vs.zr, &vs.zv, &vs.zs, &vs.rin};
     for (int i = 0; i < kNumVecs; i++) *slots[i] = V + (size_t)i * n;
 
-    // Ahat = A D^-1 (FP64 fold) and its FP32 copy
-    if ((rc = launch_fold(ctx, g, ws->march, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
-    k_to_f32<<<eb, 256, 0, ctx->stream>>>(ws->ahat, lw->ahat32, 6 * n);
-    DARE_LAUNCHED(ctx);
+    // Ahat = A D^-1, folded straight to FP32
+    if ((rc = launch_fold32(ctx, g, ws->march, s->diag, ws->invd, lw->ahat32, ws->st, ws->partials))) return rc;
     DARE_CUDA(ctx, cudaMemsetAsync(lw->st, 0, sizeof(SolverState), ctx->stream));
     k_bnorm<<<eb, 256, 0, ctx->stream>>>(n, s->rhs, lw->st, lw->partials, lw->scal);
     DARE_LAUNCHED(ctx);

@@ -317,6 +317,26 @@ struct FFold {
     __device__ void done(SolverState*, const double*) const {}
 };
 
+// The same, rounded to FP32: the operator of the FP32 inner solves, written
+// without an FP64 copy
+struct FFold32 {
+    using type = double;
+    static constexpr int Q = 0, NZ = 1, NP = 6;
+    static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
+    const double* zs[2];   // invd
+    const double* ps[NP];  // the 6 off-diagonals of A
+    float* ahat;
+    int64_t n;
+    __device__ void load(const SolverState*) {}
+    __device__ double zc(double a, double) const { return a; }
+    __device__ void center(int64_t c, const double (&zz)[7], const double* p, double*) const {
+#pragma unroll
+        for (int q = 0; q < 6; q++) ahat[q * n + c] = (float)(p[q] * zz[q + 1]);
+    }
+    __device__ void done(SolverState*, const double*) const {}
+};
+
 // ---------------------------------------------------------------------------
 // item reduction: partials are indexed by item; the item whose counter
 // increment completes the set sums them in item order.

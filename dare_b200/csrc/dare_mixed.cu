@@ -29,10 +29,6 @@ void dare_mixed_ws_free(dare_solver_ws* ws) {
 
 namespace dare_gpu {
 
-static __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
-        b[c] = (float)a[c];
-}
 
 // x += D^-1 dy
 static __global__ void k_correct(int64_t n, const double* __restrict__ invd, const float* __restrict__ dy,
@@ -112,10 +108,8 @@ int dare_bicgstab2_refine(dare_system* s, const dare_solver_params* p, dare_solv
     const int eb = grid_blocks(ctx, n, 256, 8);
     OpT<double> full{s->diag, s->diag + n, n};
 
-    // Ahat = A D^-1 in FP64, then its FP32 copy
-    if ((rc = launch_fold(ctx, g, m, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
-    k_to_f32<<<eb, 256, 0, ctx->stream>>>(ws->ahat, ws->ahat32, 6 * n);
-    DARE_LAUNCHED(ctx);
+    // Ahat = A D^-1, folded straight to FP32
+    if ((rc = launch_fold32(ctx, g, m, s->diag, ws->invd, ws->ahat32, ws->st, ws->partials))) return rc;
     OpT<float> op32{nullptr, ws->ahat32, n};
     float* dy = ws->vec32 + 11 * n;
     float* r32 = ws->vec32 + 12 * n;
