@@ -52,6 +52,12 @@ class AssemblyDesc(C.Structure):
                 ("face_vel", C.c_void_p * 3), ("scheme", C.c_int)]
 
 
+class TermDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("op", C.c_int), ("component", C.c_int), ("dt", C.c_double), ("D", C.c_double),
+                ("face_D", C.c_void_p * 3), ("vel", C.c_double * 3), ("face_vel", C.c_void_p * 3),
+                ("limiter", C.c_int), ("scheme", C.c_int)]
+
+
 class SolverParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_it", C.c_int), ("precond", C.c_int), ("precision", C.c_int),
                 ("inner_rel_tol", C.c_double), ("inner_max_it", C.c_int), ("max_refinements", C.c_int),
@@ -109,6 +115,8 @@ _SIGS = [
     ("dare_system_destroy", C.c_int, [_P]),
     ("dare_system_set_bc", C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
     ("dare_assemble", C.c_int, [_P, C.POINTER(AssemblyDesc), _P]),
+    ("dare_system_set_bc_component", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_double]),
+    ("dare_assemble_terms", C.c_int, [_P, C.POINTER(TermDesc), C.c_int, _P]),
     ("dare_system_set_coefficients", C.c_int, [_P, _P, _P, _P]),
     ("dare_system_get_coefficients", C.c_int, [_P, _P, _P]),
     ("dare_system_set_initial_guess", C.c_int, [_P, _P]),
@@ -421,6 +429,49 @@ class Assembly:
         return a
 
 
+
+TERM_KINDS = {"DDT": 0, "DIFFUSION": 1, "CONVECTION": 2}
+TERM_OPS = {"SET": 0, "ADD": 1, "SUB": 2}
+
+
+@dataclass
+class Term:
+    """One MatrixBlock expression of a composed functor (see dare_term):
+    ``Term("DDT", "SET", dt=dt)`` is ``mb = ddt(field)``, ``Term("DIFFUSION",
+    "SUB")`` is ``mb -= div(grad(mb))``, ``Term("CONVECTION", "ADD", component=0,
+    vel=(u, v, 0))`` is ``mb.Add(0, div(TVD(u) * field).GetSlice(0))``."""
+    kind: str
+    op: str = "ADD"
+    component: int = -1
+    dt: float = 0.0
+    D: float = 1.0
+    face_D: tuple | None = None
+    vel: tuple | None = None
+    face_vel: tuple | None = None
+    limiter: str = "VANLEER"
+    scheme: str = "EULER_BACKWARD"
+
+    def to_c(self) -> TermDesc:
+        t = TermDesc()
+        t.kind = TERM_KINDS[self.kind.upper()]
+        t.op = TERM_OPS[self.op.upper()]
+        t.component = int(self.component)
+        t.dt = float(self.dt)
+        t.D = float(self.D)
+        if self.face_D is not None:
+            for d, p in enumerate(self.face_D):
+                t.face_D[d] = p.ptr if isinstance(p, DeviceArray) else p
+        if self.vel is not None:
+            for d, v in enumerate(self.vel):
+                t.vel[d] = float(v)
+        if self.face_vel is not None:
+            for d, p in enumerate(self.face_vel):
+                t.face_vel[d] = p.ptr if isinstance(p, DeviceArray) else p
+        t.limiter = LIMITER[self.limiter]
+        t.scheme = SCHEME[self.scheme]
+        return t
+
+
 class MatrixSystem:
     """Structured 7-diagonal system A x = B (Matrix::Trilinos<SC>); with N
     components one stencil per component, rows and columns cell * N + c."""
@@ -438,13 +489,26 @@ class MatrixSystem:
             lib().dare_system_destroy(self.h)
             self.h = None
 
-    def set_bc(self, face: int, kind: int, value: float = 0.0):
-        _check(lib().dare_system_set_bc(self.h, face, kind, value), self.grid.ctx.h, "set_bc")
+    def set_bc(self, face: int, kind: int, value: float = 0.0, component: int = -1):
+        """Condition of a face, for every component or for one."""
+        if component < 0:
+            _check(lib().dare_system_set_bc(self.h, face, kind, value), self.grid.ctx.h, "set_bc")
+        else:
+            _check(lib().dare_system_set_bc_component(self.h, component, face, kind, value), self.grid.ctx.h,
+                   "set_bc_component")
 
-    def build(self, field: Field, assembly: Assembly):
-        """Trilinos<SC>::Build with the fused functor; x0 = field level 0."""
-        desc = assembly.to_c()
-        _check(lib().dare_assemble(self.h, C.byref(desc), field.h), self.grid.ctx.h, "assemble")
+    def build(self, field: Field, assembly):
+        """Trilinos<SC>::Build; x0 = field level 0.  ``assembly`` is the fused
+        functor (an Assembly) or a composed one (a sequence of Term)."""
+        if isinstance(assembly, Assembly):
+            desc = assembly.to_c()
+            _check(lib().dare_assemble(self.h, C.byref(desc), field.h), self.grid.ctx.h, "assemble")
+            return
+        terms = list(assembly)
+        arr = (TermDesc * max(1, len(terms)))()
+        for i, t in enumerate(terms):
+            arr[i] = t.to_c()
+        _check(lib().dare_assemble_terms(self.h, arr, len(terms), field.h), self.grid.ctx.h, "assemble_terms")
 
     def set_coefficients(self, diag: np.ndarray | None, rhs: np.ndarray | None = None, x0: np.ndarray | None = None):
         d = None if diag is None else np.ascontiguousarray(diag, dtype=np.float64)

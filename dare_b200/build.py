@@ -74,7 +74,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-EXAMPLES = {"example_diffusion": os.path.join(HERE, "cxx", "example_diffusion.cpp")}
+EXAMPLES = {"example_diffusion": os.path.join(HERE, "cxx", "example_diffusion.cpp"),
+            "example_counter_diffusion": os.path.join(HERE, "cxx", "example_counter_diffusion.cpp")}
 BIN = os.path.join(HERE, "bin")
 
 

@@ -117,13 +117,18 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
         const int64_t fx_up = (int64_t)upper_face(g, 0, i) * nplane + jk;
         double coef[7];
 #pragma unroll
-        for (int p = 0; p < 7; p++) coef[p] = 0.;
-        double rhs = 0.;
+        for (int p = 0; p < 7; p++) coef[p] = a.acc ? diag[p * n + c] : 0.;
+        double rhs = a.acc ? rhs_out[c] : 0.;
 
         if (a.dt > 0.) {                                   // DDT, weights (1, 1)
             const double tt = a.tt;
-            coef[DARE_CENTER] = tt;
-            rhs = 0. + tt * phi_old[loc];
+            if (a.sgn_ddt > 0.) {                           // from zero: C = tt, rhs = 0 + tt phi_old
+                coef[DARE_CENTER] += tt;
+                rhs += tt * phi_old[loc];
+            } else {                                        // MatrixBlock -=: += (-1 s)
+                coef[DARE_CENTER] += -1. * tt;
+                rhs += -1. * (tt * phi_old[loc]);
+            }
         }
 
         if (a.convection) {                                // TVD * field, then divergence
@@ -174,9 +179,15 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
                 if (DIM > 1) srhs += a.w[t] * g.area[1] * (rr[DARE_NORTH] - rr[DARE_SOUTH]);
                 if (DIM > 2) srhs += a.w[t] * g.area[2] * (rr[DARE_TOP] - rr[DARE_BOTTOM]);
             }
+            if (a.sgn_conv > 0.) {                           // MatrixBlock::Add
 #pragma unroll
-            for (int p = 0; p < 7; p++) coef[p] += sc[p];       // MatrixBlock::Add
-            rhs += srhs;
+                for (int p = 0; p < 7; p++) coef[p] += sc[p];
+                rhs += srhs;
+            } else {                                        // MatrixBlock -=
+#pragma unroll
+                for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
+                rhs += -1. * srhs;
+            }
         }
 
         if (a.diffusion) {                                 // mb -= div(D, grad(mb))
@@ -208,15 +219,20 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             apply_divergence<DIM>(g, nb, cf, sc);
 #pragma unroll
             for (int p = 0; p < 7; p++) sc[p] *= a.w[0];           // s_c *= weight[0]
+            if (a.sgn_diff < 0.) {                           // mb -= div(D grad(mb))
 #pragma unroll
-            for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
-            rhs += -1. * 0.;
+                for (int p = 0; p < 7; p++) coef[p] += -1. * sc[p];
+                rhs += -1. * 0.;
+            } else {
+#pragma unroll
+                for (int p = 0; p < 7; p++) coef[p] += sc[p];
+            }
         }
 
         const int idx[3] = {i, jj, kk};
 #pragma unroll
         for (int d = 0; d < DIM; d++) {                    // boundary folding
-            if (g.periodic[d]) continue;
+            if (g.periodic[d] || !a.fold) continue;
 #pragma unroll
             for (int side = 0; side < 2; side++) {
                 const int face = 2 * d + 1 + side;
@@ -256,38 +272,26 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
     }
 }
 
-int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old) {
+// The conditions on the boundary faces of component c
+static void component_bc(const dare_system* s, int c, AsmParams& a) {
+    const bool own = !s->bc_type_c.empty();
+    for (int f = 0; f < 6; f++) {
+        a.bc_type[f] = own ? s->bc_type_c[(size_t)c * 6 + f] : s->bc_type[f];
+        a.bc_value[f] = own ? s->bc_value_c[(size_t)c * 6 + f] : s->bc_value[f];
+    }
+}
+
+// Launch the assembly kernel of the grid's dimension for field component c
+// (its field values, its rows).
+static int launch_component(dare_system* s, const AsmParams& a, int c, const double* phi, const double* phi_old) {
     dare_ctx* ctx = s->grid->ctx;
     const GridDev& g = s->grid->dev;
-    AsmParams a{};
-    a.dt = desc->dt;
-    a.diffusion = desc->diffusion;
-    a.D = desc->D;
-    a.convection = desc->convection;
-    a.limiter = desc->limiter;
-    for (int d = 0; d < 3; d++) {
-        a.face_D[d] = desc->face_D[d];
-        a.face_vel[d] = desc->face_vel[d];
-        a.vel[d] = desc->vel[d];
-    }
-    for (int f = 0; f < 6; f++) {
-        a.bc_type[f] = s->bc_type[f];
-        a.bc_value[f] = s->bc_value[f];
-    }
-    a.tt = a.dt > 0. ? (g.volume * 1.) / a.dt : 0.;
-    a.dstride = s->sdev.ncell;
-    a.scheme = desc->scheme;
-    a.nexp = scheme_weights(desc->scheme, a.w);
-    if (a.nexp < 0) return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: unknown time scheme");
-    for (int d = 0; d < 3; d++) a.dn[d] = 1. / g.dx[d];
-    for (int d = 0; d < g.dim; d++) {
-        if (a.diffusion == 2 && !a.face_D[d]) return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: face_D missing");
-        if (a.convection == 2 && !a.face_vel[d])
-            return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: face_vel missing");
-    }
-    if (a.diffusion < 0 || a.diffusion > 2 || a.convection < 0 || a.convection > 2 || a.limiter < 0 ||
-        a.limiter > DARE_LIMITER_VANLEER)
-        return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble: bad descriptor");
+    const double* pc = phi + (size_t)c * g.ncell_ghosted;
+    const double* po = phi_old + (size_t)c * g.ncell_ghosted;
+    double* dc = s->diag + (size_t)c * g.ncell;
+    double* rc = s->rhs + (size_t)c * g.ncell;
+    double* xc = s->x + (size_t)c * g.ncell;
+    if (g.dim == 3) return launch_assemble3(ctx, g, a, pc, po, dc, rc, xc);
     // (j,k) tiles of tk x tj columns, runs of `planes` i-planes per block
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     const int tk = n2 > 16 ? 32 : n2 > 8 ? 16 : n2 > 4 ? 8 : n2 > 2 ? 4 : 1;
@@ -302,27 +306,118 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
     if (planes < 2 && n0 >= 2) planes = 2;
     nchunk = (n0 + planes - 1) / planes;
     const dim3 grid(gx, gy, (unsigned)nchunk), block(tk, tj, 1);
-    if (g.dim == 3) {
-        // one launch per field component (its field values, its rows)
-        for (int c = 0; c < s->ncomp; c++) {
-            int rc = launch_assemble3(ctx, g, a, phi + (size_t)c * g.ncell_ghosted,
-                                      phi_old + (size_t)c * g.ncell_ghosted, s->diag + (size_t)c * g.ncell,
-                                      s->rhs + (size_t)c * g.ncell, s->x + (size_t)c * g.ncell);
-            if (rc) return rc;
-        }
-        return DARE_OK;
+    if (g.dim == 2)
+        k_assemble<2><<<grid, block, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, planes);
+    else
+        k_assemble<1><<<grid, block, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, planes);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+// Geometry, scheme weights and checks shared by both entry points.
+static int base_params(dare_system* s, AsmParams& a, const char* who) {
+    dare_ctx* ctx = s->grid->ctx;
+    const GridDev& g = s->grid->dev;
+    a.tt = a.dt > 0. ? (g.volume * 1.) / a.dt : 0.;
+    a.dstride = s->sdev.ncell;
+    a.nexp = scheme_weights(a.scheme, a.w);
+    if (a.nexp < 0) return set_error(ctx, DARE_ERR_BAD_ARG, std::string(who) + ": unknown time scheme");
+    for (int d = 0; d < 3; d++) a.dn[d] = 1. / g.dx[d];
+    for (int d = 0; d < g.dim; d++) {
+        if (a.diffusion == 2 && !a.face_D[d]) return set_error(ctx, DARE_ERR_BAD_ARG, std::string(who) + ": face_D missing");
+        if (a.convection == 2 && !a.face_vel[d])
+            return set_error(ctx, DARE_ERR_BAD_ARG, std::string(who) + ": face_vel missing");
     }
+    if (a.diffusion < 0 || a.diffusion > 2 || a.convection < 0 || a.convection > 2 || a.limiter < 0 ||
+        a.limiter > DARE_LIMITER_VANLEER || !(a.dt >= 0.))
+        return set_error(ctx, DARE_ERR_BAD_ARG, std::string(who) + ": bad descriptor");
+    return DARE_OK;
+}
+
+int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old) {
+    AsmParams a{};
+    a.dt = desc->dt;
+    a.diffusion = desc->diffusion;
+    a.D = desc->D;
+    a.convection = desc->convection;
+    a.limiter = desc->limiter;
+    for (int d = 0; d < 3; d++) {
+        a.face_D[d] = desc->face_D[d];
+        a.face_vel[d] = desc->face_vel[d];
+        a.vel[d] = desc->vel[d];
+    }
+    a.scheme = desc->scheme;
+    // the fused functor: mb = ddt; mb += div(TVD * field); mb -= div(D grad); fold
+    a.sgn_ddt = 1.;
+    a.sgn_conv = 1.;
+    a.sgn_diff = -1.;
+    a.acc = 0;
+    a.fold = 1;
+    int rc = base_params(s, a, "dare_assemble");
+    if (rc) return rc;
     for (int c = 0; c < s->ncomp; c++) {
-        const double* pc = phi + (size_t)c * g.ncell_ghosted;
-        const double* po = phi_old + (size_t)c * g.ncell_ghosted;
-        double* dc = s->diag + (size_t)c * g.ncell;
-        double* rc = s->rhs + (size_t)c * g.ncell;
-        double* xc = s->x + (size_t)c * g.ncell;
-        if (g.dim == 2)
-            k_assemble<2><<<grid, block, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, planes);
-        else
-            k_assemble<1><<<grid, block, 0, ctx->stream>>>(g, a, pc, po, dc, rc, xc, planes);
-        DARE_LAUNCHED(ctx);
+        component_bc(s, c, a);
+        if ((rc = launch_component(s, a, c, phi, phi_old))) return rc;
+    }
+    return DARE_OK;
+}
+
+// A composed functor (dare_assemble_terms): per component, its terms in
+// order -- each one launch that sets or adds its coefficients -- then one
+// pass that folds the boundary faces.
+static int launch_terms(dare_system* s, const dare_term* terms, int nterms, const double* phi, const double* phi_old) {
+    dare_ctx* ctx = s->grid->ctx;
+    for (int t = 0; t < nterms; t++) {
+        const dare_term& T = terms[t];
+        if (T.kind < DARE_TERM_DDT || T.kind > DARE_TERM_CONVECTION || T.op < DARE_OP_SET || T.op > DARE_OP_SUB ||
+            T.component < -1 || T.component >= s->ncomp)
+            return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble_terms: bad term");
+        if (T.kind == DARE_TERM_DDT && !(T.dt > 0.))
+            return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble_terms: DDT needs dt > 0");
+    }
+    int rc;
+    for (int c = 0; c < s->ncomp; c++) {
+        bool started = false;
+        for (int t = 0; t < nterms; t++) {
+            const dare_term& T = terms[t];
+            if (T.component >= 0 && T.component != c) continue;
+            AsmParams a{};
+            a.scheme = T.scheme;
+            a.limiter = T.limiter;
+            const double sgn = T.op == DARE_OP_SUB ? -1. : 1.;
+            a.sgn_ddt = a.sgn_conv = a.sgn_diff = sgn;
+            if (T.kind == DARE_TERM_DDT) a.dt = T.dt;
+            if (T.kind == DARE_TERM_DIFFUSION) {
+                const bool faces = T.face_D[0] || T.face_D[1] || T.face_D[2];
+                a.diffusion = faces ? 2 : 1;
+                a.D = T.D;
+                for (int d = 0; d < 3; d++) a.face_D[d] = T.face_D[d];
+            }
+            if (T.kind == DARE_TERM_CONVECTION) {
+                const bool faces = T.face_vel[0] || T.face_vel[1] || T.face_vel[2];
+                a.convection = faces ? 2 : 1;
+                for (int d = 0; d < 3; d++) {
+                    a.vel[d] = T.vel[d];
+                    a.face_vel[d] = T.face_vel[d];
+                }
+            }
+            a.acc = started && T.op != DARE_OP_SET;   // Set starts the component's block afresh
+            a.fold = 0;
+            if ((rc = base_params(s, a, "dare_assemble_terms"))) return rc;
+            component_bc(s, c, a);
+            if ((rc = launch_component(s, a, c, phi, phi_old))) return rc;
+            started = true;
+        }
+        // the fold pass (it also zeroes a component that no term touched)
+        AsmParams a{};
+        a.sgn_ddt = a.sgn_conv = 1.;
+        a.sgn_diff = -1.;
+        a.acc = started;
+        a.fold = 1;
+        a.limiter = DARE_LIMITER_CDS;
+        if ((rc = base_params(s, a, "dare_assemble_terms"))) return rc;
+        component_bc(s, c, a);
+        if ((rc = launch_component(s, a, c, phi, phi_old))) return rc;
     }
     return DARE_OK;
 }
@@ -335,4 +430,13 @@ extern "C" int dare_assemble(dare_system* s, const dare_assembly_desc* desc, dar
     const double* phi = field->level[0];
     const double* phi_old = field->num_levels > 1 ? field->level[1] : field->level[0];
     return dare_gpu::launch_assemble(s, desc, phi, phi_old);
+}
+
+extern "C" int dare_assemble_terms(dare_system* s, const dare_term* terms, int nterms, dare_field* field) {
+    if (!s || (!terms && nterms > 0) || nterms < 0 || !field || field->grid != s->grid || field->ncomp != s->ncomp)
+        return DARE_ERR_BAD_ARG;
+    cudaSetDevice(s->grid->ctx->device);
+    const double* phi = field->level[0];
+    const double* phi_old = field->num_levels > 1 ? field->level[1] : field->level[0];
+    return dare_gpu::launch_terms(s, terms, nterms, phi, phi_old);
 }

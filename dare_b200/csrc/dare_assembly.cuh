@@ -23,6 +23,13 @@ struct AsmParams {
     int scheme;     // DARE_SCHEME_* of the div(...) terms
     int nexp;       // its explicit levels T
     double w[3];    // its weights w[0..T] (TimeDiscretizationSchemes.h:29-76)
+    // composition (MatrixBlock::Set / Add / operator-=): the sign each part
+    // enters with (the fused descriptor: DDT +1, convection +1, diffusion -1),
+    // whether the parts add to the coefficients already in the system, and
+    // whether the boundary faces are folded at the end
+    double sgn_ddt, sgn_conv, sgn_diff;
+    int acc;
+    int fold;
 };
 
 // Weights of the Divergence time schemes (TimeDiscretizationSchemes.h:29-76);

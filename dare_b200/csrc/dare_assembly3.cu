@@ -84,6 +84,8 @@ struct A3Params {
     int64_t dstride;
     const double* face_vel[3];
     const double* face_D[3];
+    int acc;            // add to the coefficients already in the system
+    int fold;           // fold the boundary faces at the end
 };
 
 // a / b for normal, finite b by Newton-Raphson refinement of the hardware
@@ -327,10 +329,15 @@ __global__ void __launch_bounds__(256, FD ? 2 : 3)
         }
         if (active) {
             double coef[7] = {cC, cW, cE, cS, cN, cB, cT};
+            if (a.acc) {                                  // a term added to an earlier one
+#pragma unroll
+                for (int p = 0; p < 7; p++) coef[p] += diag[p * a.dstride + c];
+                rhs += rhs_out[c];
+            }
             const int idx[3] = {i, jj, kk};
 #pragma unroll
             for (int d = 0; d < 3; d++) {                 // boundary folding
-                if (g.periodic[d]) continue;
+                if (g.periodic[d] || !a.fold) continue;
 #pragma unroll
                 for (int side = 0; side < 2; side++) {
                     const int face = 2 * d + 1 + side;
@@ -402,16 +409,20 @@ int launch_assemble3(dare_ctx* ctx, const GridDev& g, const AsmParams& a, const 
                      double* diag, double* rhs, double* x0) {
     A3Params p{};
     p.ddt = a.dt > 0.;
-    p.tt = a.tt;
+    p.tt = a.sgn_ddt * a.tt;
     p.conv = a.convection;
     p.diff = a.diffusion;
+    p.acc = a.acc;
+    p.fold = a.fold;
     double wsum = 1.;
     for (int t = 1; t <= a.nexp; t++) wsum += a.w[t];
+    // the parts' signs enter through their factors: the kernel subtracts the
+    // diffusion factors (the fused functor's mb -= div(D grad))
     for (int d = 0; d < 3; d++) {
         p.vel[d] = a.vel[d];
-        p.cA[d] = a.w[0] * g.area[d];
-        p.rA[d] = wsum * g.area[d];
-        p.kD[d] = a.w[0] * g.area[d] * a.dn[d] * (a.diffusion == 1 ? a.D : 1.);
+        p.cA[d] = a.sgn_conv * (a.w[0] * g.area[d]);
+        p.rA[d] = a.sgn_conv * (wsum * g.area[d]);
+        p.kD[d] = -a.sgn_diff * (a.w[0] * g.area[d] * a.dn[d] * (a.diffusion == 1 ? a.D : 1.));
         p.face_vel[d] = a.face_vel[d];
         p.face_D[d] = a.face_D[d];
     }

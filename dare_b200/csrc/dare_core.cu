@@ -427,6 +427,39 @@ int dare_system_set_bc(dare_system* s, int face, int type, double value) {
     }
     s->bc_type[face - 1] = type;
     s->bc_value[face - 1] = value;
+    for (int c = 0; c < (int)s->bc_type_c.size() / 6; c++) {   // every component
+        s->bc_type_c[c * 6 + face - 1] = type;
+        s->bc_value_c[c * 6 + face - 1] = value;
+    }
+    return DARE_OK;
+}
+
+int dare_system_set_bc_component(dare_system* s, int component, int face, int type, double value) {
+    if (!s || face < DARE_WEST || face > DARE_TOP) return DARE_ERR_BAD_ARG;
+    if (component < 0) return dare_system_set_bc(s, face, type, value);
+    if (component >= s->ncomp)
+        return set_error(s->grid->ctx, DARE_ERR_BAD_ARG, "dare_system_set_bc_component: no such component");
+    const GridDev& g = s->grid->dev;
+    const int d = (face - 1) / 2;
+    if (d >= g.dim) return set_error(s->grid->ctx, DARE_ERR_BAD_ARG, "dare_system_set_bc_component: inactive dimension");
+    if (g.periodic[d]) {
+        if (type != DARE_BC_PERIODIC)
+            return set_error(s->grid->ctx, DARE_ERR_BAD_ARG, "dare_system_set_bc_component: dimension is periodic");
+    } else if (type != DARE_BC_DIRICHLET && type != DARE_BC_NEUMANN) {
+        return set_error(s->grid->ctx, DARE_ERR_BAD_ARG,
+                         "dare_system_set_bc_component: non-periodic face needs Dirichlet or Neumann");
+    }
+    if (s->bc_type_c.empty()) {   // start from the whole-system conditions
+        s->bc_type_c.resize((size_t)s->ncomp * 6);
+        s->bc_value_c.resize((size_t)s->ncomp * 6);
+        for (int c = 0; c < s->ncomp; c++)
+            for (int f = 0; f < 6; f++) {
+                s->bc_type_c[c * 6 + f] = s->bc_type[f];
+                s->bc_value_c[c * 6 + f] = s->bc_value[f];
+            }
+    }
+    s->bc_type_c[(size_t)component * 6 + face - 1] = type;
+    s->bc_value_c[(size_t)component * 6 + face - 1] = value;
     return DARE_OK;
 }
 

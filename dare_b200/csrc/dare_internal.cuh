@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/dare_gpu.h"
 
@@ -89,8 +90,12 @@ struct dare_system {
     dare_grid* grid = nullptr;
     int ncomp = 1;               // field components (block-diagonal, one 7-point stencil each)
     dare_gpu::GridDev sdev{};    // the solver's view: components stacked along i
-    int bc_type[6] = {0, 0, 0, 0, 0, 0};
+    int bc_type[6] = {0, 0, 0, 0, 0, 0};        // the faces' conditions of every component ...
     double bc_value[6] = {0, 0, 0, 0, 0, 0};
+    // ... unless a component has its own (dare_system_set_bc_component):
+    // per component, 6 faces each; empty until the first per-component call
+    std::vector<int> bc_type_c;
+    std::vector<double> bc_value_c;
     double* diag = nullptr;   // [7][ncomp][ncell], component-major within a slot
     double* rhs = nullptr;    // [ncomp][ncell]
     double* x = nullptr;

@@ -122,6 +122,33 @@ typedef struct {
     int scheme;                      /* DARE_SCHEME_*, time scheme of both div(...) terms */
 } dare_assembly_desc;
 
+/* One term of a composed assembly functor: the MatrixBlock expressions of a
+ * user functor for Trilinos<SC>::Build (MatrixSystem/Trilinos.h:107-111),
+ *     (*mblock) = ddt(field);                  DDT, DARE_OP_SET
+ *     (*mblock) -= div(grad(*mblock));         DIFFUSION with D = 1, DARE_OP_SUB
+ *     mblock->Add(n, div(u * field).GetSlice(n));   CONVECTION for component n, DARE_OP_ADD
+ * (MatrixBlock_Cartesian.inl:480-593; counter_diffusion1D.cpp:107-148,
+ * advection_periodic2D.cpp:108-126).  The terms apply in order to every
+ * component (component = -1) or to one; SET starts a component's block
+ * afresh, ADD and SUB add the term or its negative.  After the last term the
+ * non-periodic faces are folded with each component's conditions
+ * (dare_system_set_bc, dare_system_set_bc_component).  Face arrays as in
+ * dare_assembly_desc. */
+enum { DARE_TERM_DDT = 0, DARE_TERM_DIFFUSION = 1, DARE_TERM_CONVECTION = 2 };
+enum { DARE_OP_SET = 0, DARE_OP_ADD = 1, DARE_OP_SUB = 2 };
+typedef struct {
+    int kind;                        /* DARE_TERM_* */
+    int op;                          /* DARE_OP_* */
+    int component;                   /* -1: every component; else that component only */
+    double dt;                       /* DDT: time step (> 0) */
+    double D;                        /* DIFFUSION: div(D grad(mb)); 1 for div(grad(mb)) */
+    const double* face_D[3];         /* DIFFUSION: face diffusivities instead of D (all three or none) */
+    double vel[3];                   /* CONVECTION: constant velocity ... */
+    const double* face_vel[3];       /* ... or face velocities (all three or none) */
+    int limiter;                     /* CONVECTION: DARE_LIMITER_* */
+    int scheme;                      /* DIFFUSION / CONVECTION: DARE_SCHEME_* of the div(...) */
+} dare_term;
+
 typedef struct {
     double tol;             /* ABSOLUTE tolerance on ||r||_2 (stop criterion RNORM,
                                BiCGStab2.inl:34,561-565); tol_abs = rel * ||b|| for a relative one */
@@ -226,10 +253,19 @@ DARE_API int dare_system_num_components(const dare_system* s);
 DARE_API int dare_system_destroy(dare_system* s);
 /* face: DARE_WEST..DARE_TOP; non-periodic faces need DIRICHLET or NEUMANN */
 DARE_API int dare_system_set_bc(dare_system* s, int face, int type, double value);
+/* The condition of one field component on one face (component -1: every
+ * component, as dare_system_set_bc).  A functor that folds the components
+ * differently, e.g. counter_diffusion1D.cpp:123-146 (Dirichlet for component 0
+ * and Neumann for component 1 on the west face, the reverse on the east). */
+DARE_API int dare_system_set_bc_component(dare_system* s, int component, int face, int type, double value);
 /* Trilinos<SC>::Build -> BuildNew (Trilinos.inl:48-60,285-385) with the fused
  * functor above; x0 = field level 0 (the initial guess). DDT reads level 1 when
  * the field has 2+ levels, else level 0; convection reads level 0. */
 DARE_API int dare_assemble(dare_system* s, const dare_assembly_desc* desc, dare_field* field);
+/* Trilinos<SC>::Build with a composed functor given as `nterms` terms (see
+ * dare_term); x0 = field level 0.  DDT reads level 1 when the field has 2+
+ * levels; convection reads level 0. */
+DARE_API int dare_assemble_terms(dare_system* s, const dare_term* terms, int nterms, dare_field* field);
 /* Replace coefficients with user-built MatrixBlocks (host SoA: diag[7][ncells]
  * in slot order CENTER..TOP, removed entries 0), rhs and initial guess. */
 DARE_API int dare_system_set_coefficients(dare_system* s, const double* diag7, const double* rhs,
@@ -306,9 +342,11 @@ DARE_API int dare_batch_get_tuning(const dare_batch* bt, int* block, int vec_by_
 
 /* ---- residual norm without device allocation -------------------------------
  * No counterpart in the reference (DaRe computes residuals inside Tpetra).
- * ||b - A x||_2 of a structured 7-point system given as plain device arrays
- * (diag7: 7 x ncells in slot order CENTER..TOP, x, b over internal cells,
- * ordinal (i*ny + j)*nz + k; neighbours past a non-periodic face are ignored),
+ * ||b - A x||_2 of a structured 7-point system of ONE field component given
+ * as plain device arrays (diag7: 7 x ncells in slot order CENTER..TOP, x, b
+ * over internal cells, ordinal (i*ny + j)*nz + k; neighbours past a
+ * non-periodic face are ignored).  Systems with several components per cell
+ * are not supported here (their slots interleave the components).  The result is
  * written as one double to the device pointer norm_out, on `stream` (a
  * cudaStream_t, NULL = legacy default stream).  It is for callers that cannot
  * call cudaMalloc mid-run -- host codes whose device memory is owned by their
@@ -320,7 +358,9 @@ DARE_API int dare_batch_get_tuning(const dare_batch* bt, int* block, int vec_by_
  * with DARE_ERR_UNSUPPORTED and a message in `err` (may be NULL).  All calls
  * on a device share that array: calls that overlap on the GPU race and must
  * be serialized by the caller.  The first call on a device looks up the
- * array's device address, so make it before capturing any stream there. */
+ * array's device address and keeps it for the life of the process, so make
+ * that call before capturing any stream there, and do not call it again on a
+ * device after cudaDeviceReset (the array's address may change). */
 DARE_API int dare_residual_norm_noalloc(int dim, const int64_t n[3], const int periodic[3], const double* diag7,
                                         const double* x, const double* b, double* norm_out, void* stream,
                                         char* err, int err_len);

@@ -6,7 +6,9 @@
 //   dare::Grid::Cartesian<Dim>          -> dare_b200::Cartesian      (CartesianMesh.h:177-379)
 //   dare::Data::Field<Grid,SC,1>        -> dare_b200::Field          (Data/Field.h:47-138)
 //   dare::Matrix::Trilinos<SC>          -> dare_b200::Trilinos       (MatrixSystem/Trilinos.h:51-314)
-//   dare::Matrix::MatrixBlock (functor) -> dare_b200::Assembly       (the fused per-cell functor)
+//   dare::Matrix::MatrixBlock (functor) -> dare_b200::Assembly       (the fused per-cell functor),
+//                                          dare_b200::MatrixBlock    (a composed functor: ddt, div(grad),
+//                                                                     div(TVD * field) terms with =, +=, -=, Add)
 //                                          or Trilinos::SetBlocks    (host-built coefficients)
 //   dare::Matrix::BiCGStab2 / TrilinosSolver::Solve("BICGSTAB2")
 //                                       -> dare_b200::BiCGStab2      (BiCGStab2.h:58-206)
@@ -189,6 +191,80 @@ struct Assembly {
     }
 };
 
+// One operator of a composed functor (Equations/Operators.h: DDT,
+// Divergence of Gradient, Divergence of TVD * field), to be placed into a
+// MatrixBlock with =, +=, -= or Add(component, ...).
+struct Term {
+    dare_term t{};
+};
+// ddt(field): implicit Euler with step dt (DDT.inl:39-81)
+inline Term DDT(double dt) {
+    Term r;
+    r.t.kind = DARE_TERM_DDT;
+    r.t.dt = dt;
+    return r;
+}
+// div(D, grad(mb)) (D = 1: div(grad(mb))), or with device face diffusivities
+inline Term DivGrad(double D = 1., TimeScheme scheme = TimeScheme::EULER_BACKWARD) {
+    Term r;
+    r.t.kind = DARE_TERM_DIFFUSION;
+    r.t.D = D;
+    r.t.scheme = (int)scheme;
+    return r;
+}
+inline Term DivGrad(const double* const face_D[3], TimeScheme scheme = TimeScheme::EULER_BACKWARD) {
+    Term r = DivGrad(1., scheme);
+    for (int d = 0; d < 3; d++) r.t.face_D[d] = face_D[d];
+    return r;
+}
+// div(TVD(u) * field) with a constant velocity or device face velocities
+inline Term DivTVD(const std::array<double, 3>& u, Limiter limiter = Limiter::VANLEER,
+                   TimeScheme scheme = TimeScheme::EULER_BACKWARD) {
+    Term r;
+    r.t.kind = DARE_TERM_CONVECTION;
+    for (int d = 0; d < 3; d++) r.t.vel[d] = u[d];
+    r.t.limiter = (int)limiter;
+    r.t.scheme = (int)scheme;
+    return r;
+}
+inline Term DivTVD(const double* const face_velocity[3], Limiter limiter = Limiter::VANLEER,
+                   TimeScheme scheme = TimeScheme::EULER_BACKWARD) {
+    Term r = DivTVD(std::array<double, 3>{0., 0., 0.}, limiter, scheme);
+    for (int d = 0; d < 3; d++) r.t.face_vel[d] = face_velocity[d];
+    return r;
+}
+
+// A composed per-cell functor written the way a DaRe functor writes its
+// MatrixBlock (MatrixBlock_Cartesian.inl:480-593):
+//     MatrixBlock mb;
+//     mb = DDT(dt);                           // (*mblock) = ddt(field)
+//     mb -= DivGrad();                        // (*mblock) -= div(grad(*mblock))
+//     mb.Add(0, DivTVD({1., 0., 0.}));        // mblock->Add(0, div(u_0 * field).GetSlice(0))
+//     system.Build(field, mb);
+// The device evaluates the terms in order for every cell (dare_assemble_terms);
+// per-component boundary folding comes from Trilinos::SetBC.
+class MatrixBlock {
+public:
+    MatrixBlock& operator=(const Term& term) { return push(term, DARE_OP_SET, -1); }
+    MatrixBlock& operator+=(const Term& term) { return push(term, DARE_OP_ADD, -1); }
+    MatrixBlock& operator-=(const Term& term) { return push(term, DARE_OP_SUB, -1); }
+    MatrixBlock& Set(int component, const Term& term) { return push(term, DARE_OP_SET, component); }
+    MatrixBlock& Add(int component, const Term& term) { return push(term, DARE_OP_ADD, component); }
+    MatrixBlock& Subtract(int component, const Term& term) { return push(term, DARE_OP_SUB, component); }
+    const std::vector<dare_term>& Terms() const { return terms_; }
+    void Clear() { terms_.clear(); }
+
+private:
+    MatrixBlock& push(const Term& term, int op, int component) {
+        dare_term t = term.t;
+        t.op = op;
+        t.component = component;
+        terms_.push_back(t);
+        return *this;
+    }
+    std::vector<dare_term> terms_;
+};
+
 // Matrix::Trilinos<SC>: A, x, B of the structured system on the device.
 class Trilinos {
 public:
@@ -203,14 +279,20 @@ public:
     Trilinos& operator=(const Trilinos&) = delete;
     dare_system* get() const { return h_; }
 
-    // Dirichlet / Neumann folding of a non-periodic face (DARE_WEST..DARE_TOP)
-    void SetBC(int face, int type, double value = 0.) {
-        check(dare_system_set_bc(h_, face, type, value), ctx(), "dare_system_set_bc");
+    // Dirichlet / Neumann folding of a non-periodic face (DARE_WEST..DARE_TOP),
+    // for every component or for one
+    void SetBC(int face, int type, double value = 0., int component = -1) {
+        check(dare_system_set_bc_component(h_, component, face, type, value), ctx(), "dare_system_set_bc");
     }
     // Trilinos<SC>::Build(grep, field, functor) with the fused functor
     void Build(Field& field, const Assembly& functor) {
         dare_assembly_desc d = functor.Desc();
         check(dare_assemble(h_, &d, field.get()), ctx(), "dare_assemble");
+    }
+    // ... and with a composed functor
+    void Build(Field& field, const MatrixBlock& functor) {
+        const auto& t = functor.Terms();
+        check(dare_assemble_terms(h_, t.data(), (int)t.size(), field.get()), ctx(), "dare_assemble_terms");
     }
     // Host-built MatrixBlocks: SoA diag[7][cells * N] (slots CENTER..TOP, rows
     // cell * N + c), rhs, x0
@@ -266,6 +348,15 @@ public:
         dare_assembly_desc d = functor.Desc();
         check(dare_timestep(sys.get(), field.get(), &d, &p_, &rep_), nullptr, "dare_timestep");
         return rep_.converged ? ReturnType::Converged : ReturnType::Unconverged;
+    }
+    // ... with a composed functor
+    ReturnType TimeStep(Trilinos& sys, Field& field, const MatrixBlock& functor) {
+        sys.Build(field, functor);
+        const ReturnType r = Solve(sys);
+        sys.CopyTo(field);
+        field.ExchangeHaloCells();
+        field.CopyDataVectorsToOldTimeStep();
+        return r;
     }
     int getNumIters() const { return rep_.iters; }
     double achievedTol() const { return rep_.res_abs; }

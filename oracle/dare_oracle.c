@@ -415,6 +415,8 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
             const int face = 2 * d + 1 + side;
             const int on_boundary = side == 0 ? (idx[d] == 0) : (idx[d] == g->n[d] - 1);
             if (!on_boundary) continue;
+            mask &= (uint8_t)~(1u << face);
+            if (a->no_fold) continue;
             const double X = coef[face];
             if (a->bc_type[face - 1] == DOR_BC_DIRICHLET) {
                 coef[DOR_C] -= X;
@@ -423,7 +425,6 @@ static void assemble_cell(const dor_assembly* a, const double dx[3], double V, c
                 coef[DOR_C] += X;
             }
             coef[face] = 0.;
-            mask &= (uint8_t)~(1u << face);
         }
     }
     *rhs_out = rhs;

@@ -58,6 +58,8 @@ typedef struct {
     int bc_type[6];             /* faces W,E,S,N,B,T */
     double bc_value[6];
     int scheme;                 /* time scheme of the Divergence operators: DOR_SCHEME_* */
+    int no_fold;                /* 1: leave the boundary faces unfolded (one term of a composed
+                                   functor, folded by the caller after the last term) */
 } dor_assembly;
 
 /* Time discretisation of the Divergence operators (TimeDiscretizationSchemes.h:29-76):

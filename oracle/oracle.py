@@ -52,6 +52,7 @@ class Assembly(C.Structure):
         ("bc_type", C.c_int * 6),
         ("bc_value", C.c_double * 6),
         ("scheme", C.c_int),
+        ("no_fold", C.c_int),
     ]
 
 
@@ -184,9 +185,10 @@ class AssemblyDesc:
     """Python-side description mirroring ``dor_assembly``; keeps arrays alive."""
 
     def __init__(self, grid: Grid, dt=0.0, D=None, face_D=None, vel=None, face_vel=None,
-                 limiter=LIM_VANLEER, bc=None, scheme=SCHEME_EULER_BACKWARD):
+                 limiter=LIM_VANLEER, bc=None, scheme=SCHEME_EULER_BACKWARD, no_fold=False):
         self.grid = grid
         self.scheme = scheme
+        self.no_fold = no_fold
         self.dt = dt
         self.D = D
         self.face_D = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
@@ -218,6 +220,7 @@ class AssemblyDesc:
                 a.vel[d] = float(self.vel[d])
         a.limiter = self.limiter
         a.scheme = self.scheme
+        a.no_fold = int(self.no_fold)
         for face, (kind, value) in self.bc.items():
             a.bc_type[face - 1] = kind
             a.bc_value[face - 1] = value

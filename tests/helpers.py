@@ -156,3 +156,78 @@ def interleave_csr(csrs):
             vals.append(va[a:b])
     rowptr = np.concatenate([[0], np.cumsum(rows)]).astype(np.int64)
     return rowptr, np.concatenate(cols).astype(np.int64), np.concatenate(vals)
+
+
+# ---- composed functors (dare_assemble_terms) on the oracle -----------------------
+ORACLE_LIM = {"CDS": O.LIM_CDS, "UPWIND": O.LIM_UPWIND, "VANALBADA": O.LIM_VANALBADA, "MINMOD": O.LIM_MINMOD,
+              "VANLEER": O.LIM_VANLEER}
+
+
+def fold_faces(og_n, periodic, dim, diag, rhs, bc):
+    """The boundary folding of counter_diffusion1D.cpp:123-146 on one
+    component's coefficients, faces in the order W, E, S, N, B, T: Dirichlet
+    C -= X, rhs -= 2 bc X; Neumann C += X; the face's coefficient removed."""
+    n = list(og_n) + [1] * (3 - len(og_n))
+    idx = np.indices(n).reshape(3, -1)
+    for d in range(dim):
+        if periodic[d]:
+            continue
+        for side in (0, 1):
+            face = 2 * d + 1 + side
+            on = idx[d] == 0 if side == 0 else idx[d] == n[d] - 1
+            X = diag[face][on].copy()
+            kind, value = bc[face]
+            if kind == O.BC_DIRICHLET:
+                diag[0][on] -= X
+                rhs[on] -= 2. * value * X
+            else:
+                diag[0][on] += X
+            diag[face][on] = 0.0
+    return diag, rhs
+
+
+def oracle_terms(og, case, terms, phis, olds, bcs):
+    """A composed functor on the oracle, per component: each term's unfolded
+    contribution (the oracle's parts enter as DDT +, convection +, diffusion -,
+    i.e. mb -= div(D grad)) combined in order -- SET starts afresh, ADD adds,
+    SUB adds the negative (MatrixBlock_Cartesian.inl:480-593) -- then the
+    component's boundary folding.  Returns diag (7, ncell * N) and rhs with
+    rows cell * N + c, as the system exports them, the per-component
+    coefficients and the pattern mask."""
+    N = len(phis)
+    dim = len(case["n"])
+    per = list(case.get("periodic") or [0] * dim) + [0] * (3 - dim)
+    neutral = {f: (O.BC_NEUMANN, 0.0) for f in range(1, 7)}
+    diags, rhss = [], []
+    for c in range(N):
+        acc_d = acc_r = None
+        for t in terms:
+            if t["component"] not in (-1, c):
+                continue
+            kind = t["kind"]
+            desc = O.AssemblyDesc(og, dt=t.get("dt", 0.0) if kind == "DDT" else 0.0,
+                                  D=t.get("D", 1.0) if kind == "DIFFUSION" else None,
+                                  vel=t.get("vel") if kind == "CONVECTION" else None,
+                                  limiter=ORACLE_LIM[t.get("limiter", "VANLEER")], bc=neutral, no_fold=True)
+            d, r, mask = O.assemble(desc, np.ascontiguousarray(phis[c]), np.ascontiguousarray(olds[c]))
+            native = -1.0 if kind == "DIFFUSION" else 1.0
+            want = -1.0 if t["op"] == "SUB" else 1.0
+            if want != native:
+                d, r = -d, -r
+            if acc_d is None or t["op"] == "SET":
+                acc_d, acc_r = d.copy(), r.copy()
+            else:
+                acc_d += d
+                acc_r += r
+        ncell = int(np.prod(case["n"]))
+        if acc_d is None:
+            acc_d, acc_r = np.zeros((7, ncell)), np.zeros(ncell)
+        acc_d, acc_r = fold_faces(case["n"], per, dim, acc_d, acc_r, bcs[c])
+        diags.append(acc_d)
+        rhss.append(acc_r)
+    ncell = diags[0].shape[1]
+    diag = np.stack(diags, axis=-1).reshape(7, ncell * N)
+    rhs = np.stack(rhss, axis=-1).reshape(-1)
+    ghost = np.zeros(int(np.prod(O.ghosted_shape(og))))
+    mask = O.assemble(O.AssemblyDesc(og, dt=1.0, bc=neutral), ghost)[2]   # the pattern: removed boundary faces
+    return diag, rhs, (diags, rhss), mask
