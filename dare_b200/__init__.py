@@ -43,7 +43,8 @@ KERNEL_IDS = {"assemble": 0, "step1": 3, "step2": 4, "step3": 5, "step4": 6, "st
 class GridInfo(C.Structure):
     _fields_ = [("dim", C.c_int), ("num_ghost", C.c_int), ("n", C.c_int64 * 3), ("n_ghosted", C.c_int64 * 3),
                 ("num_cells", C.c_int64), ("num_cells_ghosted", C.c_int64), ("dx", C.c_double * 3),
-                ("volume", C.c_double), ("area", C.c_double * 3), ("periodic", C.c_int * 3)]
+                ("volume", C.c_double), ("area", C.c_double * 3), ("periodic", C.c_int * 3),
+                ("staggered", C.c_int * 3), ("origin", C.c_double * 3)]
 
 
 class AssemblyDesc(C.Structure):
@@ -93,6 +94,8 @@ _SIGS = [
     ("dare_ctx_timer_stop", C.c_int, [_P, C.POINTER(C.c_double)]),
     ("dare_grid_create", C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int,
                                    C.POINTER(C.c_int), C.POINTER(_P)]),
+    ("dare_grid_create_staggered", C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_double), C.c_int,
+                                             C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_P)]),
     ("dare_grid_destroy", C.c_int, [_P]),
     ("dare_grid_get_info", C.c_int, [_P, C.POINTER(GridInfo)]),
     ("dare_field_create", C.c_int, [_P, C.c_int, C.POINTER(_P)]),
@@ -290,7 +293,10 @@ class Context:
 class Grid:
     """Cartesian grid on one rank (Grid::Cartesian<Dim> + CartesianRepresentation)."""
 
-    def __init__(self, ctx: Context, n, size=None, num_ghost: int = 2, periodic=None):
+    def __init__(self, ctx: Context, n, size=None, num_ghost: int = 2, periodic=None, staggered=None):
+        """``n`` and ``size`` describe the (base) grid; ``staggered`` (one flag
+        per direction) selects a staggered representation: one more cell
+        along each staggered, non-periodic direction, shifted by half a cell."""
         dim = len(n)
         self.ctx = ctx
         nn = (C.c_int64 * 3)(*(list(n) + [1] * (3 - dim)))
@@ -299,7 +305,12 @@ class Grid:
         pp_ = list(periodic) if periodic is not None else [0] * dim
         pp = (C.c_int * 3)(*([int(x) for x in pp_] + [0] * (3 - dim)))
         h = C.c_void_p()
-        _check(lib().dare_grid_create(ctx.h, dim, nn, ss, num_ghost, pp, C.byref(h)), ctx.h, "grid_create")
+        if staggered is None:
+            _check(lib().dare_grid_create(ctx.h, dim, nn, ss, num_ghost, pp, C.byref(h)), ctx.h, "grid_create")
+        else:
+            st = (C.c_int * 3)(*([int(x) for x in staggered] + [0] * (3 - dim)))
+            _check(lib().dare_grid_create_staggered(ctx.h, dim, nn, ss, num_ghost, pp, st, C.byref(h)), ctx.h,
+                   "grid_create")
         self.h = h
         info = GridInfo()
         lib().dare_grid_get_info(h, C.byref(info))
@@ -318,6 +329,10 @@ class Grid:
     @property
     def dx(self):
         return [self.info.dx[d] for d in range(3)]
+
+    @property
+    def origin(self):
+        return [self.info.origin[d] for d in range(3)]
 
     @property
     def volume(self):

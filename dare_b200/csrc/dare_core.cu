@@ -185,8 +185,8 @@ const char* dare_ctx_last_error(const dare_ctx* ctx) { return ctx ? ctx->last_er
 
 int64_t dare_ctx_launch_count(const dare_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
-int dare_grid_create(dare_ctx* ctx, int dim, const int64_t n[3], const double size[3], int num_ghost,
-                     const int periodic[3], dare_grid** out) {
+int dare_grid_create_staggered(dare_ctx* ctx, int dim, const int64_t n[3], const double size[3], int num_ghost,
+                               const int periodic[3], const int staggered[3], dare_grid** out) {
     if (!ctx || !out || !n || !size || dim < 1 || dim > 3 || num_ghost < 2)
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_grid_create: bad arguments (dim 1..3, num_ghost >= 2)");
     *out = nullptr;
@@ -196,14 +196,18 @@ int dare_grid_create(dare_ctx* ctx, int dim, const int64_t n[3], const double si
     int64_t total = 1, total_g = 1;
     for (int d = 0; d < 3; d++) {
         const bool active = d < dim;
-        const int64_t nd = active ? n[d] : 1;
+        const int64_t nb = active ? n[d] : 1;
         // CartesianMesh.inl:60-69: resolution must exceed the ghost count
-        if (active && (nd <= num_ghost || nd > (1 << 30)))
+        if (active && (nb <= num_ghost || nb > (1 << 30)))
             return set_error(ctx, DARE_ERR_BAD_ARG, "dare_grid_create: resolution must be > num_ghost");
+        g.periodic[d] = active && periodic ? (periodic[d] != 0) : 0;
+        // CartesianRepresentation.inl:67-76: a staggered direction gains the
+        // cell at its upper end, on non-periodic grids only
+        g.staggered[d] = active && staggered ? (staggered[d] != 0) : 0;
+        const int64_t nd = nb + (g.staggered[d] && !g.periodic[d] ? 1 : 0);
         g.n[d] = (int)nd;
         g.og[d] = active ? num_ghost : 0;
         g.gn[d] = (int)(nd + 2 * g.og[d]);
-        g.periodic[d] = active && periodic ? (periodic[d] != 0) : 0;
         total *= nd;
         total_g *= g.gn[d];
     }
@@ -211,19 +215,25 @@ int dare_grid_create(dare_ctx* ctx, int dim, const int64_t n[3], const double si
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_grid_create: grid exceeds 2^31 ghosted cells");
     g.ncell = total;
     g.ncell_ghosted = total_g;
-    // CartesianMesh.inl:75-83
+    // CartesianMesh.inl:75-83: the cell width of the base grid
     double vol = 1.;
     for (int d = 0; d < 3; d++) g.dx[d] = 1.;
     for (int d = 0; d < dim; d++) g.dx[d] = size[d] / (double)n[d];
     for (int d = 0; d < dim; d++) vol *= g.dx[d];
     for (int d = 0; d < 3; d++) g.area[d] = d < dim ? vol / g.dx[d] : 0.;
     g.volume = vol;
+    for (int d = 0; d < 3; d++) g.origin[d] = g.staggered[d] && !g.periodic[d] ? -g.dx[d] * 0.5 : 0.;
     dare_grid* gr = new (std::nothrow) dare_grid();
     if (!gr) return DARE_ERR_OOM;
     gr->ctx = ctx;
     gr->dev = g;
     *out = gr;
     return DARE_OK;
+}
+
+int dare_grid_create(dare_ctx* ctx, int dim, const int64_t n[3], const double size[3], int num_ghost,
+                     const int periodic[3], dare_grid** out) {
+    return dare_grid_create_staggered(ctx, dim, n, size, num_ghost, periodic, nullptr, out);
 }
 
 int dare_grid_destroy(dare_grid* g) {
@@ -242,6 +252,8 @@ int dare_grid_get_info(const dare_grid* g, dare_grid_info* info) {
         info->dx[i] = d.dx[i];
         info->area[i] = d.area[i];
         info->periodic[i] = d.periodic[i];
+        info->staggered[i] = d.staggered[i];
+        info->origin[i] = d.origin[i];
     }
     info->num_cells = d.ncell;
     info->num_cells_ghosted = d.ncell_ghosted;

@@ -33,6 +33,12 @@ struct GridDev {             // passed by value to kernels
     double dx[3];
     double volume;
     double area[3];
+    // Staggered representation (CartesianRepresentation.inl:33-76): one more
+    // cell along a staggered, non-periodic direction, the cell width of the
+    // base grid, and the domain starting half a cell earlier (origin = -dx/2;
+    // 0 otherwise).
+    int staggered[3];
+    double origin[3];
     // Solver view of a system with several field components: the components
     // are stacked along i (n[0] = ncomp x the grid's n0, ncell likewise), each
     // component's planes wrapping among themselves on a periodic x.

@@ -101,14 +101,14 @@ struct Geometry {
     double off[3] = {0., 0., 0.};
 };
 
-Geometry make_geometry(int dim, const int64_t n[3], const double dn[3], int ng) {
+Geometry make_geometry(int dim, const int64_t n[3], const double dn[3], const double origin[3], int ng) {
     Geometry G;
     G.dim = dim;
     G.ng = ng;
     for (int d = 0; d < dim; d++) {
         G.ext[d] = n[d] + 2 * ng;
         G.dn[d] = dn[d];
-        G.off[d] = 0. - (double)ng * G.dn[d];     // offset_size - num_ghost * dn (VTKOptions_Cartesian.h:160-162)
+        G.off[d] = origin[d] - (double)ng * G.dn[d];   // offset_size - num_ghost * dn (VTKOptions_Cartesian.h:160-162)
     }
     if (dim == 1) {                                 // pseudo 2-D grid for 1-D (VTKOptions_Cartesian.h:172-176)
         G.ext[1] = 1;
@@ -123,13 +123,14 @@ std::string extent_str(const Geometry& G) {
     return os.str();
 }
 
-int write_vtk(int dim, const int64_t n[3], const double dn[3], int num_ghost, const double* const* data,
+int write_vtk(int dim, const int64_t n[3], const double dn[3], const double origin[3], int num_ghost,
+              const double* const* data,
               const char* const* names, int count, const char* base_path, const char* grid_name, int step,
               double time) {
     if (!data || !names || count < 1 || !base_path || !grid_name || !grid_name[0]) return DARE_ERR_BAD_ARG;
     for (int f = 0; f < count; f++)
         if (!data[f] || !names[f] || !names[f][0]) return DARE_ERR_BAD_ARG;
-    const Geometry G = make_geometry(dim, n, dn, num_ghost);
+    const Geometry G = make_geometry(dim, n, dn, origin, num_ghost);
 
     // the grid's ghosted numbering: (i gn1 + j) gn2 + k over its active dims
     int64_t gn[3] = {1, 1, 1};
@@ -237,7 +238,8 @@ extern "C" int dare_vtk_write_host(int dim, const int64_t n[3], const double siz
         nn[d] = n[d];
         dn[d] = size[d] / (double)n[d];  // cell width, CartesianMesh.inl:75-77
     }
-    return write_vtk(dim, nn, dn, num_ghost, data, names, count, base_path, grid_name, step, time);
+    const double origin[3] = {0., 0., 0.};
+    return write_vtk(dim, nn, dn, origin, num_ghost, data, names, count, base_path, grid_name, step, time);
 }
 
 extern "C" int dare_vtk_write(dare_field* const* fields, int level, const char* const* names, int count,
@@ -263,7 +265,7 @@ extern "C" int dare_vtk_write(dare_field* const* fields, int level, const char* 
         n[k] = d.n[k];
         dn[k] = d.dx[k];
     }
-    const int rc = write_vtk(d.dim, n, dn, d.ng, ptr.data(), names, count, base_path, grid_name, step, time);
+    const int rc = write_vtk(d.dim, n, dn, d.origin, d.ng, ptr.data(), names, count, base_path, grid_name, step, time);
     if (rc) return dare_gpu::set_error(ctx, rc, "dare_vtk_write: cannot write to the output path");
     return DARE_OK;
 }

@@ -100,6 +100,8 @@ typedef struct {
     double volume;
     double area[3];
     int periodic[3];
+    int staggered[3];          /* staggered representation (dare_grid_create_staggered) */
+    double origin[3];          /* position of the lower face of internal cell 0 (-dx/2 when staggered) */
 } dare_grid_info;
 
 /* Assembly description: the composed user functor of the reference's time
@@ -202,6 +204,15 @@ DARE_API int dare_ctx_timer_stop(dare_ctx* ctx, double* ms);
  *      Grid/Cartesian/CartesianMesh.inl:33-112, CartesianRepresentation.inl:31-227 */
 DARE_API int dare_grid_create(dare_ctx* ctx, int dim, const int64_t n[3], const double size[3],
                      int num_ghost, const int periodic[3], dare_grid** out);
+/* A staggered representation, grid->GetRepresentation(Options)
+ * (CartesianRepresentation.inl:33-76): n[] and size[] describe the base grid;
+ * along every direction with staggered[d] != 0 that is not periodic the
+ * representation has n[d] + 1 cells of the base width size[d] / n[d], the
+ * first one centred on the base grid's lower face (origin -dx/2).  Fields,
+ * systems and solves on it work as on any grid. */
+DARE_API int dare_grid_create_staggered(dare_ctx* ctx, int dim, const int64_t n[3], const double size[3],
+                                        int num_ghost, const int periodic[3], const int staggered[3],
+                                        dare_grid** out);
 DARE_API int dare_grid_destroy(dare_grid* g);
 DARE_API int dare_grid_get_info(const dare_grid* g, dare_grid_info* info);
 
