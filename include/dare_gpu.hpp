@@ -63,19 +63,22 @@ private:
 // Grid::Cartesian<Dim> with its representation (np = 1, not staggered).
 class Cartesian {
 public:
+    // staggered: the representation grid->GetRepresentation(Options(staggered...))
+    // (CartesianRepresentation.inl:33-76); empty for the cell-centred one
     Cartesian(Context& ctx, std::vector<int64_t> resolution, std::vector<double> size, int num_ghost = 2,
-              std::vector<int> periodic = {})
+              std::vector<int> periodic = {}, std::vector<int> staggered = {})
         : ctx_(&ctx) {
         const int dim = (int)resolution.size();
         int64_t n[3] = {1, 1, 1};
         double s[3] = {1., 1., 1.};
-        int p[3] = {0, 0, 0};
+        int p[3] = {0, 0, 0}, st[3] = {0, 0, 0};
         for (int d = 0; d < dim && d < 3; d++) {
             n[d] = resolution[d];
             s[d] = d < (int)size.size() ? size[d] : 1.;
             p[d] = d < (int)periodic.size() ? periodic[d] : 0;
+            st[d] = d < (int)staggered.size() ? staggered[d] : 0;
         }
-        check(dare_grid_create(ctx.get(), dim, n, s, num_ghost, p, &h_), ctx.get(), "dare_grid_create");
+        check(dare_grid_create_staggered(ctx.get(), dim, n, s, num_ghost, p, st, &h_), ctx.get(), "dare_grid_create");
         check(dare_grid_get_info(h_, &info_), ctx.get(), "dare_grid_get_info");
     }
     ~Cartesian() {
