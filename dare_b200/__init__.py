@@ -167,6 +167,8 @@ _SIGS += [
     ("dare_learned_params_default", None, [C.POINTER(LearnedParams)]),
     ("dare_unet_create", C.c_int, [_P, C.POINTER(C.c_int), C.c_uint64, C.POINTER(_P)]),
     ("dare_unet_create_coarse", C.c_int, [_P, C.POINTER(C.c_int), C.c_uint64, C.POINTER(_P)]),
+    ("dare_unet_set_wait_limit", C.c_int, [_P, C.c_int64]),
+    ("dare_unet_debug_skip_plane", C.c_int, [_P]),
     ("dare_unet_system_shape", C.c_int, [_P, C.POINTER(C.c_int)]),
     ("dare_unet_destroy", C.c_int, [_P]),
     ("dare_unet_num_params", C.c_int64, [_P]),
@@ -740,6 +742,14 @@ class LearnedPreconditioner:
         for k, v in kw.items():
             setattr(p, k, v)
         return p
+
+    def set_wait_limit(self, polls: int = 0):
+        """Polls of the convolutions' role-to-role waits (0: the default)."""
+        _check(lib().dare_unet_set_wait_limit(self.h, int(polls)), self.ctx.h, "unet_set_wait_limit")
+
+    def debug_skip_plane(self):
+        """Test hook: the next forward convolution's first CTA leaves one plane unstaged."""
+        _check(lib().dare_unet_debug_skip_plane(self.h), self.ctx.h, "unet_debug_skip_plane")
 
     def get_weights(self) -> np.ndarray:
         w = np.empty(self.num_params, dtype=np.float32)

@@ -166,13 +166,20 @@ struct FwdArgs {
     int ppc;
     int slots;       // ring depth (shared-memory slots of staged planes)
     int* err;
+    uint32_t wait_limit;   // polls of the role-to-role waits (role_wait)
+    int skip_plane;        // test hook: CTA 0 leaves its first plane unstaged
 };
 
-// Bounded mbarrier wait that also gives up when another role has aborted.
+// Bounded mbarrier wait between the roles of a CTA (producer, MMA issuer,
+// epilogue) that also gives up when another role has aborted.  `limit` polls
+// (the network's run-time wait limit, kWaitLimit by default).  The waits of a
+// role for its own asynchronous work (its MMAs, its copies in flight) keep
+// the default limit, so an aborting CTA still releases TMEM and shared memory
+// only after that work has landed.
 __device__ __forceinline__ bool role_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
-                                          int code) {
+                                          int code, uint32_t limit) {
     const uint32_t addr = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; it++) {
+    for (uint32_t it = 0; it < limit; it++) {
         if (mbar_try_wait(addr, parity)) return true;
         if ((it & 63) == 63 && *abort_flag) return false;
     }
@@ -315,16 +322,29 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
         if (lane == 0) {
             const uint32_t bytes = (uint32_t)KC * RP * 16;
             uint32_t eph = 0xFFu;  // parity of the next wait on empty[s] (fresh slots pass)
+            uint32_t armed = 0, apar = 0;  // slots armed so far; parity of each slot's next full phase
+            // test hook (dare_unet_debug_skip_plane): the first CTA leaves its
+            // first plane unstaged -- no arrive, no copies -- so the MMA
+            // issuer's bounded wait for it runs out and the CTA aborts
+            const bool skip = a.skip_plane && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
             for (int p = I0 - 1; p <= I1 + 1; p++) {
                 const int sl = p % S;
-                if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 5)) break;
+                if (!role_wait(&empty[sl], (eph >> sl) & 1u, abort_flag, a.err, 5, a.wait_limit)) break;
                 eph ^= 1u << sl;
+                if (skip && p == I0 - 1) continue;
                 mbar_arrive_expect_tx(&full[sl], bytes);
+                armed |= 1u << sl;
+                apar ^= 1u << sl;
                 const int64_t y0 = (int64_t)p * g.plane + pbase;
                 for (int kc = 0; kc < KC; kc++)
                     bulk_load(slots + sl * SB + (size_t)kc * RP * 16, a.in + act_off(g.total, y0, kc),
                               (uint32_t)RP * 16, &full[sl]);
             }
+            // the copies in flight land before the CTA releases its shared
+            // memory: wait for the last phase armed on every slot (already
+            // complete unless the CTA is aborting)
+            for (int sl = 0; sl < S; sl++)
+                if ((armed >> sl) & 1u) mbar_wait(&full[sl], ((apar >> sl) & 1u) ^ 1u, nullptr, 0);
         }
         __syncwarp();
     } else if (warp >= 5) {
@@ -341,10 +361,10 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
                 const int buf = (I - I0) & 1;
                 for (int p = (I == I0 ? I0 - 1 : I + 1); p <= I + 1 && ok; p++) {
                     const int sp = p % S;
-                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 6);
+                    ok = role_wait(&full[sp], (fph >> sp) & 1u, abort_flag, a.err, 6, a.wait_limit);
                     fph ^= 1u << sp;
                 }
-                if (ok) ok = role_wait(&acce[buf], (aph >> buf) & 1u, abort_flag, a.err, 7);
+                if (ok) ok = role_wait(&acce[buf], (aph >> buf) & 1u, abort_flag, a.err, 7, a.wait_limit);
                 aph ^= 1u << buf;
                 if (!ok) break;
                 fence_after_sync();
@@ -404,7 +424,7 @@ __global__ void __launch_bounds__(fwd_threads(MT)) k_conv_fwd(FwdArgs a) {
         uint32_t fph = 0;
         for (int I = I0; I <= I1; I++) {
             const int buf = (I - I0) & 1;
-            const bool ok = role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 9);
+            const bool ok = role_wait(&accf[buf], (fph >> buf) & 1u, abort_flag, a.err, 9, a.wait_limit);
             if (epi_any(!ok)) break;  // the four warps leave together
             fph ^= 1u << buf;
             fence_after_sync();
@@ -560,6 +580,7 @@ struct InArgs {
     float pool_scale;
     int ppc;            // even: a CTA's output planes start on an odd plane I and pair up
     int* err;
+    uint32_t wait_limit;   // polls of the role-to-role waits (role_wait)
     CUtensorMap x;      // FP32 input [n0][n1][pitch >= n2], boxes kInBoxK x (16 MT + 3) x kInB
 };
 
@@ -642,7 +663,7 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
             int q = 0;
             for (; q < ng; q++) {
                 const int sl = q % kInRaw;
-                if (!role_wait(&rawe[sl], ((q / kInRaw) & 1) ^ 1, abort_flag, a.err, 11)) break;
+                if (!role_wait(&rawe[sl], ((q / kInRaw) & 1) ^ 1, abort_flag, a.err, 11, a.wait_limit)) break;
                 mbar_arrive_expect_tx(&rawf[sl], kInB * BOXP);
                 tma_load_3d(raw + sl * RAWS, &a.x, 8 * kb - 4, 16 * MT * jb - 1, I0 - 2 + kInB * q, &rawf[sl]);
             }
@@ -655,8 +676,8 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
         const int bt = tid - 9 * 32;
         for (int q = 0; q < ng; q++) {
             const int sr = q % kInRaw, sw = q % kInWin;
-            bool ok = role_wait(&rawf[sr], (q / kInRaw) & 1, abort_flag, a.err, 12);
-            if (ok) ok = role_wait(&empty[sw], ((q / kInWin) & 1) ^ 1, abort_flag, a.err, 12);
+            bool ok = role_wait(&rawf[sr], (q / kInRaw) & 1, abort_flag, a.err, 12, a.wait_limit);
+            if (ok) ok = role_wait(&empty[sw], ((q / kInWin) & 1) ^ 1, abort_flag, a.err, 12, a.wait_limit);
             if (!__all_sync(0xffffffffu, ok)) break;  // the warp leaves together (__syncwarp below)
             const float* x = reinterpret_cast<const float*>(raw + sr * RAWS);
             uint8_t* wp = win + sw * kInB * WINB;
@@ -685,8 +706,8 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
             bool ok = true;
             for (int q = 0; q < ng && ok; q++) {
                 const int sw = q % kInWin, ab = q & (kInAcc - 1);
-                ok = role_wait(&full[sw], (q / kInWin) & 1, abort_flag, a.err, 13);
-                if (ok) ok = role_wait(&acce[ab], ((q / kInAcc) & 1) ^ 1, abort_flag, a.err, 14);
+                ok = role_wait(&full[sw], (q / kInWin) & 1, abort_flag, a.err, 13, a.wait_limit);
+                if (ok) ok = role_wait(&acce[ab], ((q / kInAcc) & 1) ^ 1, abort_flag, a.err, 14, a.wait_limit);
                 if (!ok) break;
                 fence_after_sync();
 #pragma unroll
@@ -721,7 +742,7 @@ __global__ void __launch_bounds__(in_threads()) k_conv_in(const __grid_constant_
         float pooled[MT][8];  // 2x2 sum of the first (odd) plane of a pair, on the lanes with j, k even
         for (int q = 0; q < ng; q++) {
             const int ab = q & (kInAcc - 1);
-            const bool okw = role_wait(&accf[ab], (q / kInAcc) & 1, abort_flag, a.err, 17);
+            const bool okw = role_wait(&accf[ab], (q / kInAcc) & 1, abort_flag, a.err, 17, a.wait_limit);
             if (!__all_sync(0xffffffffu, okw)) break;  // tcgen05.ld below is warp-collective
             fence_after_sync();
             uint32_t r[kInB][MT][3][8];
@@ -813,6 +834,7 @@ struct OutArgs {
     const float* res32; // added to the output (may be null)
     int ppc, slots;
     int* err;
+    uint32_t wait_limit;   // polls of the role-to-role waits (role_wait)
 };
 
 // 4 epilogue warps, producer, one MMA warp per M tile
@@ -892,9 +914,10 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
         // I1 + 1 in the last group are not copied (their slot keeps stale
         // rows whose accumulators are never read) ----
         if (lane == 0) {
-            for (int q = 0; q < ng; q++) {
+            int q = 0;
+            for (; q < ng; q++) {
                 const int sl = q % S;
-                if (!role_wait(&empty[sl], ((q / S) & 1) ^ 1, abort_flag, a.err, 21)) break;
+                if (!role_wait(&empty[sl], ((q / S) & 1) ^ 1, abort_flag, a.err, 21, a.wait_limit)) break;
                 const int nb = min(kOutB, np - kOutB * q);
                 mbar_arrive_expect_tx(&full[sl], (uint32_t)nb * 2u * RP * 16);
                 for (int b = 0; b < nb; b++) {
@@ -904,6 +927,8 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
                                   a.in + act_off(g.total, y0, kc), (uint32_t)RP * 16, &full[sl]);
                 }
             }
+            // the copies in flight land before the CTA releases its shared memory
+            for (int r = max(0, q - S); r < q; r++) mbar_wait(&full[r % S], (r / S) & 1, nullptr, 0);
         }
         __syncwarp();
     } else if (warp >= 5) {
@@ -917,8 +942,8 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
             bool ok = true;
             for (int q = 0; q < ng && ok; q++) {
                 const int sl = q % S, ag = q & (kOutG - 1);
-                ok = role_wait(&full[sl], (q / S) & 1, abort_flag, a.err, 22);
-                if (ok) ok = role_wait(&acce[ag], ((q / kOutG) & 1) ^ 1, abort_flag, a.err, 23);
+                ok = role_wait(&full[sl], (q / S) & 1, abort_flag, a.err, 22, a.wait_limit);
+                if (ok) ok = role_wait(&acce[ag], ((q / kOutG) & 1) ^ 1, abort_flag, a.err, 23, a.wait_limit);
                 if (!ok) break;
                 fence_after_sync();
 #pragma unroll
@@ -962,7 +987,7 @@ __global__ void __launch_bounds__(out_threads(MT)) k_conv_out(OutArgs a) {
         float cur[MT][3] = {}, nxt[MT][3] = {};
         for (int q = 0; q < ng; q++) {
             const int ag = q & (kOutG - 1);
-            const bool okw = role_wait(&accf[ag], (q / kOutG) & 1, abort_flag, a.err, 25);
+            const bool okw = role_wait(&accf[ag], (q / kOutG) & 1, abort_flag, a.err, 25, a.wait_limit);
             if (epi_any(!okw)) break;  // the four warps leave together
             fence_after_sync();
             uint32_t r[kOutB][MT][16];
@@ -1023,6 +1048,7 @@ struct WgrArgs {
     int ppc, tpg;
     uint32_t cols;
     int* err;
+    uint32_t wait_limit;   // polls of the role-to-role waits (role_wait)
 };
 
 template <int C>
@@ -1828,6 +1854,7 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
         a.cg = net->geo[1];
         a.pool_scale = 0.125f;
         a.err = net->err;
+        a.wait_limit = net->wait_limit;
         return launch_in(net->ctx, L.fwd, a, in32, net->X0);
     }
     if (l == DEC0) {
@@ -1838,6 +1865,7 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
         a.out32 = out32;
         a.res32 = res32;
         a.err = net->err;
+        a.wait_limit = net->wait_limit;
         return launch_out(net->ctx, L.fwd, a);
     }
     FwdArgs a{};
@@ -1849,6 +1877,9 @@ static int conv_forward(dare_unet* net, int l, const bf16* in, const float* in32
     a.out = out;
     a.fine = fine;
     a.err = net->err;
+    a.wait_limit = net->wait_limit;
+    a.skip_plane = net->debug_skip;   // one-shot test hook
+    net->debug_skip = 0;
     return launch_fwd(net->ctx, L.fwd, L.cink, L.nt, L.coutk / L.nt, outm, a);
 }
 
@@ -1864,6 +1895,7 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
         a.cg = net->geo[1];
         a.pool_scale = 1.f;
         a.err = net->err;
+        a.wait_limit = net->wait_limit;
         return launch_in(net->ctx, L.bwd, a, dy32, net->X0);
     }
     FwdArgs a{};
@@ -1873,6 +1905,7 @@ static int conv_dgrad(dare_unet* net, int l, const bf16* dy, const float* dy32, 
     a.cout = L.cink;
     a.out = dx;
     a.err = net->err;
+    a.wait_limit = net->wait_limit;
     return launch_fwd(net->ctx, L.bwd, L.coutk, L.ntb, L.cink / L.ntb, OUT_STORE, a);
 }
 
@@ -2029,11 +2062,17 @@ static int pack_weights(dare_unet* net) {
     return DARE_OK;
 }
 
+// Reads the device error word of the launches so far; a reported time-out is
+// cleared, so the network stays usable for the next call.
 static int check_err(dare_unet* net) {
     int e = 0;
     DARE_CUDA(net->ctx, cudaMemcpyAsync(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost, net->ctx->stream));
     DARE_CUDA(net->ctx, cudaStreamSynchronize(net->ctx->stream));
-    if (e) return set_error(net->ctx, DARE_ERR_CUDA, "unet: a tensor-core wait timed out (code " + std::to_string(e) + ")");
+    if (e) {
+        DARE_CUDA(net->ctx, cudaMemsetAsync(net->err, 0, sizeof(int), net->ctx->stream));
+        return set_error(net->ctx, DARE_ERR_TIMEOUT,
+                         "unet: a tensor-core wait timed out (code " + std::to_string(e) + ")");
+    }
     return DARE_OK;
 }
 
@@ -2267,6 +2306,18 @@ int dare_unet_system_shape(const dare_unet* net, int n[3]) {
     if (!net || !n) return DARE_ERR_BAD_ARG;
     for (int d = 0; d < 3; d++) n[d] = net->coarse ? net->fine[d] : net->n[d];
     return net->coarse;
+}
+
+int dare_unet_set_wait_limit(dare_unet* net, int64_t polls) {
+    if (!net || polls < 0 || polls > 0xFFFFFFFFll) return DARE_ERR_BAD_ARG;
+    net->wait_limit = polls == 0 ? kWaitLimit : (uint32_t)polls;
+    return DARE_OK;
+}
+
+int dare_unet_debug_skip_plane(dare_unet* net) {
+    if (!net) return DARE_ERR_BAD_ARG;
+    net->debug_skip = 1;
+    return DARE_OK;
 }
 
 int dare_unet_destroy(dare_unet* net) {

@@ -161,6 +161,8 @@ struct dare_unet {
     size_t part_floats = 0;
     double* dscal = nullptr;              // [0] loss accumulator
     int* err = nullptr;                   // device error word (bounded waits)
+    uint32_t wait_limit = 1u << 22;       // polls of the role-to-role waits (= tc::kWaitLimit; dare_unet_set_wait_limit)
+    int debug_skip = 0;                   // one-shot test hook (dare_unet_debug_skip_plane)
     // training ring of (residual, error) pairs
     float* ring_r = nullptr;
     float* ring_e = nullptr;

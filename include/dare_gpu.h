@@ -35,6 +35,7 @@ extern "C" {
 #define DARE_ERR_OOM (-3)
 #define DARE_ERR_STATE (-4)
 #define DARE_ERR_UNSUPPORTED (-5)
+#define DARE_ERR_TIMEOUT (-6)       /* a bounded device wait ran out (the call returned; the context stays usable) */
 
 /* ---- neighbour slots: CartesianNeighbor (Grid/Cartesian/CartesianMesh.h:67-77) */
 #define DARE_CENTER 0
@@ -443,6 +444,18 @@ DARE_API int dare_unet_create_coarse(dare_ctx* ctx, const int n_fine[3], uint64_
  * full-resolution form, < 0 on a bad argument.  No reference counterpart. */
 DARE_API int dare_unet_system_shape(const dare_unet* net, int n[3]);
 DARE_API int dare_unet_destroy(dare_unet* net);
+/* Polls after which a bounded wait between the roles of a tensor-core
+ * convolution CTA (producer, MMA issuer, epilogue) gives up: the CTA raises
+ * its abort flag, waits for its own MMAs and copies in flight, frees its
+ * tensor memory and returns; the call then reports DARE_ERR_TIMEOUT and the
+ * network stays usable.  0 restores the default (2^22 polls).  No reference
+ * counterpart. */
+DARE_API int dare_unet_set_wait_limit(dare_unet* net, int64_t polls);
+/* Test hook for that failure path: in the next forward convolution of 16 or
+ * more input channels, the first CTA's producer leaves its first input plane
+ * unstaged (no arrive, no copies), so that CTA's bounded waits run out.  One
+ * shot.  No reference counterpart. */
+DARE_API int dare_unet_debug_skip_plane(dare_unet* net);
 DARE_API int64_t dare_unet_num_params(const dare_unet* net);
 DARE_API int dare_unet_get_weights(dare_unet* net, float* host, int64_t count);
 DARE_API int dare_unet_set_weights(dare_unet* net, const float* host, int64_t count);

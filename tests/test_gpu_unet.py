@@ -307,3 +307,34 @@ def test_coarse_learned_solver(ctx):
     print({"loss_first": first, "loss_last": last, "iters": its})
     assert last < first
     assert sum(its["trained"]) <= sum(its["identity"])
+
+
+def test_bounded_wait_times_out_and_the_network_recovers(ctx):
+    """Failure detection without a GPU fault.  A one-shot test hook leaves one
+    input plane of one CTA of the next forward convolution unstaged, so that
+    CTA's MMA issuer waits for a phase that never completes.  With a short
+    run-time limit (1000 polls) the wait runs out: the CTA raises its abort
+    flag, its roles leave their loops, it waits for its own work in flight,
+    frees its tensor memory and returns.  The call reports DARE_ERR_TIMEOUT
+    with the message on the context, and the next call on the same network
+    and context gives the correct output bit for bit (its CTAs allocate
+    tensor memory again, so none was left held)."""
+    import dare_b200 as D
+    torch = _torch()
+    n = (16, 24, 32)
+    net = D.LearnedPreconditioner(ctx, n, seed=3)
+    net.set_weights(_weights(15, net.num_params))
+    N = int(np.prod(n))
+    u = torch.randn(N, generator=torch.Generator().manual_seed(4), dtype=torch.float32).cuda()
+    z0, z1, z2 = (torch.empty_like(u) for _ in range(3))
+    net.apply(u.data_ptr(), z0.data_ptr())
+    net.set_wait_limit(1000)
+    net.debug_skip_plane()
+    with pytest.raises(D.DareError) as err:
+        net.apply(u.data_ptr(), z1.data_ptr())
+    assert "timed out" in str(err.value) and "status -6" in str(err.value)
+    assert "timed out" in D.lib().dare_ctx_last_error(ctx.h).decode()
+    net.set_wait_limit(0)
+    net.apply(u.data_ptr(), z2.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(z2, z0)
