@@ -133,6 +133,22 @@ _SIGS = [
     ("dare_timestep", C.c_int, [_P, _P, C.POINTER(AssemblyDesc), C.POINTER(SolverParams),
                                 C.POINTER(SolveReport)]),
     ("dare_face_average", C.c_int, [_P, _P, C.POINTER(_P)]),
+    ("dare_slabs_create", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P)]),
+    ("dare_slabs_destroy", C.c_int, [_P]),
+    ("dare_slabs_count", C.c_int, [_P]),
+    ("dare_slabs_range", C.c_int, [_P, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    ("dare_slabs_system", _P, [_P, C.c_int]),
+    ("dare_slabs_field", _P, [_P, C.c_int]),
+    ("dare_slabs_set_bc", C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
+    ("dare_slabs_scatter", C.c_int, [_P, _P]),
+    ("dare_slabs_gather", C.c_int, [_P, _P]),
+    ("dare_slabs_exchange_halo", C.c_int, [_P]),
+    ("dare_slabs_copy_to_old", C.c_int, [_P]),
+    ("dare_slabs_assemble", C.c_int, [_P, C.POINTER(AssemblyDesc)]),
+    ("dare_slabs_solve", C.c_int, [_P, C.POINTER(SolverParams), C.POINTER(SolveReport)]),
+    ("dare_slabs_copy_to", C.c_int, [_P]),
+    ("dare_slabs_timestep", C.c_int, [_P, C.POINTER(AssemblyDesc), C.POINTER(SolverParams),
+                                      C.POINTER(SolveReport)]),
     ("dare_residual_norm_noalloc", C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int), _P, _P, _P, _P,
                                              _P, C.c_char_p, C.c_int]),
     ("dare_batch_create", C.c_int, [_P, C.c_int, _P, C.POINTER(_P)]),
@@ -502,9 +518,9 @@ class MatrixSystem:
         self.rows = grid.num_cells * components
 
     def __del__(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "_owned", True):
             lib().dare_system_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def set_bc(self, face: int, kind: int, value: float = 0.0, component: int = -1):
         """Condition of a face, for every component or for one."""
@@ -592,6 +608,114 @@ class BiCGStab2:
 
     def get_num_iters(self) -> int:
         return self.report["iters"] if self.report else 0
+
+
+class Slabs:
+    """The grid of ``system`` split into slabs of i-planes on its device: the
+    reference's distribution over ranks (CartesianDistribution.h:94-380)
+    with its halo exchange (HaloBuffer.inl:30-208) and a sum over all slabs
+    in every dot product of the solve.  Slab s owns planes ``ranges[s]`` with
+    its own field, rows and solver vectors; boundary planes cross to the x
+    neighbours before every assembly (num_ghost planes of the field) and
+    every SpMV (one plane of the operand).  One field component, FP64."""
+
+    def __init__(self, system: MatrixSystem, num_slabs: int, num_levels: int = 2):
+        self.ctx = system.grid.ctx
+        self.grid = system.grid
+        h = C.c_void_p()
+        _check(lib().dare_slabs_create(system.h, num_slabs, num_levels, C.byref(h)), self.ctx.h, "slabs_create")
+        self.h = h
+        self.count = int(lib().dare_slabs_count(h))
+        self.ranges = []
+        for s in range(self.count):
+            a, b = C.c_int64(), C.c_int64()
+            _check(lib().dare_slabs_range(h, s, C.byref(a), C.byref(b)), self.ctx.h, "slabs_range")
+            self.ranges.append((a.value, b.value))
+        self.periodic_x = bool(self.grid.info.periodic[0])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().dare_slabs_destroy(self.h)
+            self.h = None
+
+    def system(self, s: int) -> MatrixSystem:
+        """Slab s's rows as a MatrixSystem view (coefficients, solution)."""
+        v = MatrixSystem.__new__(MatrixSystem)
+        v._owned = False
+        v.h = C.c_void_p(lib().dare_slabs_system(self.h, s))
+        v.grid = self.grid
+        v.components = 1
+        i0, i1 = self.ranges[s]
+        v.rows = (i1 - i0) * self.grid.n[1] * self.grid.n[2]
+        return v
+
+    def field_ptr(self, s: int, level: int = 0) -> int:
+        return lib().dare_field_device_ptr(lib().dare_slabs_field(self.h, s), level)
+
+    def set_bc(self, face: int, kind: int, value: float = 0.0):
+        _check(lib().dare_slabs_set_bc(self.h, face, kind, value), self.ctx.h, "slabs_set_bc")
+
+    def scatter(self, field: Field):
+        _check(lib().dare_slabs_scatter(self.h, field.h), self.ctx.h, "slabs_scatter")
+
+    def gather(self, field: Field):
+        _check(lib().dare_slabs_gather(self.h, field.h), self.ctx.h, "slabs_gather")
+
+    def exchange_halo(self):
+        _check(lib().dare_slabs_exchange_halo(self.h), self.ctx.h, "slabs_exchange_halo")
+
+    def copy_to_old(self):
+        _check(lib().dare_slabs_copy_to_old(self.h), self.ctx.h, "slabs_copy_to_old")
+
+    def copy_to(self):
+        _check(lib().dare_slabs_copy_to(self.h), self.ctx.h, "slabs_copy_to")
+
+    def face_slices(self, faces):
+        """Each slab's part of the three face arrays of the grid (host arrays
+        of shapes n + e_d): x faces i0 .. i1 (face 0 after the last plane on
+        a periodic x), the slab's planes of the y and z faces."""
+        n0 = self.grid.n[0]
+        out = []
+        for i0, i1 in self.ranges:
+            fx = np.asarray(faces[0])
+            if self.periodic_x and i1 == n0:
+                fx = np.concatenate([fx[i0:n0], fx[0:1]])
+            else:
+                fx = fx[i0:i1 + 1]
+            out.append((np.ascontiguousarray(fx), np.ascontiguousarray(np.asarray(faces[1])[i0:i1]),
+                        np.ascontiguousarray(np.asarray(faces[2])[i0:i1])))
+        return out
+
+    def _descs(self, assemblies):
+        assemblies = list(assemblies)
+        if len(assemblies) != self.count:
+            raise ValueError("one Assembly per slab")
+        arr = (AssemblyDesc * self.count)()
+        for s, a in enumerate(assemblies):
+            arr[s] = a.to_c()
+        return arr
+
+    def assemble(self, assemblies):
+        """Trilinos::Build on every slab (one Assembly per slab, its face
+        arrays from face_slices)."""
+        _check(lib().dare_slabs_assemble(self.h, self._descs(assemblies)), self.ctx.h, "slabs_assemble")
+
+    def solve(self, solver: "BiCGStab2") -> dict:
+        rep = SolveReport()
+        _check(lib().dare_slabs_solve(self.h, C.byref(solver.params), C.byref(rep)), self.ctx.h, "slabs_solve")
+        solver.report = rep.as_dict()
+        return solver.report
+
+    def timestep(self, assemblies, solver: "BiCGStab2") -> dict:
+        rep = SolveReport()
+        _check(lib().dare_slabs_timestep(self.h, self._descs(assemblies), C.byref(solver.params), C.byref(rep)),
+               self.ctx.h, "slabs_timestep")
+        solver.report = rep.as_dict()
+        return solver.report
+
+    def solution(self) -> np.ndarray:
+        """The slabs' solutions in the grid's cell order."""
+        return np.concatenate([self.system(s).solution() for s in range(self.count)])
 
 
 def timestep(system: MatrixSystem, field: Field, assembly: Assembly, solver: BiCGStab2) -> dict:

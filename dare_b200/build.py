@@ -33,6 +33,7 @@ SOURCES = {
     "dare_core.cu": [],
     "dare_assembly.cu": ["--fmad=false"],
     "dare_assembly3.cu": [],
+    "dare_slabs.cu": [],
     "dare_bicgstab2.cu": [],
     "dare_mixed.cu": [],
     "dare_step.cu": [],

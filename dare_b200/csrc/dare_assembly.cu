@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256) k_assemble(GridDev g, AsmParams a, const 
             for (int side = 0; side < 2; side++) {
                 const int face = 2 * d + 1 + side;
                 const bool on_boundary = side == 0 ? (idx[d] == 0) : (idx[d] == g.n[d] - 1);
-                if (!on_boundary) continue;
+                if (!on_boundary || (d == 0 && ((a.xint >> side) & 1))) continue;
                 const double X = coef[face];
                 if (a.bc_type[face - 1] == DARE_BC_DIRICHLET) {
                     coef[DARE_CENTER] -= X;
@@ -320,6 +320,7 @@ static int base_params(dare_system* s, AsmParams& a, const char* who) {
     const GridDev& g = s->grid->dev;
     a.tt = a.dt > 0. ? (g.volume * 1.) / a.dt : 0.;
     a.dstride = s->sdev.ncell;
+    a.xint = s->xint;
     a.nexp = scheme_weights(a.scheme, a.w);
     if (a.nexp < 0) return set_error(ctx, DARE_ERR_BAD_ARG, std::string(who) + ": unknown time scheme");
     for (int d = 0; d < 3; d++) a.dn[d] = 1. / g.dx[d];

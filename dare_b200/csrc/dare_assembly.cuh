@@ -30,6 +30,9 @@ struct AsmParams {
     double sgn_ddt, sgn_conv, sgn_diff;
     int acc;
     int fold;
+    // x ends the system shares with a neighbouring slab (bit 0 the low end,
+    // bit 1 the high end): their faces are interior faces and stay unfolded
+    int xint;
 };
 
 // Weights of the Divergence time schemes (TimeDiscretizationSchemes.h:29-76);

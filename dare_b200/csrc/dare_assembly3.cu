@@ -86,6 +86,7 @@ struct A3Params {
     const double* face_D[3];
     int acc;            // add to the coefficients already in the system
     int fold;           // fold the boundary faces at the end
+    int xint;           // x ends shared with a neighbouring slab (bit 0 low, bit 1 high): not folded
 };
 
 // a / b for normal, finite b by Newton-Raphson refinement of the hardware
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(256, FD ? 2 : 3)
                 for (int side = 0; side < 2; side++) {
                     const int face = 2 * d + 1 + side;
                     const bool on_boundary = side == 0 ? (idx[d] == 0) : (idx[d] == g.n[d] - 1);
-                    if (!on_boundary) continue;
+                    if (!on_boundary || (d == 0 && ((a.xint >> side) & 1))) continue;
                     const double X = coef[face];
                     if (a.bc_type[face - 1] == DARE_BC_DIRICHLET) {
                         coef[0] -= X;
@@ -414,6 +415,7 @@ int launch_assemble3(dare_ctx* ctx, const GridDev& g, const AsmParams& a, const 
     p.diff = a.diffusion;
     p.acc = a.acc;
     p.fold = a.fold;
+    p.xint = a.xint;
     double wsum = 1.;
     for (int t = 1; t <= a.nexp; t++) wsum += a.w[t];
     // the parts' signs enter through their factors: the kernel subtracts the

@@ -50,7 +50,7 @@ namespace dare_gpu {
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem) {
+MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem, int max_items) {
     MarchCfg m;
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     int tk = n2 > 16 ? 32 : n2 > 8 ? 16 : n2 > 4 ? 8 : n2 > 2 ? 4 : 1;
@@ -74,7 +74,7 @@ MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem) {
     const int64_t want = (int64_t)ctx->num_sms * 3 * 4;
     int planes = 32;
     while (planes > 4 && tiles * nc * ((n0c + planes - 1) / planes) < want) planes /= 2;
-    while (tiles * nc * ((n0c + planes - 1) / planes) > kMaxBlocks && planes < n0c) planes *= 2;
+    while (tiles * nc * ((n0c + planes - 1) / planes) > max_items && planes < n0c) planes *= 2;
     if (planes > n0c) planes = n0c;
     m.planes = planes;
     m.cpc = (n0c + planes - 1) / planes;
@@ -133,17 +133,7 @@ template VecsT<float> carve_vecs<float>(float*, int64_t, float*, const float*);
 template <typename T, bool UNIT>
 int launch_init(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const OpT<T>& op, const VecsT<T>& vs,
                 SolverState* st, double* partials) {
-    using F = FInit<T, UNIT>;
-    F f{};
-    f.zs[0] = vs.x;
-    set_coef_streams<T, UNIT, F::NP>(op, f.ps);
-    f.ps[F::NC] = vs.b;
-    f.r = vs.r[0];
-    f.rh = vs.rh;
-    f.u = vs.u[0];
-    f.v = vs.v[0];
-    f.w = vs.w;
-    return launch_march(ctx, g, m, f, st, partials);
+    return launch_march(ctx, g, m, make_init<T, UNIT>(op, vs), st, partials);
 }
 template int launch_init<double, true>(dare_ctx*, const GridDev&, const MarchCfg&, const OpT<double>&,
                                        const VecsT<double>&, SolverState*, double*);
@@ -160,57 +150,17 @@ int launch_iteration(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbl
     const int a = par, b = 1 - par;
     cudaStream_t sm = ctx->stream;
     int rc;
-    using F1 = FStep1<T, UNIT>;
-    using F2 = FStep2<T, UNIT>;
-    using F3 = FStep3<T, UNIT>;
-    using F4 = FStep4<T, UNIT>;
-    constexpr int NC = NCoef<UNIT>::value;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[0], sm));
-    F1 f1{};
-    f1.zs[0] = vs.r[a];
-    f1.zs[1] = vs.u[a];
-    set_coef_streams<T, UNIT, F1::NP>(op, f1.ps);
-    f1.ps[NC] = vs.rh;
-    f1.u_out = vs.u[b];
-    f1.v = vs.v[0];
-    if ((rc = launch_march(ctx, g, m, f1, st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step1<T, UNIT>(op, vs, a, b), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[1], sm));
-    F2 f2{};
-    f2.zs[0] = vs.v[0];
-    f2.zs[1] = vs.r[a];
-    set_coef_streams<T, UNIT, F2::NP>(op, f2.ps);
-    f2.ps[NC] = vs.rh;
-    f2.ps[NC + 1] = vs.u[b];
-    f2.ps[NC + 2] = vs.x;
-    f2.r_out = vs.r[b];
-    f2.s = vs.s[0];
-    f2.x = vs.x;
-    if ((rc = launch_march(ctx, g, m, f2, st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step2<T, UNIT>(op, vs, a, b), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[2], sm));
-    F3 f3{};
-    f3.zs[0] = vs.s[0];
-    f3.zs[1] = vs.v[0];
-    set_coef_streams<T, UNIT, F3::NP>(op, f3.ps);
-    f3.ps[NC] = vs.rh;
-    f3.v_out = vs.v[1];
-    f3.w = vs.w;
-    if ((rc = launch_march(ctx, g, m, f3, st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step3<T, UNIT>(op, vs), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[3], sm));
-    F4 f4{};
-    f4.zs[0] = vs.w;
-    f4.zs[1] = vs.s[0];
-    set_coef_streams<T, UNIT, F4::NP>(op, f4.ps);
-    f4.ps[NC] = vs.r[b];
-    f4.ps[NC + 1] = vs.u[b];
-    f4.ps[NC + 2] = vs.v[1];
-    f4.u = vs.u[b];
-    f4.r = vs.r[b];
-    f4.s_out = vs.s[1];
-    f4.t = vs.t;
-    if ((rc = launch_march(ctx, g, m, f4, st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step4<T, UNIT>(op, vs, b), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[4], sm));
     k_step5<T><<<sblocks, 256, 0, sm>>>(g.ncell, vs.x, vs.r[b], vs.s[1], vs.t, vs.u[b], vs.v[1], vs.w, vs.rh, st,
-                                        partials);
+                                        partials, 0, 0);
     DARE_LAUNCHED(ctx);
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[5], sm));
     return DARE_OK;
@@ -224,12 +174,7 @@ template int launch_iteration<float, true>(dare_ctx*, const GridDev&, const Marc
 
 int launch_true_residual(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const OpT<double>& op,
                          const double* x, const double* b, SolverState* st, double* partials, double* out) {
-    FResidual<double> f{};
-    f.zs[0] = x;
-    set_coef_streams<double, false, 8>(op, f.ps);
-    f.ps[7] = b;
-    f.out = out;
-    return launch_march(ctx, g, m, f, st, partials);
+    return launch_march(ctx, g, m, make_residual(op, x, b, out), st, partials);
 }
 
 int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, double* ahat,
@@ -237,12 +182,7 @@ int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double
     const int eb = grid_blocks(ctx, g.ncell, 256, 8);
     k_invdiag<<<eb, 256, 0, ctx->stream>>>(diag, invd, g.ncell);
     DARE_LAUNCHED(ctx);
-    FFold f{};
-    f.zs[0] = invd;
-    for (int q = 0; q < 6; q++) f.ps[q] = diag + (q + 1) * g.ncell;
-    f.ahat = ahat;
-    f.n = g.ncell;
-    return launch_march(ctx, g, m, f, st, partials);
+    return launch_march(ctx, g, m, make_fold(diag, invd, ahat, g.ncell), st, partials);
 }
 
 int launch_fold32(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, float* ahat32,

@@ -51,6 +51,13 @@ struct MarchCfg {
     size_t smem = 0;
     int cpt = 1;      // cells per thread along k (2: paired 16-byte copies, needs an even n2)
     int cpc = 1;      // plane runs per field component (items: tiles x cpc x components)
+    // Slab decomposition (dare_slabs.cu): the first partial-sum slot of this
+    // launch's items and the items of all launches that share the reduction
+    // (0: this launch alone), and per operand input the planes below the
+    // first and above the last plane of the slab (null: wrap / zero as usual).
+    int item_base = 0;
+    int nitems_total = 0;
+    const void* halo[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
 // ---- deterministic grid reduction -----------------------------------------
@@ -88,20 +95,23 @@ __device__ __forceinline__ void block_sum(double (&v)[Q], double* sh /* [32*Q] *
 
 // Publish this block's partial sums; returns true in the last block to
 // finish, after which tot[] holds the grid-wide sums (fixed summation order,
-// so results are reproducible run to run).
+// so results are reproducible run to run).  `base` / `total`: the block's
+// slot is base + its index, and the sums span `total` slots filled by this
+// and earlier launches (0: this launch's blocks).
 template <int Q>
 __device__ bool grid_reduce(double (&v)[Q], double* __restrict__ partials, unsigned int* counter,
-                            double (&tot)[Q]) {
+                            double (&tot)[Q], int base = 0, int total = 0) {
     __shared__ double sh[32 * kMaxQ];
     __shared__ bool is_last;
+    const int span = total > 0 ? total : blocks_total();
     block_sum<Q>(v, sh);
     const int tid = thread_linear();
     if (tid == 0) {
 #pragma unroll
-        for (int q = 0; q < Q; q++) partials[q * kMaxBlocks + block_linear()] = v[q];
+        for (int q = 0; q < Q; q++) partials[q * kMaxBlocks + base + block_linear()] = v[q];
         __threadfence();
         const unsigned prev = atomicAdd(counter, 1u);
-        is_last = (prev == (unsigned)blocks_total() - 1);
+        is_last = (prev == (unsigned)span - 1);
     }
     __syncthreads();
     if (!is_last) return false;
@@ -110,7 +120,7 @@ __device__ bool grid_reduce(double (&v)[Q], double* __restrict__ partials, unsig
 #pragma unroll
     for (int q = 0; q < Q; q++) a[q] = 0.;
     const int nt = blockDim.x * blockDim.y;
-    for (int b = tid; b < blocks_total(); b += nt) {
+    for (int b = tid; b < span; b += nt) {
 #pragma unroll
         for (int q = 0; q < Q; q++) a[q] += __ldcg(partials + q * kMaxBlocks + b);
     }
@@ -122,7 +132,9 @@ __device__ bool grid_reduce(double (&v)[Q], double* __restrict__ partials, unsig
 }
 
 // ---- host-side launch helpers (dare_bicgstab2.cu) -------------------------
-MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem);
+// `max_items`: the partial-sum slots the launch may use (fewer when several
+// launches share one reduction)
+MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem, int max_items = kMaxBlocks);
 int ensure_solver_ws(dare_system* s);
 
 template <typename T>

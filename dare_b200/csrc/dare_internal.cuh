@@ -102,6 +102,9 @@ struct dare_system {
     // per component, 6 faces each; empty until the first per-component call
     std::vector<int> bc_type_c;
     std::vector<double> bc_value_c;
+    // A slab of a larger grid (dare_slabs.cu): x ends shared with a
+    // neighbouring slab (bit 0 low, bit 1 high), whose faces are not folded.
+    int xint = 0;
     double* diag = nullptr;   // [7][ncomp][ncell], component-major within a slot
     double* rhs = nullptr;    // [ncomp][ncell]
     double* x = nullptr;

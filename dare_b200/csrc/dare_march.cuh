@@ -338,6 +338,95 @@ struct FFold32 {
 };
 
 // ---------------------------------------------------------------------------
+// the functors of the init kernel and of one iteration over the vectors vs
+// (halves a of r / u current, b = 1 - a written), shared by the single-grid
+// and the slab drivers
+// ---------------------------------------------------------------------------
+template <typename T, bool UNIT>
+FInit<T, UNIT> make_init(const OpT<T>& op, const VecsT<T>& vs) {
+    using F = FInit<T, UNIT>;
+    F f{};
+    f.zs[0] = vs.x;
+    set_coef_streams<T, UNIT, F::NP>(op, f.ps);
+    f.ps[F::NC] = vs.b;
+    f.r = vs.r[0];
+    f.rh = vs.rh;
+    f.u = vs.u[0];
+    f.v = vs.v[0];
+    f.w = vs.w;
+    return f;
+}
+template <typename T, bool UNIT>
+FStep1<T, UNIT> make_step1(const OpT<T>& op, const VecsT<T>& vs, int a, int b) {
+    FStep1<T, UNIT> f{};
+    f.zs[0] = vs.r[a];
+    f.zs[1] = vs.u[a];
+    set_coef_streams<T, UNIT, FStep1<T, UNIT>::NP>(op, f.ps);
+    f.ps[NCoef<UNIT>::value] = vs.rh;
+    f.u_out = vs.u[b];
+    f.v = vs.v[0];
+    return f;
+}
+template <typename T, bool UNIT>
+FStep2<T, UNIT> make_step2(const OpT<T>& op, const VecsT<T>& vs, int a, int b) {
+    constexpr int NC = NCoef<UNIT>::value;
+    FStep2<T, UNIT> f{};
+    f.zs[0] = vs.v[0];
+    f.zs[1] = vs.r[a];
+    set_coef_streams<T, UNIT, FStep2<T, UNIT>::NP>(op, f.ps);
+    f.ps[NC] = vs.rh;
+    f.ps[NC + 1] = vs.u[b];
+    f.ps[NC + 2] = vs.x;
+    f.r_out = vs.r[b];
+    f.s = vs.s[0];
+    f.x = vs.x;
+    return f;
+}
+template <typename T, bool UNIT>
+FStep3<T, UNIT> make_step3(const OpT<T>& op, const VecsT<T>& vs) {
+    FStep3<T, UNIT> f{};
+    f.zs[0] = vs.s[0];
+    f.zs[1] = vs.v[0];
+    set_coef_streams<T, UNIT, FStep3<T, UNIT>::NP>(op, f.ps);
+    f.ps[NCoef<UNIT>::value] = vs.rh;
+    f.v_out = vs.v[1];
+    f.w = vs.w;
+    return f;
+}
+template <typename T, bool UNIT>
+FStep4<T, UNIT> make_step4(const OpT<T>& op, const VecsT<T>& vs, int b) {
+    constexpr int NC = NCoef<UNIT>::value;
+    FStep4<T, UNIT> f{};
+    f.zs[0] = vs.w;
+    f.zs[1] = vs.s[0];
+    set_coef_streams<T, UNIT, FStep4<T, UNIT>::NP>(op, f.ps);
+    f.ps[NC] = vs.r[b];
+    f.ps[NC + 1] = vs.u[b];
+    f.ps[NC + 2] = vs.v[1];
+    f.u = vs.u[b];
+    f.r = vs.r[b];
+    f.s_out = vs.s[1];
+    f.t = vs.t;
+    return f;
+}
+inline FResidual<double> make_residual(const OpT<double>& op, const double* x, const double* b, double* out) {
+    FResidual<double> f{};
+    f.zs[0] = x;
+    set_coef_streams<double, false, 8>(op, f.ps);
+    f.ps[7] = b;
+    f.out = out;
+    return f;
+}
+inline FFold make_fold(const double* diag, const double* invd, double* ahat, int64_t n) {
+    FFold f{};
+    f.zs[0] = invd;
+    for (int q = 0; q < 6; q++) f.ps[q] = diag + (q + 1) * n;
+    f.ahat = ahat;
+    f.n = n;
+    return f;
+}
+
+// ---------------------------------------------------------------------------
 // item reduction: partials are indexed by item; the item whose counter
 // increment completes the set sums them in item order.
 // ---------------------------------------------------------------------------
@@ -430,7 +519,9 @@ __device__ __forceinline__ Pair<T> ld_pair(const T* p) {
 // 0.343 / 0.353 ms to 0.408 / 0.433 ms, also when the maximum shared-memory
 // carveout then let three blocks in; that carveout also slowed steps 1 and 3
 // to 0.354 ms, so the default carveout stays).
-template <class K, int CPT = 1>
+// HALO (slabs): the planes before the first and after the last plane of the
+// grid come from m.halo when set.
+template <class K, int CPT = 1, bool HALO = false>
 __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K kern, SolverState* st, double* partials,
                                                                    MarchCfg m) {
     using T = typename K::type;
@@ -530,16 +621,26 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
         for (int z = 0; z < NZ; z++) {
             const T* src = k.zs[z];
             T* zt = sb + z * ZT;
-            cp_async<CB>(zt + (ty + 1) * W + col, src + base + (G.o_c < 0 ? 0 : G.o_c), pv && G.o_c >= 0);
-            if (G.hS) cp_async<CB>(zt + col, src + base + (G.o_s < 0 ? 0 : G.o_s), pv && G.o_s >= 0);
+            int64_t zb = base;
+            bool zv = pv;
+            if constexpr (HALO) {
+                const int hside = p - G.cb < 0 ? 0 : (p - G.cb >= n0c ? 1 : -1);   // a plane past the slab
+                if (hside >= 0 && m.halo[z][hside]) {   // the neighbour's plane, exchanged into a local buffer
+                    src = static_cast<const T*>(m.halo[z][hside]);
+                    zb = 0;
+                    zv = true;
+                }
+            }
+            cp_async<CB>(zt + (ty + 1) * W + col, src + zb + (G.o_c < 0 ? 0 : G.o_c), zv && G.o_c >= 0);
+            if (G.hS) cp_async<CB>(zt + col, src + zb + (G.o_s < 0 ? 0 : G.o_s), zv && G.o_s >= 0);
             if (G.hN)
-                cp_async<CB>(zt + (TJ + 1) * W + col, src + base + (G.o_n < 0 ? 0 : G.o_n), pv && G.o_n >= 0);
+                cp_async<CB>(zt + (TJ + 1) * W + col, src + zb + (G.o_n < 0 ? 0 : G.o_n), zv && G.o_n >= 0);
             if (G.hB)
-                cp_async<sizeof(T)>(zt + (ty + 1) * W + IC - 1, src + base + (G.o_b < 0 ? 0 : G.o_b),
-                                    pv && G.o_b >= 0);
+                cp_async<sizeof(T)>(zt + (ty + 1) * W + IC - 1, src + zb + (G.o_b < 0 ? 0 : G.o_b),
+                                    zv && G.o_b >= 0);
             if (G.hT)
-                cp_async<sizeof(T)>(zt + (ty + 1) * W + IC + TW, src + base + (G.o_t < 0 ? 0 : G.o_t),
-                                    pv && G.o_t >= 0);
+                cp_async<sizeof(T)>(zt + (ty + 1) * W + IC + TW, src + zb + (G.o_t < 0 ? 0 : G.o_t),
+                                    zv && G.o_t >= 0);
         }
         if (full && G.inside) {
             T* pt = sb + NZ * ZT + ty * TW + CPT * tx;
@@ -646,7 +747,10 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
         }
         if constexpr (K::Q > 0) {
             double tot[K::Q];
-            if (item_reduce<K::Q>(acc, partials, item, m.nitems, &st->count, tot) && tid == 0) k.done(st, tot);
+            if (item_reduce<K::Q>(acc, partials, m.item_base + item, m.nitems_total ? m.nitems_total : m.nitems,
+                                  &st->count, tot) &&
+                tid == 0)
+                k.done(st, tot);
         }
         __syncthreads();                        // s_next is rewritten at the next item's start
         item = next;
@@ -664,7 +768,7 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
     }
 }
 
-template <class K, int CPT>
+template <class K, int CPT, bool HALO>
 inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
                           double* partials) {
     const size_t smem = march_smem_bytes<K>(m);
@@ -672,14 +776,15 @@ inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, co
     static size_t per_sm_smem = 0;
     if (per_sm == 0 || per_sm_smem != smem) {
         if (smem > 48 * 1024)
-            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K, CPT>, m.block.x * m.block.y, smem);
+            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K, CPT, HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K, CPT, HALO>, m.block.x * m.block.y, smem);
         if (per_sm < 1) per_sm = 1;
         per_sm_smem = smem;
     }
     int blocks = per_sm * ctx->num_sms;
     if (blocks > m.nitems) blocks = m.nitems;
-    k_march<K, CPT><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, m);
+    k_march<K, CPT, HALO><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, m);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
@@ -689,26 +794,30 @@ inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, co
 // (steps 2 and 4), or many outputs per cell (init, fold), the halved warp
 // count per SM no longer hides the work (step 2: 0.34 -> 0.45 ms, init: 0.29
 // -> 0.38 ms), so those run one cell per thread on the same 32 x 8 tiles.
-template <class K>
+// HALO: the slab variant, which reads m.halo (ignored otherwise).
+template <class K, bool HALO = false>
 inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
                         double* partials) {
-    if (m.nitems > kMaxBlocks) return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
-    if (m.cpt == 2 && K::kPairs) return launch_march_t<K, 2>(ctx, g, m, kern, st, partials);
-    if (m.cpt == 1) return launch_march_t<K, 1>(ctx, g, m, kern, st, partials);
+    if (m.nitems > kMaxBlocks || m.item_base + m.nitems > kMaxBlocks || m.nitems_total > kMaxBlocks)
+        return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
+    if (m.cpt == 2 && K::kPairs) return launch_march_t<K, 2, HALO>(ctx, g, m, kern, st, partials);
+    if (m.cpt == 1) return launch_march_t<K, 1, HALO>(ctx, g, m, kern, st, partials);
     MarchCfg m1 = m;   // the same tiles, one cell per thread
     m1.cpt = 1;
     m1.block = dim3(m.block.x * m.cpt, m.block.y, 1);
-    return launch_march_t<K, 1>(ctx, g, m1, kern, st, partials);
+    return launch_march_t<K, 1, HALO>(ctx, g, m1, kern, st, partials);
 }
 
 // K5: (24) x = x + w1 r + w2 s + alpha u; (25) r = r - w1 s - w2 t; ||r||;
 //     u = u - w1 v - w2 w; then the next iteration's (3), (4).
+//     `base` / `total`: partial-sum slots shared with other launches (slabs;
+//     0, 0: this launch alone).
 template <typename T>
 __global__ void __launch_bounds__(256) k_step5(int64_t n, T* __restrict__ x, T* __restrict__ r,
                                                const T* __restrict__ s, const T* __restrict__ t,
                                                T* __restrict__ u, const T* __restrict__ v,
                                                const T* __restrict__ w, const T* __restrict__ rh,
-                                               SolverState* st, double* partials) {
+                                               SolverState* st, double* partials, int base, int total) {
     if (st->done) return;
     const T w1 = (T)st->omega1, w2 = (T)st->omega2, alpha = (T)st->alpha;
     double acc[2] = {0., 0.};
@@ -724,7 +833,7 @@ __global__ void __launch_bounds__(256) k_step5(int64_t n, T* __restrict__ x, T* 
         acc[1] += (double)rh[c] * (double)rn;
     }
     double tot[2];
-    if (!grid_reduce<2>(acc, partials, &st->count, tot)) return;
+    if (!grid_reduce<2>(acc, partials, &st->count, tot, base, total)) return;
     if (threadIdx.x == 0) finish_update(st, tot);
 }
 

@@ -304,6 +304,47 @@ DARE_API int dare_bicgstab2_solve(dare_system* s, const dare_solver_params* p, d
 DARE_API int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
                   const dare_solver_params* p, dare_solve_report* rep);
 
+/* ---- slabs of i-planes: the grid distributed as the reference distributes
+ *      it over ranks (Grid/Cartesian/CartesianDistribution.h:94-380,
+ *      MPI/HaloBuffer.inl:30-208, Tpetra's sum over ranks in every dot of
+ *      BiCGStab2.inl:339-559), all slabs on the system's device.
+ * Slab s owns planes [i0, i1) (n0 split into runs, the first n0 % S one
+ * plane longer) with its own field (every time level, ghosted), system rows
+ * and solver vectors.  Before an assembly num_ghost boundary planes of the
+ * field cross to each x neighbour; before every SpMV one boundary plane of
+ * the operand; every dot product sums all slabs' partials.  One field
+ * component, FP64 solves (plain or Jacobi), 1 to 8 slabs of at least
+ * max(num_ghost, 2) planes.  The slabs inherit the system's grid and face
+ * conditions; x faces shared by two slabs (every x face of a periodic x)
+ * stay unfolded. */
+typedef struct dare_slabs dare_slabs;
+DARE_API int dare_slabs_create(dare_system* s, int num_slabs, int num_levels, dare_slabs** out);
+DARE_API int dare_slabs_destroy(dare_slabs* sl);
+DARE_API int dare_slabs_count(const dare_slabs* sl);
+DARE_API int dare_slabs_range(const dare_slabs* sl, int slab, int64_t* i0, int64_t* i1);
+/* The slab's own system and field (owned by the slabs; read and write them
+ * with the dare_system_* / dare_field_* calls, do not destroy them). */
+DARE_API dare_system* dare_slabs_system(dare_slabs* sl, int slab);
+DARE_API dare_field* dare_slabs_field(dare_slabs* sl, int slab);
+DARE_API int dare_slabs_set_bc(dare_slabs* sl, int face, int type, double value);
+/* Every level of a field of the system's grid into the slabs (each slab its
+ * planes and num_ghost planes either side) / the slabs back into it. */
+DARE_API int dare_slabs_scatter(dare_slabs* sl, dare_field* f);
+DARE_API int dare_slabs_gather(dare_slabs* sl, dare_field* f);
+/* Field::ExchangeHaloCells: periodic j / k ghosts in each slab, then the x
+ * ghost planes from the neighbouring slabs (wrapping on a periodic x). */
+DARE_API int dare_slabs_exchange_halo(dare_slabs* sl);
+DARE_API int dare_slabs_copy_to_old(dare_slabs* sl);
+/* Trilinos::Build on every slab; descs[s] describes slab s, its face arrays
+ * covering its own planes (n_s + 1 x faces: global faces i0 .. i1, face 0
+ * for the last one on a periodic x; the slab's planes of the y and z faces). */
+DARE_API int dare_slabs_assemble(dare_slabs* sl, const dare_assembly_desc* descs);
+DARE_API int dare_slabs_solve(dare_slabs* sl, const dare_solver_params* p, dare_solve_report* rep);
+DARE_API int dare_slabs_copy_to(dare_slabs* sl);
+/* Build, Solve, CopyTo, ExchangeHaloCells, CopyDataVectorsToOldTimeStep */
+DARE_API int dare_slabs_timestep(dare_slabs* sl, const dare_assembly_desc* descs, const dare_solver_params* p,
+                                 dare_solve_report* rep);
+
 /* Face diffusivity as the linear interpolation of cell values to faces
  * (Interpolation_Cartesian.h:139-158: (D_lo + D_hi) * 1/2, periodic wrap on
  * periodic faces, boundary faces take the adjacent cell value).
