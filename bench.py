@@ -66,6 +66,7 @@ def parse_args(argv=None):
     ap.add_argument("--batch", type=int, default=4096)
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
+    ap.add_argument("--no-slabs", action="store_true", help="skip the slab comparison")
     ap.add_argument("--learn-operators", type=int, default=64,
                     help="128^3 operators of the training distribution the preconditioner is trained on")
     ap.add_argument("--learn-steps", type=int, default=76,
@@ -357,6 +358,10 @@ def run_dare(args):
                   "max_abs": float(np.abs(diff).max()), "iters_gpu": giters, "iters_cpu": citers,
                   "bar": "rel_l2 < 1e-9 (solutions at the same 1e-10 relative residual)"}
 
+    slabs = None
+    if rank == 0 and world == 1 and not args.no_slabs:
+        slabs = slab_comparison(D, ctx, system, field, asm, case, phi0, args)
+
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
         learned = learned_comparison(D, ctx, system, field, asm, n, args)
@@ -378,11 +383,57 @@ def run_dare(args):
             "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e; iterations replayed from CUDA graphs); "
                       "learned-preconditioned solve in 'learned'",
             "learned": learned,
+            "slabs": slabs,
             "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     ranks.close()
     return 0
+
+
+def slab_comparison(D, ctx, system, field, asm, case, phi0, args, num_slabs=2, steps=2):
+    """The same steps on slabs of i-planes (both on this device, run one after
+    the other, planes exchanged by device copies) against the single grid
+    from the same initial field: time per step and the final fields."""
+    import torch
+    field.upload(phi0, 0)
+    field.upload(phi0, 1)
+    single_iters = [D.timestep(system, field, asm, D.BiCGStab2(dict(_SOLVER)))["iters"] for _ in range(steps)]
+    ref = field.download(0)
+    sl = D.Slabs(system, num_slabs, 2)
+    n0 = case["n"][0]
+    keep, slab_asm = [], []
+    for i0, i1 in sl.ranges:
+        fx = case["face_vel"][0]
+        fx = torch.cat([fx[i0:n0], fx[0:1]]) if (case["periodic"][0] and i1 == n0) else fx[i0:i1 + 1]
+        arrs = [D.DeviceArray.from_tensor(fx), D.DeviceArray.from_tensor(case["face_vel"][1][i0:i1]),
+                D.DeviceArray.from_tensor(case["face_vel"][2][i0:i1])]
+        keep += arrs
+        slab_asm.append(D.Assembly(dt=case["dt"], D=case["D"], face_vel=tuple(arrs), limiter="VANLEER"))
+    solver = D.BiCGStab2(dict(_SOLVER))
+    field.upload(phi0, 0)
+    field.upload(phi0, 1)
+    sl.scatter(field)
+    sl.timestep(slab_asm, solver)          # captures the slab graphs
+    sl.scatter(field)
+    ctx.synchronize()
+    ctx.timer_start()
+    iters = [sl.timestep(slab_asm, solver)["iters"] for _ in range(steps)]
+    ms = ctx.timer_stop()
+    sl.gather(field)
+    got = field.download(0)
+    g = system.grid
+    inner = lambda a: a.reshape(g.ghosted_shape)[2:-2, 2:-2, 2:-2]
+    rel = float(np.linalg.norm(inner(got) - inner(ref)) / np.linalg.norm(inner(ref)))
+    del sl
+    return {"slabs": num_slabs, "steps": steps, "ms_per_step": ms / steps, "iters": iters,
+            "iters_single_grid": single_iters, "rel_l2_vs_single_grid": rel,
+            "setup": "all slabs on this one B200, launched one after the other; boundary planes cross by "
+                     "device-to-device copies; the multi-GPU form (NCCL send/recv, all-reduce) is unmeasured "
+                     "on hardware"}
+
+
+_SOLVER = {"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1}
 
 
 def _timed_solve(ctx, system, field, asm, fn, reps=2):
