@@ -303,6 +303,7 @@ public:
         check(dare_system_set_coefficients(h_, diag7.data(), rhs.data(), x0.data()), ctx(), "set_coefficients");
     }
     int GetNumComponents() const { return dare_system_num_components(h_); }
+    Cartesian& GetGrid() const { return *grid_; }
     std::vector<double> GetX() const {
         std::vector<double> x((size_t)(grid_->GetNumberLocalCellsInternal() * GetNumComponents()));
         check(dare_system_get_solution(h_, x.data()), ctx(), "get_solution");
@@ -368,6 +369,62 @@ public:
 private:
     dare_solver_params p_{};
     dare_solve_report rep_{};
+};
+
+// The grid of a system distributed over slabs of i-planes, as the reference
+// distributes it over ranks (CartesianDistribution.h:94-380), all slabs on
+// the system's device: per slab its own field, rows and solver vectors.
+class Slabs {
+public:
+    Slabs(Trilinos& sys, int num_slabs, int num_levels = 2) : ctx_(sys.GetGrid().GetContext().get()) {
+        check(dare_slabs_create(sys.get(), num_slabs, num_levels, &h_), ctx_, "dare_slabs_create");
+    }
+    ~Slabs() {
+        if (h_) dare_slabs_destroy(h_);
+    }
+    Slabs(const Slabs&) = delete;
+    Slabs& operator=(const Slabs&) = delete;
+    dare_slabs* get() const { return h_; }
+    int Count() const { return dare_slabs_count(h_); }
+    // planes [i0, i1) of slab s
+    std::array<int64_t, 2> Range(int s) const {
+        std::array<int64_t, 2> r{};
+        check(dare_slabs_range(h_, s, &r[0], &r[1]), ctx_, "dare_slabs_range");
+        return r;
+    }
+    void Scatter(Field& field) { check(dare_slabs_scatter(h_, field.get()), ctx_, "dare_slabs_scatter"); }
+    void Gather(Field& field) { check(dare_slabs_gather(h_, field.get()), ctx_, "dare_slabs_gather"); }
+    void ExchangeHaloCells() { check(dare_slabs_exchange_halo(h_), ctx_, "dare_slabs_exchange_halo"); }
+    // Trilinos::Build on every slab, descs[s] holding slab s's face arrays
+    void Build(const std::vector<Assembly>& functors) {
+        const std::vector<dare_assembly_desc> d = Descs(functors);
+        check(dare_slabs_assemble(h_, d.data()), ctx_, "dare_slabs_assemble");
+    }
+    BiCGStab2::ReturnType Solve(BiCGStab2& solver, dare_solve_report* rep = nullptr) {
+        dare_solve_report r{};
+        check(dare_slabs_solve(h_, &solver.Params(), &r), ctx_, "dare_slabs_solve");
+        if (rep) *rep = r;
+        return r.converged ? BiCGStab2::ReturnType::Converged : BiCGStab2::ReturnType::Unconverged;
+    }
+    // Build, Solve, CopyTo, ExchangeHaloCells, CopyDataVectorsToOldTimeStep on every slab
+    BiCGStab2::ReturnType TimeStep(BiCGStab2& solver, const std::vector<Assembly>& functors,
+                                   dare_solve_report* rep = nullptr) {
+        const std::vector<dare_assembly_desc> d = Descs(functors);
+        dare_solve_report r{};
+        check(dare_slabs_timestep(h_, d.data(), &solver.Params(), &r), ctx_, "dare_slabs_timestep");
+        if (rep) *rep = r;
+        return r.converged ? BiCGStab2::ReturnType::Converged : BiCGStab2::ReturnType::Unconverged;
+    }
+
+private:
+    std::vector<dare_assembly_desc> Descs(const std::vector<Assembly>& functors) const {
+        if ((int)functors.size() != Count()) throw Error("Slabs: one functor per slab", DARE_ERR_BAD_ARG);
+        std::vector<dare_assembly_desc> d;
+        for (const auto& f : functors) d.push_back(f.Desc());
+        return d;
+    }
+    dare_ctx* ctx_;
+    dare_slabs* h_ = nullptr;
 };
 
 }  // namespace dare_b200
