@@ -67,6 +67,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
     ap.add_argument("--no-slabs", action="store_true", help="skip the slab comparison")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 64^3 trajectory, 512^3 mixed-precision and 4096-box batch measurements")
     ap.add_argument("--learn-operators", type=int, default=64,
                     help="128^3 operators of the training distribution the preconditioner is trained on")
     ap.add_argument("--learn-steps", type=int, default=76,
@@ -358,6 +360,15 @@ def run_dare(args):
                   "max_abs": float(np.abs(diff).max()), "iters_gpu": giters, "iters_cpu": citers,
                   "bar": "rel_l2 < 1e-9 (solutions at the same 1e-10 relative residual)"}
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        # the other configurations of the workload family, each measured here
+        # on the same device (one warm-up, then timed)
+        configs = {"gauss64": measure_gauss64(D, ctx, args.seed),
+                   "hetero512": measure_hetero(D, ctx, 512 if n >= 256 else 2 * n, args.seed),
+                   "batched4096": measure_batched(D, ctx, 4096 if n >= 256 else 64, args.seed,
+                                                  cpu_sample=16)}
+
     slabs = None
     if rank == 0 and world == 1 and not args.no_slabs:
         slabs = slab_comparison(D, ctx, system, field, asm, case, phi0, args)
@@ -384,6 +395,7 @@ def run_dare(args):
                       "learned-preconditioned solve in 'learned'",
             "learned": learned,
             "slabs": slabs,
+            "configs": configs,
             "gpu_launches": launches, "clocks": clk, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -525,32 +537,32 @@ def _gpu_setup_field(D, ctx, case):
     return grid, field
 
 
-def run_gauss64(args):
-    """64^3 transient diffusion (Gaussian bump, Dirichlet x, Neumann elsewhere), 10 steps."""
-    import dare_b200 as D
+def measure_gauss64(D, ctx, seed=0, warmup=1):
+    """64^3 transient diffusion (Gaussian bump, Dirichlet x, Neumann elsewhere):
+    10 implicit steps on the GPU against the oracle's loop from the same field."""
     from dare_b200 import workloads as W
     from oracle import oracle as O
     from tests.helpers import oracle_timeloop
-    case = W.gaussian_diffusion(n=64, seed=args.seed, steps=10)
-    ctx = D.Context(0)
+    case = W.gaussian_diffusion(n=64, seed=seed, steps=10)
     grid, field = _gpu_setup_field(D, ctx, case)
     system = D.MatrixSystem(grid)
     for face, (kind, val) in case["bc"].items():
         system.set_bc(face, kind, val)
     asm = D.Assembly(dt=case["dt"], D=case["D"])
-    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    solver = D.BiCGStab2(dict(_SOLVER))
     phi0 = np.ascontiguousarray(case["phi0"].reshape(-1))
 
     def trajectory():
         field.upload(phi0, 0)
         field.upload(phi0, 1)
         its = []
+        ctx.synchronize()
         ctx.timer_start()
         for _ in range(case["steps"]):
             its.append(D.timestep(system, field, asm, solver)["iters"])
         return ctx.timer_stop(), its
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         trajectory()
     ms, its = trajectory()
     got = field.download(0)
@@ -558,25 +570,27 @@ def run_gauss64(args):
     hist, oits = oracle_timeloop(case, case["steps"])
     cpu_s = time.perf_counter() - t0
     err = float(np.linalg.norm(got - hist[-1]) / np.linalg.norm(hist[-1]))
-    print(json.dumps({"workload": "gaussian diffusion 64^3, 10 implicit steps, Jacobi-BiCGStab2 1e-10",
-                      "metric": "implicit steps/s", "value": case["steps"] / (ms * 1e-3), "ms_total": ms,
-                      "iterations": its, "oracle_iterations": oits, "rel_l2_vs_oracle": err,
-                      "cpu_baseline": {"value": case["steps"] / cpu_s, "unit": "steps/s", "cores": O.num_threads(),
-                                       "kind": "port"}}), flush=True)
+    return {"workload": "gaussian diffusion 64^3, 10 implicit steps, Jacobi-BiCGStab2 1e-10",
+            "metric": "implicit steps/s", "value": case["steps"] / (ms * 1e-3), "ms_total": ms,
+            "iterations": its, "oracle_iterations": oits, "rel_l2_vs_oracle": err,
+            "cpu_baseline": {"value": case["steps"] / cpu_s, "unit": "steps/s", "cores": O.num_threads(),
+                             "kind": "port"}}
+
+
+def run_gauss64(args):
+    import dare_b200 as D
+    print(json.dumps(measure_gauss64(D, D.Context(0), args.seed, args.warmup)), flush=True)
     return 0
 
 
-def run_hetero(args):
+def measure_hetero(D, ctx, n=512, seed=0, warmup=1, steps=2):
     """Heterogeneous-D TVD operator (log-normal D, box-filtered): FP64 plain vs
     FP32-inner / FP64-refinement per step, error of the latter vs the former."""
     import torch
 
-    import dare_b200 as D
     from dare_b200 import workloads as W
-    n = args.n
-    dev = "cuda:0"
-    case = W.heterogeneous(n=n, seed=args.seed, device=dev)
-    ctx = D.Context(0)
+    dev = f"cuda:{torch.cuda.current_device()}"
+    case = W.heterogeneous(n=n, seed=seed, device=dev)
     grid, field = _gpu_setup_field(D, ctx, case)
     phi0 = case["phi0"].reshape(-1).cpu().numpy()
     field.upload(phi0, 0)
@@ -587,39 +601,46 @@ def run_hetero(args):
     D.face_average(grid, cell_D.data_ptr(), faceD)
     vel = [D.DeviceArray.from_tensor(case["face_vel"][d]) for d in range(3)]
     dt = case["dt"]
-    del case
+    del case, cell_D, phi0
     torch.cuda.empty_cache()
     system = D.MatrixSystem(grid)
     asm = D.Assembly(dt=dt, face_D=tuple(faceD), face_vel=tuple(vel))
-    p64 = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
-    p32 = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1},
-                      precision="FP32_REFINE")
-    x64 = torch.empty(grid.num_cells, dtype=torch.float64, device=dev)
+    p64 = D.BiCGStab2(dict(_SOLVER))
+    p32 = D.BiCGStab2(dict(_SOLVER), precision="FP32_REFINE")
     rows = []
-    for step in range(args.warmup + args.steps):
+    for step in range(warmup + steps):
         system.build(field, asm)
+        ctx.synchronize()
         ctx.timer_start()
         r64 = p64.solve(system)
         t64 = ctx.timer_stop()
-        x64.copy_(torch.from_numpy(system.solution()).to(dev))
+        x64 = system.solution()
         system.build(field, asm)
+        ctx.synchronize()
         ctx.timer_start()
         r32 = p32.solve(system)
         t32 = ctx.timer_stop()
-        x32 = torch.from_numpy(system.solution()).to(dev)
-        err = float((x32 - x64).norm() / x64.norm())
+        x32 = system.solution()
+        err = float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
+        del x64, x32
         system.copy_to(field)
         field.exchange_halo()
         field.copy_to_old()
-        if step >= args.warmup:
+        if step >= warmup:
             rows.append({"fp64_ms": t64, "fp64_iters": r64["iters"], "refine_ms": t32,
                          "refinements": r32["refinements"], "inner_iters": r32["inner_iters"],
                          "fallback": r32["fallback_used"], "rel_l2_vs_fp64": err,
                          "true_res_rel": r32["true_res_abs"] / r32["b_norm"]})
-    print(json.dumps({"workload": f"heterogeneous-D TVD convection-diffusion {n}^3 periodic, Pe 5 at median D",
-                      "steps": rows,
-                      "fp64_ms_mean": statistics.mean(r["fp64_ms"] for r in rows),
-                      "refine_ms_mean": statistics.mean(r["refine_ms"] for r in rows)}), flush=True)
+    return {"workload": f"heterogeneous-D TVD convection-diffusion {n}^3 periodic, Pe 5 at median D",
+            "steps": rows,
+            "fp64_ms_mean": statistics.mean(r["fp64_ms"] for r in rows),
+            "refine_ms_mean": statistics.mean(r["refine_ms"] for r in rows)}
+
+
+def run_hetero(args):
+    import dare_b200 as D
+    ctx = D.Context(0)
+    print(json.dumps(measure_hetero(D, ctx, args.n, args.seed, args.warmup, args.steps)), flush=True)
     return 0
 
 
@@ -663,22 +684,22 @@ def run_unet(args):
     return 0
 
 
-def run_batched(args):
-    """4096 independent diffusion boxes (sides 16-64), one implicit step each, one launch."""
-    import dare_b200 as D
+def measure_batched(D, ctx, count=4096, seed=0, warmup=3, steps=10, autotune=True, cpu_sample=64):
+    """`count` independent diffusion boxes (sides 16-64), one implicit step
+    each, one persistent launch; the CPU oracle on a bounded sample, scaled
+    by cells."""
     from dare_b200 import workloads as W
     from oracle import oracle as O
-    inst =W.batched_diffusion(count=args.batch, seed=args.seed)
+    inst = W.batched_diffusion(count=count, seed=seed)
     cells = int(sum(np.prod(i["n"]) for i in inst))
-    ctx = D.Context(0)
     bt = D.Batch(ctx, inst)
     solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 10000, "tol_relative": 1})
-    tuning = bt.autotune(solver) if not args.no_autotune else None
-    for _ in range(args.warmup):
+    tuning = bt.autotune(solver) if autotune else None
+    for _ in range(warmup):
         bt.zero_fields()
         bt.solve(solver, reports=False)
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         bt.zero_fields()
         ctx.synchronize()
         ctx.timer_start()
@@ -687,9 +708,8 @@ def run_batched(args):
     bt.zero_fields()
     reps = bt.solve(solver)
     its = [r["iters"] for r in reps]
-    # CPU baseline on a bounded sample of the batch, scaled by cells
     rng = np.random.default_rng(1)
-    sample = rng.choice(len(inst), size=min(64, len(inst)), replace=False)
+    sample = rng.choice(len(inst), size=min(cpu_sample, len(inst)), replace=False)
     t0 = time.perf_counter()
     scells = 0
     for q in sample:
@@ -702,13 +722,20 @@ def run_batched(args):
         scells += int(np.prod(ins["n"]))
     cpu_s = (time.perf_counter() - t0) * cells / scells
     ms = statistics.median(times)
-    print(json.dumps({"workload": f"{len(inst)} diffusion boxes, sides 16-64, one implicit step each, "
-                                  "Jacobi-BiCGStab2 1e-10, one persistent launch",
-                      "cells": cells, "ms_per_batch": ms, "ms_all": times, "cell_steps_per_s": cells / (ms * 1e-3),
-                      "converged": sum(r["converged"] for r in reps), "iters_min": min(its), "iters_max": max(its),
-                      "iters_mean": statistics.mean(its), "tuning": tuning,
-                      "cpu_baseline": {"value_s_per_batch": cpu_s, "cores": O.num_threads(), "kind": "port",
-                                       "sample": f"{len(sample)} instances, scaled by cells"}}), flush=True)
+    return {"workload": f"{len(inst)} diffusion boxes, sides 16-64, one implicit step each, "
+                        "Jacobi-BiCGStab2 1e-10, one persistent launch",
+            "cells": cells, "ms_per_batch": ms, "ms_all": times, "cell_steps_per_s": cells / (ms * 1e-3),
+            "converged": sum(r["converged"] for r in reps), "iters_min": min(its), "iters_max": max(its),
+            "iters_mean": statistics.mean(its), "tuning": tuning,
+            "cpu_baseline": {"value_s_per_batch": cpu_s, "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{len(sample)} instances, scaled by cells"}}
+
+
+def run_batched(args):
+    import dare_b200 as D
+    ctx = D.Context(0)
+    print(json.dumps(measure_batched(D, ctx, args.batch, args.seed, args.warmup, args.steps,
+                                     not args.no_autotune)), flush=True)
     return 0
 
 
