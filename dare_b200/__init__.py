@@ -132,6 +132,8 @@ _SIGS = [
     ("dare_bicgstab2_solve", C.c_int, [_P, C.POINTER(SolverParams), C.POINTER(SolveReport)]),
     ("dare_timestep", C.c_int, [_P, _P, C.POINTER(AssemblyDesc), C.POINTER(SolverParams),
                                 C.POINTER(SolveReport)]),
+    ("dare_timesteps_host", C.c_int, [_P, _P, C.POINTER(AssemblyDesc), C.POINTER(SolverParams), C.c_int, _P,
+                                      C.POINTER(SolveReport)]),
     ("dare_face_average", C.c_int, [_P, _P, C.POINTER(_P)]),
     ("dare_slabs_create", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P)]),
     ("dare_slabs_destroy", C.c_int, [_P]),
@@ -726,6 +728,24 @@ def timestep(system: MatrixSystem, field: Field, assembly: Assembly, solver: BiC
            system.grid.ctx.h, "timestep")
     solver.report = rep.as_dict()
     return solver.report
+
+
+def timesteps_host(system: MatrixSystem, field: Field, assembly: Assembly, solver: BiCGStab2, steps: int,
+                   host: np.ndarray) -> list:
+    """`steps` implicit steps of a field kept in host memory (``host``: pinned,
+    the field's device layout, float64): each step reads its input from
+    ``host`` and writes its result back, the result of one step travelling
+    down while the input of the next travels up."""
+    size = field.grid.num_cells_ghosted * field.components
+    if host.size != size or host.dtype != np.float64 or not host.flags["C_CONTIGUOUS"]:
+        raise ValueError("timesteps_host expects a contiguous float64 buffer of the field's ghosted size")
+    desc = assembly.to_c()
+    reps = (SolveReport * steps)()
+    _check(lib().dare_timesteps_host(system.h, field.h, C.byref(desc), C.byref(solver.params), steps, _ptr(host),
+                                     reps), system.grid.ctx.h, "timesteps_host")
+    out = [r.as_dict() for r in reps]
+    solver.report = out[-1]
+    return out
 
 
 def write_vtk(fields, names, base_path: str, grid_name: str, step: int, time: float = -1.0, level: int = 0):

@@ -48,6 +48,82 @@ int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
     return dare_field_copy_to_old(f);                                // CopyDataVectorsToOldTimeStep
 }
 
+// nsteps steps of a field that lives in host memory: before step k the
+// field's level 0 is read from `host` and level 1 set from it; after the step
+// the result goes back to `host`.  The host buffer is in the field's device
+// layout (component-major ghosted levels) and must be pinned.  The result of
+// step k travels to the host and the input of step k + 1 back to the device
+// in kHostChunks slices on two streams: slice c goes up as soon as it has
+// come down, so the two PCIe directions run at the same time instead of one
+// after the other.  Every step still moves the whole field both ways.
+int dare_timesteps_host(dare_system* s, dare_field* f, const dare_assembly_desc* desc, const dare_solver_params* p,
+                        int nsteps, double* host, dare_solve_report* reps) {
+    if (!s || !f || !desc || !p || !host || nsteps < 1 || f->grid != s->grid || f->ncomp != s->ncomp)
+        return DARE_ERR_BAD_ARG;
+    dare_ctx* ctx = s->grid->ctx;
+    cudaSetDevice(ctx->device);
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, host) != cudaSuccess || attr.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        return set_error(ctx, DARE_ERR_BAD_ARG, "dare_timesteps_host: the host buffer must be pinned");
+    }
+    constexpr int kHostChunks = 16;
+    const size_t total = (size_t)f->grid->dev.ncell_ghosted * f->ncomp * sizeof(double);
+    size_t chunk = (total + kHostChunks - 1) / kHostChunks;
+    chunk = (chunk + 4095) / 4096 * 4096;
+    char* dev = reinterpret_cast<char*>(f->level[0]);
+    char* hb = reinterpret_cast<char*>(host);
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_step = nullptr, ev_out[kHostChunks] = {nullptr};
+    int rc = DARE_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&down, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_step, cudaEventDisableTiming);
+    for (int c = 0; c < kHostChunks && e == cudaSuccess; c++) e = cudaEventCreateWithFlags(&ev_out[c], cudaEventDisableTiming);
+    if (e != cudaSuccess) rc = check_cuda(ctx, e, "dare_timesteps_host: streams");
+    dare_solve_report last{};
+    for (int k = 0; k < nsteps && rc == DARE_OK; k++) {
+        // the input of step k: slice c waits for the slice's result of step k - 1
+        for (int c = 0; c < kHostChunks && e == cudaSuccess; c++) {
+            const size_t off = (size_t)c * chunk;
+            if (off >= total) break;
+            const size_t len = off + chunk > total ? total - off : chunk;
+            if (k > 0) e = cudaStreamWaitEvent(up, ev_out[c], 0);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dev + off, hb + off, len, cudaMemcpyHostToDevice, up);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev_in, up);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ev_in, 0);
+        if (e != cudaSuccess) {
+            rc = check_cuda(ctx, e, "dare_timesteps_host: upload");
+            break;
+        }
+        if ((rc = dare_field_copy_to_old(f))) break;
+        if ((rc = dare_timestep(s, f, desc, p, reps ? &reps[k] : &last))) break;
+        // its result, slice by slice
+        e = cudaEventRecord(ev_step, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(down, ev_step, 0);
+        for (int c = 0; c < kHostChunks && e == cudaSuccess; c++) {
+            const size_t off = (size_t)c * chunk;
+            if (off >= total) break;
+            const size_t len = off + chunk > total ? total - off : chunk;
+            e = cudaMemcpyAsync(hb + off, dev + off, len, cudaMemcpyDeviceToHost, down);
+            if (e == cudaSuccess) e = cudaEventRecord(ev_out[c], down);
+        }
+        if (e != cudaSuccess) rc = check_cuda(ctx, e, "dare_timesteps_host: download");
+    }
+    // the last result is on the host before returning (also after an error)
+    if (down) cudaStreamSynchronize(down);
+    if (up) cudaStreamSynchronize(up);
+    for (auto& ev : ev_out)
+        if (ev) cudaEventDestroy(ev);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_step) cudaEventDestroy(ev_step);
+    if (up) cudaStreamDestroy(up);
+    if (down) cudaStreamDestroy(down);
+    return rc;
+}
+
 int dare_ctx_set_profiling(dare_ctx* ctx, int on) {
     if (!ctx) return DARE_ERR_BAD_ARG;
     if (on) {

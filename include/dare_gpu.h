@@ -303,6 +303,16 @@ DARE_API int dare_bicgstab2_solve(dare_system* s, const dare_solver_params* p, d
  * ExchangeHaloCells, CopyDataVectorsToOldTimeStep. */
 DARE_API int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
                   const dare_solver_params* p, dare_solve_report* rep);
+/* nsteps such steps of a field kept in host memory: before each step the
+ * field (level 0, and level 1 from it) is read from `host`, after it the
+ * result is written back to `host`.  `host`: pinned, the field's device
+ * layout (component-major ghosted levels; for one component the ghosted
+ * layout).  The download of one step's result and the upload of the next
+ * step's input are pipelined in slices on two streams (PCIe carries both
+ * directions at once); every step moves the whole field both ways.
+ * reps: nsteps reports, or NULL.  Returns with the last result in `host`. */
+DARE_API int dare_timesteps_host(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
+                                 const dare_solver_params* p, int nsteps, double* host, dare_solve_report* reps);
 
 /* ---- slabs of i-planes: the grid distributed as the reference distributes
  *      it over ranks (Grid/Cartesian/CartesianDistribution.h:94-380,

@@ -532,3 +532,30 @@ def test_multicomponent_assembly_and_timeloop(ctx, periodic):
         for c in range(N):
             assert rel_l2(interior(got[:, c], g.ghosted_shape), interior(ocomps[c], g.ghosted_shape)) < SOL_TOL
         assert abs(rep["iters"] - info["iters"]) <= 2
+
+
+def test_host_resident_steps_match_single_calls(ctx):
+    """dare_timesteps_host (each step's field from pinned host memory, the
+    result back to it, transfers of consecutive steps pipelined in slices)
+    gives the loop of single upload / copy-to-old / timestep / download calls
+    bit for bit; an unpinned buffer is refused."""
+    import torch
+    case = W.tvd_convection_diffusion(n=24, steps=3)
+    g, f, s, asm, keep, dim = _gpu_case(ctx, case)
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    phi0 = f.download(0)
+    host = torch.empty(g.num_cells_ghosted, dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = phi0
+    reps = D.timesteps_host(s, f, asm, solver, 3, host)
+    assert len(reps) == 3 and all(r["converged"] for r in reps)
+    ref = phi0.copy()
+    iters = []
+    for _ in range(3):
+        f.upload(ref, 0)
+        f.copy_to_old()
+        iters.append(D.timestep(s, f, asm, solver)["iters"])
+        ref = f.download(0)
+    assert [r["iters"] for r in reps] == iters
+    assert np.array_equal(host, ref)
+    with pytest.raises(D.DareError):
+        D.timesteps_host(s, f, asm, solver, 1, np.zeros(g.num_cells_ghosted))
