@@ -39,10 +39,10 @@ UNIT = "steps/s"
 BYTES_PER_CELL = {
     "assemble": 8 + 8 + 24 + 56 + 8 + 8,   # phi, phi_old, 3 face velocities; 7 diagonals, rhs, x0
     "step1": 88,    # r, u, 6 off-diagonals, r_hat; u', v
-    "step2": 112,   # r, v, 6 off-diagonals, u, x, r_hat; r', s, x
+    "step2": 88,    # r, v, 6 off-diagonals, r_hat; r', s
     "step3": 88,    # s, v, 6 off-diagonals, r_hat; v', w
-    "step4": 120,   # s, w, 6 off-diagonals, r, u, v; u, r, s', t
-    "step5": 88,    # x, r, s, t, u, v, w, r_hat; x, r, u
+    "step4": 104,   # s, w, 6 off-diagonals, r', v'; r'', s', t
+    "step5": 96,    # x, r'', s', t, u', r', v', w, r_hat; x, r, u
 }
 
 

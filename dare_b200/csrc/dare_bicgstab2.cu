@@ -13,8 +13,10 @@
 //     keeping the fused input of planes i-1, i, i+1 in registers and plane i
 //     (with its j/k halo) in shared memory, so each operand is read from HBM
 //     once and each fused value is evaluated once per cell (plus the halo).
-//     Vectors written that way are double buffered (u and r flip every
-//     iteration, v and s have a fixed pair), so a graph holds two iterations.
+//     Each of r, u, v and s has a second buffer for the value of the middle
+//     of an iteration: step (10), x += alpha u, and step (15),
+//     u = r - beta u, wait for the last kernel, which reads both buffers.
+//     A graph holds two iterations.
 //   * Scalars (alpha, beta, rho, omega, ...) never leave the device: the last
 //     block of each kernel reduces the per-block partials in a fixed order
 //     (deterministic, no floating-point atomics), evaluates the reference's
@@ -142,25 +144,26 @@ template int launch_init<double, false>(dare_ctx*, const GridDev&, const MarchCf
 template int launch_init<float, true>(dare_ctx*, const GridDev&, const MarchCfg&, const OpT<float>&,
                                       const VecsT<float>&, SolverState*, double*);
 
-// One iteration; `par` selects which halves of r/u are current.  `ev`
-// (optional, profiling): ev[0] before the first kernel, ev[1..5] after each.
+// One iteration (`par`: its place in the pair a graph holds; every iteration
+// uses the same buffers).  `ev` (optional, profiling): ev[0] before the first
+// kernel, ev[1..5] after each.
 template <typename T, bool UNIT>
 int launch_iteration(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                      const VecsT<T>& vs, SolverState* st, double* partials, int par, cudaEvent_t* ev) {
-    const int a = par, b = 1 - par;
+    (void)par;
     cudaStream_t sm = ctx->stream;
     int rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[0], sm));
-    if ((rc = launch_march(ctx, g, m, make_step1<T, UNIT>(op, vs, a, b), st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step1<T, UNIT>(op, vs), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[1], sm));
-    if ((rc = launch_march(ctx, g, m, make_step2<T, UNIT>(op, vs, a, b), st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step2<T, UNIT>(op, vs), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[2], sm));
     if ((rc = launch_march(ctx, g, m, make_step3<T, UNIT>(op, vs), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[3], sm));
-    if ((rc = launch_march(ctx, g, m, make_step4<T, UNIT>(op, vs, b), st, partials))) return rc;
+    if ((rc = launch_march(ctx, g, m, make_step4<T, UNIT>(op, vs), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[4], sm));
-    k_step5<T><<<sblocks, 256, 0, sm>>>(g.ncell, vs.x, vs.r[b], vs.s[1], vs.t, vs.u[b], vs.v[1], vs.w, vs.rh, st,
-                                        partials, 0, 0);
+    k_step5<T><<<sblocks, 256, 0, sm>>>(g.ncell, vs.x, vs.r[0], vs.s[1], vs.t, vs.u[0], vs.u[1], vs.r[1], vs.v[1],
+                                        vs.w, vs.rh, st, partials, 0, 0);
     DARE_LAUNCHED(ctx);
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[5], sm));
     return DARE_OK;
@@ -197,6 +200,16 @@ int launch_fold32(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const doub
     f.n = g.ncell;
     return launch_march(ctx, g, m, f, st, partials);
 }
+
+template <typename T>
+int finish_step10(dare_ctx* ctx, int64_t n, const SolverState& st_host, const SolverState* st, const VecsT<T>& vs) {
+    if (!step10_pending(st_host)) return DARE_OK;
+    k_step10<T><<<grid_blocks(ctx, n, 256, 8), 256, 0, ctx->stream>>>(n, st, vs.u[1], vs.x);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+template int finish_step10<double>(dare_ctx*, int64_t, const SolverState&, const SolverState*, const VecsT<double>&);
+template int finish_step10<float>(dare_ctx*, int64_t, const SolverState&, const SolverState*, const VecsT<float>&);
 
 int launch_scale(dare_ctx* ctx, int64_t n, const double* invd, double* x) {
     const int eb = grid_blocks(ctx, n, 256, 8);
@@ -335,6 +348,7 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
                                                 ws->partials, &ws->graph[0][0], p->max_it, p->check_every, KID_STEP1);
     if (rc) return rc;
     SolverState st = *ws->st_host;
+    if ((rc = finish_step10(ctx, n, st, ws->st, vs))) return rc;
 
     std::memset(rep, 0, sizeof(*rep));
     rep->iters = st.k;

@@ -33,8 +33,8 @@ struct VecsT {
     T* x;        // y in the preconditioned variable, x at the end
     const T* b;
     T* rh;       // r_hat_0
-    T* r[2];
-    T* u[2];
+    T* r[2];     // r[0] the iterate's r, r[1] step (8)'s r until K5 has used it
+    T* u[2];     // u[0] the iterate's u, u[1] step (5)'s u until K5 has used it
     T* v[2];
     T* s[2];
     T* w;
@@ -161,6 +161,10 @@ int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double
 int launch_fold32(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, float* ahat32,
                   SolverState* st, double* partials);
 int launch_scale(dare_ctx* ctx, int64_t n, const double* invd, double* x);
+// Apply step (10) when the solve stopped between it and the last kernel of
+// its iteration (st_host: the final state read back)
+template <typename T>
+int finish_step10(dare_ctx* ctx, int64_t n, const SolverState& st_host, const SolverState* st, const VecsT<T>& vs);
 
 }  // namespace dare_gpu
 

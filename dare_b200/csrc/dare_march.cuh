@@ -72,6 +72,7 @@ __device__ inline void finish_gamma(SolverState* st, const double* tot, int step
         return;
     }
     st->alpha = st->rho0 / st->gamma;
+    if (step == 7) st->alpha1 = st->alpha;   // the alpha of step (10), applied in the last kernel
 }
 
 __device__ inline void finish_rho(SolverState* st, const double* tot) {               // (11)
@@ -151,7 +152,9 @@ __host__ __device__ inline void set_coef_streams(const OpT<T>& op, const T* (&ps
 //   done(st, tot):       the scalar step, by the block finishing the last item
 // ---------------------------------------------------------------------------
 
-// K0: r = b - Op x; r_hat_0 = r; u = v = w = 0; sums <r,r>, <b,b>
+// K0: r = b - Op x; r_hat_0 = r; u = 0; sums <r,r>, <b,b>.  (The reference
+// also zeroes v and w in step (1); every iteration writes both before it
+// reads them -- v in step (6), w in step (13) -- so they are left alone.)
 template <typename T, bool UNIT>
 struct FInit {
     using type = T;
@@ -160,7 +163,7 @@ struct FInit {
     static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const T* zs[2];   // x
     const T* ps[NP];  // coefficients, b
-    T *r, *rh, *u, *v, *w;
+    T *r, *rh, *u;
     __device__ void load(const SolverState*) {}
     __device__ T zc(T a, T) const { return a; }
     __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
@@ -169,8 +172,6 @@ struct FInit {
         r[c] = rr;
         rh[c] = rr;
         u[c] = T(0);
-        v[c] = T(0);
-        w[c] = T(0);
         acc[0] += (double)rr * (double)rr;
         acc[1] += (double)bc * (double)bc;
     }
@@ -199,16 +200,18 @@ struct FStep1 {
     __device__ void done(SolverState* st, const double* tot) const { finish_gamma(st, tot, 7); }
 };
 
-// K2: (8) r = r - alpha v; (9) s = Op r; (10) x = x + alpha u; (11) rho1 = <r_hat_0, s>
+// K2: (8) r = r - alpha v; (9) s = Op r; (11) rho1 = <r_hat_0, s>.  Step
+// (10), x = x + alpha u, waits for K5 (x is read by nothing in between and
+// step (15) leaves this u in place), which saves x's read and write here.
 template <typename T, bool UNIT>
 struct FStep2 {
     using type = T;
-    static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 3;
+    static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
-    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
+    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
     const T* zs[2];   // v, r
-    const T* ps[NP];  // coefficients, r_hat_0, u, x
-    T *r_out, *s, *x;
+    const T* ps[NP];  // coefficients, r_hat_0
+    T *r_out, *s;
     T alpha;
     __device__ void load(const SolverState* st) { alpha = (T)st->alpha; }
     __device__ T zc(T v, T r) const { return -alpha * v + r; }
@@ -216,7 +219,6 @@ struct FStep2 {
         r_out[c] = zz[0];
         const T sc = apply_pre<T, UNIT>(p, zz);
         s[c] = sc;
-        x[c] = alpha * p[NC + 1] + p[NC + 2];
         acc[0] += (double)p[NC] * (double)sc;
     }
     __device__ void done(SolverState* st, const double* tot) const { finish_rho(st, tot); }
@@ -244,28 +246,25 @@ struct FStep3 {
     __device__ void done(SolverState* st, const double* tot) const { finish_gamma(st, tot, 14); }
 };
 
-// K4: (15) u = r - beta u; (16) r = r - alpha v; (17) s = s - alpha w;
-//     (18) t = Op s; (19)-(20) <r,s>, <s,s>, <s,t>, <t,t>, <r,t>; (21)-(23)
+// K4: (16) r = r - alpha v; (17) s = s - alpha w; (18) t = Op s;
+//     (19)-(20) <r,s>, <s,s>, <s,t>, <t,t>, <r,t>; (21)-(23).  The new r
+//     goes to the other r buffer, so K5 can still form step (15)'s
+//     u = r - beta u from this kernel's input r.
 template <typename T, bool UNIT>
 struct FStep4 {
     using type = T;
-    static constexpr int Q = 5, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 3;
+    static constexpr int Q = 5, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 2;
     static constexpr bool kCheckDone = true;
     static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
     const T* zs[2];   // w, s
-    const T* ps[NP];  // coefficients, r, u, v
-    T *u, *r, *s_out, *t;
-    T alpha, beta;
-    __device__ void load(const SolverState* st) {
-        alpha = (T)st->alpha;
-        beta = (T)st->beta;
-    }
+    const T* ps[NP];  // coefficients, r (of step (8)), v
+    T *r_out, *s_out, *t;
+    T alpha;
+    __device__ void load(const SolverState* st) { alpha = (T)st->alpha; }
     __device__ T zc(T w, T s) const { return -alpha * w + s; }
     __device__ void center(int64_t c, const T (&zz)[7], const T* p, double* acc) const {
-        const T rc = p[NC];
-        u[c] = rc - beta * p[NC + 1];
-        const T rn = -alpha * p[NC + 2] + rc;
-        r[c] = rn;
+        const T rn = -alpha * p[NC + 1] + p[NC];
+        r_out[c] = rn;
         s_out[c] = zz[0];
         const T tc = apply_pre<T, UNIT>(p, zz);
         t[c] = tc;
@@ -352,34 +351,29 @@ FInit<T, UNIT> make_init(const OpT<T>& op, const VecsT<T>& vs) {
     f.r = vs.r[0];
     f.rh = vs.rh;
     f.u = vs.u[0];
-    f.v = vs.v[0];
-    f.w = vs.w;
     return f;
 }
 template <typename T, bool UNIT>
-FStep1<T, UNIT> make_step1(const OpT<T>& op, const VecsT<T>& vs, int a, int b) {
+FStep1<T, UNIT> make_step1(const OpT<T>& op, const VecsT<T>& vs) {
     FStep1<T, UNIT> f{};
-    f.zs[0] = vs.r[a];
-    f.zs[1] = vs.u[a];
+    f.zs[0] = vs.r[0];
+    f.zs[1] = vs.u[0];
     set_coef_streams<T, UNIT, FStep1<T, UNIT>::NP>(op, f.ps);
     f.ps[NCoef<UNIT>::value] = vs.rh;
-    f.u_out = vs.u[b];
+    f.u_out = vs.u[1];
     f.v = vs.v[0];
     return f;
 }
 template <typename T, bool UNIT>
-FStep2<T, UNIT> make_step2(const OpT<T>& op, const VecsT<T>& vs, int a, int b) {
+FStep2<T, UNIT> make_step2(const OpT<T>& op, const VecsT<T>& vs) {
     constexpr int NC = NCoef<UNIT>::value;
     FStep2<T, UNIT> f{};
     f.zs[0] = vs.v[0];
-    f.zs[1] = vs.r[a];
+    f.zs[1] = vs.r[0];
     set_coef_streams<T, UNIT, FStep2<T, UNIT>::NP>(op, f.ps);
     f.ps[NC] = vs.rh;
-    f.ps[NC + 1] = vs.u[b];
-    f.ps[NC + 2] = vs.x;
-    f.r_out = vs.r[b];
+    f.r_out = vs.r[1];
     f.s = vs.s[0];
-    f.x = vs.x;
     return f;
 }
 template <typename T, bool UNIT>
@@ -394,17 +388,15 @@ FStep3<T, UNIT> make_step3(const OpT<T>& op, const VecsT<T>& vs) {
     return f;
 }
 template <typename T, bool UNIT>
-FStep4<T, UNIT> make_step4(const OpT<T>& op, const VecsT<T>& vs, int b) {
+FStep4<T, UNIT> make_step4(const OpT<T>& op, const VecsT<T>& vs) {
     constexpr int NC = NCoef<UNIT>::value;
     FStep4<T, UNIT> f{};
     f.zs[0] = vs.w;
     f.zs[1] = vs.s[0];
     set_coef_streams<T, UNIT, FStep4<T, UNIT>::NP>(op, f.ps);
-    f.ps[NC] = vs.r[b];
-    f.ps[NC + 1] = vs.u[b];
-    f.ps[NC + 2] = vs.v[1];
-    f.u = vs.u[b];
-    f.r = vs.r[b];
+    f.ps[NC] = vs.r[1];
+    f.ps[NC + 1] = vs.v[1];
+    f.r_out = vs.r[0];
     f.s_out = vs.s[1];
     f.t = vs.t;
     return f;
@@ -789,11 +781,12 @@ inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, co
     return DARE_OK;
 }
 
-// Two cells per thread (K::kPairs) pays off for steps 1 and 3 (256^3: 0.291
-// -> 0.257 ms and 0.289 -> 0.253 ms); with nine streams and five dot products
-// (steps 2 and 4), or many outputs per cell (init, fold), the halved warp
-// count per SM no longer hides the work (step 2: 0.34 -> 0.45 ms, init: 0.29
-// -> 0.38 ms), so those run one cell per thread on the same 32 x 8 tiles.
+// Two cells per thread (K::kPairs) pays off for steps 1, 2 and 3 (seven
+// streams, one dot product; 256^3: 0.291 -> 0.257 ms for step 1, step 2
+// 0.258 ms with pairs); with eight streams and five dot products (step 4:
+// 0.316 -> 0.404 ms with pairs), or many outputs per cell (init: 0.29 ->
+// 0.38 ms, fold), the halved warp count per SM no longer hides the work, so
+// those run one cell per thread on the same 32 x 8 tiles.
 // HALO: the slab variant, which reads m.halo (ignored otherwise).
 template <class K, bool HALO = false>
 inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
@@ -808,33 +801,51 @@ inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, cons
     return launch_march_t<K, 1, HALO>(ctx, g, m1, kern, st, partials);
 }
 
-// K5: (24) x = x + w1 r + w2 s + alpha u; (25) r = r - w1 s - w2 t; ||r||;
+// K5: the deferred steps (10) x = x + alpha1 u1 and (15) u = r1 - beta u1
+//     (u1 the u of step (5), r1 the r of step (8)), then (24)
+//     x = x + w1 r + w2 s + alpha u; (25) r = r - w1 s - w2 t; ||r||;
 //     u = u - w1 v - w2 w; then the next iteration's (3), (4).
 //     `base` / `total`: partial-sum slots shared with other launches (slabs;
 //     0, 0: this launch alone).
 template <typename T>
 __global__ void __launch_bounds__(256) k_step5(int64_t n, T* __restrict__ x, T* __restrict__ r,
                                                const T* __restrict__ s, const T* __restrict__ t,
-                                               T* __restrict__ u, const T* __restrict__ v,
-                                               const T* __restrict__ w, const T* __restrict__ rh,
-                                               SolverState* st, double* partials, int base, int total) {
+                                               T* __restrict__ u, const T* __restrict__ u1,
+                                               const T* __restrict__ r1, const T* __restrict__ v,
+                                               const T* __restrict__ w, const T* __restrict__ rh, SolverState* st,
+                                               double* partials, int base, int total) {
     if (st->done) return;
-    const T w1 = (T)st->omega1, w2 = (T)st->omega2, alpha = (T)st->alpha;
+    const T w1 = (T)st->omega1, w2 = (T)st->omega2, alpha = (T)st->alpha, alpha1 = (T)st->alpha1;
+    const T beta = (T)st->beta;
     double acc[2] = {0., 0.};
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
-        const T rc = r[c], sc = s[c];
-        T xc = w1 * rc + w2 * sc + x[c];
-        xc = alpha * u[c] + xc;
+        const T rc = r[c], sc = s[c], u1c = u1[c];
+        const T x10 = alpha1 * u1c + x[c];
+        const T u15 = r1[c] - beta * u1c;
+        T xc = w1 * rc + w2 * sc + x10;
+        xc = alpha * u15 + xc;
         x[c] = xc;
         const T rn = -w1 * sc + -w2 * t[c] + rc;
         r[c] = rn;
-        u[c] = -w1 * v[c] + -w2 * w[c] + u[c];
+        u[c] = -w1 * v[c] + -w2 * w[c] + u15;
         acc[0] += (double)rn * (double)rn;
         acc[1] += (double)rh[c] * (double)rn;
     }
     double tot[2];
     if (!grid_reduce<2>(acc, partials, &st->count, tot, base, total)) return;
     if (threadIdx.x == 0) finish_update(st, tot);
+}
+
+// Step (10) of an iteration that stopped after it and before K5 (a
+// breakdown in steps (14), (20) or (21)): x = x + alpha1 u1.
+template <typename T>
+__global__ void k_step10(int64_t n, const SolverState* st, const T* __restrict__ u1, T* __restrict__ x) {
+    const T alpha1 = (T)st->alpha1;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+        x[c] = alpha1 * u1[c] + x[c];
+}
+inline bool step10_pending(const SolverState& st) {
+    return st.status == ST_TAU0 || (st.status == ST_BREAKDOWN && (st.step == 14 || st.step == 20));
 }
 
 static __global__ void k_invdiag(const double* __restrict__ dc, double* __restrict__ invd, int64_t n) {

@@ -162,6 +162,7 @@ int dare_bicgstab2_refine(dare_system* s, const dare_solver_params* p, dare_solv
         if (ws->st_host->status == ST_NAN) {
             break;
         }
+        if ((rc = finish_step10(ctx, n, *ws->st_host, ws->st, vs32))) return rc;
         k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, dy, s->x);
         DARE_LAUNCHED(ctx);
         refinements++;

@@ -132,8 +132,7 @@ SlabVecs slab_vectors(dare_slabs* sl, bool jacobi) {
 }
 
 template <bool UNIT>
-int slab_iteration(dare_slabs* sl, const SlabVecs& v, int par) {
-    const int a = par, b = 1 - par;
+int slab_iteration(dare_slabs* sl, const SlabVecs& v) {
     const int S = sl->S;
     int rc;
     std::vector<FStep1<double, UNIT>> k1;
@@ -141,10 +140,10 @@ int slab_iteration(dare_slabs* sl, const SlabVecs& v, int par) {
     std::vector<FStep3<double, UNIT>> k3;
     std::vector<FStep4<double, UNIT>> k4;
     for (int s = 0; s < S; s++) {
-        k1.push_back(make_step1<double, UNIT>(v.op[s], v.vs[s], a, b));
-        k2.push_back(make_step2<double, UNIT>(v.op[s], v.vs[s], a, b));
+        k1.push_back(make_step1<double, UNIT>(v.op[s], v.vs[s]));
+        k2.push_back(make_step2<double, UNIT>(v.op[s], v.vs[s]));
         k3.push_back(make_step3<double, UNIT>(v.op[s], v.vs[s]));
-        k4.push_back(make_step4<double, UNIT>(v.op[s], v.vs[s], b));
+        k4.push_back(make_step4<double, UNIT>(v.op[s], v.vs[s]));
     }
     if ((rc = march_slabs(sl, k1))) return rc;
     if ((rc = march_slabs(sl, k2))) return rc;
@@ -153,8 +152,8 @@ int slab_iteration(dare_slabs* sl, const SlabVecs& v, int par) {
     for (int s = 0; s < S; s++) {
         const VecsT<double>& vs = v.vs[s];
         k_step5<double><<<sl->sblocks[s], 256, 0, sl->ctx->stream>>>(
-            sl->systems[s]->sdev.ncell, vs.x, vs.r[b], vs.s[1], vs.t, vs.u[b], vs.v[1], vs.w, vs.rh, sl->st,
-            sl->partials, sl->sblock_base[s], sl->sblocks_total);
+            sl->systems[s]->sdev.ncell, vs.x, vs.r[0], vs.s[1], vs.t, vs.u[0], vs.u[1], vs.r[1], vs.v[1], vs.w, vs.rh,
+            sl->st, sl->partials, sl->sblock_base[s], sl->sblocks_total);
         DARE_LAUNCHED(sl->ctx);
     }
     return DARE_OK;
@@ -172,8 +171,8 @@ int slab_graph(dare_slabs* sl, const SlabVecs& v, cudaGraphExec_t* out) {
     const int64_t launches0 = ctx->launches;
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        rc = slab_iteration<UNIT>(sl, v, 0);
-        if (rc == DARE_OK) rc = slab_iteration<UNIT>(sl, v, 1);
+        rc = slab_iteration<UNIT>(sl, v);
+        if (rc == DARE_OK) rc = slab_iteration<UNIT>(sl, v);
         const cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
         if (e == cudaSuccess) e = e2;
     }
@@ -540,6 +539,8 @@ int dare_slabs_solve(dare_slabs* sl, const dare_solver_params* p, dare_solve_rep
     rc = jacobi ? slab_run<true>(sl, v, p->max_it, p->check_every) : slab_run<false>(sl, v, p->max_it, p->check_every);
     if (rc) return rc;
     const SolverState st = *sl->st_host;
+    for (int s = 0; s < S; s++)
+        if ((rc = finish_step10(ctx, sl->systems[s]->sdev.ncell, st, sl->st, v.vs[s]))) return rc;
     std::memset(rep, 0, sizeof(*rep));
     rep->iters = st.k;
     rep->b_norm = sqrt(st.bnorm2);
