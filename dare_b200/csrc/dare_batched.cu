@@ -58,6 +58,7 @@ struct BVecs {
 
 struct dare_batch {
     dare_ctx* ctx = nullptr;
+    int device = 0;   // for dare_batch_destroy, which does not touch ctx
     int count = 0;
     int64_t total = 0;
     std::vector<dare_gpu::BInst> host;
@@ -518,6 +519,7 @@ int dare_batch_create(dare_ctx* ctx, int count, const dare_batch_instance* inst,
     dare_batch* bt = new (std::nothrow) dare_batch();
     if (!bt) return DARE_ERR_OOM;
     bt->ctx = ctx;
+    bt->device = ctx->device;
     bt->count = count;
     bt->host.resize(count);
     std::vector<double> work(count);
@@ -564,7 +566,7 @@ int dare_batch_create(dare_ctx* ctx, int count, const dare_batch_instance* inst,
 
 int dare_batch_destroy(dare_batch* bt) {
     if (!bt) return DARE_ERR_BAD_ARG;
-    cudaSetDevice(bt->ctx->device);
+    cudaSetDevice(bt->device);
     cudaFree(bt->d_inst);
     cudaFree(bt->d_order);
     cudaFree(bt->d_out);

@@ -273,6 +273,7 @@ int dare_field_create_n(dare_grid* g, int num_levels, int num_components, dare_f
     dare_field* f = new (std::nothrow) dare_field();
     if (!f) return DARE_ERR_OOM;
     f->grid = g;
+    f->device = ctx->device;
     f->num_levels = num_levels;
     f->ncomp = num_components;
     cudaSetDevice(ctx->device);
@@ -292,7 +293,7 @@ int dare_field_create_n(dare_grid* g, int num_levels, int num_components, dare_f
 
 int dare_field_destroy(dare_field* f) {
     if (!f) return DARE_ERR_BAD_ARG;
-    cudaSetDevice(f->grid->ctx->device);
+    cudaSetDevice(f->device);
     for (int l = 0; l < f->num_levels; l++) cudaFree(f->level[l]);
     delete f;
     return DARE_OK;
@@ -386,6 +387,7 @@ int dare_system_create_n(dare_grid* g, int num_components, dare_system** out) {
     dare_system* s = new (std::nothrow) dare_system();
     if (!s) return DARE_ERR_OOM;
     s->grid = g;
+    s->device = ctx->device;
     s->ncomp = num_components;
     s->sdev = g->dev;
     s->sdev.ncomp = num_components;
@@ -417,7 +419,7 @@ int dare_system_create_n(dare_grid* g, int num_components, dare_system** out) {
 
 int dare_system_destroy(dare_system* s) {
     if (!s) return DARE_ERR_BAD_ARG;
-    cudaSetDevice(s->grid->ctx->device);
+    cudaSetDevice(s->device);
     dare_solver_ws_free(s->ws);
     cudaFree(s->diag);
     cudaFree(s->rhs);

@@ -82,8 +82,12 @@ struct dare_grid {
     dare_gpu::GridDev dev{};
 };
 
+// Every handle records its device at creation: its destroy function uses
+// that, never the context or grid it was made from, so handles may be
+// destroyed in any order (a garbage collector's, for instance).
 struct dare_field {
     dare_grid* grid = nullptr;
+    int device = 0;
     int num_levels = 0;
     int ncomp = 1;                // components, stored component-major: level[l][c * ncell_ghosted + cell]
     double* level[8] = {nullptr};
@@ -94,6 +98,7 @@ void dare_solver_ws_free(dare_solver_ws* ws);
 
 struct dare_system {
     dare_grid* grid = nullptr;
+    int device = 0;
     int ncomp = 1;               // field components (block-diagonal, one 7-point stencil each)
     dare_gpu::GridDev sdev{};    // the solver's view: components stacked along i
     int bc_type[6] = {0, 0, 0, 0, 0, 0};        // the faces' conditions of every component ...

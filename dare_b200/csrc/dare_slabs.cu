@@ -44,6 +44,7 @@ constexpr int kMaxSlabs = 8;
 
 struct dare_slabs {
     dare_ctx* ctx = nullptr;
+    int device = 0;                  // for dare_slabs_destroy, which does not touch ctx
     GridDev global{};
     int S = 0;
     int periodic_x = 0;
@@ -277,6 +278,7 @@ int dare_slabs_create(dare_system* sys, int num_slabs, int num_levels, dare_slab
     dare_slabs* sl = new (std::nothrow) dare_slabs();
     if (!sl) return DARE_ERR_OOM;
     sl->ctx = ctx;
+    sl->device = ctx->device;
     sl->global = G;
     sl->S = num_slabs;
     sl->periodic_x = G.periodic[0];
@@ -349,7 +351,7 @@ int dare_slabs_create(dare_system* sys, int num_slabs, int num_levels, dare_slab
 
 int dare_slabs_destroy(dare_slabs* sl) {
     if (!sl) return DARE_ERR_BAD_ARG;
-    cudaSetDevice(sl->ctx->device);
+    cudaSetDevice(sl->device);
     slabs_free(sl);
     return DARE_OK;
 }

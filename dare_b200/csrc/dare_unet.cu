@@ -2178,6 +2178,7 @@ int dare_unet_create(dare_ctx* ctx, const int n[3], uint64_t seed, dare_unet** o
     cudaSetDevice(ctx->device);
     dare_unet* net = new dare_unet();
     net->ctx = ctx;
+    net->device = ctx->device;
     for (int d = 0; d < 3; d++) net->n[d] = n[d];
     net->ncell = (int64_t)n[0] * n[1] * n[2];
     for (int l = 0; l < kLevels; l++) net->geo[l] = make_geom(n[0] >> l, n[1] >> l, n[2] >> l);
@@ -2322,7 +2323,7 @@ int dare_unet_debug_skip_plane(dare_unet* net) {
 
 int dare_unet_destroy(dare_unet* net) {
     if (!net) return DARE_OK;
-    cudaSetDevice(net->ctx->device);
+    cudaSetDevice(net->device);
     unet_free(net);
     delete net;
     return DARE_OK;

@@ -114,6 +114,7 @@ struct Layer {
 
 struct dare_unet {
     dare_ctx* ctx = nullptr;
+    int device = 0;            // for dare_unet_destroy, which does not touch ctx
     int n[3] = {0, 0, 0};      // the grid the convolutions run on
     int64_t ncell = 0;
     // Coarse-correction form: the network acts on the 2x restricted grid of

@@ -559,3 +559,64 @@ def test_host_resident_steps_match_single_calls(ctx):
     assert np.array_equal(host, ref)
     with pytest.raises(D.DareError):
         D.timesteps_host(s, f, asm, solver, 1, np.zeros(g.num_cells_ghosted))
+
+
+@pytest.mark.parametrize("precond", ["NONE", "JACOBI"])
+def test_breakdown_after_step10_keeps_its_update(ctx, precond):
+    """A = 2 I: alpha = 1/2 makes r' = r - alpha v exactly 0, so s = 0 and
+    gamma = 0 at step (14).  The reference leaves its loop there with step
+    (10)'s x = x0 + alpha u, the exact solution b / 2 (BiCGStab2.inl:373-392);
+    the device solve, which applies step (10) in its last kernel, must apply
+    it on this exit too.  The oracle's solve stops at the same step."""
+    n = (6, 5, 4)
+    g = D.Grid(ctx, n, None, 2, (1, 1, 1))
+    s = D.MatrixSystem(g)
+    N = g.num_cells
+    diag = np.zeros((7, N))
+    diag[0] = 2.0
+    rng = np.random.default_rng(11)
+    rhs, x0 = rng.random(N), rng.random(N)
+    s.set_coefficients(diag, rhs, x0)
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-300, "Maximum Iterations": 50}, precond=precond).solve(s)
+    assert rep["status_name"] == "breakdown" and rep["breakdown_step"] == 14, rep
+    x = s.solution()
+    # x0 + (b - 2 x0) / 2 (or D^-1 (x0 + (b - x0))): b / 2 up to the rounding
+    # of that sum; without step (10) it would be x0
+    np.testing.assert_allclose(x, rhs / 2, rtol=0, atol=2e-16)
+    if precond == "NONE":
+        # the oracle stops at the same step with the same x.  (With Jacobi its
+        # OpenMP dot products may sum in another order, alpha misses 1 by an
+        # ulp, and it goes on with steps of tiny quantities divided by tiny
+        # quantities, which end anywhere: no comparator for this exit.)
+        rp, cols, vals = s.export_csr()
+        ox, info = O.bicgstab2(rp, cols, vals, rhs, x0, 1e-300, 50, O.PREC_NONE)
+        np.testing.assert_allclose(x, ox, rtol=0, atol=1e-15)
+    # the FP32 inner solves break down the same way; their step (10) makes
+    # the correction exact, so the refinement converges without the fallback
+    s.set_coefficients(diag, rhs, x0)
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 50, "tol_relative": 1},
+                      precond="JACOBI", precision="FP32_REFINE").solve(s)
+    assert rep["converged"] and rep["fallback_used"] == 0, rep
+    np.testing.assert_allclose(s.solution(), rhs / 2, rtol=1e-6)
+
+
+def test_handles_outlive_their_context():
+    """Handles may be destroyed after the context they came from (a garbage
+    collector picks the order): each destroy uses the device it recorded,
+    and no stale CUDA error reaches the next launch."""
+    c1 = D.Context(0)
+    g = D.Grid(c1, (8, 6, 4), None, 2, (1, 1, 1))
+    f = D.Field(g, 2)
+    s = D.MatrixSystem(g)
+    sl = D.Slabs(s, 2)
+    c1.close()
+    del sl, s, f, g
+    c2 = D.Context(0)
+    g2 = D.Grid(c2, (8, 6, 4), None, 2, (1, 1, 1))
+    s2 = D.MatrixSystem(g2)
+    diag = np.zeros((7, g2.num_cells))
+    diag[0] = 7.0
+    diag[1:] = -1.0
+    s2.set_coefficients(diag, np.random.default_rng(5).random(g2.num_cells), np.zeros(g2.num_cells))
+    rep = D.BiCGStab2({"Convergence Tolerance": 1e-12, "Maximum Iterations": 100}).solve(s2)
+    assert rep["converged"]

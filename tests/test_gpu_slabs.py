@@ -211,3 +211,22 @@ def test_cxx_slabs_match_whole_grid(tmp_path):
     assert lines[1]["slabs"] == 3
     assert lines[0]["iters"] == lines[1]["iters"]
     assert rel_l2(fields[1].reshape(-1), fields[0].reshape(-1)) < 1e-10
+
+
+def test_slab_breakdown_after_step10_keeps_its_update(ctx):
+    """A = 2 I on two slabs: the solve stops at step (14) (gamma = 0) after
+    step (10), whose update every slab applies on that exit: x = b / 2."""
+    g = D.Grid(ctx, (6, 5, 4), None, 2, (1, 1, 1))
+    s = D.MatrixSystem(g)
+    sl = D.Slabs(s, 2)
+    rng = np.random.default_rng(12)
+    rhs, x0 = rng.random(g.num_cells), rng.random(g.num_cells)
+    P = 5 * 4
+    for k, (i0, i1) in enumerate(sl.ranges):
+        rows = (i1 - i0) * P
+        diag = np.zeros((7, rows))
+        diag[0] = 2.0
+        sl.system(k).set_coefficients(diag, rhs[i0 * P:i1 * P], x0[i0 * P:i1 * P])
+    rep = sl.solve(D.BiCGStab2({"Convergence Tolerance": 1e-300, "Maximum Iterations": 50}, precond="NONE"))
+    assert rep["status_name"] == "breakdown" and rep["breakdown_step"] == 14, rep
+    np.testing.assert_allclose(sl.solution(), rhs / 2, rtol=0, atol=2e-16)
