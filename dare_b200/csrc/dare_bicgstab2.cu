@@ -188,6 +188,25 @@ int launch_fold(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double
     return launch_march(ctx, g, m, make_fold(diag, invd, ahat, g.ncell), st, partials);
 }
 
+// invd = 1 / diag, then the fold and the init kernel in one pass (FFoldInit)
+int launch_fold_init(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd,
+                     double* ahat, const VecsT<double>& vs, SolverState* st, double* partials) {
+    const int64_t n = g.ncell;
+    k_invdiag<<<grid_blocks(ctx, n, 256, 8), 256, 0, ctx->stream>>>(diag, invd, n);
+    DARE_LAUNCHED(ctx);
+    FFoldInit f{};
+    f.zs[0] = invd;
+    f.zs[1] = vs.x;
+    for (int q = 0; q < 6; q++) f.ps[q] = diag + (q + 1) * n;
+    f.ps[6] = vs.b;
+    f.ahat = ahat;
+    f.r = vs.r[0];
+    f.rh = vs.rh;
+    f.u = vs.u[0];
+    f.n = n;
+    return launch_march(ctx, g, m, f, st, partials);
+}
+
 int launch_fold32(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const double* diag, double* invd, float* ahat32,
                   SolverState* st, double* partials) {
     const int eb = grid_blocks(ctx, g.ncell, 256, 8);
@@ -335,11 +354,8 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
     init.max_it = p->max_it;
     init.tol_relative = p->tol_relative;
     DARE_CUDA(ctx, cudaMemcpyAsync(ws->st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
-    if (jacobi) {
-        if ((rc = launch_fold(ctx, g, m, s->diag, ws->invd, ws->ahat, ws->st, ws->partials))) return rc;
-    }
     VecsT<double> vs = carve_vecs<double>(ws->vec, n, s->x, s->rhs);
-    rc = jacobi ? launch_init<double, true>(ctx, g, m, folded, vs, ws->st, ws->partials)
+    rc = jacobi ? launch_fold_init(ctx, g, m, s->diag, ws->invd, ws->ahat, vs, ws->st, ws->partials)
                 : launch_init<double, false>(ctx, g, m, full, vs, ws->st, ws->partials);
     if (rc) return rc;
     rc = jacobi ? run_iterations<double, true>(ctx, g, m, ws->stream_blocks, folded, vs, ws->st, ws->st_host,

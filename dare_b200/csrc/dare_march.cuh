@@ -14,6 +14,8 @@
 // last item, so results do not depend on which block took which item.
 #pragma once
 
+#include <type_traits>
+
 #include "dare_bicgstab2.cuh"
 
 namespace dare_gpu {
@@ -334,6 +336,59 @@ struct FFold32 {
         for (int q = 0; q < 6; q++) ahat[q * n + c] = (float)(p[q] * zz[q + 1]);
     }
     __device__ void done(SolverState*, const double*) const {}
+};
+
+// K0 with the Jacobi fold, one pass instead of FFold then FInit: Ahat[q][c] =
+// A[q][c] * invd[neighbour_q(c)] written, then r = b - Ahat y from those
+// values, r_hat_0 = r, u = 0; sums <r,r>, <b,b>.  The products and sums are
+// the two kernels' own, in their order, so the results are the same bits.
+// Split operands (kSplit): the kernel hands over both staged arrays' seven
+// values, invd and y, instead of one combined operand.
+struct FFoldInit {
+    using type = double;
+    static constexpr int Q = 2, NZ = 2, NP = 7;
+    static constexpr bool kCheckDone = false;
+    static constexpr bool kPairs = false;
+    static constexpr bool kSplit = true;
+    const double* zs[2];   // invd, y
+    const double* ps[NP];  // the 6 off-diagonals of A, b
+    double *ahat, *r, *rh, *u;
+    int64_t n;
+    __device__ void load(const SolverState*) {}
+    __device__ double zc(double a, double) const { return a; }   // (the combined operand is not used)
+    __device__ void center2(int64_t c, const double (&iv)[7], const double (&y)[7], const double* p,
+                            double* acc) const {
+        double a[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            a[q] = p[q] * iv[q + 1];
+            ahat[q * n + c] = a[q];
+        }
+        double yy = y[0];   // apply_pre<double, true>(a, y)
+        yy += a[0] * y[1];
+        yy += a[1] * y[2];
+        yy += a[2] * y[3];
+        yy += a[3] * y[4];
+        yy += a[4] * y[5];
+        yy += a[5] * y[6];
+        const double bc = p[6];
+        const double rr = bc - yy;
+        r[c] = rr;
+        rh[c] = rr;
+        u[c] = 0.;
+        acc[0] += rr * rr;
+        acc[1] += bc * bc;
+    }
+    __device__ void done(SolverState* st, const double* tot) const { finish_init(st, tot); }
+};
+
+template <class K, class = void>
+struct SplitOperands {
+    static constexpr bool value = false;
+};
+template <class K>
+struct SplitOperands<K, std::void_t<decltype(K::kSplit)>> {
+    static constexpr bool value = K::kSplit;
 };
 
 // ---------------------------------------------------------------------------
@@ -672,10 +727,19 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
         for (int q = 0; q < QA; q++) acc[q] = 0.;
         cp_async_wait<2>();
         __syncthreads();
+        constexpr bool SPLIT = SplitOperands<K>::value;
         T zprev[CPT];
+        T zprev_b = T(0);   // split operands: the second array's value at plane i - 1
+        if constexpr (SPLIT) {
+            const T* s0 = smem + (size_t)slot_of(G, G.i0 - 1) * STAGE + (ty + 1) * W + IC + tx;
+            zprev[0] = G.inside ? s0[0] : T(0);
+            zprev_b = G.inside ? s0[ZT] : T(0);
+        } else {
 #pragma unroll
-        for (int c = 0; c < CPT; c++)
-            zprev[c] = G.inside ? zval(smem + (size_t)slot_of(G, G.i0 - 1) * STAGE, ty + 1, IC + CPT * tx + c) : T(0);
+            for (int c = 0; c < CPT; c++)
+                zprev[c] =
+                    G.inside ? zval(smem + (size_t)slot_of(G, G.i0 - 1) * STAGE, ty + 1, IC + CPT * tx + c) : T(0);
+        }
         __syncthreads();
         for (int i = G.i0; i < G.i1; i++) {
             if (i + 2 <= G.i1) stage(G, i + 2, i + 2 < G.i1);   // reuses the slot of plane i-1
@@ -685,7 +749,22 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
             const T* sb = smem + (size_t)slot_of(G, i) * STAGE;
             const T* sn = smem + (size_t)slot_of(G, i + 1) * STAGE;
             if (G.inside) {
-                if constexpr (CPT == 1) {
+                if constexpr (SPLIT) {
+                    static_assert(CPT == 1, "split operands run one cell per thread");
+                    const int col = IC + tx;
+                    auto raw = [&](const T* b, int z, int row, int cc) { return b[z * ZT + row * W + cc]; };
+                    const T a0 = raw(sb, 0, ty + 1, col), b0 = raw(sb, 1, ty + 1, col);
+                    const T za[7] = {a0, zprev[0], raw(sn, 0, ty + 1, col), raw(sb, 0, ty, col), raw(sb, 0, ty + 2, col),
+                                     raw(sb, 0, ty + 1, col - 1), raw(sb, 0, ty + 1, col + 1)};
+                    const T zb[7] = {b0, zprev_b, raw(sn, 1, ty + 1, col), raw(sb, 1, ty, col), raw(sb, 1, ty + 2, col),
+                                     raw(sb, 1, ty + 1, col - 1), raw(sb, 1, ty + 1, col + 1)};
+                    T pv[NP];
+#pragma unroll
+                    for (int q = 0; q < NP; q++) pv[q] = sb[NZ * ZT + q * NCT + tid];
+                    k.center2((int64_t)i * plane + G.o_own, za, zb, pv, acc);
+                    zprev[0] = a0;
+                    zprev_b = b0;
+                } else if constexpr (CPT == 1) {
                     const int col = IC + tx;
                     const T zcur = zval(sb, ty + 1, col);
                     const T z7[7] = {zcur, zprev[0], zval(sn, ty + 1, col), zval(sb, ty, col), zval(sb, ty + 2, col),
@@ -793,7 +872,9 @@ inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, cons
                         double* partials) {
     if (m.nitems > kMaxBlocks || m.item_base + m.nitems > kMaxBlocks || m.nitems_total > kMaxBlocks)
         return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
-    if (m.cpt == 2 && K::kPairs) return launch_march_t<K, 2, HALO>(ctx, g, m, kern, st, partials);
+    if constexpr (K::kPairs) {
+        if (m.cpt == 2) return launch_march_t<K, 2, HALO>(ctx, g, m, kern, st, partials);
+    }
     if (m.cpt == 1) return launch_march_t<K, 1, HALO>(ctx, g, m, kern, st, partials);
     MarchCfg m1 = m;   // the same tiles, one cell per thread
     m1.cpt = 1;
