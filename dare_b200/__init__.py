@@ -684,8 +684,8 @@ class Slabs:
                 fx = np.concatenate([fx[i0:n0], fx[0:1]])
             else:
                 fx = fx[i0:i1 + 1]
-            out.append((np.ascontiguousarray(fx), np.ascontiguousarray(np.asarray(faces[1])[i0:i1]),
-                        np.ascontiguousarray(np.asarray(faces[2])[i0:i1])))
+            out.append((np.ascontiguousarray(fx),) +
+                       tuple(np.ascontiguousarray(np.asarray(f)[i0:i1]) for f in faces[1:]))
         return out
 
     def _descs(self, assemblies):

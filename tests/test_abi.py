@@ -52,6 +52,18 @@ def test_null_arguments_rejected_without_device(gpu_lib):
     assert gpu_lib.dare_field_exchange_halo(None) != 0
     assert gpu_lib.dare_system_set_bc(None, 1, 1, 0.0) != 0
     assert gpu_lib.dare_bicgstab2_solve(None, None, None) != 0
+    # the slab path and the host-resident loop check their handles first too
+    assert gpu_lib.dare_slabs_create(None, 2, 2, None) != 0
+    assert gpu_lib.dare_slabs_destroy(None) != 0
+    assert gpu_lib.dare_slabs_count(None) < 0
+    assert gpu_lib.dare_slabs_system(None, 0) is None
+    assert gpu_lib.dare_slabs_field(None, 0) is None
+    assert gpu_lib.dare_slabs_scatter(None, None) != 0
+    assert gpu_lib.dare_slabs_exchange_halo(None) != 0
+    assert gpu_lib.dare_slabs_assemble(None, None) != 0
+    assert gpu_lib.dare_slabs_solve(None, None, None) != 0
+    assert gpu_lib.dare_slabs_set_bc(None, 1, 1, 0.0) != 0
+    assert gpu_lib.dare_timesteps_host(None, None, None, None, 1, None, None) != 0
 
 
 def test_solver_defaults_match_reference():
@@ -65,7 +77,7 @@ def test_solver_defaults_match_reference():
 def test_cxx_header_compiles(tmp_path):
     src = tmp_path / "t.cpp"
     src.write_text('#include "dare_gpu.hpp"\nint main() { dare_b200::BiCGStab2 s({{"Maximum Iterations", 7}});'
-                   ' return s.Params().max_it == 7 ? 0 : 1; }\n')
+                   ' (void)sizeof(dare_b200::Slabs); return s.Params().max_it == 7 ? 0 : 1; }\n')
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
                     str(src)], check=True)
 
