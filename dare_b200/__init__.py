@@ -619,11 +619,12 @@ class Slabs:
     in every dot product of the solve.  Slab s owns planes ``ranges[s]`` with
     its own field, rows and solver vectors; boundary planes cross to the x
     neighbours before every assembly (num_ghost planes of the field) and
-    every SpMV (one plane of the operand).  One field component, FP64."""
+    every SpMV (one plane of the operand), for every field component.  FP64."""
 
     def __init__(self, system: MatrixSystem, num_slabs: int, num_levels: int = 2):
         self.ctx = system.grid.ctx
         self.grid = system.grid
+        self.components = system.components
         h = C.c_void_p()
         _check(lib().dare_slabs_create(system.h, num_slabs, num_levels, C.byref(h)), self.ctx.h, "slabs_create")
         self.h = h
@@ -646,9 +647,9 @@ class Slabs:
         v._owned = False
         v.h = C.c_void_p(lib().dare_slabs_system(self.h, s))
         v.grid = self.grid
-        v.components = 1
+        v.components = self.components
         i0, i1 = self.ranges[s]
-        v.rows = (i1 - i0) * self.grid.n[1] * self.grid.n[2]
+        v.rows = (i1 - i0) * self.grid.n[1] * self.grid.n[2] * self.components
         return v
 
     def field_ptr(self, s: int, level: int = 0) -> int:

@@ -54,7 +54,8 @@ struct MarchCfg {
     // Slab decomposition (dare_slabs.cu): the first partial-sum slot of this
     // launch's items and the items of all launches that share the reduction
     // (0: this launch alone), and per operand input the planes below the
-    // first and above the last plane of the slab (null: wrap / zero as usual).
+    // first and above the last plane of the slab, one per field component
+    // (null: wrap / zero as usual).
     int item_base = 0;
     int nitems_total = 0;
     const void* halo[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};

@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
             if constexpr (HALO) {
                 const int hside = p - G.cb < 0 ? 0 : (p - G.cb >= n0c ? 1 : -1);   // a plane past the slab
                 if (hside >= 0 && m.halo[z][hside]) {   // the neighbour's plane, exchanged into a local buffer
-                    src = static_cast<const T*>(m.halo[z][hside]);
+                    src = static_cast<const T*>(m.halo[z][hside]) + (int64_t)(G.cb / n0c) * plane;   // [component][plane]
                     zb = 0;
                     zv = true;
                 }

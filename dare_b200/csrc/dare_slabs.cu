@@ -36,8 +36,6 @@ using namespace dare_gpu;
 
 namespace dare_gpu {
 int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old);
-int launch_scatter(dare_ctx* ctx, const GridDev& g, const double* x, double* phi);
-int launch_halo(dare_ctx* ctx, const GridDev& g, double* phi);
 }  // namespace dare_gpu
 
 constexpr int kMaxSlabs = 8;
@@ -46,6 +44,7 @@ struct dare_slabs {
     dare_ctx* ctx = nullptr;
     int device = 0;                  // for dare_slabs_destroy, which does not touch ctx
     GridDev global{};
+    int ncomp = 1;                   // field components (stacked along i in the solver's vectors)
     int S = 0;
     int periodic_x = 0;
     std::vector<int> i0, i1;
@@ -56,7 +55,7 @@ struct dare_slabs {
     std::vector<MarchCfg> march;
     std::vector<int> item_base, sblocks, sblock_base;
     int items_total = 0, sblocks_total = 0;
-    double* halo = nullptr;          // per slab: [2 operand inputs][2 sides][one plane]
+    double* halo = nullptr;          // per slab: [2 operand inputs][2 sides][component][one plane]
     double* partials = nullptr;      // kMaxQ * kMaxBlocks (+ one scratch value)
     SolverState* st = nullptr;
     SolverState* st_host = nullptr;  // pinned
@@ -72,13 +71,18 @@ int64_t plane_cells(const dare_slabs* sl) { return (int64_t)sl->global.n[1] * sl
 int64_t ghosted_plane(const dare_slabs* sl) { return (int64_t)sl->global.gn[1] * sl->global.gn[2]; }
 
 double* halo_buf(dare_slabs* sl, int s, int z, int side) {
-    return sl->halo + ((size_t)(s * 2 + z) * 2 + side) * (size_t)plane_cells(sl);
+    return sl->halo + ((size_t)(s * 2 + z) * 2 + side) * (size_t)sl->ncomp * plane_cells(sl);
 }
 
-// The one transfer primitive of the slab path: `bytes` from slab memory to
-// slab memory, in stream order.
-int transfer(dare_ctx* ctx, void* dst, const void* src, size_t bytes) {
-    DARE_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+// The transfer primitive of the slab path: `count` runs of `bytes` from slab
+// memory to slab memory (runs `src_pitch` / `dst_pitch` bytes apart: one run
+// per field component), in stream order.
+int transfer(dare_ctx* ctx, void* dst, const void* src, size_t bytes, int count = 1, size_t dst_pitch = 0,
+             size_t src_pitch = 0) {
+    for (int c = 0; c < count; c++)
+        DARE_CUDA(ctx, cudaMemcpyAsync(static_cast<char*>(dst) + c * dst_pitch,
+                                       static_cast<const char*>(src) + c * src_pitch, bytes, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
     return DARE_OK;
 }
 
@@ -92,14 +96,22 @@ int march_slabs(dare_slabs* sl, const std::vector<K>& ks) {
     dare_ctx* ctx = sl->ctx;
     const int64_t P = plane_cells(sl);
     int rc;
+    const int nc = sl->ncomp;
+    const size_t pb = (size_t)P * sizeof(T);   // one plane
     for (int s = 0; s < sl->S; s++) {
         const int lo = lower(sl, s), hi = upper(sl, s);
         for (int z = 0; z < K::NZ; z++) {
+            // each component's last plane of the lower neighbour, first plane of the upper one
             if (lo >= 0) {
-                const int64_t last = (int64_t)(sl->i1[lo] - sl->i0[lo] - 1) * P;
-                if ((rc = transfer(ctx, halo_buf(sl, s, z, 0), ks[lo].zs[z] + last, P * sizeof(T)))) return rc;
+                const int nl = sl->i1[lo] - sl->i0[lo];
+                if ((rc = transfer(ctx, halo_buf(sl, s, z, 0), ks[lo].zs[z] + (int64_t)(nl - 1) * P, pb, nc, pb,
+                                   (size_t)nl * pb)))
+                    return rc;
             }
-            if (hi >= 0 && (rc = transfer(ctx, halo_buf(sl, s, z, 1), ks[hi].zs[z], P * sizeof(T)))) return rc;
+            if (hi >= 0) {
+                const int nh = sl->i1[hi] - sl->i0[hi];
+                if ((rc = transfer(ctx, halo_buf(sl, s, z, 1), ks[hi].zs[z], pb, nc, pb, (size_t)nh * pb))) return rc;
+            }
         }
     }
     for (int s = 0; s < sl->S; s++) {
@@ -267,7 +279,6 @@ int dare_slabs_create(dare_system* sys, int num_slabs, int num_levels, dare_slab
     *out = nullptr;
     dare_ctx* ctx = sys->grid->ctx;
     const GridDev& G = sys->grid->dev;
-    if (sys->ncomp != 1) return set_error(ctx, DARE_ERR_UNSUPPORTED, "dare_slabs_create: one field component");
     if (num_slabs < 1 || num_slabs > kMaxSlabs)
         return set_error(ctx, DARE_ERR_BAD_ARG, "dare_slabs_create: 1 to 8 slabs");
     // every slab holds at least ng planes (the field exchange) and two (the operand halo)
@@ -280,6 +291,7 @@ int dare_slabs_create(dare_system* sys, int num_slabs, int num_levels, dare_slab
     sl->ctx = ctx;
     sl->device = ctx->device;
     sl->global = G;
+    sl->ncomp = sys->ncomp;
     sl->S = num_slabs;
     sl->periodic_x = G.periodic[0];
     const int base = G.n[0] / num_slabs, extra = G.n[0] % num_slabs;
@@ -305,10 +317,10 @@ int dare_slabs_create(dare_system* sys, int num_slabs, int num_levels, dare_slab
         g->dev.origin[0] = G.origin[0] + i0 * G.dx[0];
         sl->grids.push_back(g);
         dare_field* f = nullptr;
-        if ((rc = dare_field_create_n(g, num_levels, 1, &f)) != DARE_OK) break;
+        if ((rc = dare_field_create_n(g, num_levels, sys->ncomp, &f)) != DARE_OK) break;
         sl->fields.push_back(f);
         dare_system* sy = nullptr;
-        if ((rc = dare_system_create_n(g, 1, &sy)) != DARE_OK) break;
+        if ((rc = dare_system_create_n(g, sys->ncomp, &sy)) != DARE_OK) break;
         sl->systems.push_back(sy);
         std::memcpy(sy->bc_type, sys->bc_type, sizeof(sy->bc_type));
         std::memcpy(sy->bc_value, sys->bc_value, sizeof(sy->bc_value));
@@ -334,7 +346,7 @@ int dare_slabs_create(dare_system* sys, int num_slabs, int num_levels, dare_slab
     }
     cudaError_t e = cudaSuccess;
     if (rc == DARE_OK) {
-        e = cudaMalloc(&sl->halo, (size_t)num_slabs * 4 * plane_cells(sl) * sizeof(double));
+        e = cudaMalloc(&sl->halo, (size_t)num_slabs * 4 * sl->ncomp * plane_cells(sl) * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&sl->partials, (size_t)kMaxQ * kMaxBlocks * sizeof(double) + 64);
         if (e == cudaSuccess) e = cudaMalloc(&sl->st, sizeof(SolverState));
         if (e == cudaSuccess) e = cudaMemsetAsync(sl->st, 0, sizeof(SolverState), ctx->stream);
@@ -395,18 +407,21 @@ int dare_slabs_set_bc(dare_slabs* sl, int face, int type, double value) {
 // its planes with ng ghost planes on either side (the global field's own
 // ghosts at a bounded end), as a rank receives its part of the initial field.
 int dare_slabs_scatter(dare_slabs* sl, dare_field* f) {
-    if (!sl || !f || f->ncomp != 1 || f->grid->dev.ncell_ghosted != sl->global.ncell_ghosted ||
+    if (!sl || !f || f->ncomp != sl->ncomp || f->grid->dev.ncell_ghosted != sl->global.ncell_ghosted ||
         f->grid->dev.n[0] != sl->global.n[0] || f->num_levels < sl->fields[0]->num_levels)
         return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = sl->ctx;
     cudaSetDevice(ctx->device);
     const int64_t GP = ghosted_plane(sl);
+    const size_t gcomp = (size_t)sl->global.ncell_ghosted * sizeof(double);   // one component of f
+    int rc;
     for (int s = 0; s < sl->S; s++) {
         dare_field* sf = sl->fields[s];
         const size_t bytes = (size_t)sf->grid->dev.ncell_ghosted * sizeof(double);
         for (int l = 0; l < sf->num_levels; l++)
-            DARE_CUDA(ctx, cudaMemcpyAsync(sf->level[l], f->level[l] + (int64_t)sl->i0[s] * GP, bytes,
-                                           cudaMemcpyDeviceToDevice, ctx->stream));
+            if ((rc = transfer(ctx, sf->level[l], f->level[l] + (int64_t)sl->i0[s] * GP, bytes, sl->ncomp, bytes,
+                               gcomp)))
+                return rc;
     }
     return DARE_OK;
 }
@@ -414,22 +429,25 @@ int dare_slabs_scatter(dare_slabs* sl, dare_field* f) {
 // The slabs' planes back into every level of the global field f (the first
 // slab's lower and the last slab's upper ghost planes included).
 int dare_slabs_gather(dare_slabs* sl, dare_field* f) {
-    if (!sl || !f || f->ncomp != 1 || f->grid->dev.ncell_ghosted != sl->global.ncell_ghosted ||
+    if (!sl || !f || f->ncomp != sl->ncomp || f->grid->dev.ncell_ghosted != sl->global.ncell_ghosted ||
         f->grid->dev.n[0] != sl->global.n[0] || f->num_levels < sl->fields[0]->num_levels)
         return DARE_ERR_BAD_ARG;
     dare_ctx* ctx = sl->ctx;
     cudaSetDevice(ctx->device);
     const int64_t GP = ghosted_plane(sl);
     const int og = sl->global.og[0];
+    const size_t gcomp = (size_t)sl->global.ncell_ghosted * sizeof(double);
+    int rc;
     for (int s = 0; s < sl->S; s++) {
         dare_field* sf = sl->fields[s];
+        const size_t scomp = (size_t)sf->grid->dev.ncell_ghosted * sizeof(double);
         const int ns = sl->i1[s] - sl->i0[s];
         const int p0 = s == 0 ? 0 : og;                            // first slab plane copied
         const int p1 = s == sl->S - 1 ? ns + 2 * og : og + ns;     // one past the last
         for (int l = 0; l < sf->num_levels; l++)
-            DARE_CUDA(ctx, cudaMemcpyAsync(f->level[l] + (int64_t)(sl->i0[s] + p0) * GP, sf->level[l] + (int64_t)p0 * GP,
-                                           (size_t)(p1 - p0) * GP * sizeof(double), cudaMemcpyDeviceToDevice,
-                                           ctx->stream));
+            if ((rc = transfer(ctx, f->level[l] + (int64_t)(sl->i0[s] + p0) * GP, sf->level[l] + (int64_t)p0 * GP,
+                               (size_t)(p1 - p0) * GP * sizeof(double), sl->ncomp, gcomp, scomp)))
+                return rc;
     }
     return DARE_OK;
 }
@@ -443,20 +461,23 @@ int dare_slabs_exchange_halo(dare_slabs* sl) {
     cudaSetDevice(ctx->device);
     int rc;
     for (int s = 0; s < sl->S; s++)
-        if ((rc = launch_halo(ctx, sl->grids[s]->dev, sl->fields[s]->level[0]))) return rc;
+        if ((rc = dare_field_exchange_halo(sl->fields[s]))) return rc;   // every component
     const int64_t GP = ghosted_plane(sl);
     const int og = sl->global.og[0];
     const size_t bytes = (size_t)og * GP * sizeof(double);
+    auto comp = [&](int s) { return (size_t)sl->fields[s]->grid->dev.ncell_ghosted * sizeof(double); };
     for (int s = 0; s < sl->S; s++) {
         const int lo = lower(sl, s), hi = upper(sl, s);
         double* own = sl->fields[s]->level[0];
         const int ns = sl->i1[s] - sl->i0[s];
         if (lo >= 0) {
             const int nl = sl->i1[lo] - sl->i0[lo];
-            if ((rc = transfer(ctx, own, sl->fields[lo]->level[0] + (int64_t)nl * GP, bytes))) return rc;
+            if ((rc = transfer(ctx, own, sl->fields[lo]->level[0] + (int64_t)nl * GP, bytes, sl->ncomp, comp(s),
+                               comp(lo))))
+                return rc;
         }
         if (hi >= 0 && (rc = transfer(ctx, own + (int64_t)(og + ns) * GP, sl->fields[hi]->level[0] + (int64_t)og * GP,
-                                      bytes)))
+                                      bytes, sl->ncomp, comp(s), comp(hi))))
             return rc;
     }
     return DARE_OK;
@@ -490,7 +511,7 @@ int dare_slabs_assemble(dare_slabs* sl, const dare_assembly_desc* descs) {
 int dare_slabs_copy_to(dare_slabs* sl) {
     if (!sl) return DARE_ERR_BAD_ARG;
     for (int s = 0; s < sl->S; s++) {
-        const int rc = launch_scatter(sl->ctx, sl->grids[s]->dev, sl->systems[s]->x, sl->fields[s]->level[0]);
+        const int rc = dare_system_copy_to(sl->systems[s], sl->fields[s]);   // every component
         if (rc) return rc;
     }
     return DARE_OK;

@@ -322,11 +322,11 @@ DARE_API int dare_timesteps_host(dare_system* s, dare_field* f, const dare_assem
  * plane longer) with its own field (every time level, ghosted), system rows
  * and solver vectors.  Before an assembly num_ghost boundary planes of the
  * field cross to each x neighbour; before every SpMV one boundary plane of
- * the operand; every dot product sums all slabs' partials.  One field
- * component, FP64 solves (plain or Jacobi), 1 to 8 slabs of at least
- * max(num_ghost, 2) planes.  The slabs inherit the system's grid and face
- * conditions; x faces shared by two slabs (every x face of a periodic x)
- * stay unfolded. */
+ * the operand (of every field component); every dot product sums all
+ * slabs' partials.  FP64 solves (plain or Jacobi), 1 to 8 slabs of at least
+ * max(num_ghost, 2) planes.  The slabs inherit the system's grid, field
+ * components and face conditions (per component too); x faces shared by two
+ * slabs (every x face of a periodic x) stay unfolded. */
 typedef struct dare_slabs dare_slabs;
 DARE_API int dare_slabs_create(dare_system* s, int num_slabs, int num_levels, dare_slabs** out);
 DARE_API int dare_slabs_destroy(dare_slabs* sl);
