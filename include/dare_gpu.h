@@ -333,7 +333,9 @@ DARE_API int dare_slabs_destroy(dare_slabs* sl);
 DARE_API int dare_slabs_count(const dare_slabs* sl);
 DARE_API int dare_slabs_range(const dare_slabs* sl, int slab, int64_t* i0, int64_t* i1);
 /* The slab's own system and field (owned by the slabs; read and write them
- * with the dare_system_* / dare_field_* calls, do not destroy them). */
+ * with the dare_system_* / dare_field_* calls, do not destroy them).  Solve
+ * the slabs together with dare_slabs_solve: a slab's system solved on its own
+ * sees zeros beyond its first and last plane. */
 DARE_API dare_system* dare_slabs_system(dare_slabs* sl, int slab);
 DARE_API dare_field* dare_slabs_field(dare_slabs* sl, int slab);
 DARE_API int dare_slabs_set_bc(dare_slabs* sl, int face, int type, double value);
