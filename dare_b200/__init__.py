@@ -240,6 +240,15 @@ class DareError(RuntimeError):
     pass
 
 
+def _destroy(fn_name: str, h) -> None:
+    """Release a handle from a finalizer.  At interpreter shutdown the module's
+    globals may already be gone, and the process is ending anyway: skip."""
+    try:
+        getattr(_lib, fn_name)(h)
+    except Exception:
+        pass
+
+
 def _check(rc: int, ctx=None, what: str = ""):
     if rc != 0:
         msg = lib().dare_ctx_last_error(ctx).decode() if ctx else ""
@@ -343,7 +352,7 @@ class Grid:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().dare_grid_destroy(self.h)
+            _destroy("dare_grid_destroy", self.h)
             self.h = None
 
     @property
@@ -383,7 +392,7 @@ class Field:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().dare_field_destroy(self.h)
+            _destroy("dare_field_destroy", self.h)
             self.h = None
 
     def upload(self, values: np.ndarray, level: int = 0):
@@ -521,7 +530,7 @@ class MatrixSystem:
 
     def __del__(self):
         if getattr(self, "h", None) and getattr(self, "_owned", True):
-            lib().dare_system_destroy(self.h)
+            _destroy("dare_system_destroy", self.h)
         self.h = None
 
     def set_bc(self, face: int, kind: int, value: float = 0.0, component: int = -1):
@@ -638,7 +647,7 @@ class Slabs:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().dare_slabs_destroy(self.h)
+            _destroy("dare_slabs_destroy", self.h)
             self.h = None
 
     def system(self, s: int) -> MatrixSystem:
@@ -810,7 +819,7 @@ class Batch:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().dare_batch_destroy(self.h)
+            _destroy("dare_batch_destroy", self.h)
             self.h = None
 
     def num_cells(self, idx: int) -> int:
@@ -877,7 +886,7 @@ class LearnedPreconditioner:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().dare_unet_destroy(self.h)
+            _destroy("dare_unet_destroy", self.h)
             self.h = None
 
     @staticmethod
