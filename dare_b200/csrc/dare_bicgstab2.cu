@@ -237,101 +237,123 @@ int launch_scale(dare_ctx* ctx, int64_t n, const double* invd, double* x) {
     return DARE_OK;
 }
 
-template <typename T, bool UNIT>
-static int build_graph(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
-                       const VecsT<T>& vs, SolverState* st, double* partials, cudaGraphExec_t* out) {
-    cudaStream_t cap;
-    DARE_CUDA(ctx, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-    cudaStream_t saved = ctx->stream;
-    ctx->stream = cap;
-    cudaGraph_t graph = nullptr;
-    int rc = DARE_OK;
-    const int64_t launches0 = ctx->launches;
-    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, 0, nullptr);
-        if (rc == DARE_OK) rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, 1, nullptr);
-        cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
-        if (e == cudaSuccess) e = e2;
-    }
-    ctx->stream = saved;
-    ctx->launches = launches0;  // captured, not executed
-    if (e == cudaSuccess && rc == DARE_OK) e = cudaGraphInstantiate(out, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(cap);
-    if (rc != DARE_OK) return rc;
-    if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2 graph capture");
+// Read the solver state back after the iterations: the launches the graph
+// ran are counted from its pair counter; a state that is not done means the
+// bound was reached without a status.
+int finish_iterations(dare_ctx* ctx, const SolverState* st, SolverState* st_host) {
+    DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
+    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->profiling == 0) ctx->launches += (int64_t)st_host->pairs * 11;   // 10 kernels and the condition
+    if (!st_host->done) return set_error(ctx, DARE_ERR_STATE, "bicgstab2: iteration bound reached without a status");
     return DARE_OK;
 }
 
-// Run iterations until the done flag is set: graph replays of two iterations
-// (or direct launches with per-kernel events when profiling), polling the
-// state every `check_every` pairs.
+// The solve graph: a conditional WHILE node whose body is two iterations and
+// the loop condition (k_loop_cond), so the whole iteration loop runs on the
+// device without host round trips; the host reads the state once at the end.
+template <typename T, bool UNIT>
+static int build_graph(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
+                       const VecsT<T>& vs, SolverState* st, double* partials, cudaGraphExec_t* out) {
+    cudaGraph_t graph = nullptr;
+    DARE_CUDA(ctx, cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node;
+    cudaStream_t cap = nullptr;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    int rc = DARE_OK;
+    cudaStream_t saved = ctx->stream;
+    const int64_t launches0 = ctx->launches;
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cap, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                          cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        ctx->stream = cap;
+        rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, 0, nullptr);
+        if (rc == DARE_OK) rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, 1, nullptr);
+        if (rc == DARE_OK) {
+            k_loop_cond<<<1, 1, 0, cap>>>(h, st);
+            e = cudaGetLastError();
+        }
+        cudaGraph_t body = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(cap, &body);
+        if (e == cudaSuccess) e = e2;
+        ctx->stream = saved;
+    }
+    ctx->launches = launches0;   // captured, not executed
+    if (e == cudaSuccess && rc == DARE_OK) e = cudaGraphInstantiate(out, graph, 0);
+    if (cap) cudaStreamDestroy(cap);
+    cudaGraphDestroy(graph);
+    if (rc != DARE_OK) return rc;
+    if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2 graph");
+    return DARE_OK;
+}
+
+// Run iterations until the done flag is set: one launch of the solve graph
+// (the loop runs on the device), or, when profiling, direct launches with
+// per-kernel events, the state polled every `check_every` pairs.
 template <typename T, bool UNIT>
 int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                    const VecsT<T>& vs, SolverState* st, SolverState* st_host, double* partials, cudaGraphExec_t* ge,
-                   int max_it, int check_every, int kid_base) {
+                   int max_it, int check_every, int kid_base, bool wait) {
     const bool prof = ctx->profiling != 0;
-    if (!prof && !*ge) {
-        int rc = build_graph<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, ge);
-        if (rc) return rc;
+    if (!prof) {
+        if (!*ge) {
+            int rc = build_graph<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, ge);
+            if (rc) return rc;
+        }
+        DARE_CUDA(ctx, cudaGraphLaunch(*ge, ctx->stream));
+        if (!wait) return DARE_OK;
+        return finish_iterations(ctx, st, st_host);
     }
-    if (check_every <= 0) {
-        const int64_t per = (int64_t)1 << 21;
-        check_every = (int)((per + g.ncell - 1) / g.ncell);
-        if (check_every < 1) check_every = 1;
-        if (check_every > 8) check_every = 8;
-    }
+    if (check_every <= 0) check_every = 1;
     // profiling checks after every pair, so each recorded duration belongs
     // to a known iteration
-    if (prof) check_every = 1;
+    check_every = 1;
     const int max_pairs = max_it / 2 + 2;
     for (int gi = 0; gi < max_pairs; gi++) {
-        if (prof) {
-            for (int par = 0; par < 2; par++) {
-                int rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, par, ctx->ev + 5 * par);
-                if (rc) return rc;
-            }
-        } else {
-            DARE_CUDA(ctx, cudaGraphLaunch(*ge, ctx->stream));
-            ctx->launches += 10;
+        for (int par = 0; par < 2; par++) {
+            int rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, par, ctx->ev + 5 * par);
+            if (rc) return rc;
         }
         if ((gi + 1) % check_every == 0 || gi + 1 == max_pairs) {
             DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
             DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            if (prof) {
-                // Iterations of this pair that ran in full: both while the
-                // solve goes on; on convergence the flag is raised by the
-                // last kernel of iteration k (k = 2 gi + 1 or 2 gi + 2), and
-                // the kernels after it returned at once.  A pair that ended
-                // in another status is not recorded.
-                int real = 2;
-                if (st_host->done) {
-                    real = st_host->status == ST_CONVERGED ? st_host->k - 2 * gi : 0;
-                    real = real < 0 ? 0 : real > 2 ? 2 : real;
-                }
-                for (int it = 0; it < real; it++)
-                    for (int q = 0; q < 5; q++) {
-                        float ms = 0.f;
-                        if (cudaEventElapsedTime(&ms, ctx->ev[it * 5 + q], ctx->ev[it * 5 + q + 1]) == cudaSuccess) {
-                            ctx->stat_ms[kid_base + q] += ms;
-                            ctx->stat_n[kid_base + q] += 1;
-                        } else {
-                            cudaGetLastError();  // timing is best effort; do not leak the error
-                        }
-                    }
+            // Iterations of this pair that ran in full: both while the
+            // solve goes on; on convergence the flag is raised by the
+            // last kernel of iteration k (k = 2 gi + 1 or 2 gi + 2), and
+            // the kernels after it returned at once.  A pair that ended
+            // in another status is not recorded.
+            int real = 2;
+            if (st_host->done) {
+                real = st_host->status == ST_CONVERGED ? st_host->k - 2 * gi : 0;
+                real = real < 0 ? 0 : real > 2 ? 2 : real;
             }
+            for (int it = 0; it < real; it++)
+                for (int q = 0; q < 5; q++) {
+                    float ms = 0.f;
+                    if (cudaEventElapsedTime(&ms, ctx->ev[it * 5 + q], ctx->ev[it * 5 + q + 1]) == cudaSuccess) {
+                        ctx->stat_ms[kid_base + q] += ms;
+                        ctx->stat_n[kid_base + q] += 1;
+                    } else {
+                        cudaGetLastError();  // timing is best effort; do not leak the error
+                    }
+                }
             if (st_host->done) break;
         }
     }
-    DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
-    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (!st_host->done) return set_error(ctx, DARE_ERR_STATE, "bicgstab2: iteration bound reached without a status");
-    return DARE_OK;
+    return finish_iterations(ctx, st, st_host);
 }
 template int run_iterations<float, true>(dare_ctx*, const GridDev&, const MarchCfg&, int, const OpT<float>&,
                                          const VecsT<float>&, SolverState*, SolverState*, double*, cudaGraphExec_t*,
-                                         int, int, int);
+                                         int, int, int, bool);
 
 }  // namespace dare_gpu
 
@@ -359,12 +381,25 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
                 : launch_init<double, false>(ctx, g, m, full, vs, ws->st, ws->partials);
     if (rc) return rc;
     rc = jacobi ? run_iterations<double, true>(ctx, g, m, ws->stream_blocks, folded, vs, ws->st, ws->st_host,
-                                               ws->partials, &ws->graph[1][0], p->max_it, p->check_every, KID_STEP1)
+                                               ws->partials, &ws->graph[1][0], p->max_it, p->check_every, KID_STEP1,
+                                               false)
                 : run_iterations<double, false>(ctx, g, m, ws->stream_blocks, full, vs, ws->st, ws->st_host,
-                                                ws->partials, &ws->graph[0][0], p->max_it, p->check_every, KID_STEP1);
+                                                ws->partials, &ws->graph[0][0], p->max_it, p->check_every, KID_STEP1,
+                                                false);
     if (rc) return rc;
+    // The exit's device work, queued behind the iterations and read back with
+    // the state in one round trip: step (10) when the solve stopped after it
+    // (decided on the device), x = M^-1 y, and the true residual of that x
+    // (the report's, and the tau = 0 exit's check).
+    k_step10<double><<<grid_blocks(ctx, n, 256, 8), 256, 0, ctx->stream>>>(n, ws->st, vs.u[1], vs.x);
+    DARE_LAUNCHED(ctx);
+    if (jacobi && (rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
+    double* tres = &ws->st->tres;
+    if (p->compute_true_residual &&
+        (rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, tres)))
+        return rc;
+    if ((rc = finish_iterations(ctx, ws->st, ws->st_host))) return rc;
     SolverState st = *ws->st_host;
-    if ((rc = finish_step10(ctx, n, st, ws->st, vs))) return rc;
 
     std::memset(rep, 0, sizeof(*rep));
     rep->iters = st.k;
@@ -372,27 +407,35 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
     rep->res_abs = st.rnorm;
     rep->breakdown_step = st.step;
     rep->tol_abs = st.tol;
-    double* dres = ws->partials + (size_t)kMaxQ * kMaxBlocks;  // scratch slot past the partials
+    if (p->compute_true_residual) rep->true_res_abs = st.tres;
     if (st.status == ST_TAU0) {
         // BiCGStab2.inl:407-424: x = M^-1 y, true residual, return if converged;
         // otherwise break to the common exit, which applies M^-1 once more.
-        if (jacobi && (rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
-        if ((rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, dres))) return rc;
-        double tr = 0.;
-        DARE_CUDA(ctx, cudaMemcpyAsync(&tr, dres, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        double tr = st.tres;
+        if (!p->compute_true_residual) {
+            if ((rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, tres))) return rc;
+            if ((rc = finish_iterations(ctx, ws->st, ws->st_host))) return rc;
+            tr = ws->st_host->tres;
+        }
         rep->res_abs = tr;
         if (tr <= st.tol) {
             rep->converged = 1;
             rep->status = DARE_SOLVE_CONVERGED;
             rep->breakdown_step = 0;
         } else {
-            if (jacobi && (rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
             rep->converged = 0;
             rep->status = DARE_SOLVE_BREAKDOWN;
+            if (jacobi) {
+                if ((rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
+                if (p->compute_true_residual) {
+                    if ((rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, tres)))
+                        return rc;
+                    if ((rc = finish_iterations(ctx, ws->st, ws->st_host))) return rc;
+                    rep->true_res_abs = ws->st_host->tres;
+                }
+            }
         }
     } else {
-        if (jacobi && (rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
         rep->converged = st.rnorm <= st.tol;
         switch (st.status) {
         case ST_CONVERGED: rep->status = DARE_SOLVE_CONVERGED; break;
@@ -400,13 +443,6 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
         case ST_NAN: rep->status = DARE_SOLVE_NAN; break;
         default: rep->status = DARE_SOLVE_BREAKDOWN; break;
         }
-    }
-    if (p->compute_true_residual) {
-        if ((rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, dres))) return rc;
-        double tr = 0.;
-        DARE_CUDA(ctx, cudaMemcpyAsync(&tr, dres, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        rep->true_res_abs = tr;
     }
     return DARE_OK;
 }

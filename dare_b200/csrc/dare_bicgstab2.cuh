@@ -19,6 +19,8 @@ struct SolverState {
     unsigned int count;   // reduction arrivals (reset by the last arrival)
     unsigned int queue;   // next work item of a marching kernel
     unsigned int exitc;   // blocks that left a marching kernel (the last resets queue)
+    unsigned int pairs;   // iteration pairs run by the device-side loop of the solve graph
+    double tres;          // ||b - A x||_2 after the solve (read back with the state)
 };
 
 template <typename T>
@@ -149,10 +151,14 @@ template <typename T, bool UNIT>
 int launch_iteration(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                      const VecsT<T>& vs, SolverState* st, double* partials, int par, cudaEvent_t* ev);
 
+// `wait`: read the final state back before returning (otherwise, on the
+// graph path, the caller enqueues more work and reads it back itself).
+int finish_iterations(dare_ctx* ctx, const SolverState* st, SolverState* st_host);
+
 template <typename T, bool UNIT>
 int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                    const VecsT<T>& vs, SolverState* st, SolverState* st_host, double* partials, cudaGraphExec_t* ge,
-                   int max_it, int check_every, int kid_base);
+                   int max_it, int check_every, int kid_base, bool wait = true);
 
 int launch_true_residual(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const OpT<double>& op,
                          const double* x, const double* b, SolverState* st, double* partials, double* out);

@@ -919,14 +919,24 @@ __global__ void __launch_bounds__(256) k_step5(int64_t n, T* __restrict__ x, T* 
 
 // Step (10) of an iteration that stopped after it and before K5 (a
 // breakdown in steps (14), (20) or (21)): x = x + alpha1 u1.
+inline __host__ __device__ bool step10_pending_state(int status, int step) {
+    return status == ST_TAU0 || (status == ST_BREAKDOWN && (step == 14 || step == 20));
+}
 template <typename T>
 __global__ void k_step10(int64_t n, const SolverState* st, const T* __restrict__ u1, T* __restrict__ x) {
+    if (!step10_pending_state(st->status, st->step)) return;   // read on the device: no host round trip
     const T alpha1 = (T)st->alpha1;
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
         x[c] = alpha1 * u1[c] + x[c];
 }
-inline bool step10_pending(const SolverState& st) {
-    return st.status == ST_TAU0 || (st.status == ST_BREAKDOWN && (st.step == 14 || st.step == 20));
+inline bool step10_pending(const SolverState& st) { return step10_pending_state(st.status, st.step); }
+
+// The loop condition of the solve graph's device-side iteration loop (a
+// conditional WHILE node): another pair of iterations while the solve runs
+// and the bound max_it / 2 + 2 pairs is not reached.
+static __global__ void k_loop_cond(cudaGraphConditionalHandle h, SolverState* st) {
+    const unsigned pairs = ++st->pairs;
+    cudaGraphSetConditional(h, (!st->done && pairs < (unsigned)(st->max_it / 2 + 2)) ? 1u : 0u);
 }
 
 static __global__ void k_invdiag(const double* __restrict__ dc, double* __restrict__ invd, int64_t n) {
