@@ -231,6 +231,7 @@ __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, SolverState* s
         st->alpha = 0.;
         st->beta = 0.;
         st->k = 1;
+        st->pairs = 0;
         st->max_it = max_it;
         st->status = ST_RUNNING;
         st->step = 0;
@@ -340,10 +341,18 @@ __global__ void __launch_bounds__(256) k_upd_final(int64_t n, Vecs vs, SolverSta
     }
 }
 
-// x += D^-1 z (FP64)
+// x += D^-1 z (FP64), unless the inner solve ended in NaN (read on the device)
 __global__ void k_correct(int64_t n, const double* __restrict__ invd, const float* __restrict__ z,
-                          double* __restrict__ x) {
+                          double* __restrict__ x, const SolverState* st) {
+    if (st->status == ST_NAN) return;
     GRID_LOOP(c, n) x[c] += invd[c] * (double)z[c];
+}
+
+// The loop condition of the inner solve's device-side loop: another
+// iteration while the inner solve runs (it stops itself after max_it).
+__global__ void k_inner_cond(cudaGraphConditionalHandle h, SolverState* st) {
+    const unsigned it = ++st->pairs;
+    cudaGraphSetConditional(h, (!st->done && it < (unsigned)st->max_it + 2) ? 1u : 0u);
 }
 
 __global__ void k_to_precond_var(int64_t n, const double* __restrict__ dc, double* __restrict__ x) {
@@ -465,27 +474,50 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     if ((rc = read_scalar(ctx, lw->scal, &bnorm))) return rc;
     const double tol_abs = p->tol_relative ? p->tol * bnorm : p->tol;
 
-    // one CUDA graph per inner iteration (captured once per network and system)
+    // the inner solve as one CUDA graph (captured once per network and
+    // system): a conditional WHILE node whose body is one inner iteration and
+    // the loop condition, so the inner iterations run without host round trips
     if (!lw->graph || lw->graph_net != net) {
         if (lw->graph) cudaGraphExecDestroy(lw->graph);
         lw->graph = nullptr;
         if ((rc = dare_gpu::unet::apply(net, vs.rin, vs.zs))) return rc;  // sets the launch configurations
         DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         cudaGraph_t graph = nullptr;
-        DARE_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        DARE_CUDA(ctx, cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle h;
+        cudaGraphNodeParams cp{};
+        cudaGraphNode_t node;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+        }
+        if (e == cudaSuccess)
+            e = cudaStreamBeginCaptureToGraph(ctx->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return check_cuda(ctx, e, "bicgstab2_learned graph");
+        }
         const int64_t before = ctx->launches;
         rc = launch_iteration(ctx, net, g, lw->march32, lw->ahat32, vs, lw->st, lw->partials);
-        lw->graph_kernels = ctx->launches - before;
-        ctx->launches = before;
-        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
-        if (rc) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc;
+        if (rc == DARE_OK) {
+            k_inner_cond<<<1, 1, 0, ctx->stream>>>(h, lw->st);
+            ctx->launches++;
+            e = cudaGetLastError();
         }
-        if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2_learned capture");
-        e = cudaGraphInstantiate(&lw->graph, graph, 0);
+        lw->graph_kernels = ctx->launches - before;   // per inner iteration
+        ctx->launches = before;
+        cudaGraph_t body = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &body);
+        if (e == cudaSuccess) e = e2;
+        if (rc == DARE_OK && e == cudaSuccess) e = cudaGraphInstantiate(&lw->graph, graph, 0);
         cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2_learned instantiate");
+        if (rc) return rc;
+        if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2_learned graph");
         lw->graph_net = net;
     }
 
@@ -495,15 +527,19 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     double rnorm = 0., prev = INFINITY;
     bool converged = false;
     int refinements = 0, inner_total = 0;
-    for (int it = 0;; it++) {
+    // r = b - A x into the inner right-hand side, its norm into out
+    auto residual = [&](double* out) {
         FLResidual fr{};
         fr.zs[0] = s->x;
         set_coef_streams<double, false, 8>(OpT<double>{s->diag, s->diag + n, n}, fr.ps);   // W..T, then C
         fr.ps[7] = s->rhs;
         fr.rin = vs.rin;
-        fr.out = lw->scal;
-        if ((rc = launch_march(ctx, g, ws->march, fr, lw->st, lw->partials))) return rc;
-        if ((rc = read_scalar(ctx, lw->scal, &rnorm))) return rc;
+        fr.out = out;
+        return launch_march(ctx, g, ws->march, fr, lw->st, lw->partials);
+    };
+    if ((rc = residual(lw->scal))) return rc;
+    if ((rc = read_scalar(ctx, lw->scal, &rnorm))) return rc;
+    for (int it = 0;; it++) {
         if (rnorm <= tol_abs) {
             converged = true;
             break;
@@ -513,21 +549,19 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         const int cap = std::min(lp->inner_max_it, lp->iteration_budget - inner_total);
         k_init<<<eb, 256, 0, ctx->stream>>>(n, vs, lw->st, lw->partials, lp->inner_rel_tol, cap);
         DARE_LAUNCHED(ctx);
-        for (int j = 0; j < cap; j++) {
-            DARE_CUDA(ctx, cudaGraphLaunch(lw->graph, ctx->stream));
-            ctx->launches += lw->graph_kernels;
-            DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
-            DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            if (lw->st_host->done) break;
-        }
+        DARE_CUDA(ctx, cudaGraphLaunch(lw->graph, ctx->stream));   // the inner iterations, on the device
+        // x += D^-1 d (skipped on the device after a NaN) and the next
+        // residual, read back with the inner solve's state in one round trip
+        k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, vs.d, s->x, lw->st);
+        DARE_LAUNCHED(ctx);
+        if ((rc = residual(&lw->st->tres))) return rc;
         DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
         DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         const SolverState st = *lw->st_host;
+        ctx->launches += (int64_t)st.pairs * lw->graph_kernels;
         inner_total += std::min(st.k, cap);
         if (st.status == ST_NAN) break;
-        // x += D^-1 d
-        k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, vs.d, s->x);
-        DARE_LAUNCHED(ctx);
+        rnorm = st.tres;
         refinements++;
     }
     rep->refinements = refinements;
