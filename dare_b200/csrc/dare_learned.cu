@@ -27,13 +27,16 @@
 // continues from the current iterate.  The reported residual is always the
 // FP64 ||b - A x||_2.
 //
-// One inner iteration is one CUDA graph: 4 network applications (13
-// tensor-core/level-transfer kernels each), 4 SpMV kernels with fused dot
-// products (plane-marching, dare_march.cuh), 6 vector kernels.  The FP64
-// residual of the refinement also runs in the marching engine.  The inner solve may stop after its first
-// iteration (the reference's `k > 1` rule applies to its own solve, not to
-// this inner correction).  Scalars live on the device; kernels after a
-// breakdown see `done` and skip their work.
+// One inner iteration: 4 network applications (13 tensor-core/level-
+// transfer kernels each), 4 SpMV kernels with fused dot products
+// (plane-marching, dare_march.cuh), 6 vector kernels.  The inner solve is one
+// CUDA graph whose conditional WHILE node repeats that iteration on the
+// device until the solve is done; the FP64 residual of the refinement also
+// runs in the marching engine and is read back with the inner solve's state.
+// The inner solve may stop after its first iteration (the reference's
+// `k > 1` rule applies to its own solve, not to this inner correction).
+// Scalars live on the device; kernels after a breakdown see `done` and skip
+// their work.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
