@@ -350,7 +350,7 @@ class Grid:
         self.num_cells = int(info.num_cells)
         self.num_cells_ghosted = int(info.num_cells_ghosted)
 
-    def __del__(self):
+    def __del__(self, _destroy=_destroy):
         if getattr(self, "h", None):
             _destroy("dare_grid_destroy", self.h)
             self.h = None
@@ -390,7 +390,7 @@ class Field:
         self.num_levels = num_levels
         self.components = components
 
-    def __del__(self):
+    def __del__(self, _destroy=_destroy):
         if getattr(self, "h", None):
             _destroy("dare_field_destroy", self.h)
             self.h = None
@@ -528,7 +528,7 @@ class MatrixSystem:
         self.components = components
         self.rows = grid.num_cells * components
 
-    def __del__(self):
+    def __del__(self, _destroy=_destroy):
         if getattr(self, "h", None) and getattr(self, "_owned", True):
             _destroy("dare_system_destroy", self.h)
         self.h = None
@@ -645,7 +645,7 @@ class Slabs:
             self.ranges.append((a.value, b.value))
         self.periodic_x = bool(self.grid.info.periodic[0])
 
-    def __del__(self):
+    def __del__(self, _destroy=_destroy):
         if getattr(self, "h", None):
             _destroy("dare_slabs_destroy", self.h)
             self.h = None
@@ -817,7 +817,7 @@ class Batch:
         self.h = h
         self.count = len(instances)
 
-    def __del__(self):
+    def __del__(self, _destroy=_destroy):
         if getattr(self, "h", None):
             _destroy("dare_batch_destroy", self.h)
             self.h = None
@@ -884,7 +884,7 @@ class LearnedPreconditioner:
         self.net_shape = tuple(x // 2 for x in self.n) if coarse else self.n
         self.net_cells = int(np.prod(self.net_shape))
 
-    def __del__(self):
+    def __del__(self, _destroy=_destroy):
         if getattr(self, "h", None):
             _destroy("dare_unet_destroy", self.h)
             self.h = None

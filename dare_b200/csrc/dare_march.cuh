@@ -257,7 +257,7 @@ struct FStep4 {
     using type = T;
     static constexpr int Q = 5, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 2;
     static constexpr bool kCheckDone = true;
-    static constexpr bool kPairs = false;   // two cells per thread (see launch_march)
+    static constexpr bool kPairs = sizeof(T) == 4;   // two cells per thread (see launch_march)
     const T* zs[2];   // w, s
     const T* ps[NP];  // coefficients, r (of step (8)), v
     T *r_out, *s_out, *t;
