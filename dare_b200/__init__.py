@@ -56,7 +56,7 @@ class AssemblyDesc(C.Structure):
 class TermDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("op", C.c_int), ("component", C.c_int), ("dt", C.c_double), ("D", C.c_double),
                 ("face_D", C.c_void_p * 3), ("vel", C.c_double * 3), ("face_vel", C.c_void_p * 3),
-                ("limiter", C.c_int), ("scheme", C.c_int)]
+                ("limiter", C.c_int), ("scheme", C.c_int), ("coef", C.c_void_p * 7), ("coef_rhs", C.c_void_p)]
 
 
 class SolverParams(C.Structure):
@@ -474,7 +474,7 @@ class Assembly:
 
 
 
-TERM_KINDS = {"DDT": 0, "DIFFUSION": 1, "CONVECTION": 2}
+TERM_KINDS = {"DDT": 0, "DIFFUSION": 1, "CONVECTION": 2, "COEFFS": 3}
 TERM_OPS = {"SET": 0, "ADD": 1, "SUB": 2}
 
 
@@ -483,7 +483,10 @@ class Term:
     """One MatrixBlock expression of a composed functor (see dare_term):
     ``Term("DDT", "SET", dt=dt)`` is ``mb = ddt(field)``, ``Term("DIFFUSION",
     "SUB")`` is ``mb -= div(grad(mb))``, ``Term("CONVECTION", "ADD", component=0,
-    vel=(u, v, 0))`` is ``mb.Add(0, div(TVD(u) * field).GetSlice(0))``."""
+    vel=(u, v, 0))`` is ``mb.Add(0, div(TVD(u) * field).GetSlice(0))``;
+    ``Term("COEFFS", "ADD", coef=(c, None, ...), rhs=b)`` adds per-cell slot
+    and right-hand-side values the caller computed on the device (device
+    pointers or DeviceArray, one component's cells each)."""
     kind: str
     op: str = "ADD"
     component: int = -1
@@ -494,6 +497,8 @@ class Term:
     face_vel: tuple | None = None
     limiter: str = "VANLEER"
     scheme: str = "EULER_BACKWARD"
+    coef: tuple | None = None          # COEFFS: 7 slot arrays (None entries: 0)
+    rhs: object = None                 # COEFFS: right-hand-side array
 
     def to_c(self) -> TermDesc:
         t = TermDesc()
@@ -513,6 +518,11 @@ class Term:
                 t.face_vel[d] = p.ptr if isinstance(p, DeviceArray) else p
         t.limiter = LIMITER[self.limiter]
         t.scheme = SCHEME[self.scheme]
+        if self.coef is not None:
+            for q, p in enumerate(self.coef):
+                t.coef[q] = p.ptr if isinstance(p, DeviceArray) else p
+        if self.rhs is not None:
+            t.coef_rhs = self.rhs.ptr if isinstance(self.rhs, DeviceArray) else self.rhs
         return t
 
 

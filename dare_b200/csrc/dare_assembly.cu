@@ -314,6 +314,28 @@ static int launch_component(dare_system* s, const AsmParams& a, int c, const dou
     return DARE_OK;
 }
 
+// A COEFFS term: the caller's per-cell values of the 7 slots and the rhs
+// (null: 0), set (acc = 0) or added with the term's sign to component c's
+// rows.
+struct CoefTerm {
+    const double* coef[7];
+    const double* rhs;
+};
+__global__ void k_term_coeffs(int64_t n, int64_t dstride, CoefTerm t, double sgn, int acc, double* __restrict__ diag,
+                              double* __restrict__ rhs) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+            const double v = t.coef[q] ? t.coef[q][c] : 0.;
+            const double sv = sgn > 0. ? v : -1. * v;
+            diag[q * dstride + c] = acc ? diag[q * dstride + c] + sv : sv;
+        }
+        const double v = t.rhs ? t.rhs[c] : 0.;
+        const double sv = sgn > 0. ? v : -1. * v;
+        rhs[c] = acc ? rhs[c] + sv : sv;
+    }
+}
+
 // Geometry, scheme weights and checks shared by both entry points.
 static int base_params(dare_system* s, AsmParams& a, const char* who) {
     dare_ctx* ctx = s->grid->ctx;
@@ -370,7 +392,7 @@ static int launch_terms(dare_system* s, const dare_term* terms, int nterms, cons
     dare_ctx* ctx = s->grid->ctx;
     for (int t = 0; t < nterms; t++) {
         const dare_term& T = terms[t];
-        if (T.kind < DARE_TERM_DDT || T.kind > DARE_TERM_CONVECTION || T.op < DARE_OP_SET || T.op > DARE_OP_SUB ||
+        if (T.kind < DARE_TERM_DDT || T.kind > DARE_TERM_COEFFS || T.op < DARE_OP_SET || T.op > DARE_OP_SUB ||
             T.component < -1 || T.component >= s->ncomp)
             return set_error(ctx, DARE_ERR_BAD_ARG, "dare_assemble_terms: bad term");
         if (T.kind == DARE_TERM_DDT && !(T.dt > 0.))
@@ -382,6 +404,18 @@ static int launch_terms(dare_system* s, const dare_term* terms, int nterms, cons
         for (int t = 0; t < nterms; t++) {
             const dare_term& T = terms[t];
             if (T.component >= 0 && T.component != c) continue;
+            if (T.kind == DARE_TERM_COEFFS) {
+                CoefTerm ct{};
+                for (int q = 0; q < 7; q++) ct.coef[q] = T.coef[q];
+                ct.rhs = T.coef_rhs;
+                const GridDev& gd = s->grid->dev;
+                k_term_coeffs<<<grid_blocks(ctx, gd.ncell, 256, 8), 256, 0, ctx->stream>>>(
+                    gd.ncell, s->sdev.ncell, ct, T.op == DARE_OP_SUB ? -1. : 1., started && T.op != DARE_OP_SET,
+                    s->diag + (size_t)c * gd.ncell, s->rhs + (size_t)c * gd.ncell);
+                DARE_LAUNCHED(ctx);
+                started = true;
+                continue;
+            }
             AsmParams a{};
             a.scheme = T.scheme;
             a.limiter = T.limiter;

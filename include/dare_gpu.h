@@ -136,8 +136,12 @@ typedef struct {
  * afresh, ADD and SUB add the term or its negative.  After the last term the
  * non-periodic faces are folded with each component's conditions
  * (dare_system_set_bc, dare_system_set_bc_component).  Face arrays as in
- * dare_assembly_desc. */
-enum { DARE_TERM_DDT = 0, DARE_TERM_DIFFUSION = 1, DARE_TERM_CONVECTION = 2 };
+ * dare_assembly_desc.  COEFFS is any other expression of a functor,
+ * evaluated by the caller on the device: per-cell values of the 7 slots
+ * (CENTER, WEST, EAST, SOUTH, NORTH, BOTTOM, TOP; NULL slots are 0) and of the
+ * right-hand side, each an array over one component's internal cells, set,
+ * added or subtracted like the other terms (and folded with them at the end). */
+enum { DARE_TERM_DDT = 0, DARE_TERM_DIFFUSION = 1, DARE_TERM_CONVECTION = 2, DARE_TERM_COEFFS = 3 };
 enum { DARE_OP_SET = 0, DARE_OP_ADD = 1, DARE_OP_SUB = 2 };
 typedef struct {
     int kind;                        /* DARE_TERM_* */
@@ -150,6 +154,8 @@ typedef struct {
     const double* face_vel[3];       /* ... or face velocities (all three or none) */
     int limiter;                     /* CONVECTION: DARE_LIMITER_* */
     int scheme;                      /* DIFFUSION / CONVECTION: DARE_SCHEME_* of the div(...) */
+    const double* coef[7];           /* COEFFS: device arrays of the 7 slots (NULL: 0) ... */
+    const double* coef_rhs;          /* ... and of the right-hand side (NULL: 0) */
 } dare_term;
 
 typedef struct {

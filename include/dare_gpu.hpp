@@ -207,6 +207,15 @@ inline Term DDT(double dt) {
     r.t.dt = dt;
     return r;
 }
+// Any other expression, evaluated by the caller on the device: per-cell
+// values of the 7 slots (CENTER .. TOP; null: 0) and of the right-hand side
+inline Term Coefficients(const double* const coef[7], const double* rhs) {
+    Term r;
+    r.t.kind = DARE_TERM_COEFFS;
+    for (int q = 0; q < 7; q++) r.t.coef[q] = coef ? coef[q] : nullptr;
+    r.t.coef_rhs = rhs;
+    return r;
+}
 // div(D, grad(mb)) (D = 1: div(grad(mb))), or with device face diffusivities
 inline Term DivGrad(double D = 1., TimeScheme scheme = TimeScheme::EULER_BACKWARD) {
     Term r;

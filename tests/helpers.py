@@ -205,12 +205,19 @@ def oracle_terms(og, case, terms, phis, olds, bcs):
             if t["component"] not in (-1, c):
                 continue
             kind = t["kind"]
-            desc = O.AssemblyDesc(og, dt=t.get("dt", 0.0) if kind == "DDT" else 0.0,
-                                  D=t.get("D", 1.0) if kind == "DIFFUSION" else None,
-                                  vel=t.get("vel") if kind == "CONVECTION" else None,
-                                  limiter=ORACLE_LIM[t.get("limiter", "VANLEER")], bc=neutral, no_fold=True)
-            d, r, mask = O.assemble(desc, np.ascontiguousarray(phis[c]), np.ascontiguousarray(olds[c]))
-            native = -1.0 if kind == "DIFFUSION" else 1.0
+            if kind == "COEFFS":   # the caller's own values: 7 slot arrays (None: 0) and the rhs
+                ncell = int(np.prod(case["n"]))
+                d = np.stack([np.zeros(ncell) if a is None else np.asarray(a, dtype=np.float64)
+                              for a in t["coef"]])
+                r = np.zeros(ncell) if t.get("rhs") is None else np.asarray(t["rhs"], dtype=np.float64).copy()
+                native = 1.0
+            else:
+                desc = O.AssemblyDesc(og, dt=t.get("dt", 0.0) if kind == "DDT" else 0.0,
+                                      D=t.get("D", 1.0) if kind == "DIFFUSION" else None,
+                                      vel=t.get("vel") if kind == "CONVECTION" else None,
+                                      limiter=ORACLE_LIM[t.get("limiter", "VANLEER")], bc=neutral, no_fold=True)
+                d, r, mask = O.assemble(desc, np.ascontiguousarray(phis[c]), np.ascontiguousarray(olds[c]))
+                native = -1.0 if kind == "DIFFUSION" else 1.0
             want = -1.0 if t["op"] == "SUB" else 1.0
             if want != native:
                 d, r = -d, -r

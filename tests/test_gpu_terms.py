@@ -229,3 +229,43 @@ def test_cxx_counter_diffusion_example(tmp_path):
     i0 = interior(got[:, 0], shape, dim=1).ravel()
     i1 = interior(got[:, 1], shape, dim=1).ravel()
     np.testing.assert_allclose(i0, i1[::-1], rtol=0, atol=1e-8)
+
+
+@pytest.mark.parametrize("n,periodic", [((18, 14), (0, 1)), ((12, 10, 9), (0, 1, 1))])
+def test_caller_coefficients_term(ctx, n, periodic):
+    """COEFFS terms (per-cell slot and rhs values the caller computed on the
+    device) composed with DDT and diffusion, for every component and for
+    one, then folded with each component's conditions: 2-D bit for bit,
+    3-D within 1e-13 of the oracle's composition of the same parts."""
+    import torch
+    rng = np.random.default_rng(41)
+    dim, N = len(n), 2
+    case = {"n": n, "size": tuple(1.0 + 0.1 * d for d in range(dim)), "periodic": periodic}
+    gh = tuple(x + 4 for x in n)
+    comps = [rng.random(gh) for _ in range(N)]
+    olds = [rng.random(gh) for _ in range(N)]
+    bcs = [{1: (O.BC_DIRICHLET, 1.0 + c), 2: (O.BC_NEUMANN, 0.0)} for c in range(N)]
+    g, f, s = _setup(ctx, case, comps, olds, bcs)
+    ncell = int(np.prod(n))
+    coef = [rng.random(ncell) + 1.0] + [-0.1 * rng.random(ncell) if q <= 2 * dim else None for q in range(1, 7)]
+    rhs = rng.normal(size=ncell)
+    extra = [rng.random(ncell)] + [None] * 6
+    dev = lambda a: None if a is None else D.DeviceArray(a)
+    coef_d, rhs_d, extra_d = [dev(a) for a in coef], dev(rhs), [dev(a) for a in extra]
+    terms = [dict(kind="DDT", op="SET", component=-1, dt=0.05),
+             dict(kind="COEFFS", op="ADD", component=-1, coef=coef, rhs=rhs),
+             dict(kind="DIFFUSION", op="SUB", component=-1, D=0.01),
+             dict(kind="COEFFS", op="SUB", component=1, coef=extra, rhs=None)]
+    gpu = [D.Term("DDT", "SET", dt=0.05),
+           D.Term("COEFFS", "ADD", coef=tuple(coef_d), rhs=rhs_d),
+           D.Term("DIFFUSION", "SUB", D=0.01),
+           D.Term("COEFFS", "SUB", component=1, coef=tuple(extra_d))]
+    s.build(f, gpu)
+    gd, gr = s.coefficients()
+    od, orhs, _, _ = oracle_terms(oracle_grid(case), case, terms, [c.reshape(-1) for c in comps],
+                                  [o.reshape(-1) for o in olds], bcs)
+    if dim < 3:
+        assert np.array_equal(gd, od) and np.array_equal(gr, orhs)
+    else:
+        assert_coef_close(gd, od)
+        assert_coef_close(gr, orhs)
