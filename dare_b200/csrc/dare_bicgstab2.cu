@@ -298,7 +298,8 @@ static int build_graph(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int s
 
 // Run iterations until the done flag is set: one launch of the solve graph
 // (the loop runs on the device), or, when profiling, direct launches with
-// per-kernel events, the state polled every `check_every` pairs.
+// per-kernel events, the state read back after every pair (`check_every`
+// is no longer used: nothing is polled on the graph path).
 template <typename T, bool UNIT>
 int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                    const VecsT<T>& vs, SolverState* st, SolverState* st_host, double* partials, cudaGraphExec_t* ge,
@@ -313,41 +314,38 @@ int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbloc
         if (!wait) return DARE_OK;
         return finish_iterations(ctx, st, st_host);
     }
-    if (check_every <= 0) check_every = 1;
+    (void)check_every;
     // profiling checks after every pair, so each recorded duration belongs
     // to a known iteration
-    check_every = 1;
     const int max_pairs = max_it / 2 + 2;
     for (int gi = 0; gi < max_pairs; gi++) {
         for (int par = 0; par < 2; par++) {
             int rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, par, ctx->ev + 5 * par);
             if (rc) return rc;
         }
-        if ((gi + 1) % check_every == 0 || gi + 1 == max_pairs) {
-            DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
-            DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            // Iterations of this pair that ran in full: both while the
-            // solve goes on; on convergence the flag is raised by the
-            // last kernel of iteration k (k = 2 gi + 1 or 2 gi + 2), and
-            // the kernels after it returned at once.  A pair that ended
-            // in another status is not recorded.
-            int real = 2;
-            if (st_host->done) {
-                real = st_host->status == ST_CONVERGED ? st_host->k - 2 * gi : 0;
-                real = real < 0 ? 0 : real > 2 ? 2 : real;
-            }
-            for (int it = 0; it < real; it++)
-                for (int q = 0; q < 5; q++) {
-                    float ms = 0.f;
-                    if (cudaEventElapsedTime(&ms, ctx->ev[it * 5 + q], ctx->ev[it * 5 + q + 1]) == cudaSuccess) {
-                        ctx->stat_ms[kid_base + q] += ms;
-                        ctx->stat_n[kid_base + q] += 1;
-                    } else {
-                        cudaGetLastError();  // timing is best effort; do not leak the error
-                    }
-                }
-            if (st_host->done) break;
+        DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
+        DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        // Iterations of this pair that ran in full: both while the
+        // solve goes on; on convergence the flag is raised by the
+        // last kernel of iteration k (k = 2 gi + 1 or 2 gi + 2), and
+        // the kernels after it returned at once.  A pair that ended
+        // in another status is not recorded.
+        int real = 2;
+        if (st_host->done) {
+            real = st_host->status == ST_CONVERGED ? st_host->k - 2 * gi : 0;
+            real = real < 0 ? 0 : real > 2 ? 2 : real;
         }
+        for (int it = 0; it < real; it++)
+            for (int q = 0; q < 5; q++) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, ctx->ev[it * 5 + q], ctx->ev[it * 5 + q + 1]) == cudaSuccess) {
+                    ctx->stat_ms[kid_base + q] += ms;
+                    ctx->stat_n[kid_base + q] += 1;
+                } else {
+                    cudaGetLastError();  // timing is best effort; do not leak the error
+                }
+            }
+        if (st_host->done) break;
     }
     return finish_iterations(ctx, st, st_host);
 }
