@@ -64,6 +64,13 @@ MarchCfg march_config(const dare_ctx* ctx, const GridDev& g, size_t elem, int ma
         tk = 16;
         tj = 8;
     }
+    if (elem == 4 && n2 % 4 == 0 && n2 >= 64) {
+        // FP32: four cells per thread, 16 x 8 threads on 64 x 8 cells (every
+        // row segment one 16-byte copy)
+        m.cpt = 4;
+        tk = 16;
+        tj = 8;
+    }
     while (tj > 1 && tj / 2 >= n1) tj /= 2;
     m.block = dim3(tk, tj, 1);
     m.tiles_x = (n2 + tk * m.cpt - 1) / (tk * m.cpt);

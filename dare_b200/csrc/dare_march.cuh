@@ -533,7 +533,7 @@ __host__ __device__ constexpr size_t march_stage_elems(int tw, int tj, int ic) {
 }
 template <class K>
 inline size_t march_smem_bytes(const MarchCfg& m) {
-    const int ic = m.cpt == 2 ? 2 : 1;
+    const int ic = m.cpt;   // first interior column: one row segment of padding
     return 3 * march_stage_elems<K>(m.block.x * m.cpt, m.block.y, ic) * sizeof(typename K::type);
 }
 
@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
     using T = typename K::type;
     constexpr int NZ = K::NZ, NP = K::NP;
     constexpr int QA = K::Q > 0 ? K::Q : 1;
-    constexpr int IC = CPT == 2 ? 2 : 1;        // first interior column of a staged operand row
+    constexpr int IC = CPT;                     // first interior column of a staged operand row
     constexpr int CB = CPT * (int)sizeof(T);    // bytes of one thread's row segment
     if (K::kCheckDone && st->done) return;
     K k = kern;
@@ -774,7 +774,7 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
                     for (int q = 0; q < NP; q++) pv[q] = sb[NZ * ZT + q * NCT + tid];
                     k.center((int64_t)i * plane + G.o_own, z7, pv, acc);
                     zprev[0] = zcur;
-                } else {
+                } else if constexpr (CPT == 2) {
                     // the thread's two cells as one 16-byte (8-byte for FP32)
                     // shared-memory load per row: consecutive threads read
                     // consecutive pairs, without bank conflicts
@@ -805,6 +805,43 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
                     k.center((int64_t)i * plane + G.o_own + 1, z71, pv1, acc);
                     zprev[0] = zc0;
                     zprev[1] = zc1;
+                } else {
+                    // four FP32 cells per thread: every row segment one 16-byte
+                    // copy and one 16-byte shared-memory load
+                    static_assert(CPT == 4 && sizeof(T) == 4, "four cells per thread: FP32");
+                    const int col = IC + 4 * tx;
+                    auto zquad = [&](const T* b, int row, T (&z)[4]) {
+                        const float4 a = *reinterpret_cast<const float4*>(b + row * W + col);
+                        float4 c2 = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if constexpr (NZ > 1) c2 = *reinterpret_cast<const float4*>(b + ZT + row * W + col);
+                        z[0] = k.zc(a.x, c2.x);
+                        z[1] = k.zc(a.y, c2.y);
+                        z[2] = k.zc(a.z, c2.z);
+                        z[3] = k.zc(a.w, c2.w);
+                    };
+                    T zc[4], zn[4], zs[4], zt[4];
+                    zquad(sb, ty + 1, zc);
+                    zquad(sn, ty + 1, zn);
+                    zquad(sb, ty, zs);
+                    zquad(sb, ty + 2, zt);
+                    const T zw = zval(sb, ty + 1, col - 1), ze = zval(sb, ty + 1, col + 4);
+                    T pv[4][NP];
+#pragma unroll
+                    for (int q = 0; q < NP; q++) {
+                        const float4 pq = *reinterpret_cast<const float4*>(sb + NZ * ZT + q * NCT + ty * TW + 4 * tx);
+                        pv[0][q] = pq.x;
+                        pv[1][q] = pq.y;
+                        pv[2][q] = pq.z;
+                        pv[3][q] = pq.w;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const T z7[7] = {zc[c], zprev[c], zn[c], zs[c], zt[c], c == 0 ? zw : zc[c - 1],
+                                         c == 3 ? ze : zc[c + 1]};
+                        k.center((int64_t)i * plane + G.o_own + c, z7, pv[c], acc);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; c++) zprev[c] = zc[c];
                 }
             }
             __syncthreads();                    // slot of plane i is free for plane i+3
@@ -872,6 +909,19 @@ inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, cons
                         double* partials) {
     if (m.nitems > kMaxBlocks || m.item_base + m.nitems > kMaxBlocks || m.nitems_total > kMaxBlocks)
         return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
+    if (m.cpt == 4) {   // FP32 grids with n2 a multiple of 4, 64-cell tiles
+        if constexpr (sizeof(typename K::type) == 4 && !SplitOperands<K>::value) {
+            if constexpr (K::kPairs) {
+                return launch_march_t<K, 4, HALO>(ctx, g, m, kern, st, partials);
+            } else {
+                MarchCfg m2 = m;   // two cells per thread on the same tiles
+                m2.cpt = 2;
+                m2.block = dim3(m.block.x * 2, m.block.y, 1);
+                return launch_march_t<K, 2, HALO>(ctx, g, m2, kern, st, partials);
+            }
+        }
+        return set_error(ctx, DARE_ERR_UNSUPPORTED, "four cells per thread are for FP32 kernels");
+    }
     if constexpr (K::kPairs) {
         if (m.cpt == 2) return launch_march_t<K, 2, HALO>(ctx, g, m, kern, st, partials);
     }
