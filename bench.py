@@ -271,7 +271,7 @@ def run_dare(args):
 
     barrier, max_over_ranks = ranks.barrier, ranks.max
 
-    # the headline: the product path (the iterations run as the solve graph's device-side loop,
+    # the headline: the product path (iterations replayed from CUDA graphs,
     # no per-kernel events), exactly K steps between two barriers
     clocks = ClockSampler(local)
     launches0 = ctx.launch_count
@@ -409,7 +409,7 @@ def run_dare(args):
             "parity": parity,
             "time_to_residual_ms": ms / args.steps, "iterations_per_step": statistics.mean(iters),
             "cell_updates_per_s": value * n ** 3,
-            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e; iterations as a device-side graph loop); "
+            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e; iterations replayed from CUDA graphs); "
                       "learned-preconditioned solve in 'learned'",
             "learned": learned,
             "slabs": slabs,

@@ -23,6 +23,7 @@
 //     scalar recurrence and its breakdown checks, and sets a done flag that
 //     turns every later kernel into a no-op.  The host polls that flag.
 //   * The reference keeps omega/mu/nu/tau in long double; here they are FP64.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -244,87 +245,83 @@ int launch_scale(dare_ctx* ctx, int64_t n, const double* invd, double* x) {
     return DARE_OK;
 }
 
-// Read the solver state back after the iterations: the launches the graph
-// ran are counted from its pair counter; a state that is not done means the
-// bound was reached without a status.
+// Read the solver state back after the iterations; a state that is not done
+// means the bound was reached without a status.
 int finish_iterations(dare_ctx* ctx, const SolverState* st, SolverState* st_host) {
     DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
     DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (ctx->profiling == 0) ctx->launches += (int64_t)st_host->pairs * 11;   // 10 kernels and the condition
     if (!st_host->done) return set_error(ctx, DARE_ERR_STATE, "bicgstab2: iteration bound reached without a status");
     return DARE_OK;
 }
 
-// The solve graph: a conditional WHILE node whose body is two iterations and
-// the loop condition (k_loop_cond), so the whole iteration loop runs on the
-// device without host round trips; the host reads the state once at the end.
+// Two iterations captured as one CUDA graph.  (A device-side loop, a
+// conditional WHILE node around them, was measured as well: no faster on
+// the boxes measured, and ncu does not profile kernels of graphs that can
+// hold conditional nodes, so the host replays this graph and polls.)
 template <typename T, bool UNIT>
 static int build_graph(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                        const VecsT<T>& vs, SolverState* st, double* partials, cudaGraphExec_t* out) {
-    cudaGraph_t graph = nullptr;
-    DARE_CUDA(ctx, cudaGraphCreate(&graph, 0));
-    cudaGraphConditionalHandle h;
-    cudaGraphNodeParams cp{};
-    cudaGraphNode_t node;
-    cudaStream_t cap = nullptr;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) {
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
-    }
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    int rc = DARE_OK;
+    cudaStream_t cap;
+    DARE_CUDA(ctx, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaStream_t saved = ctx->stream;
+    ctx->stream = cap;
+    cudaGraph_t graph = nullptr;
+    int rc = DARE_OK;
     const int64_t launches0 = ctx->launches;
-    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cap, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                                          cudaStreamCaptureModeThreadLocal);
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        ctx->stream = cap;
         rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, 0, nullptr);
         if (rc == DARE_OK) rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, 1, nullptr);
-        if (rc == DARE_OK) {
-            k_loop_cond<<<1, 1, 0, cap>>>(h, st);
-            e = cudaGetLastError();
-        }
-        cudaGraph_t body = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(cap, &body);
+        cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
         if (e == cudaSuccess) e = e2;
-        ctx->stream = saved;
     }
-    ctx->launches = launches0;   // captured, not executed
+    ctx->stream = saved;
+    ctx->launches = launches0;  // captured, not executed
     if (e == cudaSuccess && rc == DARE_OK) e = cudaGraphInstantiate(out, graph, 0);
-    if (cap) cudaStreamDestroy(cap);
-    cudaGraphDestroy(graph);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cap);
     if (rc != DARE_OK) return rc;
-    if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2 graph");
+    if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2 graph capture");
     return DARE_OK;
 }
 
-// Run iterations until the done flag is set: one launch of the solve graph
-// (the loop runs on the device), or, when profiling, direct launches with
-// per-kernel events, the state read back after every pair (`check_every`
-// is no longer used: nothing is polled on the graph path).
+// Run iterations until the done flag is set: replays of the two-iteration
+// graph, the state read back every `check_every` pairs (0: by grid size), or,
+// when profiling, direct launches with per-kernel events and a read after
+// every pair.  `wait`: read the final state back again before returning
+// (otherwise the caller queues more work and reads it with the state).
 template <typename T, bool UNIT>
 int run_iterations(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sblocks, const OpT<T>& op,
                    const VecsT<T>& vs, SolverState* st, SolverState* st_host, double* partials, cudaGraphExec_t* ge,
                    int max_it, int check_every, int kid_base, bool wait) {
     const bool prof = ctx->profiling != 0;
+    const int max_pairs = max_it / 2 + 2;
     if (!prof) {
         if (!*ge) {
             int rc = build_graph<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, ge);
             if (rc) return rc;
         }
-        DARE_CUDA(ctx, cudaGraphLaunch(*ge, ctx->stream));
-        if (!wait) return DARE_OK;
+        if (check_every <= 0) {
+            const int64_t per = (int64_t)1 << 21;
+            check_every = (int)std::min<int64_t>(8, std::max<int64_t>(1, (per + g.ncell - 1) / g.ncell));
+        }
+        for (int gi = 0; gi < max_pairs; gi++) {
+            DARE_CUDA(ctx, cudaGraphLaunch(*ge, ctx->stream));
+            ctx->launches += 10;
+            if ((gi + 1) % check_every == 0 || gi + 1 == max_pairs) {
+                DARE_CUDA(ctx, cudaMemcpyAsync(st_host, st, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                               ctx->stream));
+                DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+                if (st_host->done) break;
+            }
+        }
+        if (!wait) return st_host->done ? DARE_OK
+                                        : set_error(ctx, DARE_ERR_STATE,
+                                                    "bicgstab2: iteration bound reached without a status");
         return finish_iterations(ctx, st, st_host);
     }
-    (void)check_every;
     // profiling checks after every pair, so each recorded duration belongs
     // to a known iteration
-    const int max_pairs = max_it / 2 + 2;
     for (int gi = 0; gi < max_pairs; gi++) {
         for (int par = 0; par < 2; par++) {
             int rc = launch_iteration<T, UNIT>(ctx, g, m, sblocks, op, vs, st, partials, par, ctx->ev + 5 * par);

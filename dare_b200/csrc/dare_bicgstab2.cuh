@@ -19,7 +19,6 @@ struct SolverState {
     unsigned int count;   // reduction arrivals (reset by the last arrival)
     unsigned int queue;   // next work item of a marching kernel
     unsigned int exitc;   // blocks that left a marching kernel (the last resets queue)
-    unsigned int pairs;   // iteration pairs run by the device-side loop of the solve graph
     double tres;          // ||b - A x||_2 after the solve (read back with the state)
 };
 

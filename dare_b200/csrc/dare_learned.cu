@@ -27,12 +27,11 @@
 // continues from the current iterate.  The reported residual is always the
 // FP64 ||b - A x||_2.
 //
-// One inner iteration: 4 network applications (13 tensor-core/level-
-// transfer kernels each), 4 SpMV kernels with fused dot products
-// (plane-marching, dare_march.cuh), 6 vector kernels.  The inner solve is one
-// CUDA graph whose conditional WHILE node repeats that iteration on the
-// device until the solve is done; the FP64 residual of the refinement also
-// runs in the marching engine and is read back with the inner solve's state.
+// One inner iteration is one CUDA graph: 4 network applications (13
+// tensor-core/level-transfer kernels each), 4 SpMV kernels with fused dot
+// products (plane-marching, dare_march.cuh), 6 vector kernels.  The FP64
+// residual of the refinement also runs in the marching engine and is read
+// back with the inner solve's state.
 // The inner solve may stop after its first iteration (the reference's
 // `k > 1` rule applies to its own solve, not to this inner correction).
 // Scalars live on the device; kernels after a breakdown see `done` and skip
@@ -234,7 +233,6 @@ __global__ void __launch_bounds__(256) k_init(int64_t n, Vecs vs, SolverState* s
         st->alpha = 0.;
         st->beta = 0.;
         st->k = 1;
-        st->pairs = 0;
         st->max_it = max_it;
         st->status = ST_RUNNING;
         st->step = 0;
@@ -351,12 +349,6 @@ __global__ void k_correct(int64_t n, const double* __restrict__ invd, const floa
     GRID_LOOP(c, n) x[c] += invd[c] * (double)z[c];
 }
 
-// The loop condition of the inner solve's device-side loop: another
-// iteration while the inner solve runs (it stops itself after max_it).
-__global__ void k_inner_cond(cudaGraphConditionalHandle h, SolverState* st) {
-    const unsigned it = ++st->pairs;
-    cudaGraphSetConditional(h, (!st->done && it < (unsigned)st->max_it + 2) ? 1u : 0u);
-}
 
 __global__ void k_to_precond_var(int64_t n, const double* __restrict__ dc, double* __restrict__ x) {
     GRID_LOOP(c, n) x[c] = dc[c] * x[c];
@@ -477,50 +469,28 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
     if ((rc = read_scalar(ctx, lw->scal, &bnorm))) return rc;
     const double tol_abs = p->tol_relative ? p->tol * bnorm : p->tol;
 
-    // the inner solve as one CUDA graph (captured once per network and
-    // system): a conditional WHILE node whose body is one inner iteration and
-    // the loop condition, so the inner iterations run without host round trips
+    // one CUDA graph per inner iteration (captured once per network and
+    // system); the host replays it and polls the state
     if (!lw->graph || lw->graph_net != net) {
         if (lw->graph) cudaGraphExecDestroy(lw->graph);
         lw->graph = nullptr;
         if ((rc = dare_gpu::unet::apply(net, vs.rin, vs.zs))) return rc;  // sets the launch configurations
         DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         cudaGraph_t graph = nullptr;
-        DARE_CUDA(ctx, cudaGraphCreate(&graph, 0));
-        cudaGraphConditionalHandle h;
-        cudaGraphNodeParams cp{};
-        cudaGraphNode_t node;
-        cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
-        if (e == cudaSuccess) {
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = h;
-            cp.conditional.type = cudaGraphCondTypeWhile;
-            cp.conditional.size = 1;
-            e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
-        }
-        if (e == cudaSuccess)
-            e = cudaStreamBeginCaptureToGraph(ctx->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                              cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) {
-            cudaGraphDestroy(graph);
-            return check_cuda(ctx, e, "bicgstab2_learned graph");
-        }
+        DARE_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         const int64_t before = ctx->launches;
         rc = launch_iteration(ctx, net, g, lw->march32, lw->ahat32, vs, lw->st, lw->partials);
-        if (rc == DARE_OK) {
-            k_inner_cond<<<1, 1, 0, ctx->stream>>>(h, lw->st);
-            ctx->launches++;
-            e = cudaGetLastError();
-        }
-        lw->graph_kernels = ctx->launches - before;   // per inner iteration
+        lw->graph_kernels = ctx->launches - before;
         ctx->launches = before;
-        cudaGraph_t body = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &body);
-        if (e == cudaSuccess) e = e2;
-        if (rc == DARE_OK && e == cudaSuccess) e = cudaGraphInstantiate(&lw->graph, graph, 0);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2_learned capture");
+        e = cudaGraphInstantiate(&lw->graph, graph, 0);
         cudaGraphDestroy(graph);
-        if (rc) return rc;
-        if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2_learned graph");
+        if (e != cudaSuccess) return check_cuda(ctx, e, "bicgstab2_learned instantiate");
         lw->graph_net = net;
     }
 
@@ -552,7 +522,13 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         const int cap = std::min(lp->inner_max_it, lp->iteration_budget - inner_total);
         k_init<<<eb, 256, 0, ctx->stream>>>(n, vs, lw->st, lw->partials, lp->inner_rel_tol, cap);
         DARE_LAUNCHED(ctx);
-        DARE_CUDA(ctx, cudaGraphLaunch(lw->graph, ctx->stream));   // the inner iterations, on the device
+        for (int j = 0; j < cap; j++) {
+            DARE_CUDA(ctx, cudaGraphLaunch(lw->graph, ctx->stream));
+            ctx->launches += lw->graph_kernels;
+            DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
+            DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            if (lw->st_host->done) break;
+        }
         // x += D^-1 d (skipped on the device after a NaN) and the next
         // residual, read back with the inner solve's state in one round trip
         k_correct<<<eb, 256, 0, ctx->stream>>>(n, ws->invd, vs.d, s->x, lw->st);
@@ -561,7 +537,6 @@ extern "C" int dare_bicgstab2_learned(dare_system* s, dare_unet* net, const dare
         DARE_CUDA(ctx, cudaMemcpyAsync(lw->st_host, lw->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
         DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         const SolverState st = *lw->st_host;
-        ctx->launches += (int64_t)st.pairs * lw->graph_kernels;
         inner_total += std::min(st.k, cap);
         if (st.status == ST_NAN) break;
         rnorm = st.tres;

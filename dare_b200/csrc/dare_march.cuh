@@ -981,13 +981,6 @@ __global__ void k_step10(int64_t n, const SolverState* st, const T* __restrict__
 }
 inline bool step10_pending(const SolverState& st) { return step10_pending_state(st.status, st.step); }
 
-// The loop condition of the solve graph's device-side iteration loop (a
-// conditional WHILE node): another pair of iterations while the solve runs
-// and the bound max_it / 2 + 2 pairs is not reached.
-static __global__ void k_loop_cond(cudaGraphConditionalHandle h, SolverState* st) {
-    const unsigned pairs = ++st->pairs;
-    cudaGraphSetConditional(h, (!st->done && pairs < (unsigned)(st->max_it / 2 + 2)) ? 1u : 0u);
-}
 
 static __global__ void k_invdiag(const double* __restrict__ dc, double* __restrict__ invd, int64_t n) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)

@@ -172,65 +172,58 @@ int slab_iteration(dare_slabs* sl, const SlabVecs& v) {
     return DARE_OK;
 }
 
-// The slab solve graph: a conditional WHILE node whose body is two
-// iterations over every slab and the loop condition (the single-grid solve's
-// device-side loop).
+// Two iterations over every slab, captured as one CUDA graph.
 template <bool UNIT>
 int slab_graph(dare_slabs* sl, const SlabVecs& v, cudaGraphExec_t* out) {
     dare_ctx* ctx = sl->ctx;
-    cudaGraph_t graph = nullptr;
-    DARE_CUDA(ctx, cudaGraphCreate(&graph, 0));
-    cudaGraphConditionalHandle h;
-    cudaGraphNodeParams cp{};
-    cudaGraphNode_t node;
-    cudaStream_t cap = nullptr;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) {
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
-    }
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    int rc = DARE_OK;
+    cudaStream_t cap;
+    DARE_CUDA(ctx, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cudaStream_t saved = ctx->stream;
+    ctx->stream = cap;
+    cudaGraph_t graph = nullptr;
+    int rc = DARE_OK;
     const int64_t launches0 = ctx->launches;
-    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cap, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                                          cudaStreamCaptureModeThreadLocal);
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        ctx->stream = cap;
         rc = slab_iteration<UNIT>(sl, v);
         if (rc == DARE_OK) rc = slab_iteration<UNIT>(sl, v);
-        if (rc == DARE_OK) {
-            k_loop_cond<<<1, 1, 0, cap>>>(h, sl->st);
-            e = cudaGetLastError();
-        }
-        cudaGraph_t body = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(cap, &body);
+        const cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
         if (e == cudaSuccess) e = e2;
-        ctx->stream = saved;
     }
+    ctx->stream = saved;
     ctx->launches = launches0;   // captured, not executed
     if (e == cudaSuccess && rc == DARE_OK) e = cudaGraphInstantiate(out, graph, 0);
-    if (cap) cudaStreamDestroy(cap);
-    cudaGraphDestroy(graph);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cap);
     if (rc != DARE_OK) return rc;
-    if (e != cudaSuccess) return check_cuda(ctx, e, "slab graph");
+    if (e != cudaSuccess) return check_cuda(ctx, e, "slab graph capture");
     return DARE_OK;
 }
 
-// The iterations: one launch of the slab solve graph, then the state.
+// Iterations until the shared done flag is set (graph replays of two
+// iterations, the state polled every few pairs).
 template <bool UNIT>
-int slab_run(dare_slabs* sl, const SlabVecs& v) {
+int slab_run(dare_slabs* sl, const SlabVecs& v, int max_it, int check_every) {
     dare_ctx* ctx = sl->ctx;
     cudaGraphExec_t* ge = &sl->graph[UNIT ? 1 : 0];
     int rc;
     if (!*ge && (rc = slab_graph<UNIT>(sl, v, ge))) return rc;
-    DARE_CUDA(ctx, cudaGraphLaunch(*ge, ctx->stream));
-    DARE_CUDA(ctx, cudaMemcpyAsync(sl->st_host, sl->st, sizeof(SolverState), cudaMemcpyDeviceToHost, ctx->stream));
-    DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    ctx->launches += (int64_t)sl->st_host->pairs * (2 * 5 * sl->S + 1);
+    if (check_every <= 0) {
+        const int64_t per = (int64_t)1 << 21;
+        check_every = (int)std::min<int64_t>(8, std::max<int64_t>(1, (per + sl->global.ncell - 1) / sl->global.ncell));
+    }
+    const int launches_per_pair = 2 * (4 * sl->S + sl->S);
+    const int max_pairs = max_it / 2 + 2;
+    for (int gi = 0; gi < max_pairs; gi++) {
+        DARE_CUDA(ctx, cudaGraphLaunch(*ge, ctx->stream));
+        ctx->launches += launches_per_pair;
+        if ((gi + 1) % check_every == 0 || gi + 1 == max_pairs) {
+            DARE_CUDA(ctx, cudaMemcpyAsync(sl->st_host, sl->st, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+            DARE_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            if (sl->st_host->done) break;
+        }
+    }
     if (!sl->st_host->done) return set_error(ctx, DARE_ERR_STATE, "slab bicgstab2: iteration bound reached without a status");
     return DARE_OK;
 }
@@ -565,7 +558,7 @@ int dare_slabs_solve(dare_slabs* sl, const dare_solver_params* p, dare_solve_rep
         rc = march_slabs(sl, ki);
     }
     if (rc) return rc;
-    rc = jacobi ? slab_run<true>(sl, v) : slab_run<false>(sl, v);
+    rc = jacobi ? slab_run<true>(sl, v, p->max_it, p->check_every) : slab_run<false>(sl, v, p->max_it, p->check_every);
     if (rc) return rc;
     const SolverState st = *sl->st_host;
     for (int s = 0; s < S; s++)

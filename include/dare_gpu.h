@@ -167,7 +167,7 @@ typedef struct {
     double inner_rel_tol;   /* FP32 inner solve: relative reduction per refinement (e.g. 1e-5) */
     int inner_max_it;       /* FP32 inner solve iteration cap per refinement */
     int max_refinements;
-    int check_every;        /* unused: the iterations run as a device-side loop (kept for the layout) */
+    int check_every;        /* iteration pairs between host status polls (0 = by grid size) */
     int compute_true_residual; /* report ||b - A x||_2 in FP64 after the solve */
     int tol_relative;       /* 1: stop on ||r|| <= tol * ||b||_2 (||b|| computed on the device) */
 } dare_solver_params;
