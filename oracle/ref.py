@@ -1,0 +1,89 @@
+"""ctypes binding of oracle/_ref/libdare_ref.so: the reference's own assembly
+code (its Grid/Cartesian, Equations, Data and MatrixSystem headers, compiled
+against the single-rank stand-ins in oracle/ref_shim/), used to check the C
+restatement in dare_oracle.c.  Test infrastructure only; built by
+``make -C oracle ref`` where the reference's sources are present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libdare_ref.so")
+
+LIMITERS = {"CDS": 0, "UPWIND": 1, "VANALBADA": 2, "MINMOD": 3, "VANLEER": 4}
+SCHEMES = {"EULER_BACKWARD": 0, "EULER_FORWARD": 1, "CRANK_NICHOLSON": 2, "ADAMS_BASHFORT": 3}
+
+
+class Desc(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n", C.c_int64 * 3), ("L", C.c_double * 3), ("periodic", C.c_int * 3),
+                ("dt", C.c_double), ("diffusion", C.c_int), ("D", C.c_double),
+                ("face_D", C.c_void_p * 3), ("convection", C.c_int), ("vel", C.c_double * 3),
+                ("limiter", C.c_int), ("scheme", C.c_int), ("bc_type", C.c_int * 6), ("bc_value", C.c_double * 6)]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(LIB_PATH)
+        _lib.dref_assemble.restype = C.c_int
+        _lib.dref_assemble.argtypes = [C.POINTER(Desc)] + [C.c_void_p] * 7 + [C.c_int64]
+    return _lib
+
+
+def assemble(dim, n, L, periodic, phi_conv, phi_old, dt=0.0, D=None, face_D=None, vel=None,
+             limiter="VANLEER", scheme="EULER_BACKWARD", bc=None):
+    """CSR (rowptr, cols, vals), rhs and initial guess of one implicit step,
+    assembled by the reference's code.  bc: {face 1..6: (1 Dirichlet | 2
+    Neumann, value)}; fields are ghosted (two layers) in the oracle's layout."""
+    d = Desc()
+    d.dim = dim
+    for q in range(3):
+        d.n[q] = int(n[q]) if q < dim else 1
+        d.L[q] = float(L[q]) if q < dim else 1.0
+        d.periodic[q] = int(periodic[q]) if q < dim else 0
+    d.dt = dt
+    keep = []
+    if face_D is not None:
+        d.diffusion = 2
+        for q in range(dim):
+            a = np.ascontiguousarray(face_D[q], dtype=np.float64)
+            keep.append(a)
+            d.face_D[q] = a.ctypes.data
+    elif D is not None:
+        d.diffusion = 1
+        d.D = float(D)
+    if vel is not None:
+        d.convection = 1
+        for q in range(dim):
+            d.vel[q] = float(vel[q])
+    d.limiter = LIMITERS[limiter]
+    d.scheme = SCHEMES[scheme]
+    for face, (kind, value) in (bc or {}).items():
+        d.bc_type[face - 1] = kind
+        d.bc_value[face - 1] = value
+    ncell = int(np.prod([d.n[q] for q in range(3)]))
+    phi_conv = np.ascontiguousarray(phi_conv, dtype=np.float64)
+    phi_old = np.ascontiguousarray(phi_old, dtype=np.float64)
+    rowptr = np.zeros(ncell + 1, dtype=np.int64)
+    cap = 7 * ncell
+    cols = np.zeros(cap, dtype=np.int64)
+    vals = np.zeros(cap, dtype=np.float64)
+    rhs = np.zeros(ncell, dtype=np.float64)
+    x0 = np.zeros(ncell, dtype=np.float64)
+    rc = lib().dref_assemble(C.byref(d), phi_conv.ctypes.data, phi_old.ctypes.data, rowptr.ctypes.data,
+                             cols.ctypes.data, vals.ctypes.data, rhs.ctypes.data, x0.ctypes.data, cap)
+    if rc != 0:
+        raise ValueError(f"reference assembly failed ({rc})")
+    nnz = int(rowptr[-1])
+    return rowptr, cols[:nnz], vals[:nnz], rhs, x0
