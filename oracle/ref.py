@@ -1,8 +1,9 @@
 """ctypes binding of oracle/_ref/libdare_ref.so: the reference's own assembly
-code (its Grid/Cartesian, Equations, Data and MatrixSystem headers, compiled
-against the single-rank stand-ins in oracle/ref_shim/), used to check the C
-restatement in dare_oracle.c.  Test infrastructure only; built by
-``make -C oracle ref`` where the reference's sources are present.
+code (its Grid/Cartesian, Equations, Data and MatrixSystem headers) and its
+BiCGStab2 solver, compiled against the single-rank stand-ins in
+oracle/ref_shim/, used to check the C restatement in dare_oracle.c.  Test
+infrastructure only; built by ``make -C oracle ref`` where the reference's
+sources are present.
 """
 from __future__ import annotations
 
@@ -38,6 +39,9 @@ def lib():
         _lib = C.CDLL(LIB_PATH)
         _lib.dref_assemble.restype = C.c_int
         _lib.dref_assemble.argtypes = [C.POINTER(Desc)] + [C.c_void_p] * 7 + [C.c_int64]
+        _lib.dref_bicgstab2.restype = C.c_int
+        _lib.dref_bicgstab2.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_double, C.c_int, C.c_int,
+                                                                          C.POINTER(C.c_int), C.POINTER(C.c_int)]
     return _lib
 
 
@@ -87,3 +91,21 @@ def assemble(dim, n, L, periodic, phi_conv, phi_old, dt=0.0, D=None, face_D=None
         raise ValueError(f"reference assembly failed ({rc})")
     nnz = int(rowptr[-1])
     return rowptr, cols[:nnz], vals[:nnz], rhs, x0
+
+
+def bicgstab2(rowptr, cols, vals, b, x0, tol, max_it=5000, jacobi=True):
+    """The reference's BiCGStab2::solve on a CSR system: (x, iterations,
+    converged).  tol is absolute (its RNORM criterion)."""
+    n = len(rowptr) - 1
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    iters, conv = C.c_int(0), C.c_int(0)
+    rc = lib().dref_bicgstab2(n, rowptr.ctypes.data, cols.ctypes.data, vals.ctypes.data, b.ctypes.data,
+                              x.ctypes.data, float(tol), int(max_it), int(bool(jacobi)), C.byref(iters),
+                              C.byref(conv))
+    if rc != 0:
+        raise RuntimeError("the reference's BiCGStab2 threw")
+    return x, iters.value, bool(conv.value)

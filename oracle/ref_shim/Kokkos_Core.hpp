@@ -1,6 +1,7 @@
-// Host-only stand-in for the few Kokkos types the reference's GridVector and
-// MatrixBlock headers name (View<T*>, DualView<T*>, deep_copy), so that those
-// headers compile unmodified into the parity checker (oracle/_ref).  Test
+// Host-only stand-in for the few Kokkos types the reference's GridVector,
+// MatrixBlock and BiCGStab2 headers name (View<T*>, DualView<T*>, deep_copy),
+// so that those headers compile unmodified into the parity checker
+// (oracle/_ref).  Test
 // infrastructure only.  A View is a reference-counted host array; a DualView
 // holds one such array as both its host and its device view.
 #pragma once
@@ -18,11 +19,11 @@ struct HostSpace {
 using DefaultExecutionSpace = HostSpace;
 using DefaultHostExecutionSpace = HostSpace;
 
-template <class T>
+template <class T, class... Props>
 class View;
 
-template <class T>
-class View<T*> {
+template <class T, class... Props>
+class View<T*, Props...> {
 public:
     using value_type = T;
     View() : v(std::make_shared<std::vector<T>>()) {}
@@ -40,12 +41,12 @@ private:
     std::shared_ptr<std::vector<T>> v;
 };
 
-template <class T>
-void deep_copy(const View<T*>& dst, const View<T*>& src) {
+template <class T, class... P, class... Q>
+void deep_copy(const View<T*, P...>& dst, const View<T*, Q...>& src) {
     for (std::size_t i = 0; i < src.size() && i < dst.size(); i++) dst[i] = src[i];
 }
-template <class T>
-void deep_copy(const View<T*>& dst, const T& value) {
+template <class T, class... P>
+void deep_copy(const View<T*, P...>& dst, const T& value) {
     for (std::size_t i = 0; i < dst.size(); i++) dst[i] = value;
 }
 }  // namespace Kokkos

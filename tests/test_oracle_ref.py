@@ -1,4 +1,4 @@
-"""The oracle's assembly against the reference's own code.
+"""The oracle's assembly and solve against the reference's own code.
 
 oracle/_ref/libdare_ref.so is the reference's DDT / Gradient / Divergence /
 TVD / MatrixBlock code (Grid/Cartesian, Equations, Data, MatrixSystem),
@@ -10,8 +10,13 @@ restatement in oracle/dare_oracle.c must reproduce it bit for bit: row
 pointers, sorted columns, coefficients, right-hand side and initial guess, on
 seeded random grids in one to three dimensions with every limiter, every time
 scheme the reference compiles, scalar and face diffusivities and Dirichlet /
-Neumann faces.  The library is built where the reference's sources are
-present (``make -C oracle ref``).
+Neumann faces.  The same library holds the reference's BiCGStab2
+(MatrixSystem/BiCGStab2.h, .inl) over a CSR operator and vectors that restate
+Tpetra's update / dot / norm2 / apply, with Ifpack2's Jacobi on the right; the
+oracle's solve (one thread, so its sums run in index order) must give the same
+iterates bit for bit: iteration count, convergence flag and solution.  The
+library is built where the reference's sources are present
+(``make -C oracle ref``).
 """
 import numpy as np
 import pytest
@@ -132,3 +137,67 @@ def test_heterogeneous_face_diffusivity_3d():
     compare(3, n, (1, 1, 1), rng, dt=3.8e-3, face_D=face_arrays(rng, 3, n, 1e-5, 1e-2), vel=(0.2, 0.1, -0.3))
     compare(3, n, (0, 0, 1), rng, dt=3.8e-3, face_D=face_arrays(rng, 3, n, 1e-5, 1e-2), vel=(-0.2, 0.1, 0.3),
             bc={1: (1, 0.2), 2: (2, 0.0), 3: (1, 0.7), 4: (1, -0.1)})
+
+
+def solve_both(rp, cols, vals, rhs, x0, tol, max_it, jacobi):
+    threads = O.num_threads()
+    O.set_threads(1)
+    try:
+        xo, info = O.bicgstab2(rp, cols, vals, rhs, x0, tol, max_it,
+                               precond=O.PREC_JACOBI if jacobi else O.PREC_NONE)
+    finally:
+        O.set_threads(threads)
+    xr, iters, conv = R.bicgstab2(rp, cols, vals, rhs, x0, tol, max_it, jacobi=jacobi)
+    assert info["iters"] == iters
+    assert bool(info["converged"]) == conv
+    assert np.array_equal(xo, xr), np.max(np.abs(xo - xr))
+    return iters, conv
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_bicgstab2_matches_reference_solver(seed):
+    """Seeded systems of the assembly above, from diagonally dominant (a few
+    iterations) to diffusion-dominated (tens of iterations), with and without
+    Jacobi, the stop at tol = 1e-10 ||b|| absolute as the workloads use it."""
+    rng = np.random.default_rng(500 + seed)
+    dim = 1 + seed % 3
+    periodic = tuple(int(rng.integers(0, 2)) for _ in range(dim))
+    n = tuple(int(rng.integers(6, 12 if dim == 3 else 40)) for _ in range(dim))
+    og = O.make_grid(dim, n, [1.0] * dim, 2, periodic)
+    phi = field(rng, og, "normal")
+    D = float(10.0 ** rng.uniform(-3, 0))          # D dt / dx^2 from ~0.1 to ~1e3
+    vel = tuple(float(rng.uniform(-1, 1)) for _ in range(dim)) if seed % 2 else None
+    desc = O.AssemblyDesc(og, dt=1e-2, D=D, vel=vel, limiter=LIMS[seed % 5][1], bc=random_bc(rng, dim, periodic))
+    diag, rhs, mask = O.assemble(desc, phi, phi)
+    rp, cols, vals = O.export_csr(og, diag, mask)
+    x0 = O.field_to_vector(og, phi)
+    tol = 1e-10 * float(np.linalg.norm(rhs))
+    for jacobi in (True, False):
+        iters, conv = solve_both(rp, cols, vals, rhs, x0, tol, 2000, jacobi)
+        assert conv and iters >= 1
+
+
+def test_bicgstab2_edge_exits_match_reference_solver():
+    """The iteration cap (unconverged return), an initial guess that already
+    meets the tolerance (k = 0 without a preconditioner; with Jacobi the
+    reference first replaces the guess by M^-1 x0, BiCGStab2.inl:258-261, and
+    iterates again), and a loose tolerance met in the first iteration (the
+    k > 1 rule)."""
+    rng = np.random.default_rng(9)
+    og = O.make_grid(3, (12, 12, 12), [1.0] * 3, 2, (0, 0, 0))
+    phi = field(rng, og, "normal")
+    bc = {f: (1, 0.5) for f in range(1, 7)}
+    desc = O.AssemblyDesc(og, dt=1e-2, D=1.0, bc=bc)
+    diag, rhs, mask = O.assemble(desc, phi, phi)
+    rp, cols, vals = O.export_csr(og, diag, mask)
+    x0 = O.field_to_vector(og, phi)
+    tol = 1e-10 * float(np.linalg.norm(rhs))
+    iters, conv = solve_both(rp, cols, vals, rhs, x0, tol, 3, True)
+    assert not conv
+    xs, _, _ = R.bicgstab2(rp, cols, vals, rhs, x0, tol, 2000, jacobi=False)
+    iters, conv = solve_both(rp, cols, vals, rhs, xs, 1e3 * tol, 2000, False)
+    assert conv and iters == 0
+    iters, conv = solve_both(rp, cols, vals, rhs, xs, 1e3 * tol, 2000, True)
+    assert conv and iters > 0
+    iters, conv = solve_both(rp, cols, vals, rhs, x0, 0.5 * float(np.linalg.norm(rhs)), 2000, True)
+    assert conv and iters >= 1
