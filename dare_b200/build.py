@@ -11,6 +11,7 @@ in-tree so it travels with the repository.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -56,16 +57,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "dare_gpu.h"))
-    objs = []
+    objs, cmds = [], []
     for src, extra in SOURCES.items():
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [path] + headers):
-            cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", path, "-o", obj]
+            cmds.append([NVCC, *ARCH, *COMMON, *extra, "-c", path, "-o", obj])
+    # translation units compile independently: one nvcc per host core
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for cmd in cmds:
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcuda"]
         if verbose:
