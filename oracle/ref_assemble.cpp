@@ -186,6 +186,7 @@ int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, 
 
     const LO ncell = grep.GetNumberLocalCellsInternal();
     std::vector<MB> blocks(ncell);
+#pragma omp parallel for                        // as Trilinos.inl:308
     for (LO node = 0; node < ncell; node++) {   // Trilinos.inl:309-328
         MB* mb = &blocks[node];
         const GO node_global = grep.MapLocalToGlobalInternal(node);

@@ -9,11 +9,12 @@
 // CrsMatrix (Trilinos 15), restating the definitions the solve relies on:
 //   update(a, A, b):        this = a A + b this         (KokkosBlas axpby)
 //   update(a, A, b, B, c):  this = a A + b B + c this   (KokkosBlas update)
-//   dot / norm2:            sums in index order (one rank, one thread)
+//   dot / norm2:            OpenMP sums (in index order with one thread)
 //   apply(x, y):            y_i = sum over the row's sorted columns of a_ip x_p
 // and the right preconditioner is Ifpack2's RELAXATION Jacobi (one sweep,
 // damping 1, zero start): y = D^-1 x with D^-1 = 1 / diag(A), as
-// TrilinosSolver.inl:84-85,164-176 sets it up.
+// TrilinosSolver.inl:84-85,164-176 sets it up.  The loops are spread over the
+// host threads as Tpetra's OpenMP node spreads them.
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -44,24 +45,34 @@ public:
     Teuchos::RCP<const map_type> getMap() const { return map_; }
     void assign(const ShimVector& o) { v = o.v; }
     void putScalar(double a) {
-        for (auto& e : v) e = a;
+        const int64_t n = (int64_t)v.size();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; i++) v[i] = a;
     }
     void update(double a, const ShimVector& A, double b) {
-        for (std::size_t i = 0; i < v.size(); i++) v[i] = a * A.v[i] + b * v[i];
+        const int64_t n = (int64_t)v.size();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; i++) v[i] = a * A.v[i] + b * v[i];
     }
     void update(double a, const ShimVector& A, double b, const ShimVector& B, double c) {
-        for (std::size_t i = 0; i < v.size(); i++) v[i] = a * A.v[i] + b * B.v[i] + c * v[i];
+        const int64_t n = (int64_t)v.size();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; i++) v[i] = a * A.v[i] + b * B.v[i] + c * v[i];
     }
     template <class View>
     void dot(const ShimVector& o, const View& out) const {
+        const int64_t n = (int64_t)v.size();
         double s = 0.;
-        for (std::size_t i = 0; i < v.size(); i++) s += v[i] * o.v[i];
+#pragma omp parallel for reduction(+ : s) schedule(static)
+        for (int64_t i = 0; i < n; i++) s += v[i] * o.v[i];
         out[0] = s;
     }
     template <class View>
     void norm2(const View& out) const {
+        const int64_t n = (int64_t)v.size();
         double s = 0.;
-        for (std::size_t i = 0; i < v.size(); i++) s += v[i] * v[i];
+#pragma omp parallel for reduction(+ : s) schedule(static)
+        for (int64_t i = 0; i < n; i++) s += v[i] * v[i];
         out[0] = std::sqrt(s);
     }
 
@@ -77,6 +88,7 @@ struct ShimCsr {
     const int64_t* cols;
     const double* vals;
     void apply(const ShimVector& x, ShimVector& y) const {
+#pragma omp parallel for schedule(static)
         for (int64_t r = 0; r < n; r++) {
             double s = 0.;
             for (int64_t p = rowptr[r]; p < rowptr[r + 1]; p++) s += vals[p] * x.v[cols[p]];
@@ -116,7 +128,9 @@ int dref_bicgstab2(int64_t n, const int64_t* rowptr, const int64_t* cols, const 
             inv_diag[r] = 1. / d;
         }
         problem->setRightPrec([&inv_diag](const ShimVector& in, ShimVector& out) {
-            for (std::size_t i = 0; i < in.v.size(); i++) out.v[i] = inv_diag[i] * in.v[i];
+            const int64_t m = (int64_t)in.v.size();
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < m; i++) out.v[i] = inv_diag[i] * in.v[i];
         });
     }
     auto params = Teuchos::rcp(new Teuchos::ParameterList());

@@ -46,6 +46,40 @@ def oracle_timeloop(case, steps, precond=O.PREC_JACOBI, face_D=None, max_it=5000
     return history, iters
 
 
+def ref_timeloop(case, steps, max_it=5000):
+    """The same driver loop with the reference's own assembly and BiCGStab2
+    (oracle/_ref: its Grid/Cartesian, Equations, MatrixBlock and BiCGStab2
+    code) for a case without face fields (scalar D, constant or no velocity).
+    The copy back and the periodic ghost fill are the oracle's.  Returns the
+    field history, the iterations and the seconds spent in assembly and
+    solve."""
+    import time
+
+    from oracle import ref as R
+    og = oracle_grid(case)
+    n = tuple(case["n"])
+    dim = len(n)
+    lim = case.get("limiter", "VANLEER")
+    phi = np.ascontiguousarray(np.asarray(case["phi0"], dtype=np.float64).reshape(-1)).copy()
+    old = phi.copy()
+    bc = {int(k): v for k, v in case.get("bc", {}).items()}
+    history, iters, secs = [], [], 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        rp, cols, vals, rhs, x0 = R.assemble(dim, n, case.get("size", (1.0,) * dim), case.get("periodic", (0,) * dim),
+                                             phi, old, dt=case.get("dt", 0.0), D=case.get("D"), vel=case.get("vel"),
+                                             limiter=lim, bc=bc)
+        tol = case.get("rel_tol", 1e-10) * float(np.linalg.norm(rhs))
+        x, it, conv = R.bicgstab2(rp, cols, vals, rhs, x0, tol, max_it, jacobi=True)
+        secs += time.perf_counter() - t0
+        O.copy_to_field(og, x, phi)
+        O.exchange_halo(og, phi)
+        old[:] = phi
+        history.append(phi.copy())
+        iters.append(it)
+    return history, iters, secs
+
+
 def interior(phi, shape, ng=2, dim=3):
     a = np.asarray(phi).reshape(shape)
     sl = tuple(slice(ng, s - ng) if d < dim else slice(None) for d, s in enumerate(shape))

@@ -141,13 +141,13 @@ def test_heterogeneous_face_diffusivity_3d():
 
 def solve_both(rp, cols, vals, rhs, x0, tol, max_it, jacobi):
     threads = O.num_threads()
-    O.set_threads(1)
+    O.set_threads(1)   # one OpenMP thread for both libraries: sums in index order
     try:
         xo, info = O.bicgstab2(rp, cols, vals, rhs, x0, tol, max_it,
                                precond=O.PREC_JACOBI if jacobi else O.PREC_NONE)
+        xr, iters, conv = R.bicgstab2(rp, cols, vals, rhs, x0, tol, max_it, jacobi=jacobi)
     finally:
         O.set_threads(threads)
-    xr, iters, conv = R.bicgstab2(rp, cols, vals, rhs, x0, tol, max_it, jacobi=jacobi)
     assert info["iters"] == iters
     assert bool(info["converged"]) == conv
     assert np.array_equal(xo, xr), np.max(np.abs(xo - xr))
