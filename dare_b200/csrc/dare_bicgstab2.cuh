@@ -52,7 +52,6 @@ struct MarchCfg {
     size_t smem = 0;
     int cpt = 1;      // cells per thread along k (2: paired 16-byte copies, needs an even n2)
     int cpc = 1;      // plane runs per field component (items: tiles x cpc x components)
-    int pair16 = 0;   // FP64, one cell per thread: stage the per-cell streams as 16-byte pairs (set at launch)
     // Slab decomposition (dare_slabs.cu): the first partial-sum slot of this
     // launch's items and the items of all launches that share the reduction
     // (0: this launch alone), and per operand input the planes below the

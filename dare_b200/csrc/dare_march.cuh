@@ -568,13 +568,14 @@ __device__ __forceinline__ Pair<T> ld_pair(const T* p) {
 // to 0.354 ms, so the default carveout stays).
 // HALO (slabs): the planes before the first and after the last plane of the
 // grid come from m.halo when set.
-template <class K, int CPT = 1, bool HALO = false>
+template <class K, int CPT = 1, bool HALO = false, bool PAIR = false>
 __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K kern, SolverState* st, double* partials,
                                                                    MarchCfg m) {
     using T = typename K::type;
     constexpr int NZ = K::NZ, NP = K::NP;
     constexpr int QA = K::Q > 0 ? K::Q : 1;
-    constexpr int IC = CPT;                     // first interior column of a staged operand row
+    static_assert(!PAIR || (CPT == 1 && sizeof(typename K::type) == 8), "16-byte pairs: FP64, one cell per thread");
+    constexpr int IC = PAIR ? 2 : CPT;          // first interior column of a staged operand row
     constexpr int CB = CPT * (int)sizeof(T);    // bytes of one thread's row segment
     if (K::kCheckDone && st->done) return;
     K k = kern;
@@ -602,18 +603,41 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
         int cb;        // first stacked plane of this item's component
         bool inside, hS, hN, hB, hT;
         int64_t o_c, o_s, o_n, o_b, o_t, o_own;
-        int64_t o_pair;   // pair16: in-plane offset of this thread's cell pair (-1: outside)
+        int64_t o_pair;   // PAIR: in-plane offset of this thread's pair of stream cells (-1: outside)
+        int64_t o_op;     // PAIR: in-plane offset of this thread's operand copy (-1: zero)
     };
-    // pair16 (FP64, one cell per thread, even n2): the per-cell streams are
+    // PAIR (FP64, one cell per thread, even n2): the per-cell streams are
     // staged as 16-byte pairs of cells, the first half of the threads copying
     // the even-numbered streams and the second half the odd ones -- half the
     // copies and address arithmetic of one 8-byte copy per thread and stream
-    // (256^3 step 4: 0.316 -> 0.300 ms, 125 -> 119 registers)
+    // (256^3 step 4: 0.316 -> 0.298 ms)
     const int npairs = NCT / 2;
     const int par = tid >= npairs;
     const int e_pair = tid - par * npairs;
-    const int hw = TW / 2 > 0 ? TW / 2 : 1;   // pairs per row (pair16 needs an even TW)
+    const int hw = TW / 2 > 0 ? TW / 2 : 1;   // pairs per row (PAIR needs an even TW)
     const int pr_row = e_pair / hw, pr_col = 2 * (e_pair - pr_row * hw);
+    // PAIR: the operand tiles' rows 0 .. TJ+1 (j0-1 .. j0+TJ) as 16-byte pairs,
+    // then the single halo cells k0-1 and k0+TW of rows 1 .. TJ; thread tid
+    // copies one element of every operand array (op_kind 2: a pair, 1: one
+    // cell, 0: none) -- (TJ+2) TW/2 + 2 TJ copies, all threads alike, in place
+    // of one copy per cell plus the halo copies of the edge threads (256^3
+    // step 4: 0.298 -> 0.285 ms, 6.1 TB/s)
+    int op_kind = 0, op_row = 0, op_col = 0, op_dk = 0;
+    if constexpr (PAIR) {
+        const int npr = (TJ + 2) * hw;
+        if (tid < npr) {
+            op_kind = 2;
+            op_row = tid / hw;
+            op_dk = 2 * (tid - op_row * hw);
+            op_col = IC + op_dk;
+        } else if (tid < npr + 2 * TJ) {
+            const int e = tid - npr;
+            op_kind = 1;
+            op_row = 1 + (e >> 1);
+            op_dk = (e & 1) ? TW : -1;
+            op_col = IC + op_dk;
+        }
+    }
     // in-plane position (j, kx) -> wrapped offset, or -1 when outside (zero)
     auto jk_offset = [&](int j, int kx) -> int64_t {
         if (j < 0) {
@@ -657,9 +681,14 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
         G.o_b = G.hB ? jk_offset(jj, kk - 1) : -1;
         G.o_t = G.hT ? jk_offset(jj, kk + CPT) : -1;
         G.o_own = G.inside ? (int64_t)jj * n2 + kk : 0;
-        {
-            const int pj = (tile_id / m.tiles_x) * TJ + pr_row, pk = (tile_id % m.tiles_x) * TW + pr_col;
+        G.o_pair = G.o_op = -1;
+        if constexpr (PAIR) {
+            const int tj0 = (tile_id / m.tiles_x) * TJ, tk0 = (tile_id % m.tiles_x) * TW;
+            const int pj = tj0 + pr_row, pk = tk0 + pr_col;
             G.o_pair = (pj < n1 && pk < n2) ? (int64_t)pj * n2 + pk : -1;
+            // a pair past n2 starts at the wrapped (or removed) first cell; its
+            // second cell is never read
+            if (op_kind) G.o_op = jk_offset(tj0 - 1 + op_row, tk0 + op_dk);
         }
         return G;
     };
@@ -693,6 +722,13 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
                     zv = true;
                 }
             }
+            if constexpr (PAIR) {
+                if (op_kind == 2)
+                    cp_async<16>(zt + op_row * W + op_col, src + zb + (G.o_op < 0 ? 0 : G.o_op), zv && G.o_op >= 0);
+                else if (op_kind == 1)
+                    cp_async<8>(zt + op_row * W + op_col, src + zb + (G.o_op < 0 ? 0 : G.o_op), zv && G.o_op >= 0);
+                continue;
+            }
             cp_async<CB>(zt + (ty + 1) * W + col, src + zb + (G.o_c < 0 ? 0 : G.o_c), zv && G.o_c >= 0);
             if (G.hS) cp_async<CB>(zt + col, src + zb + (G.o_s < 0 ? 0 : G.o_s), zv && G.o_s >= 0);
             if (G.hN)
@@ -704,17 +740,15 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
                 cp_async<sizeof(T)>(zt + (ty + 1) * W + IC + TW, src + zb + (G.o_t < 0 ? 0 : G.o_t),
                                     zv && G.o_t >= 0);
         }
-        if constexpr (CPT == 1 && sizeof(T) == 8) {
-            if (m.pair16) {
-                if (full) {
-                    T* pt = sb + NZ * ZT + pr_row * TW + pr_col;
+        if constexpr (PAIR) {
+            if (full) {
+                T* pt = sb + NZ * ZT + pr_row * TW + pr_col;
 #pragma unroll
-                    for (int q = 0; q < NP; q++)
-                        if ((q & 1) == par)
-                            cp_async<16>(pt + q * NCT, k.ps[q] + base + (G.o_pair < 0 ? 0 : G.o_pair), G.o_pair >= 0);
-                }
-                return;
+                for (int q = 0; q < NP; q++)
+                    if ((q & 1) == par)
+                        cp_async<16>(pt + q * NCT, k.ps[q] + base + (G.o_pair < 0 ? 0 : G.o_pair), G.o_pair >= 0);
             }
+            return;
         }
         if (full && G.inside) {
             T* pt = sb + NZ * ZT + ty * TW + CPT * tx;
@@ -903,33 +937,51 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
     }
 }
 
-template <class K, int CPT, bool HALO>
-inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
+template <class K, int CPT, bool HALO, bool PAIR>
+inline int launch_march_k(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
                           double* partials) {
-    const size_t smem = march_smem_bytes<K>(m);
+    const int ic = PAIR ? 2 : m.cpt;   // first interior column of a staged operand row
+    const size_t smem = 3 * march_stage_elems<K>(m.block.x * m.cpt, m.block.y, ic) * sizeof(typename K::type);
     static int per_sm = 0;
     static size_t per_sm_smem = 0;
     if (per_sm == 0 || per_sm_smem != smem) {
         if (smem > 48 * 1024)
-            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K, CPT, HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K, CPT, HALO>, m.block.x * m.block.y, smem);
+            DARE_CUDA(ctx, cudaFuncSetAttribute(k_march<K, CPT, HALO, PAIR>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_march<K, CPT, HALO, PAIR>, m.block.x * m.block.y,
+                                                      smem);
         if (per_sm < 1) per_sm = 1;
         per_sm_smem = smem;
     }
     int blocks = per_sm * ctx->num_sms;
     if (blocks > m.nitems) blocks = m.nitems;
-    MarchCfg mk = m;
-    mk.pair16 = 0;
-    if constexpr (CPT == 1 && sizeof(typename K::type) == 8) {
-        // 16-byte pairs need an even row length and 16-byte aligned streams
-        bool ok = g.n[2] % 2 == 0 && (m.block.x * m.block.y) % 2 == 0 && m.block.x % 2 == 0;
-        for (int q = 0; q < K::NP; q++) ok = ok && ((uintptr_t)kern.ps[q] & 15) == 0;
-        mk.pair16 = ok;
-    }
-    k_march<K, CPT, HALO><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, mk);
+    k_march<K, CPT, HALO, PAIR><<<blocks, m.block, smem, ctx->stream>>>(g, kern, st, partials, m);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
+}
+
+// 16-byte pairs (FP64, one cell per thread): an even row length and tile
+// width, enough threads for the operand copies, and 16-byte aligned arrays
+template <class K, bool HALO>
+inline bool march_pairs_ok(const GridDev& g, const MarchCfg& m, const K& kern) {
+    const int tw = (int)m.block.x, tj = (int)m.block.y;
+    bool ok = g.n[2] % 2 == 0 && tw % 2 == 0 && (tj + 2) * (tw / 2) + 2 * tj <= tw * tj;
+    for (int q = 0; q < K::NP; q++) ok = ok && ((uintptr_t)kern.ps[q] & 15) == 0;
+    for (int z = 0; z < K::NZ; z++) {
+        ok = ok && ((uintptr_t)kern.zs[z] & 15) == 0;
+        if (HALO)
+            for (int h = 0; h < 2; h++) ok = ok && ((uintptr_t)m.halo[z][h] & 15) == 0;
+    }
+    return ok;
+}
+
+template <class K, int CPT, bool HALO>
+inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
+                          double* partials) {
+    if constexpr (CPT == 1 && sizeof(typename K::type) == 8) {
+        if (march_pairs_ok<K, HALO>(g, m, kern)) return launch_march_k<K, CPT, HALO, true>(ctx, g, m, kern, st, partials);
+    }
+    return launch_march_k<K, CPT, HALO, false>(ctx, g, m, kern, st, partials);
 }
 
 // Two cells per thread (K::kPairs) pays off for steps 1, 2 and 3 (seven
