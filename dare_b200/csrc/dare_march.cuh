@@ -186,7 +186,7 @@ struct FStep1 {
     using type = T;
     static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
-    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
+    static constexpr bool kPairs = sizeof(T) == 4;   // two cells per thread (see launch_march)
     const T* zs[2];   // r, u
     const T* ps[NP];  // coefficients, r_hat_0
     T *u_out, *v;
@@ -210,7 +210,7 @@ struct FStep2 {
     using type = T;
     static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
-    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
+    static constexpr bool kPairs = sizeof(T) == 4;   // two cells per thread (see launch_march)
     const T* zs[2];   // v, r
     const T* ps[NP];  // coefficients, r_hat_0
     T *r_out, *s;
@@ -232,7 +232,7 @@ struct FStep3 {
     using type = T;
     static constexpr int Q = 1, NZ = 2, NC = NCoef<UNIT>::value, NP = NC + 1;
     static constexpr bool kCheckDone = true;
-    static constexpr bool kPairs = true;   // two cells per thread (see launch_march)
+    static constexpr bool kPairs = sizeof(T) == 4;   // two cells per thread (see launch_march)
     const T* zs[2];   // s, v
     const T* ps[NP];  // coefficients, r_hat_0
     T *v_out, *w;
@@ -984,12 +984,15 @@ inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, co
     return launch_march_k<K, CPT, HALO, false>(ctx, g, m, kern, st, partials);
 }
 
-// Two cells per thread (K::kPairs) pays off for steps 1, 2 and 3 (seven
-// streams, one dot product; 256^3: 0.291 -> 0.257 ms for step 1, step 2
-// 0.258 ms with pairs); with eight streams and five dot products (step 4:
-// 0.316 -> 0.404 ms with pairs), or many outputs per cell (init: 0.29 ->
-// 0.38 ms, fold), the halved warp count per SM no longer hides the work, so
-// those run one cell per thread on the same 32 x 8 tiles.
+// Two cells per thread (K::kPairs) paid off for steps 1, 2 and 3 while one
+// cell per thread staged every value with its own 8-byte copy (256^3: 0.291
+// -> 0.257 ms for step 1).  With the 16-byte paired staging of the FP64
+// one-cell kernels (PAIR in k_march) one cell per thread is ahead again
+// (step 1 0.255 -> 0.252 ms, step 2 0.254 -> 0.249, step 3 0.252 -> 0.249),
+// so the FP64 steps run one cell per thread on 32 x 8 tiles; the FP32
+// kernels keep two or four cells per thread.  With eight streams and five
+// dot products (step 4: 0.316 -> 0.404 ms with two cells), or many outputs
+// per cell (init: 0.29 -> 0.38 ms, fold), two cells per thread never paid.
 // HALO: the slab variant, which reads m.halo (ignored otherwise).
 template <class K, bool HALO = false>
 inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
