@@ -574,8 +574,9 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
     using T = typename K::type;
     constexpr int NZ = K::NZ, NP = K::NP;
     constexpr int QA = K::Q > 0 ? K::Q : 1;
-    static_assert(!PAIR || (CPT == 1 && sizeof(typename K::type) == 8), "16-byte pairs: FP64, one cell per thread");
-    constexpr int IC = PAIR ? 2 : CPT;          // first interior column of a staged operand row
+    constexpr int VEC = 16 / (int)sizeof(T);    // cells of one 16-byte copy
+    static_assert(!PAIR || VEC % CPT == 0, "16-byte staging: a copy covers whole thread segments");
+    constexpr int IC = PAIR ? VEC : CPT;        // first interior column of a staged operand row
     constexpr int CB = CPT * (int)sizeof(T);    // bytes of one thread's row segment
     if (K::kCheckDone && st->done) return;
     K k = kern;
@@ -606,29 +607,33 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
         int64_t o_pair;   // PAIR: in-plane offset of this thread's pair of stream cells (-1: outside)
         int64_t o_op;     // PAIR: in-plane offset of this thread's operand copy (-1: zero)
     };
-    // PAIR (FP64, one cell per thread, even n2): the per-cell streams are
-    // staged as 16-byte pairs of cells, the first half of the threads copying
-    // the even-numbered streams and the second half the odd ones -- half the
-    // copies and address arithmetic of one 8-byte copy per thread and stream
-    // (256^3 step 4: 0.316 -> 0.298 ms)
-    const int npairs = NCT / 2;
+    // PAIR: every value staged as part of a 16-byte copy of VEC cells (FP64
+    // with one cell per thread, FP32 with two: row length and tile width
+    // multiples of VEC).  The per-cell streams: the first half of the threads
+    // copies the even-numbered streams and the second half the odd ones, one
+    // 16-byte copy each -- half the copies and address arithmetic of one
+    // copy per thread and stream (256^3 FP64 step 4: 0.316 -> 0.298 ms).
+    static_assert(!PAIR || VEC / CPT == 2, "16-byte staging: two thread sets");
+    const int npairs = NCT / VEC;               // 16-byte copies per stream and plane (half the threads)
     const int par = tid >= npairs;
     const int e_pair = tid - par * npairs;
-    const int hw = TW / 2 > 0 ? TW / 2 : 1;   // pairs per row (PAIR needs an even TW)
-    const int pr_row = e_pair / hw, pr_col = 2 * (e_pair - pr_row * hw);
-    // PAIR: the operand tiles' rows 0 .. TJ+1 (j0-1 .. j0+TJ) as 16-byte pairs,
+    const int hw = TW / VEC > 0 ? TW / VEC : 1;   // copies per row (PAIR needs TW % VEC == 0)
+    const int pr_row = e_pair / hw, pr_col = VEC * (e_pair - pr_row * hw);
+    // PAIR: the operand tiles' rows 0 .. TJ+1 (j0-1 .. j0+TJ) as 16-byte copies,
     // then the single halo cells k0-1 and k0+TW of rows 1 .. TJ; thread tid
-    // copies one element of every operand array (op_kind 2: a pair, 1: one
-    // cell, 0: none) -- (TJ+2) TW/2 + 2 TJ copies, all threads alike, in place
+    // makes one copy of every operand array (op_kind 2: 16 bytes, 1: one
+    // cell, 0: none) -- (TJ+2) TW/VEC + 2 TJ copies, all threads alike, in place
     // of one copy per cell plus the halo copies of the edge threads (256^3
-    // step 4: 0.298 -> 0.285 ms, 6.1 TB/s)
+    // FP64 step 4: 0.298 -> 0.285 ms, 6.1 TB/s; the FP32 kernels on 64 x 8
+    // tiles run two cells per thread this way, 512^3 FP32-refine solve 52.8
+    // -> 51.7 ms)
     int op_kind = 0, op_row = 0, op_col = 0, op_dk = 0;
     if constexpr (PAIR) {
         const int npr = (TJ + 2) * hw;
         if (tid < npr) {
             op_kind = 2;
             op_row = tid / hw;
-            op_dk = 2 * (tid - op_row * hw);
+            op_dk = VEC * (tid - op_row * hw);
             op_col = IC + op_dk;
         } else if (tid < npr + 2 * TJ) {
             const int e = tid - npr;
@@ -726,7 +731,8 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
                 if (op_kind == 2)
                     cp_async<16>(zt + op_row * W + op_col, src + zb + (G.o_op < 0 ? 0 : G.o_op), zv && G.o_op >= 0);
                 else if (op_kind == 1)
-                    cp_async<8>(zt + op_row * W + op_col, src + zb + (G.o_op < 0 ? 0 : G.o_op), zv && G.o_op >= 0);
+                    cp_async<(int)sizeof(T)>(zt + op_row * W + op_col, src + zb + (G.o_op < 0 ? 0 : G.o_op),
+                                             zv && G.o_op >= 0);
                 continue;
             }
             cp_async<CB>(zt + (ty + 1) * W + col, src + zb + (G.o_c < 0 ? 0 : G.o_c), zv && G.o_c >= 0);
@@ -940,7 +946,7 @@ __global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K ke
 template <class K, int CPT, bool HALO, bool PAIR>
 inline int launch_march_k(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
                           double* partials) {
-    const int ic = PAIR ? 2 : m.cpt;   // first interior column of a staged operand row
+    const int ic = PAIR ? 16 / (int)sizeof(typename K::type) : m.cpt;   // first interior column of an operand row
     const size_t smem = 3 * march_stage_elems<K>(m.block.x * m.cpt, m.block.y, ic) * sizeof(typename K::type);
     static int per_sm = 0;
     static size_t per_sm_smem = 0;
@@ -960,12 +966,14 @@ inline int launch_march_k(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, co
     return DARE_OK;
 }
 
-// 16-byte pairs (FP64, one cell per thread): an even row length and tile
-// width, enough threads for the operand copies, and 16-byte aligned arrays
+// 16-byte staging (one copy = 16 / sizeof(T) cells): a row length and tile
+// width that are multiples of it, enough threads for the operand copies, and
+// 16-byte aligned arrays
 template <class K, bool HALO>
-inline bool march_pairs_ok(const GridDev& g, const MarchCfg& m, const K& kern) {
-    const int tw = (int)m.block.x, tj = (int)m.block.y;
-    bool ok = g.n[2] % 2 == 0 && tw % 2 == 0 && (tj + 2) * (tw / 2) + 2 * tj <= tw * tj;
+inline bool march_pairs_ok(const GridDev& g, const MarchCfg& m, const K& kern, int cpt) {
+    const int vec = 16 / (int)sizeof(typename K::type);
+    const int nt = (int)(m.block.x * m.block.y), tw = (int)m.block.x * cpt, tj = (int)m.block.y;
+    bool ok = g.n[2] % vec == 0 && tw % vec == 0 && (tj + 2) * (tw / vec) + 2 * tj <= nt;
     for (int q = 0; q < K::NP; q++) ok = ok && ((uintptr_t)kern.ps[q] & 15) == 0;
     for (int z = 0; z < K::NZ; z++) {
         ok = ok && ((uintptr_t)kern.zs[z] & 15) == 0;
@@ -978,8 +986,9 @@ inline bool march_pairs_ok(const GridDev& g, const MarchCfg& m, const K& kern) {
 template <class K, int CPT, bool HALO>
 inline int launch_march_t(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, const K& kern, SolverState* st,
                           double* partials) {
-    if constexpr (CPT == 1 && sizeof(typename K::type) == 8) {
-        if (march_pairs_ok<K, HALO>(g, m, kern)) return launch_march_k<K, CPT, HALO, true>(ctx, g, m, kern, st, partials);
+    if constexpr ((CPT == 1 && sizeof(typename K::type) == 8) || (CPT == 2 && sizeof(typename K::type) == 4)) {
+        if (march_pairs_ok<K, HALO>(g, m, kern, CPT))
+            return launch_march_k<K, CPT, HALO, true>(ctx, g, m, kern, st, partials);
     }
     return launch_march_k<K, CPT, HALO, false>(ctx, g, m, kern, st, partials);
 }
@@ -1001,6 +1010,10 @@ inline int launch_march(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, cons
         return set_error(ctx, DARE_ERR_UNSUPPORTED, "grid too large for the reduction");
     if (m.cpt == 4) {   // FP32 grids with n2 a multiple of 4, 64-cell tiles
         if constexpr (sizeof(typename K::type) == 4 && !SplitOperands<K>::value) {
+            MarchCfg m2 = m;   // two cells per thread on the same tiles, 16-byte staging
+            m2.cpt = 2;
+            m2.block = dim3(m.block.x * 2, m.block.y, 1);
+            if (march_pairs_ok<K, HALO>(g, m2, kern, 2)) return launch_march_k<K, 2, HALO, true>(ctx, g, m2, kern, st, partials);
             if constexpr (K::kPairs) {
                 return launch_march_t<K, 4, HALO>(ctx, g, m, kern, st, partials);
             } else {
