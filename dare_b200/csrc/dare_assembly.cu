@@ -357,8 +357,7 @@ static int base_params(dare_system* s, AsmParams& a, const char* who) {
     return DARE_OK;
 }
 
-int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old) {
-    AsmParams a{};
+static void fused_params(const dare_assembly_desc* desc, AsmParams& a) {
     a.dt = desc->dt;
     a.diffusion = desc->diffusion;
     a.D = desc->D;
@@ -376,6 +375,11 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
     a.sgn_diff = -1.;
     a.acc = 0;
     a.fold = 1;
+}
+
+int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old) {
+    AsmParams a{};
+    fused_params(desc, a);
     int rc = base_params(s, a, "dare_assemble");
     if (rc) return rc;
     for (int c = 0; c < s->ncomp; c++) {
@@ -383,6 +387,21 @@ int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double
         if ((rc = launch_component(s, a, c, phi, phi_old))) return rc;
     }
     return DARE_OK;
+}
+
+// The fused functor on the planes ib .. ie - 1 of a single-component 3-D
+// grid: each plane's coefficients are those of the whole-grid launch, bit for
+// bit.  DARE_ERR_UNSUPPORTED on other grids.
+int launch_assemble_planes(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old,
+                           int ib, int ie) {
+    const GridDev& g = s->grid->dev;
+    if (g.dim != 3 || s->ncomp != 1) return DARE_ERR_UNSUPPORTED;
+    AsmParams a{};
+    fused_params(desc, a);
+    int rc = base_params(s, a, "dare_assemble");
+    if (rc) return rc;
+    component_bc(s, 0, a);
+    return launch_assemble3(s->grid->ctx, g, a, phi, phi_old, s->diag, s->rhs, s->x, ib, ie);
 }
 
 // A composed functor (dare_assemble_terms): per component, its terms in

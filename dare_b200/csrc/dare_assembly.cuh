@@ -78,8 +78,9 @@ __device__ __forceinline__ int upper_face(const GridDev& g, int d, int i) {
     return (g.periodic[d] && i + 1 == g.n[d]) ? 0 : i + 1;
 }
 
-// The 3-D assembly (dare_assembly3.cu): one launch per field component.
+// The 3-D assembly (dare_assembly3.cu): one launch per field component, over
+// the planes ib .. ie - 1 (ie < 0: through the last plane).
 int launch_assemble3(dare_ctx* ctx, const GridDev& g, const AsmParams& a, const double* phi,
-                     const double* phi_old, double* diag, double* rhs, double* x0);
+                     const double* phi_old, double* diag, double* rhs, double* x0, int ib = 0, int ie = -1);
 
 }  // namespace dare_gpu

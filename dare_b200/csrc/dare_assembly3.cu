@@ -146,19 +146,20 @@ struct A3Copy {
 template <int LIM, bool FD>
 __global__ void __launch_bounds__(256, FD ? 2 : 3)
     k_assemble3(GridDev g, A3Params a, const double* __restrict__ phi, const double* __restrict__ phi_old,
-                double* __restrict__ diag, double* __restrict__ rhs_out, double* __restrict__ x0, int planes) {
+                double* __restrict__ diag, double* __restrict__ rhs_out, double* __restrict__ x0, int planes,
+                int ibase, int iend) {
     constexpr int STAGE = a3_stage<FD>();
     extern __shared__ __align__(16) double sm3[];
     __shared__ double rrN_s[2][kA3J][kA3K];
     const int lane = threadIdx.x, ty = threadIdx.y, tid = lane + kA3K * ty;
-    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int n1 = g.n[1], n2 = g.n[2];
     const int gn1 = g.gn[1], gn2 = g.gn[2];
     const int og0 = g.og[0], og1 = g.og[1], og2 = g.og[2];
     const int k0 = blockIdx.x * kA3K, j0 = blockIdx.y * kA3J;
     const int kk = k0 + lane, jj = j0 + ty;
     const bool active = kk < n2 && jj < n1;
-    const int i0 = blockIdx.z * planes;
-    const int i1 = min(i0 + planes, n0);
+    const int i0 = ibase + blockIdx.z * planes;   // this block's run of the planes ibase .. iend - 1
+    const int i1 = min(i0 + planes, iend);
     const int P = (i1 - i0) + 4;                    // staged planes i0-2 .. i1+1
     const int64_t gplane = (int64_t)gn1 * gn2;
     const int64_t xplane = (int64_t)n1 * n2, yplane = (int64_t)(n1 + 1) * n2, zplane = (int64_t)n1 * (n2 + 1);
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(256, FD ? 2 : 3)
 
 template <int LIM, bool FD>
 static int launch3_t(dare_ctx* ctx, const GridDev& g, const A3Params& p, const double* phi, const double* phi_old,
-                     double* diag, double* rhs, double* x0) {
+                     double* diag, double* rhs, double* x0, int ib, int ie) {
     const size_t smem = (size_t)a3_stage<FD>() * kA3Ring * sizeof(double);
     static int resident = 0;
     if (!resident) {
@@ -386,7 +387,7 @@ static int launch3_t(dare_ctx* ctx, const GridDev& g, const A3Params& p, const d
     }
     // runs of i-planes sized so the waves of resident blocks come out even;
     // a run re-stages 4 planes of phi (its x halo)
-    const int n0 = g.n[0];
+    const int n0 = ie - ib;   // the planes of this launch
     const int gx = (g.n[2] + kA3K - 1) / kA3K, gy = (g.n[1] + kA3J - 1) / kA3J;
     const int64_t units = (int64_t)gx * gy;
     int best = n0;
@@ -401,13 +402,15 @@ static int launch3_t(dare_ctx* ctx, const GridDev& g, const A3Params& p, const d
         }
     }
     const dim3 grid(gx, gy, (unsigned)((n0 + best - 1) / best)), block(kA3K, kA3J, 1);
-    k_assemble3<LIM, FD><<<grid, block, smem, ctx->stream>>>(g, p, phi, phi_old, diag, rhs, x0, best);
+    k_assemble3<LIM, FD><<<grid, block, smem, ctx->stream>>>(g, p, phi, phi_old, diag, rhs, x0, best, ib, ie);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }
 
 int launch_assemble3(dare_ctx* ctx, const GridDev& g, const AsmParams& a, const double* phi, const double* phi_old,
-                     double* diag, double* rhs, double* x0) {
+                     double* diag, double* rhs, double* x0, int ib, int ie) {
+    if (ie < 0) ie = g.n[0];
+    if (ib < 0 || ib >= ie || ie > g.n[0]) return DARE_OK;   // an empty range
     A3Params p{};
     p.ddt = a.dt > 0.;
     p.tt = a.sgn_ddt * a.tt;
@@ -437,8 +440,8 @@ int launch_assemble3(dare_ctx* ctx, const GridDev& g, const AsmParams& a, const 
     switch (a.limiter) {
 #define DARE_A3(L)                                                                                   \
     case L:                                                                                          \
-        return fd ? launch3_t<L, true>(ctx, g, p, phi, phi_old, diag, rhs, x0)                       \
-                  : launch3_t<L, false>(ctx, g, p, phi, phi_old, diag, rhs, x0);
+        return fd ? launch3_t<L, true>(ctx, g, p, phi, phi_old, diag, rhs, x0, ib, ie)               \
+                  : launch3_t<L, false>(ctx, g, p, phi, phi_old, diag, rhs, x0, ib, ie);
         DARE_A3(DARE_LIMITER_CDS)
         DARE_A3(DARE_LIMITER_UPWIND)
         DARE_A3(DARE_LIMITER_VANALBADA)

@@ -534,13 +534,18 @@ def test_multicomponent_assembly_and_timeloop(ctx, periodic):
         assert abs(rep["iters"] - info["iters"]) <= 2
 
 
-def test_host_resident_steps_match_single_calls(ctx):
+@pytest.mark.parametrize("kind", ["tvd-periodic", "gaussian-bounded"])
+def test_host_resident_steps_match_single_calls(ctx, kind):
     """dare_timesteps_host (each step's field from pinned host memory, the
-    result back to it, transfers of consecutive steps pipelined in slices)
-    gives the loop of single upload / copy-to-old / timestep / download calls
-    bit for bit; an unpinned buffer is refused."""
+    result back to it, transfers of consecutive steps pipelined in slices,
+    each slice's planes assembled as it lands) gives the loop of single
+    upload / copy-to-old / timestep / download calls bit for bit, the old
+    level included; an unpinned buffer is refused."""
     import torch
-    case = W.tvd_convection_diffusion(n=24, steps=3)
+    if kind == "tvd-periodic":
+        case = W.tvd_convection_diffusion(n=24, steps=3)
+    else:
+        case = W.gaussian_diffusion(n=20, steps=3)
     g, f, s, asm, keep, dim = _gpu_case(ctx, case)
     solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
     phi0 = f.download(0)
@@ -548,6 +553,8 @@ def test_host_resident_steps_match_single_calls(ctx):
     host[:] = phi0
     reps = D.timesteps_host(s, f, asm, solver, 3, host)
     assert len(reps) == 3 and all(r["converged"] for r in reps)
+    np.testing.assert_array_equal(f.download(0), host)
+    np.testing.assert_array_equal(f.download(1), host)   # CopyDataVectorsToOldTimeStep of the last step
     ref = phi0.copy()
     iters = []
     for _ in range(3):
