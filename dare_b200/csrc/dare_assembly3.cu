@@ -143,7 +143,7 @@ struct A3Copy {
     int sm;      // element in the stage
 };
 
-template <int LIM, bool FD>
+template <int LIM, bool FD, bool PAIR>
 __global__ void __launch_bounds__(256, FD ? 2 : 3)
     k_assemble3(GridDev g, A3Params a, const double* __restrict__ phi, const double* __restrict__ phi_old,
                 double* __restrict__ diag, double* __restrict__ rhs_out, double* __restrict__ x0, int planes,
@@ -196,6 +196,43 @@ __global__ void __launch_bounds__(256, FD ? 2 : 3)
     cpo.off = active ? jj * n2 + kk : -1;
     const int cell_gh = (jj + og1) * gn2 + kk + og2;     // the cell's ghosted in-plane offset (active cells)
 
+    // PAIR (even n2 and ghost width, 16-byte aligned arrays): the same
+    // elements staged as 16-byte pairs of cells.  Each thread: one pair of the
+    // phi tile (216 pairs), one pair of phi_old (threads 0-127) or of the x
+    // faces (128-255), one pair of the y faces (0-143); the z faces (rows of
+    // n2 + 1) stay single.  The shared-memory layout is the one above.
+    A3Copy pph{-1, 0}, pov{-1, 0}, pvy{-1, 0}, pdx{-1, 0};
+    if constexpr (PAIR) {
+        if (tid < kA3Phi / 2) {
+            const int row = tid / (kA3PW / 2), col = 2 * (tid - row * (kA3PW / 2));
+            pph.sm = row * kA3PW + col;
+            const int j = j0 - 2 + row, k = k0 - 2 + col;
+            if (j + og1 >= 0 && j + og1 < gn1 && k + og2 >= 0 && k + og2 < gn2) pph.off = (j + og1) * gn2 + k + og2;
+        }
+        {
+            const int t2 = tid & 127, row = t2 >> 4, c2 = 2 * (t2 & 15);
+            const int pj = j0 + row, pk = k0 + c2;
+            const bool act = pj < n1 && pk < n2;
+            if (tid < 128) {   // phi_old (ghosted) and, with face D, the x faces of D
+                pov.sm = kOffPO + row * kA3K + c2;
+                pov.off = act ? (pj + og1) * gn2 + pk + og2 : -1;
+                pdx.sm = kOffDX + row * kA3K + c2;
+                pdx.off = act ? pj * n2 + pk : -1;
+            } else {           // the x faces of the velocity
+                pov.sm = kOffVX + row * kA3K + c2;
+                pov.off = act ? pj * n2 + pk : -1;
+            }
+        }
+        if (tid < kA3FY / 2) {
+            const int row = tid >> 4, c2 = 2 * (tid & 15);
+            int f = j0 + row;
+            const int k = k0 + c2;
+            if (f == n1 && g.periodic[1]) f = 0;
+            pvy.sm = kOffVY + row * kA3K + c2;
+            pvy.off = (f <= n1 && k < n2) ? f * n2 + k : -1;
+        }
+    }
+
     auto slot = [&](int s) { return sm3 + (size_t)(s % kA3Ring) * STAGE; };
     // stage sequence index s: plane i0 - 2 + s
     auto stage = [&](int s) {
@@ -203,36 +240,68 @@ __global__ void __launch_bounds__(256, FD ? 2 : 3)
         const int p = i0 - 2 + s;
         double* sb = slot(s);
         const double* src = phi + (int64_t)(p + og0) * gplane;
+        if constexpr (PAIR) {
+            if (tid < kA3Phi / 2) cp_async<16>(sb + pph.sm, src + (pph.off < 0 ? 0 : pph.off), pph.off >= 0);
+            if (p < i0 || p >= i1) return;                // halo planes: phi only
+            const int pu = upper_face(g, 0, p);
+            if (tid < 128)
+                cp_async<16>(sb + pov.sm, phi_old + (int64_t)(p + og0) * gplane + (pov.off < 0 ? 0 : pov.off),
+                             pov.off >= 0);
+            if (fvel) {
+                if (tid >= 128)
+                    cp_async<16>(sb + pov.sm, a.face_vel[0] + pu * xplane + (pov.off < 0 ? 0 : pov.off), pov.off >= 0);
+                if (tid < kA3FY / 2)
+                    cp_async<16>(sb + pvy.sm, a.face_vel[1] + p * yplane + (pvy.off < 0 ? 0 : pvy.off), pvy.off >= 0);
 #pragma unroll
-        for (int h = 0; h < 2; h++)
-            if (cph[h].sm < kA3Phi) cp_async<8>(sb + cph[h].sm, src + (cph[h].off < 0 ? 0 : cph[h].off), cph[h].off >= 0);
-        if (p < i0 || p >= i1) return;                    // halo planes: phi only
-        cp_async<8>(sb + kOffPO + tid, phi_old + (int64_t)(p + og0) * gplane + (cpo.off < 0 ? 0 : cell_gh),
-                    cpo.off >= 0);
-        const int pu = upper_face(g, 0, p);
-        if (fvel) {
-            cp_async<8>(sb + kOffVX + tid, a.face_vel[0] + pu * xplane + (cpo.off < 0 ? 0 : cpo.off), cpo.off >= 0);
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                if (cy[h].sm < kOffVY + kA3FY)
-                    cp_async<8>(sb + cy[h].sm, a.face_vel[1] + p * yplane + (cy[h].off < 0 ? 0 : cy[h].off),
-                                cy[h].off >= 0);
-                if (cz[h].sm < kOffVZ + kA3FZ)
-                    cp_async<8>(sb + cz[h].sm, a.face_vel[2] + p * zplane + (cz[h].off < 0 ? 0 : cz[h].off),
-                                cz[h].off >= 0);
+                for (int h = 0; h < 2; h++)
+                    if (cz[h].sm < kOffVZ + kA3FZ)
+                        cp_async<8>(sb + cz[h].sm, a.face_vel[2] + p * zplane + (cz[h].off < 0 ? 0 : cz[h].off),
+                                    cz[h].off >= 0);
             }
-        }
-        if constexpr (FD) {
-            constexpr int dy = kOffDY - kOffVY, dz = kOffDZ - kOffVZ;
-            cp_async<8>(sb + kOffDX + tid, a.face_D[0] + pu * xplane + (cpo.off < 0 ? 0 : cpo.off), cpo.off >= 0);
+            if constexpr (FD) {
+                constexpr int dy = kOffDY - kOffVY, dz = kOffDZ - kOffVZ;
+                if (tid < 128)
+                    cp_async<16>(sb + pdx.sm, a.face_D[0] + pu * xplane + (pdx.off < 0 ? 0 : pdx.off), pdx.off >= 0);
+                if (tid < kA3FY / 2)
+                    cp_async<16>(sb + pvy.sm + dy, a.face_D[1] + p * yplane + (pvy.off < 0 ? 0 : pvy.off), pvy.off >= 0);
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                if (cy[h].sm < kOffVY + kA3FY)
-                    cp_async<8>(sb + cy[h].sm + dy, a.face_D[1] + p * yplane + (cy[h].off < 0 ? 0 : cy[h].off),
-                                cy[h].off >= 0);
-                if (cz[h].sm < kOffVZ + kA3FZ)
-                    cp_async<8>(sb + cz[h].sm + dz, a.face_D[2] + p * zplane + (cz[h].off < 0 ? 0 : cz[h].off),
-                                cz[h].off >= 0);
+                for (int h = 0; h < 2; h++)
+                    if (cz[h].sm < kOffVZ + kA3FZ)
+                        cp_async<8>(sb + cz[h].sm + dz, a.face_D[2] + p * zplane + (cz[h].off < 0 ? 0 : cz[h].off),
+                                    cz[h].off >= 0);
+            }
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (cph[h].sm < kA3Phi) cp_async<8>(sb + cph[h].sm, src + (cph[h].off < 0 ? 0 : cph[h].off), cph[h].off >= 0);
+            if (p < i0 || p >= i1) return;                    // halo planes: phi only
+            cp_async<8>(sb + kOffPO + tid, phi_old + (int64_t)(p + og0) * gplane + (cpo.off < 0 ? 0 : cell_gh),
+                        cpo.off >= 0);
+            const int pu = upper_face(g, 0, p);
+            if (fvel) {
+                cp_async<8>(sb + kOffVX + tid, a.face_vel[0] + pu * xplane + (cpo.off < 0 ? 0 : cpo.off), cpo.off >= 0);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    if (cy[h].sm < kOffVY + kA3FY)
+                        cp_async<8>(sb + cy[h].sm, a.face_vel[1] + p * yplane + (cy[h].off < 0 ? 0 : cy[h].off),
+                                    cy[h].off >= 0);
+                    if (cz[h].sm < kOffVZ + kA3FZ)
+                        cp_async<8>(sb + cz[h].sm, a.face_vel[2] + p * zplane + (cz[h].off < 0 ? 0 : cz[h].off),
+                                    cz[h].off >= 0);
+                }
+            }
+            if constexpr (FD) {
+                constexpr int dy = kOffDY - kOffVY, dz = kOffDZ - kOffVZ;
+                cp_async<8>(sb + kOffDX + tid, a.face_D[0] + pu * xplane + (cpo.off < 0 ? 0 : cpo.off), cpo.off >= 0);
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    if (cy[h].sm < kOffVY + kA3FY)
+                        cp_async<8>(sb + cy[h].sm + dy, a.face_D[1] + p * yplane + (cy[h].off < 0 ? 0 : cy[h].off),
+                                    cy[h].off >= 0);
+                    if (cz[h].sm < kOffVZ + kA3FZ)
+                        cp_async<8>(sb + cz[h].sm + dz, a.face_D[2] + p * zplane + (cz[h].off < 0 ? 0 : cz[h].off),
+                                    cz[h].off >= 0);
+                }
             }
         }
     };
@@ -370,16 +439,16 @@ __global__ void __launch_bounds__(256, FD ? 2 : 3)
     cp_async_wait<0>();
 }
 
-template <int LIM, bool FD>
-static int launch3_t(dare_ctx* ctx, const GridDev& g, const A3Params& p, const double* phi, const double* phi_old,
+template <int LIM, bool FD, bool PAIR>
+static int launch3_k(dare_ctx* ctx, const GridDev& g, const A3Params& p, const double* phi, const double* phi_old,
                      double* diag, double* rhs, double* x0, int ib, int ie) {
     const size_t smem = (size_t)a3_stage<FD>() * kA3Ring * sizeof(double);
     static int resident = 0;
     if (!resident) {
-        DARE_CUDA(ctx, cudaFuncSetAttribute(k_assemble3<LIM, FD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        DARE_CUDA(ctx, cudaFuncSetAttribute(k_assemble3<LIM, FD, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
         int occ = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_assemble3<LIM, FD>, kA3K * kA3J, smem) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_assemble3<LIM, FD, PAIR>, kA3K * kA3J, smem) !=
                 cudaSuccess ||
             occ < 1)
             occ = 1;
@@ -402,9 +471,23 @@ static int launch3_t(dare_ctx* ctx, const GridDev& g, const A3Params& p, const d
         }
     }
     const dim3 grid(gx, gy, (unsigned)((n0 + best - 1) / best)), block(kA3K, kA3J, 1);
-    k_assemble3<LIM, FD><<<grid, block, smem, ctx->stream>>>(g, p, phi, phi_old, diag, rhs, x0, best, ib, ie);
+    k_assemble3<LIM, FD, PAIR><<<grid, block, smem, ctx->stream>>>(g, p, phi, phi_old, diag, rhs, x0, best, ib, ie);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
+}
+
+// PAIR applies with an even n2 and ghost width (the ghosted rows and the
+// tile's first column then start on 16-byte boundaries) and 16-byte aligned
+// arrays
+template <int LIM, bool FD>
+static int launch3_t(dare_ctx* ctx, const GridDev& g, const A3Params& p, const double* phi, const double* phi_old,
+                     double* diag, double* rhs, double* x0, int ib, int ie) {
+    auto al = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
+    bool pair = g.n[2] % 2 == 0 && g.og[2] % 2 == 0 && al(phi) && al(phi_old);
+    if (p.conv == 2) pair = pair && al(p.face_vel[0]) && al(p.face_vel[1]);
+    if (FD) pair = pair && al(p.face_D[0]) && al(p.face_D[1]);
+    return pair ? launch3_k<LIM, FD, true>(ctx, g, p, phi, phi_old, diag, rhs, x0, ib, ie)
+                : launch3_k<LIM, FD, false>(ctx, g, p, phi, phi_old, diag, rhs, x0, ib, ie);
 }
 
 int launch_assemble3(dare_ctx* ctx, const GridDev& g, const AsmParams& a, const double* phi, const double* phi_old,
