@@ -23,7 +23,8 @@ class Desc(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int64 * 3), ("L", C.c_double * 3), ("periodic", C.c_int * 3),
                 ("dt", C.c_double), ("diffusion", C.c_int), ("D", C.c_double),
                 ("face_D", C.c_void_p * 3), ("convection", C.c_int), ("vel", C.c_double * 3),
-                ("limiter", C.c_int), ("scheme", C.c_int), ("bc_type", C.c_int * 6), ("bc_value", C.c_double * 6)]
+                ("limiter", C.c_int), ("scheme", C.c_int), ("bc_type", C.c_int * 6), ("bc_value", C.c_double * 6),
+                ("ncomp", C.c_int), ("bc_type1", C.c_int * 6), ("bc_value1", C.c_double * 6)]
 
 
 _lib = None
@@ -46,10 +47,12 @@ def lib():
 
 
 def assemble(dim, n, L, periodic, phi_conv, phi_old, dt=0.0, D=None, face_D=None, vel=None,
-             limiter="VANLEER", scheme="EULER_BACKWARD", bc=None):
+             limiter="VANLEER", scheme="EULER_BACKWARD", bc=None, ncomp=1, bc1=None):
     """CSR (rowptr, cols, vals), rhs and initial guess of one implicit step,
     assembled by the reference's code.  bc: {face 1..6: (1 Dirichlet | 2
-    Neumann, value)}; fields are ghosted (two layers) in the oracle's layout."""
+    Neumann, value)}, bc1 the same for component 1 when ncomp = 2; fields
+    are ghosted (two layers) in the oracle's layout, component after
+    component; rows are cell * ncomp + component."""
     d = Desc()
     d.dim = dim
     for q in range(3):
@@ -76,7 +79,11 @@ def assemble(dim, n, L, periodic, phi_conv, phi_old, dt=0.0, D=None, face_D=None
     for face, (kind, value) in (bc or {}).items():
         d.bc_type[face - 1] = kind
         d.bc_value[face - 1] = value
-    ncell = int(np.prod([d.n[q] for q in range(3)]))
+    d.ncomp = ncomp
+    for face, (kind, value) in (bc1 or {}).items():
+        d.bc_type1[face - 1] = kind
+        d.bc_value1[face - 1] = value
+    ncell = int(np.prod([d.n[q] for q in range(3)])) * ncomp
     phi_conv = np.ascontiguousarray(phi_conv, dtype=np.float64)
     phi_old = np.ascontiguousarray(phi_old, dtype=np.float64)
     rowptr = np.zeros(ncell + 1, dtype=np.int64)

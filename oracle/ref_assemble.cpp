@@ -49,6 +49,9 @@ struct dref_desc {
                                // 3 ADAMS_BASHFORT, 4 ADAMS_MOULTON
     int bc_type[6];            // faces W,E,S,N,B,T: 1 Dirichlet, 2 Neumann
     double bc_value[6];
+    int ncomp;                 // 1 or 2 field components (0 reads as 1)
+    int bc_type1[6];           // component 1's conditions (ncomp 2)
+    double bc_value1[6];
 };
 }
 
@@ -87,16 +90,16 @@ int64_t upper_face(const dref_desc* d, int dd, int64_t i) {
 
 int grid_counter = 0;
 
-template <std::size_t Dim, class Limiter, class Scheme>
+template <std::size_t Dim, class Limiter, class Scheme, std::size_t N>
 int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, int64_t* rowptr, int64_t* cols,
              double* vals, double* rhs, double* x0, int64_t nnz_cap) {
     using SC = double;
     using GO = dare::defaults::GlobalOrdinalType;
     using LO = dare::defaults::LocalOrdinalType;
     using Grid = dare::Grid::Cartesian<Dim>;
-    using Field = dare::Data::Field<Grid, SC, 1>;
+    using Field = dare::Data::Field<Grid, SC, N>;
     using CNB = typename Grid::NeighborID;
-    using MB = dare::Matrix::MatrixBlock<Grid, GO, SC, 1>;
+    using MB = dare::Matrix::MatrixBlock<Grid, GO, SC, N>;
 
     const int num_ghost = 2;
     dare::mpi::ExecutionManager exman(MPI_COMM_WORLD, dare::mpi::Verbosity::None);
@@ -116,15 +119,20 @@ int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, 
     // dimensions, 1 along the others, last dimension fastest
     int64_t gn[3] = {1, 1, 1};
     for (std::size_t q = 0; q < Dim; q++) gn[q] = d->n[q] + 2 * num_ghost;
+    // N components: the fields are given component after component, each in
+    // the ghosted layout
     Field field("phi", grep, 2);
     const LO nloc = grep.GetNumberLocalCells();
+    const int64_t gcells = gn[0] * gn[1] * gn[2];
     for (LO lo = 0; lo < nloc; lo++) {
         const auto ind = grep.MapOrdinalToIndexLocal(lo);
         int64_t idx[3] = {0, 0, 0};
         for (std::size_t q = 0; q < Dim; q++) idx[q] = ind[q];
         const int64_t off = (idx[0] * gn[1] + idx[1]) * gn[2] + idx[2];
-        field.GetDataVector(0).At(lo, 0) = phi_conv[off];
-        field.GetDataVector(1).At(lo, 0) = phi_old[off];
+        for (std::size_t n = 0; n < N; n++) {
+            field.GetDataVector(0).At(lo, n) = phi_conv[n * gcells + off];
+            field.GetDataVector(1).At(lo, n) = phi_old[n * gcells + off];
+        }
     }
 
     typename Grid::VecSC velocity;
@@ -156,12 +164,16 @@ int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, 
             Divergence div(*g_r, loc_o);
             (*mb) -= div(d->D, grad(*mb));
         } else if (d->diffusion == 2) {
-            dare::Data::FaceValueStencil<Grid, SC, 1> dface;
+            dare::Data::FaceValueStencil<Grid, SC, N> dface;   // the same face D for every component
             for (std::size_t q = 0; q < Dim; q++) {
                 int64_t fi[3] = {gi[0], gi[1], gi[2]};
-                dface.SetValue(faces[2 * q], 0, d->face_D[q][face_index(d, (int)q, fi[0], fi[1], fi[2])]);
+                const double lo = d->face_D[q][face_index(d, (int)q, fi[0], fi[1], fi[2])];
                 fi[q] = upper_face(d, (int)q, fi[q]);
-                dface.SetValue(faces[2 * q + 1], 0, d->face_D[q][face_index(d, (int)q, fi[0], fi[1], fi[2])]);
+                const double up = d->face_D[q][face_index(d, (int)q, fi[0], fi[1], fi[2])];
+                for (std::size_t n = 0; n < N; n++) {
+                    dface.SetValue(faces[2 * q], n, lo);
+                    dface.SetValue(faces[2 * q + 1], n, up);
+                }
             }
             Gradient grad(*g_r, loc_o);
             Divergence div(*g_r, loc_o);
@@ -172,14 +184,18 @@ int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, 
             for (int side = 0; side < 2; side++) {
                 const int f = 2 * (int)q + side;
                 if (!(side == 0 ? gi[q] == 0 : gi[q] == nn[q] - 1)) continue;
-                const SC X = mb->Get(0, faces[f]);
-                if (d->bc_type[f] == 1) {
-                    mb->Get(0, CNB::CENTER) -= X;
-                    mb->GetRhs(0) -= 2. * d->bc_value[f] * X;
-                } else {
-                    mb->Get(0, CNB::CENTER) += X;
+                for (std::size_t n = 0; n < N; n++) {   // counter_diffusion1D.cpp:123-146, per component
+                    const int type = n == 0 ? d->bc_type[f] : d->bc_type1[f];
+                    const double value = n == 0 ? d->bc_value[f] : d->bc_value1[f];
+                    const SC X = mb->Get(n, faces[f]);
+                    if (type == 1) {
+                        mb->Get(n, CNB::CENTER) -= X;
+                        mb->GetRhs(n) -= 2. * value * X;
+                    } else {
+                        mb->Get(n, CNB::CENTER) += X;
+                    }
+                    mb->Remove(n, faces[f]);
                 }
-                mb->Remove(0, faces[f]);
             }
         }
     };
@@ -191,7 +207,8 @@ int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, 
         MB* mb = &blocks[node];
         const GO node_global = grep.MapLocalToGlobalInternal(node);
         mb->Initialize(&grep, node_global);
-        mb->SetInitialGuess(0, field.GetDataVector().At(grep.MapInternalToLocal(node), 0));
+        for (std::size_t n = 0; n < N; n++)
+            mb->SetInitialGuess(n, field.GetDataVector().At(grep.MapInternalToLocal(node), n));
         functor(mb);
         mb->Finalize();
     }
@@ -203,35 +220,46 @@ int assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, 
         mb.Finalize();
         const GO r = grep.MapLocalToGlobalInternal(node);
         if (r != node) return -3;                // one rank: local and global internal ordinals agree
-        const auto& c = mb.GetColumnOrdinals(0);
-        const auto& v = mb.GetColumnValues(0);
-        row.clear();
-        for (std::size_t e = 0; e < c.size(); e++) row.emplace_back(c[e], v[e]);
-        std::stable_sort(row.begin(), row.end(),
-                         [](const std::pair<GO, SC>& a, const std::pair<GO, SC>& b) { return a.first < b.first; });
-        for (std::size_t e = 0; e + 1 < row.size(); e++)
-            if (row[e].first == row[e + 1].first) return -4;   // duplicate columns (a periodic extent < 3)
-        if (nnz + (int64_t)row.size() > nnz_cap) return -2;
-        for (const auto& cv : row) {
-            cols[nnz] = cv.first;
-            vals[nnz] = cv.second;
-            nnz++;
+        for (std::size_t n = 0; n < N; n++) {    // row node * N + n (MatrixBlockBase::GetRow)
+            const auto& c = mb.GetColumnOrdinals(n);
+            const auto& v = mb.GetColumnValues(n);
+            row.clear();
+            for (std::size_t e = 0; e < c.size(); e++) row.emplace_back(c[e], v[e]);
+            std::stable_sort(row.begin(), row.end(),
+                             [](const std::pair<GO, SC>& a, const std::pair<GO, SC>& b) { return a.first < b.first; });
+            for (std::size_t e = 0; e + 1 < row.size(); e++)
+                if (row[e].first == row[e + 1].first) return -4;   // duplicate columns (a periodic extent < 3)
+            if (nnz + (int64_t)row.size() > nnz_cap) return -2;
+            for (const auto& cv : row) {
+                cols[nnz] = cv.first;
+                vals[nnz] = cv.second;
+                nnz++;
+            }
+            const int64_t rr = (int64_t)node * N + n;
+            rowptr[rr + 1] = nnz;
+            rhs[rr] = mb.GetRhs(n);
+            x0[rr] = mb.GetInitialGuess(n);
         }
-        rowptr[node + 1] = nnz;
-        rhs[node] = mb.GetRhs(0);
-        x0[node] = mb.GetInitialGuess(0);
     }
     return 0;
+}
+
+template <std::size_t Dim, class Limiter, class Scheme>
+int by_ncomp(const dref_desc* d, const double* a, const double* b, int64_t* rp, int64_t* c, double* v, double* r,
+             double* x, int64_t cap) {
+    if (d->ncomp == 2) return assemble<Dim, Limiter, Scheme, 2>(d, a, b, rp, c, v, r, x, cap);
+    if (d->ncomp <= 1) return assemble<Dim, Limiter, Scheme, 1>(d, a, b, rp, c, v, r, x, cap);
+    return -1;
 }
 
 template <std::size_t Dim, class Limiter>
 int by_scheme(const dref_desc* d, const double* a, const double* b, int64_t* rp, int64_t* c, double* v, double* r,
               double* x, int64_t cap) {
     switch (d->scheme) {
-    case 0: return assemble<Dim, Limiter, dare::Matrix::EULER_BACKWARD>(d, a, b, rp, c, v, r, x, cap);
-    case 1: return assemble<Dim, Limiter, dare::Matrix::EULER_FORWARD>(d, a, b, rp, c, v, r, x, cap);
-    case 2: return assemble<Dim, Limiter, dare::Matrix::CRANK_NICHOLSON>(d, a, b, rp, c, v, r, x, cap);
-    case 3: return assemble<Dim, Limiter, dare::Matrix::ADAMS_BASHFORT>(d, a, b, rp, c, v, r, x, cap);
+    case 0: return by_ncomp<Dim, Limiter, dare::Matrix::EULER_BACKWARD>(d, a, b, rp, c, v, r, x, cap);
+    case 1: return by_ncomp<Dim, Limiter, dare::Matrix::EULER_FORWARD>(d, a, b, rp, c, v, r, x, cap);
+    case 2: return by_ncomp<Dim, Limiter, dare::Matrix::CRANK_NICHOLSON>(d, a, b, rp, c, v, r, x, cap);
+    case 3: return by_ncomp<Dim, Limiter, dare::Matrix::ADAMS_BASHFORT>(d, a, b, rp, c, v, r, x, cap);
     // ADAMS_MOULTON does not compile in the reference: its GetWeights is not
     // static (Equations/TimeDiscretizationSchemes.h:70), and Divergence calls
     // it as a static member (Divergence_Cartesian.inl:183).
@@ -257,8 +285,9 @@ int by_limiter(const dref_desc* d, const double* a, const double* b, int64_t* rp
 extern "C" {
 // Assembles the system of one implicit step with the reference's own
 // operators.  phi_conv / phi_old: ghosted fields (two ghost layers) in the
-// oracle's layout.  Outputs: CSR rows (rowptr n+1, cols / vals up to nnz_cap),
-// rhs and initial guess per internal cell.  Returns 0, or -1 (bad
+// oracle's layout, component after component.  Outputs: CSR rows (rowptr
+// rows+1, cols / vals up to nnz_cap),
+// rhs and initial guess per row (cell * ncomp + component).  Returns 0, or -1 (bad
 // description, or a scheme the reference does not compile), -2 (nnz_cap too
 // small), -3 / -4 (unsupported layout).
 int dref_assemble(const dref_desc* d, const double* phi_conv, const double* phi_old, int64_t* rowptr, int64_t* cols,
