@@ -272,7 +272,7 @@ def run_dare(args):
     system = D.MatrixSystem(grid)
     vel = [D.DeviceArray.from_tensor(case["face_vel"][d]) for d in range(3)]
     asm = D.Assembly(dt=case["dt"], D=case["D"], face_vel=tuple(vel), limiter="VANLEER")
-    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1})
+    solver = D.BiCGStab2(dict(_STEP_SOLVER))
 
     for _ in range(args.warmup):
         D.timestep(system, field, asm, solver)
@@ -306,9 +306,13 @@ def run_dare(args):
     # stream); every iteration that ran is counted, the last one included
     ctx.set_profiling(True)
     ctx.reset_kernel_stats()
-    prof_iters = []
+    prof_iters, true_res = [], None
+    checked = D.BiCGStab2(dict(_SOLVER))       # the same solve, plus ||b - A x|| at its exit
     for _ in range(args.profile_steps):
-        prof_iters.append(D.timestep(system, field, asm, solver)["iters"])
+        prep = D.timestep(system, field, asm, checked)
+        prof_iters.append(prep["iters"])
+        true_res = {"true_res_rel": prep["true_res_abs"] / prep["b_norm"], "res_rel": prep["res_abs"] / prep["b_norm"],
+                    "of": "the last untimed profiling step"}
     ctx.synchronize()
     kstats = {}
     for name in BYTES_PER_CELL:
@@ -418,8 +422,9 @@ def run_dare(args):
             "parity": parity,
             "time_to_residual_ms": ms / args.steps, "iterations_per_step": statistics.mean(iters),
             "cell_updates_per_s": value * n ** 3,
-            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e; iterations replayed from CUDA graphs); "
-                      "learned-preconditioned solve in 'learned'",
+            "solver": "plain FP64 Jacobi-BiCGStab2 (value, e2e; iterations replayed from CUDA graphs; no true "
+                      "residual at the exit, as the reference's solve); learned-preconditioned solve in 'learned'",
+            "final_residual": true_res,
             "learned": learned,
             "slabs": slabs,
             "configs": configs,
@@ -473,6 +478,10 @@ def slab_comparison(D, ctx, system, field, asm, case, phi0, args, num_slabs=2, s
 
 
 _SOLVER = {"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1}
+# The time-step loops' solver: the reference's BiCGStab2::Solve computes no
+# true residual ||b - A x|| at its common exit (MatrixSystem/BiCGStab2.inl:
+# 571-582), only at the tau = 0 exit (:407-424), which this solver keeps.
+_STEP_SOLVER = dict(_SOLVER, compute_true_residual=0)
 
 
 def _timed_solve(ctx, system, field, asm, fn, reps=2):
@@ -576,7 +585,7 @@ def measure_gauss64(D, ctx, seed=0, warmup=1):
     for face, (kind, val) in case["bc"].items():
         system.set_bc(face, kind, val)
     asm = D.Assembly(dt=case["dt"], D=case["D"])
-    solver = D.BiCGStab2(dict(_SOLVER))
+    solver = D.BiCGStab2(dict(_STEP_SOLVER))
     phi0 = np.ascontiguousarray(case["phi0"].reshape(-1))
 
     def trajectory():
