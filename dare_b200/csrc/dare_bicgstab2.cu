@@ -359,9 +359,19 @@ template int run_iterations<float, true>(dare_ctx*, const GridDev&, const MarchC
 
 }  // namespace dare_gpu
 
-// Plain FP64 solve (BiCGStab2::Solve on the device).
-int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_report* rep) {
+namespace dare_gpu {
+bool solution_to_field_ok(const GridDev& g);
+int launch_solution_to_field(dare_ctx* ctx, const GridDev& g, const double* invd, double* x, double* phi);
+}  // namespace dare_gpu
+
+// Plain FP64 solve (BiCGStab2::Solve on the device).  With a field `f` (the
+// time step's), the exit's x = M^-1 y also writes x into the field's level 0
+// with its periodic face ghosts (CopyTo and ExchangeHaloCells in the same
+// pass); *field_written says whether the field holds the returned x.
+int dare_bicgstab2_fp64_to(dare_system* s, const dare_solver_params* p, dare_solve_report* rep, dare_field* f,
+                           int* field_written) {
     using namespace dare_gpu;
+    if (field_written) *field_written = 0;
     dare_ctx* ctx = s->grid->ctx;
     const GridDev& g = s->sdev;   // components stacked along i
     int rc = ensure_solver_ws(s);
@@ -395,7 +405,17 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
     // (the report's, and the tau = 0 exit's check).
     k_step10<double><<<grid_blocks(ctx, n, 256, 8), 256, 0, ctx->stream>>>(n, ws->st, vs.u[1], vs.x);
     DARE_LAUNCHED(ctx);
-    if (jacobi && (rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
+    const GridDev& gf = s->grid->dev;   // one field component
+    const bool to_field = f && field_written && f->grid == s->grid && f->ncomp == s->ncomp && solution_to_field_ok(gf);
+    if (to_field) {
+        for (int c = 0; c < s->ncomp; c++)
+            if ((rc = launch_solution_to_field(ctx, gf, jacobi ? ws->invd + (size_t)c * gf.ncell : nullptr,
+                                               s->x + (size_t)c * gf.ncell, f->level[0] + (size_t)c * gf.ncell_ghosted)))
+                return rc;
+    } else if (jacobi && (rc = launch_scale(ctx, n, ws->invd, s->x))) {
+        return rc;
+    }
+    bool field_current = to_field;
     double* tres = &ws->st->tres;
     if (p->compute_true_residual &&
         (rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, tres)))
@@ -429,6 +449,7 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
             rep->status = DARE_SOLVE_BREAKDOWN;
             if (jacobi) {
                 if ((rc = launch_scale(ctx, n, ws->invd, s->x))) return rc;
+                field_current = false;   // x changed after the field was written
                 if (p->compute_true_residual) {
                     if ((rc = launch_true_residual(ctx, g, m, full, s->x, s->rhs, ws->st, ws->partials, tres)))
                         return rc;
@@ -446,7 +467,12 @@ int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_
         default: rep->status = DARE_SOLVE_BREAKDOWN; break;
         }
     }
+    if (field_written) *field_written = field_current ? 1 : 0;
     return DARE_OK;
+}
+
+int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_report* rep) {
+    return dare_bicgstab2_fp64_to(s, p, rep, nullptr, nullptr);
 }
 
 int dare_bicgstab2_refine(dare_system* s, const dare_solver_params* p, dare_solve_report* rep);
@@ -465,6 +491,21 @@ void dare_solver_params_default(dare_solver_params* p) {
     p->max_refinements = 30;
     p->check_every = 0;
     p->compute_true_residual = 1;
+}
+
+// dare_bicgstab2_solve for a time step of field f: with the plain FP64
+// solve, the field is written at the solve's exit (*field_written = 1);
+// otherwise the caller copies x into it.
+int dare_bicgstab2_solve_to_field(dare_system* s, const dare_solver_params* p, dare_solve_report* rep,
+                                  dare_field* f, int* field_written) {
+    *field_written = 0;
+    if (!s || !p || !rep) return DARE_ERR_BAD_ARG;
+    if (p->max_it < 0 || !(p->tol >= 0.)) return dare_gpu::set_error(s->grid->ctx, DARE_ERR_BAD_ARG, "bicgstab2: bad params");
+    if (p->precond != DARE_PREC_NONE && p->precond != DARE_PREC_JACOBI)
+        return dare_gpu::set_error(s->grid->ctx, DARE_ERR_UNSUPPORTED, "bicgstab2: preconditioner not supported");
+    cudaSetDevice(s->grid->ctx->device);
+    if (p->precision == DARE_PRECISION_FP64) return dare_bicgstab2_fp64_to(s, p, rep, f, field_written);
+    return dare_bicgstab2_solve(s, p, rep);
 }
 
 int dare_bicgstab2_solve(dare_system* s, const dare_solver_params* p, dare_solve_report* rep) {

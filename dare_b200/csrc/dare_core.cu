@@ -65,6 +65,48 @@ __global__ void k_scatter_to_field(GridDev g, const double* __restrict__ x, doub
     }
 }
 
+// The end of a solve and the two calls after it in one pass: x = invd .* x
+// (applyRightPrec, skipped when invd is null), CopyTo into the field, and
+// the periodic face ghosts of ExchangeHaloCells, each ghost written by the
+// internal cell it images (internal index q < ng: the upper ghost og + n + q;
+// q >= n - ng: the lower ghost q - n + ng).  The values and the cells
+// written are those of k_scale, k_scatter_to_field and k_halo_fill in turn
+// (needs og[d] == ng and n[d] >= ng on the periodic dimensions).  Threads
+// run along k, block rows along (i, j), without 64-bit divisions.
+__global__ void k_solution_to_field(GridDev g, const double* __restrict__ invd, double* __restrict__ x,
+                                    double* __restrict__ phi) {
+    const int n1 = g.n[1], n2 = g.n[2];
+    const int64_t rows = (int64_t)g.n[0] * n1;
+    const int64_t rstep = (int64_t)gridDim.x * blockDim.y;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.y + threadIdx.y; r < rows; r += rstep) {
+        const int i = (int)(r / n1), j = (int)(r - (int64_t)i * n1);
+        const int64_t c0 = r * n2;
+        for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+            const int64_t c = c0 + k;
+            double v = x[c];
+            if (invd) {
+                v = invd[c] * v;
+                x[c] = v;
+            }
+            const int q[3] = {i, j, k};
+            const int ind[3] = {i + g.og[0], j + g.og[1], k + g.og[2]};
+            phi[((int64_t)ind[0] * g.gn[1] + ind[1]) * g.gn[2] + ind[2]] = v;
+            for (int d = 0; d < g.dim; d++) {
+                if (!g.periodic[d]) continue;
+                int t[3] = {ind[0], ind[1], ind[2]};
+                if (q[d] < g.ng) {
+                    t[d] = g.og[d] + g.n[d] + q[d];
+                    phi[((int64_t)t[0] * g.gn[1] + t[1]) * g.gn[2] + t[2]] = v;
+                }
+                if (q[d] >= g.n[d] - g.ng) {
+                    t[d] = q[d] - g.n[d] + g.ng;
+                    phi[((int64_t)t[0] * g.gn[1] + t[1]) * g.gn[2] + t[2]] = v;
+                }
+            }
+        }
+    }
+}
+
 // field (ghosted) -> x (internal): the initial guess of BuildNew
 __global__ void k_gather_from_field(GridDev g, const double* __restrict__ phi, double* __restrict__ x) {
     const int64_t nyz = (int64_t)g.n[1] * g.n[2];
@@ -112,6 +154,30 @@ int launch_gather(dare_ctx* ctx, const GridDev& g, const double* phi, double* x)
 int launch_scatter(dare_ctx* ctx, const GridDev& g, const double* x, double* phi) {
     int blocks = grid_blocks(ctx, g.ncell, 256, 8);
     k_scatter_to_field<<<blocks, 256, 0, ctx->stream>>>(g, x, phi);
+    DARE_LAUNCHED(ctx);
+    return DARE_OK;
+}
+
+bool solution_to_field_ok(const GridDev& g) {
+    for (int d = 0; d < g.dim; d++)
+        if (g.periodic[d] && (g.og[d] != g.ng || g.n[d] < g.ng)) return false;
+    return g.ncell > 0;
+}
+
+// Block shape of k_solution_to_field: threads along k up to 256 (a power of
+// two covering n2), the rest of the 256 along the rows.
+dim3 solution_to_field_block(const GridDev& g) {
+    int bx = 1;
+    while (bx < g.n[2] && bx < 256) bx *= 2;
+    return dim3(bx, 256 / bx, 1);
+}
+
+int launch_solution_to_field(dare_ctx* ctx, const GridDev& g, const double* invd, double* x, double* phi) {
+    if (!solution_to_field_ok(g)) return set_error(ctx, DARE_ERR_BAD_ARG, "solution_to_field: ghost layout");
+    const dim3 block = solution_to_field_block(g);
+    const int64_t rows = (int64_t)g.n[0] * g.n[1];
+    const int blocks = grid_blocks(ctx, rows, (int)block.y, 8);
+    k_solution_to_field<<<blocks, block, 0, ctx->stream>>>(g, invd, x, phi);
     DARE_LAUNCHED(ctx);
     return DARE_OK;
 }

@@ -9,7 +9,8 @@
 
 using namespace dare_gpu;
 
-int dare_bicgstab2_fp64(dare_system* s, const dare_solver_params* p, dare_solve_report* rep);
+extern "C" int dare_bicgstab2_solve_to_field(dare_system* s, const dare_solver_params* p, dare_solve_report* rep,
+                                             dare_field* f, int* field_written);
 namespace dare_gpu {
 int launch_assemble(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old);
 int launch_assemble_planes(dare_system* s, const dare_assembly_desc* desc, const double* phi, const double* phi_old,
@@ -32,8 +33,9 @@ int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
     int rc = launch_assemble(s, desc, phi, phi_old);                 // Trilinos::Build
     if (rc) return rc;
     if (prof) DARE_CUDA(ctx, cudaEventRecord(ctx->ev[13], ctx->stream));
-    rc = dare_bicgstab2_solve(s, p, rep);                            // TrilinosSolver::Solve
-    if (rc) return rc;
+    int written = 0;                                                 // TrilinosSolver::Solve, and with the
+    rc = dare_bicgstab2_solve_to_field(s, p, rep, f, &written);      // plain FP64 solve CopyTo and
+    if (rc) return rc;                                               // ExchangeHaloCells at its exit
     if (prof) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ctx->ev[12], ctx->ev[13]) == cudaSuccess) {
@@ -43,10 +45,12 @@ int dare_timestep(dare_system* s, dare_field* f, const dare_assembly_desc* desc,
             cudaGetLastError();
         }
     }
-    rc = dare_system_copy_to(s, f);                                   // Trilinos::CopyTo
-    if (rc) return rc;
-    rc = dare_field_exchange_halo(f);                                 // Field::ExchangeHaloCells
-    if (rc) return rc;
+    if (!written) {
+        rc = dare_system_copy_to(s, f);                               // Trilinos::CopyTo
+        if (rc) return rc;
+        rc = dare_field_exchange_halo(f);                             // Field::ExchangeHaloCells
+        if (rc) return rc;
+    }
     return dare_field_copy_to_old(f);                                // CopyDataVectorsToOldTimeStep
 }
 
@@ -56,8 +60,9 @@ namespace {
 // The rest of a step whose Build has been queued: Solve, CopyTo,
 // ExchangeHaloCells (CopyDataVectorsToOldTimeStep is the caller's).
 int solve_and_copy_back(dare_system* s, dare_field* f, const dare_solver_params* p, dare_solve_report* rep) {
-    int rc = dare_bicgstab2_solve(s, p, rep);
-    if (rc) return rc;
+    int written = 0;
+    int rc = dare_bicgstab2_solve_to_field(s, p, rep, f, &written);
+    if (rc || written) return rc;
     rc = dare_system_copy_to(s, f);
     if (rc) return rc;
     return dare_field_exchange_halo(f);

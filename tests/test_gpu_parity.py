@@ -568,6 +568,46 @@ def test_host_resident_steps_match_single_calls(ctx, kind):
         D.timesteps_host(s, f, asm, solver, 1, np.zeros(g.num_cells_ghosted))
 
 
+def _periodic_2d_case():
+    rng = np.random.default_rng(31)
+    n = (20, 18)
+    return {"n": n, "size": (1.0, 1.25), "periodic": (1, 1), "dt": 0.01, "D": 1e-3, "vel": (0.3, -0.2),
+            "limiter": "VANLEER", "phi0": rng.random((24, 22, 1)), "phi_old": rng.random((24, 22, 1)), "bc": {}}
+
+
+@pytest.mark.parametrize("kind,precond", [("tvd-periodic", "JACOBI"), ("tvd-periodic", "NONE"),
+                                          ("gaussian-bounded", "JACOBI"), ("periodic-2d", "JACOBI")])
+def test_timestep_field_write_matches_separate_calls(ctx, kind, precond):
+    """dare_timestep writes the solution into the field, with its periodic
+    face ghosts, in the pass that ends the solve (x = M^-1 y); the separate
+    calls Build, Solve, CopyTo, ExchangeHaloCells and
+    CopyDataVectorsToOldTimeStep give the same field (both levels, every
+    ghost) and the same solution vector, bit for bit."""
+    if kind == "tvd-periodic":
+        case = W.tvd_convection_diffusion(n=24, steps=1)
+    elif kind == "gaussian-bounded":
+        case = W.gaussian_diffusion(n=20, steps=1)
+    else:
+        case = _periodic_2d_case()
+    g, f, s, asm, keep, dim = _gpu_case(ctx, case)
+    solver = D.BiCGStab2({"Convergence Tolerance": 1e-10, "Maximum Iterations": 5000, "tol_relative": 1,
+                          "compute_true_residual": 0}, precond=precond)
+    phi0, old0 = f.download(0), f.download(1)
+    rep = D.timestep(s, f, asm, solver)
+    got0, got1, gx = f.download(0), f.download(1), s.solution()
+    f.upload(phi0, 0)
+    f.upload(old0, 1)
+    s.build(f, asm)
+    rep2 = solver.solve(s)
+    s.copy_to(f)
+    f.exchange_halo()
+    f.copy_to_old()
+    assert rep["converged"] and rep["iters"] == rep2["iters"]
+    np.testing.assert_array_equal(gx, s.solution())
+    np.testing.assert_array_equal(got0, f.download(0))
+    np.testing.assert_array_equal(got1, f.download(1))
+
+
 @pytest.mark.parametrize("precond", ["NONE", "JACOBI"])
 def test_breakdown_after_step10_keeps_its_update(ctx, precond):
     """A = 2 I: alpha = 1/2 makes r' = r - alpha v exactly 0, so s = 0 and
