@@ -568,8 +568,23 @@ __device__ __forceinline__ Pair<T> ld_pair(const T* p) {
 // to 0.354 ms, so the default carveout stays).
 // HALO (slabs): the planes before the first and after the last plane of the
 // grid come from m.halo when set.
+// Blocks per SM the register budget is set for: three (80 registers) with
+// two cells per thread, two (128) with one.  Step 4 (two staged operands,
+// eight streams, five FP64 dot products) takes two blocks of 128 registers
+// with two cells per thread too: held to 80, the FP32 step 4 of the
+// refinement ran 1.66 ms at 512^3 (64 % of copy bandwidth), with 128
+// registers 1.18 ms (90 %).
+template <class K, int CPT>
+struct MarchMinBlocks {
+    static constexpr int value = CPT == 2 ? 3 : 2;
+};
+template <typename T, bool UNIT, int CPT>
+struct MarchMinBlocks<FStep4<T, UNIT>, CPT> {
+    static constexpr int value = 2;
+};
+
 template <class K, int CPT = 1, bool HALO = false, bool PAIR = false>
-__global__ void __launch_bounds__(256, CPT == 2 ? 3 : 2) k_march(GridDev g, K kern, SolverState* st, double* partials,
+__global__ void __launch_bounds__(256, MarchMinBlocks<K, CPT>::value) k_march(GridDev g, K kern, SolverState* st, double* partials,
                                                                    MarchCfg m) {
     using T = typename K::type;
     constexpr int NZ = K::NZ, NP = K::NP;
