@@ -170,8 +170,15 @@ int launch_iteration(dare_ctx* ctx, const GridDev& g, const MarchCfg& m, int sbl
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[3], sm));
     if ((rc = launch_march(ctx, g, m, make_step4<T, UNIT>(op, vs), st, partials))) return rc;
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[4], sm));
+    int vec4 = 0;
+    if constexpr (sizeof(T) == 4) {
+        const void* arrs[10] = {vs.x, vs.r[0], vs.s[1], vs.t, vs.u[0], vs.u[1], vs.r[1], vs.v[1], vs.w, vs.rh};
+        vec4 = g.ncell % 4 == 0;
+        for (const void* a : arrs)
+            if (a && reinterpret_cast<uintptr_t>(a) % 16 != 0) vec4 = 0;
+    }
     k_step5<T><<<sblocks, 256, 0, sm>>>(g.ncell, vs.x, vs.r[0], vs.s[1], vs.t, vs.u[0], vs.u[1], vs.r[1], vs.v[1],
-                                        vs.w, vs.rh, st, partials, 0, 0);
+                                        vs.w, vs.rh, st, partials, 0, 0, vec4);
     DARE_LAUNCHED(ctx);
     if (ev) DARE_CUDA(ctx, cudaEventRecord(ev[5], sm));
     return DARE_OK;

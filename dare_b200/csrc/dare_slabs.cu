@@ -166,7 +166,7 @@ int slab_iteration(dare_slabs* sl, const SlabVecs& v) {
         const VecsT<double>& vs = v.vs[s];
         k_step5<double><<<sl->sblocks[s], 256, 0, sl->ctx->stream>>>(
             sl->systems[s]->sdev.ncell, vs.x, vs.r[0], vs.s[1], vs.t, vs.u[0], vs.u[1], vs.r[1], vs.v[1], vs.w, vs.rh,
-            sl->st, sl->partials, sl->sblock_base[s], sl->sblocks_total);
+            sl->st, sl->partials, sl->sblock_base[s], sl->sblocks_total, 0);
         DARE_LAUNCHED(sl->ctx);
     }
     return DARE_OK;
