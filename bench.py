@@ -683,7 +683,22 @@ def measure_hetero(D, ctx, n=512, seed=0, warmup=1, steps=2):
                          "refinements": r32["refinements"], "inner_iters": r32["inner_iters"],
                          "fallback": r32["fallback_used"], "rel_l2_vs_fp64": err,
                          "true_res_rel": r32["true_res_abs"] / r32["b_norm"]})
+    # per-kernel CUDA events of the FP32 inner iterations: one more, untimed solve
+    system.build(field, asm)
+    ctx.set_profiling(True)
+    ctx.reset_kernel_stats()
+    p32.solve(system)
+    ctx.synchronize()
+    fp32_kernels = {}
+    for name, bpc in (("fp32_step1", 44), ("fp32_step2", 44), ("fp32_step3", 44), ("fp32_step4", 52),
+                      ("fp32_step5", 48)):
+        tot, cnt = ctx.kernel_stats(name)
+        if cnt:
+            fp32_kernels[name] = {"launches": cnt, "ms_avg": tot / cnt, "bytes_per_cell": bpc,
+                                  "GBps": bpc * n ** 3 / (tot / cnt * 1e-3) / 1e9}
+    ctx.set_profiling(False)
     return {"workload": f"heterogeneous-D TVD convection-diffusion {n}^3 periodic, Pe 5 at median D",
+            "fp32_kernels": fp32_kernels,
             "steps": rows,
             "fp64_ms_mean": statistics.mean(r["fp64_ms"] for r in rows),
             "refine_ms_mean": statistics.mean(r["refine_ms"] for r in rows)}

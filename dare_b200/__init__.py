@@ -37,7 +37,9 @@ SCHEME = {"EULER_BACKWARD": 0, "EULER_FORWARD": 1, "CRANK_NICHOLSON": 2, "ADAMS_
 PREC_NONE, PREC_JACOBI = 0, 1
 PRECISION_FP64, PRECISION_FP32_REFINE = 0, 1
 SOLVE_STATUS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "nan"}
-KERNEL_IDS = {"assemble": 0, "step1": 3, "step2": 4, "step3": 5, "step4": 6, "step5": 7}
+KERNEL_IDS = {"assemble": 0, "step1": 3, "step2": 4, "step3": 5, "step4": 6, "step5": 7,
+              # the FP32 inner iterations of the refinement solve
+              "fp32_step1": 9, "fp32_step2": 10, "fp32_step3": 11, "fp32_step4": 12, "fp32_step5": 13}
 
 
 class GridInfo(C.Structure):
